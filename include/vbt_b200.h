@@ -1,0 +1,130 @@
+/*
+ * vbt_b200.h -- C-ABI of the B200 (sm_100a) decode path for VBTPACK4 assets.
+ *
+ * Plain C types only: pointers, sizes, and an opaque asset handle.  Device pointers are CUDA
+ * device addresses on the asset's device; `stream` is a cudaStream_t (NULL = legacy default).
+ * Every call returns a status (VBT_STATUS_*); a message for the last failure on the calling
+ * thread is available from vbt_last_error().  There is no CPU execution path: a process without
+ * a usable CUDA device gets VBT_STATUS_CUDA from every decode call.
+ *
+ * The reference interfaces each call replaces are cited as file:line inside the VBT project.
+ */
+#ifndef VBT_B200_H
+#define VBT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (1..13 mirror the reference's std::runtime_error messages) ---- */
+#define VBT_STATUS_OK 0
+#define VBT_STATUS_LEAF_TOO_SMALL 1       /* "render temporal leaf bytes too small" */
+#define VBT_STATUS_PREFIX_MISSING 2       /* "render temporal leaf prefix missing" */
+#define VBT_STATUS_LEAF_SHORT 3           /* "render temporal leaf shorter than computed layout" */
+#define VBT_STATUS_SHELL_OCC_OOB 4        /* "render temporal shell occupancy is out of bounds" */
+#define VBT_STATUS_SHELL_GROUP_PREFIX 5   /* "render temporal shell group prefix is inconsistent" */
+#define VBT_STATUS_SHELL_NO_ACTIVE 6      /* "render temporal shell mode contains no active voxels" */
+#define VBT_STATUS_SHELL_RESIDUAL_OOB 7   /* "render temporal shell residual stream is out of bounds" */
+#define VBT_STATUS_SHELL_TRAILING 8       /* "render temporal shell leaf contains trailing bytes" */
+#define VBT_STATUS_CONTROL_INDEX 9        /* "render temporal control index out of range" */
+#define VBT_STATUS_STREAM_OOB 10          /* "render temporal stream decode out of bounds" */
+#define VBT_STATUS_DECODE_OOB 11          /* "render temporal decode out of bounds" / std::out_of_range */
+#define VBT_STATUS_KEY_RANGE_OOB 12       /* "render temporal keyframe range out of bounds" */
+#define VBT_STATUS_KEY_INDEX 13           /* "render temporal keyframe index out of range" */
+#define VBT_STATUS_WAIT_TIMEOUT 30        /* a bounded device-side wait gave up (no hang) */
+#define VBT_STATUS_INVALID_ARGUMENT 40
+#define VBT_STATUS_FILE 41                /* the VBTPACK4 reader rejected the file (message set) */
+#define VBT_STATUS_CUDA 42                /* CUDA runtime error or no usable device (message set) */
+#define VBT_STATUS_LIMIT 43               /* request exceeds a fixed capacity of the call */
+
+typedef struct vbt_asset vbt_asset;
+
+/* VBTPACK4 header fields; replaces vbt::render::VbtFileHeader (render/src/vbt_file.h:10-23). */
+typedef struct {
+    uint32_t version, width, height, depth, frames, leaf_size, coarse_resolution, max_coarse_keep,
+        leaf_count, profile_type, coarse_ac_scale_count;
+} vbt_header;
+
+typedef struct {
+    vbt_header header;
+    uint32_t leaf_count_x, leaf_count_y, leaf_count_z;
+    uint32_t active_leaf_count;  /* from the last page-table build (synchronised read) */
+    uint64_t payload_words;
+    uint64_t device_bytes;       /* device memory held by the asset */
+    int device;
+} vbt_asset_info;
+
+const char* vbt_status_string(int status);
+const char* vbt_last_error(void);
+int vbt_device_count(void);
+
+/* Validate a whole VBTPACK4 file image with the reader's rules and messages
+ * (replaces vbt::render::loadVbtFile's checks, render/src/vbt_file.cpp:39-206). */
+int vbt_validate_file_image(const void* bytes, uint64_t len, vbt_header* out_header);
+
+/* Load an asset and keep it resident on `device`: offsets, payload, scales, leaf table, page
+ * table.  The page table is built once during the call.  Replaces loadVbtFile
+ * (render/src/vbt_file.cpp:109-210) + the Studio's upload (VBTStudio/frontend/src/
+ * volume_renderer.cpp:1593-1608). */
+int vbt_asset_open(const char* path, int device, vbt_asset** out_asset);
+int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset** out_asset);
+int vbt_asset_destroy(vbt_asset* asset);
+int vbt_asset_get_info(vbt_asset* asset, vbt_asset_info* out_info);
+
+/* Kernel (a): payload walker + active-leaf page table (compact[leaf] = ascending rank among
+ * non-EMPTY leaves, 0xFFFFFFFF for EMPTY).  Replaces parseRenderTemporalPackedLeaf
+ * (src/render_temporal_payload.cpp:234-311) per leaf and the Studio's page-table shader
+ * (VBTStudio/frontend/shaders/vbt_active_index.comp:28-57). Asynchronous on `stream`. */
+int vbt_build_page_table(vbt_asset* asset, void* stream);
+/* Device views of the page table: compact[leaf_count], active_list[rank] = leaf, and the
+ * device-resident active count (one uint32). */
+int vbt_page_table_device(vbt_asset* asset, const uint32_t** d_compact, const uint32_t** d_active_list,
+                          const uint32_t** d_active_count);
+/* Synchronous host copy of the page table (compact must hold leaf_count entries). */
+int vbt_get_page_table(vbt_asset* asset, uint32_t* compact, uint32_t* active_count);
+/* Synchronous host copy of the 32-byte leaf-table rows (8 uint32 per leaf). */
+int vbt_get_leaf_table(vbt_asset* asset, uint32_t* rows);
+
+/* Kernel (b): current-frame voxel cache for `nframes` (<= 64) frames in one launch:
+ * d_out[f * frame_stride + rank * 512 + (lz*8 + ly)*8 + lx].  Voxels outside a boundary leaf's
+ * extent are 0.  Values equal decodeFrameToDense (render/src/render_smoke_vbt_bench_main.cpp:
+ * 389-452) voxel for voxel; the Studio cache it replaces is vbt_cache.comp:176-294.
+ * `grid` = CTAs of the persistent launch (0 = one wave of the device). */
+int vbt_decode_cache(vbt_asset* asset, const int* frames, int nframes, float* d_out, uint64_t frame_stride,
+                     int grid, void* stream);
+/* Plain per-leaf launch (one CTA per leaf of the grid, one frame), for comparison. */
+int vbt_decode_cache_plain(vbt_asset* asset, int frame, float* d_out, void* stream);
+/* Dense frames d_out[f * X*Y*Z + (z*Y + y)*X + x] (decodeFrameToDense /
+ * reconstructScientificFrameCpu, render/src/scientific_decode.cpp:361-409). */
+int vbt_decode_frames(vbt_asset* asset, const int* frames, int nframes, float* d_out, int grid, void* stream);
+
+/* Kernel (c): point queries, d_xyzt = n x (x, y, z, t) uint32, 16-byte aligned.  Render family:
+ * the voxel of decodeFrameToDense(t); scientific: decodeScientificValueAtCpu
+ * (render/src/scientific_decode.cpp:335-359). */
+int vbt_query_points(vbt_asset* asset, const uint32_t* d_xyzt, uint64_t n, float* d_out, void* stream);
+/* z-slice over frames [t0, t1): d_out[(t - t0) * X*Y + y*X + x]. */
+int vbt_query_slice(vbt_asset* asset, uint32_t z, int t0, int t1, float* d_out, void* stream);
+
+/* Synchronise `stream` and return the first decode error recorded on the asset since the last
+ * call (lowest failing leaf; *bad_leaf set), then clear it. */
+int vbt_asset_sync_status(vbt_asset* asset, void* stream, uint32_t* bad_leaf);
+
+/* Host-buffer calls (end-to-end: copies in, kernels, copies out, synchronised). */
+int vbt_query_points_host(vbt_asset* asset, const uint32_t* xyzt, uint64_t n, float* out, void* stream);
+int vbt_decode_frames_host(vbt_asset* asset, const int* frames, int nframes, float* out, void* stream);
+
+/* Scalar decode of controls of one control stream already in device memory, one value per
+ * (control index, frame) pair, with every check of decodeRenderTemporalControlValue
+ * (src/render_temporal_decode.cpp:304-356); d_status[i] receives 0 or the VBT_STATUS code. */
+int vbt_decode_control_values(const uint8_t* d_stream, uint32_t stream_bytes, uint32_t codec, uint32_t control_count,
+                              uint32_t time_bins, uint32_t keyframe_count, int align4, int total_frames,
+                              const uint32_t* d_control_index, const int32_t* d_frame, uint64_t n, float* d_out,
+                              int32_t* d_status, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

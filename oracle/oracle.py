@@ -1,0 +1,285 @@
+"""ctypes bindings for the parity checker (test infrastructure only).
+
+``Oracle`` wraps liboracle.so, the C restatement of the reference decode path
+(vbt_oracle.c).  ``Reference`` wraps oracle/_ref/libvbtref.so, the reference decoder
+compiled from its own sources.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg use this module; the product (vbt_b200) never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libvbtref.so")
+
+u8p = C.POINTER(C.c_uint8)
+u32p = C.POINTER(C.c_uint32)
+f32p = C.POINTER(C.c_float)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+class VoFile(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("version", "width", "height", "depth", "frames", "leaf_size",
+                                          "coarse_res", "max_coarse_keep", "leaf_count", "profile_type",
+                                          "scale_count")] + [
+        ("scales", f32p), ("offsets", u32p), ("payload", u32p), ("payload_words", C.c_uint64)]
+
+
+class VoStream(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("desc_off", "desc_bytes", "bin_off", "bin_bytes", "key_off",
+                                          "key_bytes", "total")]
+
+
+class VoHeader(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("mode", "coarse_codec", "fine_codec", "coarse_res", "fine_res")]
+
+
+class VoLeafView(C.Structure):
+    _fields_ = [("header", VoHeader), ("coarse_kf", C.c_uint32), ("fine_kf", C.c_uint32),
+                ("coarse_off", C.c_uint32), ("fine_off", C.c_uint32), ("total", C.c_uint32),
+                ("coarse", VoStream), ("fine", VoStream), ("shell_active", C.c_uint32),
+                ("shell_residual_off", C.c_uint32), ("shell_residual_bytes", C.c_uint32)]
+
+
+def build(ref=False):
+    """Build liboracle.so (and, when the reference tree exists, oracle/_ref)."""
+    targets = ["oracle"] + (["ref"] if ref else [])
+    subprocess.check_call(["make", "-s", "-C", HERE, "-j8"] + targets)
+
+
+class Oracle:
+    def __init__(self):
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = self.lib = C.CDLL(ORACLE_SO)
+        L.vo_load_file.argtypes = [C.c_char_p, C.POINTER(VoFile), C.c_char_p, C.c_size_t]
+        L.vo_free_file.argtypes = [C.POINTER(VoFile)]
+        L.vo_decode_frame.argtypes = [C.POINTER(VoFile), C.c_int, f32p, C.c_int, u32p]
+        L.vo_build_page_table.argtypes = [C.POINTER(VoFile), u32p]
+        L.vo_build_page_table.restype = C.c_uint32
+        L.vo_decode_cache.argtypes = [C.POINTER(VoFile), C.c_int, u32p, f32p, C.c_int]
+        L.vo_query_points.argtypes = [C.POINTER(VoFile), u32p, C.c_uint64, f32p, C.c_int]
+        L.vo_sci_frame.argtypes = [C.POINTER(VoFile), C.c_uint32, f32p, C.c_int]
+        L.vo_sci_query_points.argtypes = [C.POINTER(VoFile), u32p, C.c_uint64, f32p, C.c_int]
+        L.vo_decode_control.argtypes = [u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                        C.c_int, C.c_uint32, C.c_int, f32p]
+        L.vo_decode_shell_voxel.argtypes = [u8p, C.POINTER(VoLeafView), C.c_int, C.c_uint32, C.c_int, f32p]
+        L.vo_parse_leaf.argtypes = [u8p, C.c_size_t, C.c_int, C.POINTER(VoLeafView)]
+        L.vo_decode_leaf_frame.argtypes = [u8p, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, f32p]
+        L.vo_half_to_float.argtypes = [C.c_uint16]
+        L.vo_half_to_float.restype = C.c_float
+        L.vo_float_to_half.argtypes = [C.c_float]
+        L.vo_float_to_half.restype = C.c_uint16
+        L.vo_dct_basis.restype = C.c_float
+        L.vo_dct_basis_f64.restype = C.c_double
+
+    def load(self, path):
+        return OracleFile(self, path)
+
+    def decode_control(self, stream, codec, cc, bins, kf, stream_bytes, total, ci, frame, align=True):
+        s = np.ascontiguousarray(stream, np.uint8)
+        out = C.c_float()
+        st = self.lib.vo_decode_control(_ptr(s, u8p), codec, cc, bins, kf, stream_bytes, int(align), total, ci,
+                                        frame, C.byref(out))
+        return st, out.value
+
+    def parse_leaf(self, leaf):
+        b = np.ascontiguousarray(leaf, np.uint8)
+        v = VoLeafView()
+        st = self.lib.vo_parse_leaf(_ptr(b, u8p), b.size, 1, C.byref(v))
+        return st, v
+
+    def shell_voxel(self, leaf, total, voxel, frame):
+        b = np.ascontiguousarray(leaf, np.uint8)
+        st, v = self.parse_leaf(b)
+        if st:
+            return st, 0.0
+        out = C.c_float()
+        st = self.lib.vo_decode_shell_voxel(_ptr(b, u8p), C.byref(v), total, voxel, frame, C.byref(out))
+        return st, out.value
+
+    def decode_leaf(self, leaf, total, frame, w=8, h=8, d=8):
+        b = np.ascontiguousarray(leaf, np.uint8)
+        out = np.zeros(w * h * d, np.float32)
+        st = self.lib.vo_decode_leaf_frame(_ptr(b, u8p), b.size, total, frame, w, h, d, _ptr(out, f32p))
+        return st, out
+
+
+class OracleFile:
+    def __init__(self, oracle, path):
+        self.o = oracle
+        self.f = VoFile()
+        err = C.create_string_buffer(512)
+        if oracle.lib.vo_load_file(path.encode(), C.byref(self.f), err, 512) != 0:
+            raise RuntimeError(err.value.decode())
+        self.dims = (self.f.width, self.f.height, self.f.depth)
+        self.frames = self.f.frames
+        self.leaf_count = self.f.leaf_count
+        self.profile = self.f.profile_type
+
+    def __del__(self):
+        try:
+            self.o.lib.vo_free_file(C.byref(self.f))
+        except Exception:
+            pass
+
+    def offsets(self):
+        return np.ctypeslib.as_array(self.f.offsets, (self.f.leaf_count + 1,)).copy()
+
+    def payload(self):
+        return np.ctypeslib.as_array(self.f.payload, (int(self.f.payload_words),)).copy()
+
+    def frame(self, t, threads=0):
+        X, Y, Z = self.dims
+        out = np.zeros(Z * Y * X, np.float32)
+        if self.profile == 2:
+            self.o.lib.vo_sci_frame(C.byref(self.f), t, _ptr(out, f32p), threads)
+            return out.reshape(Z, Y, X)
+        bad = C.c_uint32()
+        st = self.o.lib.vo_decode_frame(C.byref(self.f), t, _ptr(out, f32p), threads, C.byref(bad))
+        if st:
+            raise RuntimeError(f"oracle status {st} at leaf {bad.value}")
+        return out.reshape(Z, Y, X)
+
+    def page_table(self):
+        compact = np.zeros(self.f.leaf_count, np.uint32)
+        n = self.o.lib.vo_build_page_table(C.byref(self.f), _ptr(compact, u32p))
+        return compact, int(n)
+
+    def cache(self, t, threads=0):
+        compact, n = self.page_table()
+        out = np.zeros(max(n, 1) * 512, np.float32)
+        st = self.o.lib.vo_decode_cache(C.byref(self.f), t, _ptr(compact, u32p), _ptr(out, f32p), threads)
+        if st:
+            raise RuntimeError(f"oracle status {st}")
+        return out[: n * 512].reshape(n, 512)
+
+    def query(self, xyzt, threads=0):
+        q = np.ascontiguousarray(xyzt, np.uint32)
+        out = np.zeros(q.shape[0], np.float32)
+        if self.profile == 2:
+            self.o.lib.vo_sci_query_points(C.byref(self.f), _ptr(q, u32p), q.shape[0], _ptr(out, f32p), threads)
+        else:
+            st = self.o.lib.vo_query_points(C.byref(self.f), _ptr(q, u32p), q.shape[0], _ptr(out, f32p), threads)
+            if st:
+                raise RuntimeError(f"oracle status {st}")
+        return out
+
+
+class Reference:
+    """The reference decoder compiled from its sources (oracle/_ref/libvbtref.so)."""
+
+    def __init__(self):
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(REF_SO)
+        L = self.lib = C.CDLL(REF_SO)
+        L.vr_last_error.restype = C.c_char_p
+        L.vr_load.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t]
+        L.vr_load.restype = C.c_void_p
+        L.vr_free.argtypes = [C.c_void_p]
+        L.vr_decode_frame.argtypes = [C.c_void_p, C.c_int, f32p, C.c_int]
+        L.vr_sci_frame.argtypes = [C.c_void_p, C.c_uint32, f32p]
+        L.vr_sci_query.argtypes = [C.c_void_p, u32p, C.c_uint64, f32p, C.c_int]
+        L.vr_decode_control.argtypes = [u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                        C.c_int, C.c_uint32, C.c_int, f32p]
+        L.vr_parse_leaf.argtypes = [u8p, C.c_size_t, u32p]
+        L.vr_shell_voxel.argtypes = [u8p, C.c_size_t, C.c_int, C.c_uint32, C.c_int, f32p]
+        L.vr_decode_leaf.argtypes = [u8p, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, f32p]
+        L.vr_float_to_half.argtypes = [C.c_float]
+        L.vr_float_to_half.restype = C.c_uint16
+        L.vr_half_to_float.argtypes = [C.c_uint16]
+        L.vr_half_to_float.restype = C.c_float
+        L.vr_pack_stream.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, u8p, u32p, f32p,
+                                     C.c_uint32, C.c_int, u8p, C.c_size_t]
+        L.vr_pack_stream.restype = C.c_long
+        L.vr_build_leaf.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u8p, C.c_size_t, u8p, C.c_size_t, u8p,
+                                    C.c_size_t, C.c_int, u8p, C.c_size_t]
+        L.vr_build_leaf.restype = C.c_long
+
+    def error(self):
+        return self.lib.vr_last_error().decode()
+
+    def load(self, path):
+        err = C.create_string_buffer(512)
+        h = self.lib.vr_load(path.encode(), err, 512)
+        if not h:
+            raise RuntimeError(err.value.decode())
+        return h
+
+    def free(self, h):
+        self.lib.vr_free(h)
+
+    def frame(self, h, dims, t, profile=1, threads=0):
+        X, Y, Z = dims
+        out = np.zeros(Z * Y * X, np.float32)
+        if profile == 2:
+            st = self.lib.vr_sci_frame(h, t, _ptr(out, f32p))
+        else:
+            st = self.lib.vr_decode_frame(h, t, _ptr(out, f32p), threads)
+        if st:
+            raise RuntimeError(self.error())
+        return out.reshape(Z, Y, X)
+
+    def sci_query(self, h, xyzt, threads=0):
+        q = np.ascontiguousarray(xyzt, np.uint32)
+        out = np.zeros(q.shape[0], np.float32)
+        self.lib.vr_sci_query(h, _ptr(q, u32p), q.shape[0], _ptr(out, f32p), threads)
+        return out
+
+    def decode_control(self, stream, codec, cc, bins, kf, stream_bytes, total, ci, frame, align=True):
+        s = np.ascontiguousarray(stream, np.uint8)
+        out = C.c_float()
+        st = self.lib.vr_decode_control(_ptr(s, u8p), codec, cc, bins, kf, stream_bytes, int(align), total, ci,
+                                        frame, C.byref(out))
+        return (self.error() if st else None), out.value
+
+    def parse_leaf(self, leaf):
+        b = np.ascontiguousarray(leaf, np.uint8)
+        out = np.zeros(16, np.uint32)
+        st = self.lib.vr_parse_leaf(_ptr(b, u8p), b.size, _ptr(out, u32p))
+        return (self.error() if st else None), out
+
+    def shell_voxel(self, leaf, total, voxel, frame):
+        b = np.ascontiguousarray(leaf, np.uint8)
+        out = C.c_float()
+        st = self.lib.vr_shell_voxel(_ptr(b, u8p), b.size, total, voxel, frame, C.byref(out))
+        return (self.error() if st else None), out.value
+
+    def decode_leaf(self, leaf, total, frame, w=8, h=8, d=8):
+        b = np.ascontiguousarray(leaf, np.uint8)
+        out = np.zeros(w * h * d, np.float32)
+        st = self.lib.vr_decode_leaf(_ptr(b, u8p), b.size, total, frame, w, h, d, _ptr(out, f32p))
+        return (self.error() if st else None), out
+
+    def pack_stream(self, codec, desc, bin_index, key_frames, key_values, bins, max_local=255, align=True):
+        desc = np.ascontiguousarray(desc, np.uint32).reshape(-1)
+        cc = desc.size // 3
+        bi = np.ascontiguousarray(bin_index, np.uint8)
+        kfr = np.ascontiguousarray(key_frames, np.uint32)
+        kv = np.ascontiguousarray(key_values, np.float32)
+        cap = 64 + cc * (4 + bins + 4) + kfr.size * 8 + 16
+        out = np.zeros(cap, np.uint8)
+        n = self.lib.vr_pack_stream(codec, cc, bins, max_local, _ptr(desc, u32p), _ptr(bi, u8p), _ptr(kfr, u32p),
+                                    _ptr(kv, f32p), kfr.size, int(align), _ptr(out, u8p), cap)
+        if n < 0:
+            raise RuntimeError(self.error())
+        return out[:n].copy()
+
+    def build_leaf(self, packed_header, coarse_kf, fine_kf, coarse, fine, occ=None, align=True):
+        c = np.ascontiguousarray(coarse, np.uint8)
+        f = np.ascontiguousarray(fine, np.uint8)
+        o = None if occ is None else np.ascontiguousarray(occ, np.uint8)
+        cap = c.size + f.size + (0 if o is None else o.size) + 64
+        out = np.zeros(cap, np.uint8)
+        n = self.lib.vr_build_leaf(packed_header, coarse_kf, fine_kf, _ptr(c, u8p), c.size, _ptr(f, u8p), f.size,
+                                   None if o is None else _ptr(o, u8p), 0 if o is None else o.size, int(align),
+                                   _ptr(out, u8p), cap)
+        if n < 0:
+            raise RuntimeError(self.error())
+        return out[:n].copy()

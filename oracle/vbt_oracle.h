@@ -1,0 +1,104 @@
+/*
+ * vbt_oracle.h -- CPU restatement of VBT's compressed-domain temporal decode path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the parity checker for the CUDA
+ * path in vbt_b200/.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg load it; the product never links or calls it.
+ *
+ * Every function restates one function of the reference (VBT, namespace vbt /
+ * vbt::render) and cites the file:line it follows.  The restatement is pinned
+ * against (1) the known-answer cases of the reference's own tests
+ * (tests/temporal_decode_tests.cpp, tests/render_temporal_payload_tests.cpp,
+ * tests/vbt_file_tests.cpp), rebuilt as fixtures under tests/golden/, and
+ * (2) the reference decoder itself, compiled from its sources into
+ * oracle/_ref/ by oracle/Makefile and compared on every asset the tests use.
+ */
+#ifndef VBT_ORACLE_H
+#define VBT_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: identical numbering to include/vbt_b200.h (VBT_STATUS_*). */
+enum {
+    VO_OK = 0,
+    VO_ERR_LEAF_TOO_SMALL = 1,
+    VO_ERR_PREFIX_MISSING = 2,
+    VO_ERR_LEAF_SHORT = 3,
+    VO_ERR_SHELL_OCC_OOB = 4,
+    VO_ERR_SHELL_GROUP_PREFIX = 5,
+    VO_ERR_SHELL_NO_ACTIVE = 6,
+    VO_ERR_SHELL_RESIDUAL_OOB = 7,
+    VO_ERR_SHELL_TRAILING = 8,
+    VO_ERR_CONTROL_INDEX = 9,
+    VO_ERR_STREAM_OOB = 10,
+    VO_ERR_DECODE_OOB = 11,
+    VO_ERR_KEY_RANGE_OOB = 12,
+    VO_ERR_KEY_INDEX = 13,
+};
+
+typedef struct {
+    uint32_t mode, coarse_codec, fine_codec, coarse_res, fine_res;
+} vo_header;
+
+typedef struct {
+    uint32_t desc_off, desc_bytes, bin_off, bin_bytes, key_off, key_bytes, total;
+} vo_stream_layout;
+
+typedef struct {
+    vo_header header;
+    uint32_t coarse_kf, fine_kf;
+    uint32_t coarse_off, fine_off, total;
+    vo_stream_layout coarse, fine;
+    uint32_t shell_active, shell_residual_off, shell_residual_bytes;
+} vo_leaf_view;
+
+/* VBTPACK4 file as loaded by render/src/vbt_file.cpp:109-210. */
+typedef struct {
+    uint32_t version, width, height, depth, frames, leaf_size, coarse_res, max_coarse_keep,
+        leaf_count, profile_type, scale_count;
+    float* scales;
+    uint32_t* offsets;      /* leaf_count + 1 words */
+    uint32_t* payload;      /* offsets[leaf_count] words */
+    uint64_t payload_words;
+} vo_file;
+
+uint32_t vo_pack_header(const vo_header* h);
+void vo_unpack_header(uint32_t packed, vo_header* out);
+void vo_leaf_layout(const vo_header* h, uint32_t coarse_kf, uint32_t fine_kf, int align4, vo_leaf_view* out);
+int vo_parse_leaf(const uint8_t* leaf, size_t bytes, int align4, vo_leaf_view* out);
+float vo_half_to_float(uint16_t bits);
+uint16_t vo_float_to_half(float v);
+
+int vo_decode_control(const uint8_t* stream, uint32_t codec, uint32_t control_count, uint32_t bins,
+                      uint32_t kf_count, uint32_t stream_bytes, int align4, int total_frames,
+                      uint32_t control_index, int frame, float* out);
+int vo_decode_shell_voxel(const uint8_t* leaf, const vo_leaf_view* v, int total_frames,
+                          uint32_t voxel, int frame, float* out);
+int vo_decode_leaf_frame(const uint8_t* leaf, size_t bytes, int total_frames, int frame,
+                         int w, int h, int d, float* out);
+
+int vo_load_file(const char* path, vo_file* out, char* err, size_t err_len);
+void vo_free_file(vo_file* f);
+
+/* Render-temporal family (profileType 0/1). */
+int vo_decode_frame(const vo_file* f, int frame, float* out, int threads, uint32_t* bad_leaf);
+uint32_t vo_build_page_table(const vo_file* f, uint32_t* compact);
+int vo_decode_cache(const vo_file* f, int frame, const uint32_t* compact, float* cache, int threads);
+int vo_query_points(const vo_file* f, const uint32_t* xyzt, uint64_t n, float* out, int threads);
+
+/* Scientific family (profileType 2). */
+float vo_sci_value(const vo_file* f, uint32_t x, uint32_t y, uint32_t z, uint32_t t);
+void vo_sci_frame(const vo_file* f, uint32_t frame, float* out, int threads);
+void vo_sci_query_points(const vo_file* f, const uint32_t* xyzt, uint64_t n, float* out, int threads);
+double vo_dct_basis_f64(int total, int index, int k);
+float vo_dct_basis(int total, int index, int k);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,192 @@
+#!/usr/bin/env python3
+"""Build the seeded synthetic VBTPACK4 assets used by the tests and the benchmark.
+
+Each asset is a float32 field generated here with numpy from a fixed seed, written as a
+RAW file plus the metadata JSON the reference encoder reads (src/frame_metadata.h), then
+encoded by the reference encoder ``vbt_spatialfirst_probe`` (built from the reference
+sources into oracle/_ref/ by oracle/Makefile).  Outputs go to assets/<name>.vbtp
+(git-ignored; they travel to the GPU host with the working tree).  The encoder is
+deterministic, so the same seed gives byte-identical assets.
+
+Field recipes (shapes are X x Y x Z x T):
+  cfg1_blobs      64^3 x 24, 6 Gaussian blobs (sigma U(4,10), amplitude U(0.2,1)) moving on
+                  linear paths at <=1 voxel/frame, plus N(0, 0.01) noise; density profile.
+  cfg2_plume      256^3 x 96, buoyant plume: 4-octave fBm value noise inside a cone rising at
+                  1.5 voxels/frame, clamped to [0, 1], exactly 0 outside; density profile.
+  cfg4_sdf_small  64^3 x 24 level set (a scaled-down config-4 scene): sloshing plane
+                  z = 24 + 2 sin(0.2 x + 0.1 t) united with 6 ballistic spheres; Mode2 shell.
+  tiny_*          small, odd-sized fields (boundary leaves with cropped extents).
+  sci_*           scientific (generic profile, time-fastest RAW) Gaussian random fields with a
+                  k^-5/3 spectrum, phase drift, and 0.1% spikes of 10 sigma.
+
+Usage: python tests/golden/make_assets.py [names...]   (default: the small set + cfg1 + cfg2)
+"""
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+ASSETS = os.path.join(ROOT, "assets")
+ENCODER = os.path.join(ROOT, "oracle", "_ref", "vbt_spatialfirst_probe")
+
+
+# ----------------------------------------------------------------------------- fields
+def blobs(shape_xyz, frames, n_blobs, seed, noise=0.01):
+    rng = np.random.default_rng(seed)
+    X, Y, Z = shape_xyz
+    sig = rng.uniform(4.0, 10.0, n_blobs)
+    amp = rng.uniform(0.2, 1.0, n_blobs)
+    c0 = rng.uniform(0.2, 0.8, (n_blobs, 3)) * np.array([X, Y, Z])
+    d = rng.normal(size=(n_blobs, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    vel = d * rng.uniform(0.0, 1.0, (n_blobs, 1))
+    zz, yy, xx = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(X), indexing="ij")
+    out = np.empty((frames, Z, Y, X), np.float32)
+    for t in range(frames):
+        f = np.zeros((Z, Y, X), np.float64)
+        for b in range(n_blobs):
+            c = c0[b] + vel[b] * t
+            r2 = (xx - c[0]) ** 2 + (yy - c[1]) ** 2 + (zz - c[2]) ** 2
+            f += amp[b] * np.exp(-r2 / (2.0 * sig[b] ** 2))
+        f += rng.normal(0.0, noise, f.shape)
+        out[t] = f.astype(np.float32)
+    return out
+
+
+def fbm_volume(shape_zyx, octaves, base_cell, seed):
+    """4-octave fBm of trilinearly interpolated value noise on a lattice, in [0, 1]."""
+    from scipy.ndimage import zoom
+    rng = np.random.default_rng(seed)
+    Z, Y, X = shape_zyx
+    acc = np.zeros(shape_zyx, np.float32)
+    amp, norm = 1.0, 0.0
+    for o in range(octaves):
+        cell = max(1, base_cell >> o)
+        lat = rng.random((Z // cell + 2, Y // cell + 2, X // cell + 2)).astype(np.float32)
+        up = zoom(lat, cell, order=1, prefilter=False)[:Z, :Y, :X]
+        acc += amp * up
+        norm += amp
+        amp *= 0.5
+    return acc / norm
+
+
+def plume(size, frames, seed):
+    """Cone-shaped plume rising at 1.5 voxels/frame.  The fBm is advected upward by sampling
+    a static noise volume built at half-voxel z spacing (1.5 voxels = 3 half-voxel slices)."""
+    S = size
+    zpad = 3 * (frames - 1)
+    noise = fbm_volume((2 * S + zpad, S, S), 4, 32, seed)   # half-voxel z spacing
+    zz, yy, xx = np.meshgrid(np.arange(S), np.arange(S), np.arange(S), indexing="ij")
+    cx = cy = S / 2.0
+    r_xy = np.sqrt((xx - cx) ** 2 + (yy - cy) ** 2)
+    z0 = S * 0.04
+    out = np.empty((frames, S, S, S), np.float32)
+    for t in range(frames):
+        top = z0 + S * 0.25 + 1.5 * t                      # front of the rising plume
+        radius = 0.12 * S * 0.25 + 0.14 * (zz - z0)        # cone opening upward
+        inside = (zz >= z0) & (zz <= top) & (r_xy <= radius)
+        idx = 2 * zz - 3 * t + zpad                        # z - 1.5 t in half-voxel units
+        n = noise[idx, yy, xx]
+        edge = np.clip((radius - r_xy) / 6.0, 0.0, 1.0) * np.clip((top - zz) / 8.0, 0.0, 1.0)
+        val = np.clip((n - 0.35) * 2.5 * edge, 0.0, 1.0)
+        val[~inside] = 0.0
+        out[t] = val.astype(np.float32)
+    return out
+
+
+def sdf_scene(shape_xyz, frames, plane_z, plane_amp, kx, n_spheres, rmin, rmax, seed, g=0.05):
+    rng = np.random.default_rng(seed)
+    X, Y, Z = shape_xyz
+    c0 = np.stack([rng.uniform(0, X, n_spheres), rng.uniform(0, Y, n_spheres),
+                   rng.uniform(plane_z, Z * 0.9, n_spheres)], axis=1)
+    v0 = np.stack([rng.uniform(-0.5, 0.5, n_spheres), rng.uniform(-0.5, 0.5, n_spheres),
+                   rng.uniform(0.0, 1.0, n_spheres)], axis=1)
+    rad = rng.uniform(rmin, rmax, n_spheres)
+    zz, yy, xx = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(X), indexing="ij")
+    out = np.empty((frames, Z, Y, X), np.float32)
+    for t in range(frames):
+        phi = zz - (plane_z + plane_amp * np.sin(kx * xx + 0.1 * t))
+        for s in range(n_spheres):
+            c = c0[s] + v0[s] * t + np.array([0.0, 0.0, -0.5 * g * t * t])
+            d = np.sqrt((xx - c[0]) ** 2 + (yy - c[1]) ** 2 + (zz - c[2]) ** 2) - rad[s]
+            phi = np.minimum(phi, d)
+        out[t] = phi.astype(np.float32)
+    return out
+
+
+def grf_scientific(shape_xyz, frames, seed, spike_frac=0.001, spike_sigma=10.0):
+    """Gaussian random field, k^-5/3 power spectrum, evolved by a per-mode phase drift."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z = shape_xyz
+    kz = np.fft.fftfreq(Z)[:, None, None]
+    ky = np.fft.fftfreq(Y)[None, :, None]
+    kx = np.fft.fftfreq(X)[None, None, :]
+    k = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    k[0, 0, 0] = 1.0
+    amp = k ** (-5.0 / 6.0)                                  # |F|^2 ~ k^-5/3
+    amp[0, 0, 0] = 0.0
+    phase0 = rng.uniform(0, 2 * np.pi, k.shape)
+    omega = rng.normal(0.0, 0.08, k.shape)
+    out = np.empty((Z, Y, X, frames), np.float32)           # time fastest
+    for t in range(frames):
+        spec = amp * np.exp(1j * (phase0 + omega * t))
+        f = np.real(np.fft.ifftn(spec))
+        out[..., t] = f.astype(np.float32)
+    sigma = float(out.std())
+    out /= max(sigma, 1e-12)
+    n_spk = max(1, int(spike_frac * out.size))
+    idx = rng.choice(out.size, n_spk, replace=False)
+    out.reshape(-1)[idx] += np.float32(spike_sigma) * np.sign(rng.normal(size=n_spk)).astype(np.float32)
+    return out
+
+
+# ----------------------------------------------------------------------------- encode
+def encode(name, data, xyzt, profile, extra_meta=None, time_fastest=False):
+    os.makedirs(ASSETS, exist_ok=True)
+    if not os.path.exists(ENCODER):
+        subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "ref"])
+    X, Y, Z, T = xyzt
+    with tempfile.TemporaryDirectory(dir=os.environ.get("VBT_ASSET_TMP")) as td:
+        raw = os.path.join(td, name + ".raw")
+        meta = os.path.join(td, name + ".metadata.json")
+        data.astype(np.float32).tofile(raw)
+        m = {"dimensions": [X, Y, Z, T], "axis_order": ["X", "Y", "Z", "T"],
+             "time_is_fastest_dimension": bool(time_fastest), "data_type": "float32",
+             "data_min": float(data.min()), "data_max": float(data.max())}
+        if extra_meta:
+            m.update(extra_meta)
+        with open(meta, "w") as fh:
+            json.dump(m, fh)
+        out = os.path.join(ASSETS, name + ".vbtp")
+        cmd = [ENCODER, "--input-raw", raw, "--metadata", meta, "--profile", profile,
+               "--save-vbt", out, "--report", os.path.join(td, "report.md"), "--omp-threads", "8"]
+        subprocess.check_call(cmd, stdout=subprocess.DEVNULL)
+    print(f"{name}: {os.path.getsize(out)} bytes")
+    return out
+
+
+LEVELSET = {"conversion_mode": "levelset", "shell_width_voxels": 3.0, "voxel_size": 1.0}
+
+RECIPES = {
+    "tiny_density": lambda: encode("tiny_density", blobs((20, 12, 17), 9, 3, 11), (20, 12, 17, 9), "density"),
+    "tiny_levelset": lambda: encode("tiny_levelset", sdf_scene((24, 20, 28), 12, 12.0, 2.0, 0.3, 3, 2.0, 5.0, 12),
+                                    (24, 20, 28, 12), "density", LEVELSET),
+    "cfg1_blobs": lambda: encode("cfg1_blobs", blobs((64, 64, 64), 24, 6, 1), (64, 64, 64, 24), "density"),
+    "cfg4_sdf_small": lambda: encode("cfg4_sdf_small", sdf_scene((64, 64, 64), 24, 24.0, 2.0, 0.2, 6, 3.0, 8.0, 4),
+                                     (64, 64, 64, 24), "density", LEVELSET),
+    "sci_small": lambda: encode("sci_small", grf_scientific((24, 16, 20), 16, 5), (24, 16, 20, 16), "generic",
+                                time_fastest=True),
+    "sci_64": lambda: encode("sci_64", grf_scientific((64, 64, 64), 32, 6), (64, 64, 64, 32), "generic",
+                             time_fastest=True),
+    "cfg2_plume": lambda: encode("cfg2_plume", plume(256, 96, 2), (256, 256, 256, 96), "density"),
+}
+DEFAULT = ["tiny_density", "tiny_levelset", "sci_small", "cfg1_blobs", "cfg4_sdf_small", "sci_64", "cfg2_plume"]
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or DEFAULT
+    for n in names:
+        RECIPES[n]()

@@ -1,0 +1,234 @@
+"""vbt_b200 -- B200-native (sm_100a) compressed-domain temporal decode of VBTPACK4 assets.
+
+This module is a thin ctypes binding of the C-ABI in include/vbt_b200.h (libvbt_b200.so,
+built in-tree by vbt_b200/build.py).  The decode work runs only in the CUDA kernels of that
+library; there is no CPU execution path.  Importing this module fails loudly when the library
+is missing; decode calls fail with VbtError(status=VBT_STATUS_CUDA) without a usable GPU.
+
+Device buffers are passed as torch CUDA tensors (for their device pointers and streams only) or
+as raw integer device addresses.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvbt_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"vbt_b200: {LIB_PATH} is missing; build it with `python -m vbt_b200.build`")
+
+_lib = C.CDLL(LIB_PATH)
+
+STATUS = {
+    0: "OK", 1: "LEAF_TOO_SMALL", 2: "PREFIX_MISSING", 3: "LEAF_SHORT", 4: "SHELL_OCC_OOB",
+    5: "SHELL_GROUP_PREFIX", 6: "SHELL_NO_ACTIVE", 7: "SHELL_RESIDUAL_OOB", 8: "SHELL_TRAILING",
+    9: "CONTROL_INDEX", 10: "STREAM_OOB", 11: "DECODE_OOB", 12: "KEY_RANGE_OOB", 13: "KEY_INDEX",
+    30: "WAIT_TIMEOUT", 40: "INVALID_ARGUMENT", 41: "FILE", 42: "CUDA", 43: "LIMIT",
+}
+
+
+class VbtHeader(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("version", "width", "height", "depth", "frames", "leaf_size",
+                                          "coarse_resolution", "max_coarse_keep", "leaf_count", "profile_type",
+                                          "coarse_ac_scale_count")]
+
+
+class VbtAssetInfo(C.Structure):
+    _fields_ = [("header", VbtHeader), ("leaf_count_x", C.c_uint32), ("leaf_count_y", C.c_uint32),
+                ("leaf_count_z", C.c_uint32), ("active_leaf_count", C.c_uint32), ("payload_words", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("device", C.c_int)]
+
+
+_vp, _u32p, _i32p, _f32p = C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.c_void_p
+_sig = {
+    "vbt_status_string": ([C.c_int], C.c_char_p),
+    "vbt_last_error": ([], C.c_char_p),
+    "vbt_device_count": ([], C.c_int),
+    "vbt_validate_file_image": ([_vp, C.c_uint64, C.POINTER(VbtHeader)], C.c_int),
+    "vbt_asset_open": ([C.c_char_p, C.c_int, C.POINTER(_vp)], C.c_int),
+    "vbt_asset_create": ([_vp, C.c_uint64, C.c_int, C.POINTER(_vp)], C.c_int),
+    "vbt_asset_destroy": ([_vp], C.c_int),
+    "vbt_asset_get_info": ([_vp, C.POINTER(VbtAssetInfo)], C.c_int),
+    "vbt_build_page_table": ([_vp, _vp], C.c_int),
+    "vbt_page_table_device": ([_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)], C.c_int),
+    "vbt_get_page_table": ([_vp, _vp, _u32p], C.c_int),
+    "vbt_get_leaf_table": ([_vp, _vp], C.c_int),
+    "vbt_decode_cache": ([_vp, _i32p, C.c_int, _vp, C.c_uint64, C.c_int, _vp], C.c_int),
+    "vbt_decode_cache_plain": ([_vp, C.c_int, _vp, _vp], C.c_int),
+    "vbt_decode_frames": ([_vp, _i32p, C.c_int, _vp, C.c_int, _vp], C.c_int),
+    "vbt_query_points": ([_vp, _vp, C.c_uint64, _vp, _vp], C.c_int),
+    "vbt_query_slice": ([_vp, C.c_uint32, C.c_int, C.c_int, _vp, _vp], C.c_int),
+    "vbt_asset_sync_status": ([_vp, _vp, _u32p], C.c_int),
+    "vbt_query_points_host": ([_vp, _vp, C.c_uint64, _vp, _vp], C.c_int),
+    "vbt_decode_frames_host": ([_vp, _i32p, C.c_int, _vp, _vp], C.c_int),
+    "vbt_decode_control_values": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                   C.c_int, _vp, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
+}
+for _name, (_args, _res) in _sig.items():
+    _f = getattr(_lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res
+
+EXPORTS = tuple(_sig)
+
+
+class VbtError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+def _check(status):
+    if status != 0:
+        raise VbtError(status, _lib.vbt_last_error().decode(errors="replace"))
+
+
+def lib():
+    return _lib
+
+
+def device_count():
+    return _lib.vbt_device_count()
+
+
+def status_string(status):
+    return _lib.vbt_status_string(status).decode()
+
+
+def _addr(x):
+    """Device address of a torch tensor or an int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except Exception:
+            pass
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def validate_file_image(data):
+    h = VbtHeader()
+    buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+    _check(_lib.vbt_validate_file_image(C.cast(buf, _vp), len(data), C.byref(h)))
+    return h
+
+
+class Asset:
+    """A VBTPACK4 asset resident on one GPU (offsets, payload, leaf table, page table)."""
+
+    def __init__(self, path=None, data=None, device=0):
+        self._h = _vp()
+        if path is not None:
+            _check(_lib.vbt_asset_open(os.fspath(path).encode(), device, C.byref(self._h)))
+        else:
+            buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+            _check(_lib.vbt_asset_create(C.cast(buf, _vp), len(data), device, C.byref(self._h)))
+        self.refresh_info()
+
+    def refresh_info(self):
+        info = VbtAssetInfo()
+        _check(_lib.vbt_asset_get_info(self._h, C.byref(info)))
+        self.info = info
+        h = info.header
+        self.dims = (h.width, h.height, h.depth)
+        self.frames = h.frames
+        self.leaf_count = h.leaf_count
+        self.profile = h.profile_type
+        self.active_count = info.active_leaf_count
+        self.device = info.device
+        return info
+
+    def close(self):
+        if self._h:
+            _lib.vbt_asset_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # kernel (a)
+    def build_page_table(self, stream=None):
+        _check(_lib.vbt_build_page_table(self._h, _stream(stream)))
+
+    def page_table_device(self):
+        c, l, n = _vp(), _vp(), _vp()
+        _check(_lib.vbt_page_table_device(self._h, C.byref(c), C.byref(l), C.byref(n)))
+        return c.value, l.value, n.value
+
+    def page_table(self):
+        import numpy as np
+        compact = np.zeros(self.leaf_count, np.uint32)
+        n = C.c_uint32()
+        _check(_lib.vbt_get_page_table(self._h, compact.ctypes.data, C.byref(n)))
+        return compact, n.value
+
+    def leaf_table(self):
+        import numpy as np
+        rows = np.zeros((self.leaf_count, 8), np.uint32)
+        _check(_lib.vbt_get_leaf_table(self._h, rows.ctypes.data))
+        return rows
+
+    # kernel (b)
+    def decode_cache(self, frames, out, frame_stride=None, grid=0, stream=None):
+        fr = (C.c_int32 * len(frames))(*frames)
+        if frame_stride is None:
+            frame_stride = self.active_count * 512
+        _check(_lib.vbt_decode_cache(self._h, fr, len(frames), _addr(out), frame_stride, grid, _stream(stream)))
+
+    def decode_cache_plain(self, frame, out, stream=None):
+        _check(_lib.vbt_decode_cache_plain(self._h, frame, _addr(out), _stream(stream)))
+
+    def decode_frames(self, frames, out, grid=0, stream=None):
+        fr = (C.c_int32 * len(frames))(*frames)
+        _check(_lib.vbt_decode_frames(self._h, fr, len(frames), _addr(out), grid, _stream(stream)))
+
+    # kernel (c)
+    def query_points(self, xyzt, out, stream=None):
+        n = xyzt.shape[0] if hasattr(xyzt, "shape") else 0
+        _check(_lib.vbt_query_points(self._h, _addr(xyzt), n, _addr(out), _stream(stream)))
+
+    def query_slice(self, z, t0, t1, out, stream=None):
+        _check(_lib.vbt_query_slice(self._h, z, t0, t1, _addr(out), _stream(stream)))
+
+    def sync_status(self, stream=None):
+        bad = C.c_uint32()
+        st = _lib.vbt_asset_sync_status(self._h, _stream(stream), C.byref(bad))
+        if st != 0:
+            raise VbtError(st, _lib.vbt_last_error().decode(errors="replace"))
+        return True
+
+    # host-buffer (end-to-end) calls
+    def query_points_host(self, xyzt, out, stream=None):
+        _check(_lib.vbt_query_points_host(self._h, xyzt.ctypes.data, xyzt.shape[0], out.ctypes.data,
+                                          _stream(stream)))
+
+    def decode_frames_host(self, frames, out, stream=None):
+        fr = (C.c_int32 * len(frames))(*frames)
+        _check(_lib.vbt_decode_frames_host(self._h, fr, len(frames), out.ctypes.data, _stream(stream)))
+
+
+def decode_control_values(d_stream, stream_bytes, codec, control_count, bins, kf, total_frames, d_ci, d_frames, n,
+                          d_out, d_status, align=True, stream=None):
+    _check(_lib.vbt_decode_control_values(_addr(d_stream), stream_bytes, codec, control_count, bins, kf, int(align),
+                                          total_frames, _addr(d_ci), _addr(d_frames), n, _addr(d_out),
+                                          _addr(d_status), _stream(stream)))

@@ -1,0 +1,972 @@
+// kernels.cu -- the hand-written sm_100a kernels of the decode path.
+//
+//  (a) walk_kernel          payload walker: validates every leaf once, writes the 32-byte leaf
+//                           table, and builds the active-leaf page table by warp-ballot/popc
+//                           compaction with a single-pass decoupled look-back across CTAs.
+//  (b) decode_*_kernel      warp-per-leaf decode into the current-frame voxel cache (512 FP32
+//                           per active leaf) or into dense frames, several frames per launch.
+//  (c) query_*_kernel       batched (x, y, z, t) point queries and z-slice queries.
+//
+// Render-temporal arithmetic is bit-exact with the reference CPU decoder (every float op is an
+// explicitly rounded _rn intrinsic; see rt_decode.cuh).  Scientific coarse controls are summed in
+// compensated float-float arithmetic (error-free products and two-sums) to track the reference's
+// double accumulation (render/src/scientific_decode.cpp:82-97) without FP64 on the device.
+#include <cuda/atomic>
+
+#include "kernels.cuh"
+#include "rt_decode.cuh"
+
+namespace vbtb {
+
+// Axis weight table (see AxisWeight), filled once per process by upload_axis_tables().
+__constant__ AxisWeight c_axis[kAxisRes * kAxisExt * kAxisPos];
+__device__ AxisWeight g_axis[kAxisRes * kAxisExt * kAxisPos];
+// Scientific trilinear axes: [0] coarse 4^3 grid (f = x/7*3, clamp 0..2), [1] dense 3^3, [2] dense 4^3.
+__constant__ AxisWeight c_sci_axis[3][8];
+
+// ---------------------------------------------------------------------------------------------
+// host: axis tables, computed with the same float expressions as the reference
+// (render/src/render_smoke_vbt_bench_main.cpp:201-234; render/src/scientific_decode.cpp:99-123,
+// :137-149).  Host float arithmetic is IEEE binary32 with round-to-nearest and no contraction
+// (this translation unit's host code is compiled with -ffp-contract=off).
+void upload_axis_tables()
+{
+    static AxisWeight tab[kAxisRes * kAxisExt * kAxisPos];
+    for (int res = 0; res < kAxisRes; ++res)
+        for (int ext = 0; ext < kAxisExt; ++ext)
+            for (int pos = 0; pos < kAxisPos; ++pos) {
+                AxisWeight w{0, 0, 0, 0, 0.0f, 1.0f};
+                if (res >= 2) {
+                    const float scale = 7.0f / (float)(res - 1);
+                    const float maxp = (float)(ext - 1 > 0 ? ext - 1 : 0);
+                    float p = (float)pos;
+                    p = p < 0.0f ? 0.0f : (p > maxp ? maxp : p);
+                    int i1 = 1;
+                    while (i1 < res - 1 && (float)i1 * scale < p) ++i1;
+                    const int i0 = i1 - 1 > 0 ? i1 - 1 : 0;
+                    const float c0 = (float)i0 * scale, c1 = (float)i1 * scale;
+                    const volatile float num = p - c0;
+                    const volatile float den = c1 - c0;
+                    const float t = (c1 > c0) ? (num / den) : 0.0f;
+                    w.i0 = (uint8_t)i0;
+                    w.i1 = (uint8_t)i1;
+                    w.t = t;
+                    w.omt = 1.0f - t;
+                }
+                tab[axis_index(res, ext, pos)] = w;
+            }
+    cudaMemcpyToSymbol(c_axis, tab, sizeof(tab));
+    cudaMemcpyToSymbol(g_axis, tab, sizeof(tab));
+    AxisWeight sci[3][8];
+    const int grids[3] = {4, 3, 4};
+    for (int g = 0; g < 3; ++g)
+        for (int p = 0; p < 8; ++p) {
+            const int res = grids[g];
+            const volatile float q = (float)p / 7.0f;
+            const float f = q * (float)(res - 1);
+            int i0 = (int)floorf(f);
+            i0 = i0 < 0 ? 0 : (i0 > res - 2 ? res - 2 : i0);
+            const float t = f - (float)i0;
+            sci[g][p] = AxisWeight{(uint8_t)i0, (uint8_t)(i0 + 1), 0, 0, t, 1.0f - t};
+        }
+    cudaMemcpyToSymbol(c_sci_axis, sci, sizeof(sci));
+}
+
+// ---------------------------------------------------------------------------------------------
+// shared helpers
+
+__device__ __forceinline__ void record_error(unsigned long long* err, uint32_t leaf, uint32_t status)
+{
+    atomicMin(err, ((unsigned long long)leaf << 8) | status);
+}
+
+__device__ __forceinline__ void leaf_extent(const AssetGeom& g, uint32_t leaf, uint32_t& bx, uint32_t& by,
+                                            uint32_t& bz, int& w, int& h, int& d)
+{
+    bx = leaf % g.lcx;
+    by = (leaf / g.lcx) % g.lcy;
+    bz = leaf / (g.lcx * g.lcy);
+    const int ex = (int)g.width - (int)bx * 8, ey = (int)g.height - (int)by * 8, ez = (int)g.depth - (int)bz * 8;
+    w = ex < 8 ? ex : 8;
+    h = ey < 8 ? ey : 8;
+    d = ez < 8 ? ez : 8;
+}
+
+// ---------------------------------------------------------------------------------------------
+// (a) payload walker + page table
+
+// Validate one render-temporal leaf with the whole warp (src/render_temporal_payload.cpp:234-311
+// for the layout and Mode2 occupancy checks; src/render_temporal_decode.cpp:316-339 for the
+// stream-size and keyframe-range checks the decoder would make on every control it decodes).
+__device__ LeafEntry walk_rt_leaf(const DeviceAsset& a, uint32_t leaf, int lane)
+{
+    const uint32_t* __restrict__ pw = a.payload;
+    LeafEntry e{};
+    const uint32_t wb = __ldg(a.offsets + leaf), we = __ldg(a.offsets + leaf + 1);
+    const uint64_t bytes = 4ull * (we - wb);
+    e.word_off = wb;
+    e.header = ldw(pw, wb);
+    const uint32_t mode = e.header & 3u;
+    if (mode == kModeEmpty) return e;
+    uint32_t status = kOk, flags = kFlagActive;
+    if (bytes < 8u) {
+        e.info = flags | (kErrPrefixMissing << 16);
+        return e;
+    }
+    const uint32_t ccodec = (e.header >> 2) & 3u, fcodec = (e.header >> 4) & 3u;
+    const uint32_t cres = (e.header >> 6) & 7u, fres = (e.header >> 9) & 7u;
+    e.kf = ldw(pw, wb + 1);
+    const uint32_t ckf = e.kf & 0xFFFFu, fkf = e.kf >> 16;
+    const uint32_t cc = cres * cres * cres, fc = fres * fres * fres;
+    e.coarse_bytes = stream_bytes(cc, 8u, ckf, ccodec);
+    const uint32_t fine_off = 8u + e.coarse_bytes;
+    uint32_t total = fine_off;
+    if (mode == kModeFine6) {
+        e.fine_bytes = stream_bytes(fc, 8u, fkf, fcodec);
+        total = fine_off + e.fine_bytes;
+    } else if (mode == kModeFineCompact) {
+        e.fine_bytes = 80u + align4(fkf * key_stride(fcodec));
+        total = fine_off + e.fine_bytes;
+    }
+    uint32_t active = 0;
+    if (total > bytes) {
+        status = kErrLeafShort;
+    } else if (mode == kModeFineCompact) {
+        flags |= kFlagOccClamp;
+        // occupancy: u64 mask[8] at fine_off, u16 prefix[8] at fine_off + 64
+        const uint64_t ob = 4ull * wb + fine_off;
+        uint32_t pc = 0, pref = 0;
+        if (lane < 8) {
+            const uint32_t m0 = ldw(pw, (uint32_t)((ob + 8u * lane) >> 2));
+            const uint32_t m1 = ldw(pw, (uint32_t)((ob + 8u * lane + 4u) >> 2));
+            pc = __popc(m0) + __popc(m1);
+            pref = (ldw(pw, (uint32_t)((ob + 64u + 2u * lane) >> 2)) >> ((lane & 1) * 16)) & 0xFFFFu;
+        }
+        // exclusive scan of the 8 group popcounts
+        uint32_t incl = pc;
+        for (int o = 1; o < 8; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const uint32_t excl = incl - pc;
+        const unsigned bad = __ballot_sync(0xFFFFFFFFu, lane < 8 && pref != excl);
+        active = __shfl_sync(0xFFFFFFFFu, incl, 7);
+        if (bad) {
+            status = kErrShellGroupPrefix;
+        } else if (active == 0u) {
+            status = kErrShellNoActive;
+        } else {
+            const uint64_t res_off = fine_off + 80u;   // fine_off is 4-aligned
+            const uint64_t res_bytes = 4ull * active + 4ull * active + (uint64_t)align4(fkf * key_stride(fcodec));
+            if (res_off > bytes || res_bytes > bytes - res_off) status = kErrShellResidualOob;
+            else if (res_off + res_bytes != bytes) status = kErrShellTrailing;
+            e.shell_off = (uint32_t)res_off;
+            e.shell_bytes = (uint32_t)res_bytes;
+        }
+    }
+    if (status == kOk) {
+        // coarse controls: keyStart + keyCount must stay inside the keyframe pool
+        const uint64_t cbase = 4ull * wb + 8u;
+        bool bad = false;
+        for (uint32_t c = lane; c < cc; c += 32) {
+            const uint32_t dsc = ldw(pw, (uint32_t)((cbase + 4ull * c) >> 2));
+            const uint32_t kc = (dsc >> 16) & 0xFFu;
+            bad |= kc != 0u && (dsc & 0xFFFFu) + kc > ckf;
+        }
+        if (__any_sync(0xFFFFFFFFu, bad)) status = kErrKeyRangeOob;
+    }
+    const bool has_fine = fres > 0u && e.fine_bytes > 0u && mode != kModeGrid4;
+    if (status == kOk && has_fine) {
+        flags |= kFlagFine;
+        if (stream_bytes(fc, 8u, fkf, fcodec) > e.fine_bytes) {
+            status = kErrStreamOob;
+        } else {
+            const uint64_t fbase = 4ull * wb + fine_off;
+            bool bad = false;
+            for (uint32_t c = lane; c < fc; c += 32) {
+                const uint32_t dsc = ldw(pw, (uint32_t)((fbase + 4ull * c) >> 2));
+                const uint32_t kc = (dsc >> 16) & 0xFFu;
+                bad |= kc != 0u && (dsc & 0xFFFFu) + kc > fkf;
+            }
+            if (__any_sync(0xFFFFFFFFu, bad)) status = kErrKeyRangeOob;
+        }
+    }
+    if (status == kOk && mode == kModeFineCompact && !has_fine && fkf > 0u) {
+        flags |= kFlagShell;
+        // Only occupied voxels inside the leaf extent are ever decoded, so only their descriptors
+        // are checked (src/render_temporal_decode.cpp:404-450 per voxel of the cropped extent).
+        uint32_t bx, by, bz;
+        int w, h, d;
+        leaf_extent(a.g, leaf, bx, by, bz, w, h, d);
+        const uint64_t ob = 4ull * wb + fine_off;
+        const uint64_t sbase = 4ull * wb + e.shell_off;
+        bool bad = false;
+        for (uint32_t v = lane; v < 512u; v += 32) {
+            const int lx = v & 7, ly = (v >> 3) & 7, lz = v >> 6;
+            if (lx >= w || ly >= h || lz >= d) continue;
+            const uint32_t g = v >> 6, bit = v & 63u;
+            const uint32_t mw = ldw(pw, (uint32_t)((ob + 8u * g + (bit >= 32 ? 4u : 0u)) >> 2));
+            if (((mw >> (bit & 31u)) & 1u) == 0u) continue;
+            const uint32_t m0 = ldw(pw, (uint32_t)((ob + 8u * g) >> 2));
+            const uint32_t m1 = ldw(pw, (uint32_t)((ob + 8u * g + 4u) >> 2));
+            const uint64_t mask = ((uint64_t)m1 << 32) | m0;
+            const uint32_t pref = (ldw(pw, (uint32_t)((ob + 64u + 2u * g) >> 2)) >> ((g & 1u) * 16u)) & 0xFFFFu;
+            const uint32_t di = (pref + __popcll(mask & ((1ull << bit) - 1ull))) & 0xFFFFu;
+            const uint32_t dsc = ldw(pw, (uint32_t)((sbase + 4ull * di) >> 2));
+            const uint32_t kc = (dsc >> 16) & 0xFFu;
+            bad |= kc != 0u && (dsc & 0xFFFFu) + kc > fkf;
+        }
+        if (__any_sync(0xFFFFFFFFu, bad)) status = kErrKeyRangeOob;
+    }
+    e.info = (active & 0x3FFu) | flags | (status << 16);
+    return e;
+}
+
+// Scientific leaves: every leaf is active.  The decoder reads through bounds-checked accessors
+// (the reference reads through std::vector::at, render/src/scientific_decode.cpp:41-58); here the
+// walker only checks that every AC scale the leaf's keep needs exists (the reference's
+// coarseAcScales.at(k - 1), :91).
+__device__ LeafEntry walk_sci_leaf(const DeviceAsset& a, uint32_t leaf)
+{
+    LeafEntry e{};
+    e.word_off = __ldg(a.offsets + leaf);
+    e.header = e.word_off < a.g.payload_words ? ldw(a.payload, e.word_off) : 0u;
+    const uint32_t keep = ((e.header >> 2) & 0x3Fu) + 1u;
+    uint32_t status = kOk;
+    if (e.word_off >= a.g.payload_words || keep - 1u > a.g.scale_count) status = kErrDecodeOob;
+    e.info = kFlagActive | (status << 16);
+    return e;
+}
+
+__global__ void __launch_bounds__(kWalkThreads) walk_kernel(DeviceAsset a, uint32_t epoch)
+{
+    __shared__ uint8_t s_flag[kWalkTile];
+    __shared__ uint32_t s_warp[kWalkThreads / 32];
+    __shared__ uint32_t s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t leaf0 = tile * kWalkTile;
+    const uint32_t L = a.g.leaf_count;
+
+    // phase 1: one warp per leaf, 32 leaves per warp
+    for (int j = 0; j < kWalkTile / (kWalkThreads / 32); ++j) {
+        const uint32_t local = warp * (kWalkTile / (kWalkThreads / 32)) + j;
+        const uint32_t leaf = leaf0 + local;
+        if (leaf >= L) break;
+        const LeafEntry e = a.g.profile == 2u ? walk_sci_leaf(a, leaf) : walk_rt_leaf(a, leaf, lane);
+        if (lane == 0) {
+            a.entries[leaf] = e;
+            s_flag[local] = (e.info & kFlagActive) ? 1 : 0;
+        }
+    }
+    __syncthreads();
+
+    // phase 2: ballot/popc compaction of the tile's active flags
+    const uint32_t leaf = leaf0 + threadIdx.x;
+    const bool flag = leaf < L && s_flag[threadIdx.x] != 0;
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, flag);
+    const uint32_t in_warp = __popc(bal & ((1u << lane) - 1u));
+    if (lane == 0) s_warp[warp] = __popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < kWalkThreads / 32; ++w) {
+            const uint32_t c = s_warp[w];
+            s_warp[w] = run;
+            run += c;
+        }
+        // decoupled look-back: descriptor = epoch[63:34] | flag[33:32] (1 aggregate, 2 prefix) | count
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> self(a.tile_state[tile]);
+        const unsigned long long ep = (unsigned long long)(epoch & 0x3FFFFFFFu) << 34;
+        uint32_t excl = 0;
+        if (tile == 0) {
+            self.store(ep | (2ull << 32) | run, cuda::memory_order_release);
+        } else {
+            self.store(ep | (1ull << 32) | run, cuda::memory_order_release);
+            int j = (int)tile - 1;
+            uint32_t spins = 0;
+            while (j >= 0) {
+                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> st(a.tile_state[j]);
+                const unsigned long long v = st.load(cuda::memory_order_acquire);
+                if ((v >> 34) != (unsigned long long)(epoch & 0x3FFFFFFFu) || ((v >> 32) & 3ull) == 0ull) {
+                    if (++spins > (1u << 22)) {   // bounded wait: report and stop, never hang
+                        atomicOr(a.counters + 1, 1u);
+                        record_error(a.err, leaf0, kErrWaitTimeout);
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
+                }
+                excl += (uint32_t)(v & 0xFFFFFFFFull);
+                if (((v >> 32) & 3ull) == 2ull) break;
+                --j;
+            }
+            self.store(ep | (2ull << 32) | (excl + run), cuda::memory_order_release);
+        }
+        s_base = excl;
+        if (leaf0 + kWalkTile >= L) a.counters[0] = excl + run;   // last tile: total active count
+    }
+    __syncthreads();
+    if (leaf < L) {
+        const uint32_t rank = s_base + s_warp[warp] + in_warp;
+        a.compact[leaf] = flag ? rank : kNoRank;
+        if (flag) a.active_list[rank] = leaf;
+    }
+}
+
+void launch_walk(const DeviceAsset& a, uint32_t epoch, cudaStream_t s)
+{
+    const uint32_t tiles = (a.g.leaf_count + kWalkTile - 1) / kWalkTile;
+    walk_kernel<<<tiles, kWalkThreads, 0, s>>>(a, epoch);
+}
+
+// ---------------------------------------------------------------------------------------------
+// (b) render-temporal leaf decode (one warp)
+
+__device__ __forceinline__ float trilinear_rt(const float* __restrict__ g, int res, const AxisWeight& ax,
+                                              const AxisWeight& ay, const AxisWeight& az)
+{
+    if (res <= 0) return 0.0f;   // no controls (the reference dereferences an empty grid here)
+    if (res == 1) return g[0];   // one control (the reference reads past its coordinate vector)
+    const int r = res;
+    const float* gz0 = g + (az.i0 * r) * r;
+    const float* gz1 = g + (az.i1 * r) * r;
+    const float c00 = lerp_ref(gz0[ay.i0 * r + ax.i0], gz0[ay.i0 * r + ax.i1], ax.t, ax.omt);
+    const float c01 = lerp_ref(gz1[ay.i0 * r + ax.i0], gz1[ay.i0 * r + ax.i1], ax.t, ax.omt);
+    const float c10 = lerp_ref(gz0[ay.i1 * r + ax.i0], gz0[ay.i1 * r + ax.i1], ax.t, ax.omt);
+    const float c11 = lerp_ref(gz1[ay.i1 * r + ax.i0], gz1[ay.i1 * r + ax.i1], ax.t, ax.omt);
+    const float c0 = lerp_ref(c00, c10, ay.t, ay.omt);
+    const float c1 = lerp_ref(c01, c11, ay.t, ay.omt);
+    return lerp_ref(c0, c1, az.t, az.omt);
+}
+
+// Decode the controls of one leaf at one frame into s_ctrl (coarse at [0, 343), fine or shell
+// at [343, 855)).  Returns false when the leaf cannot be decoded (status recorded).
+__device__ __forceinline__ void rt_decode_controls(const DeviceAsset& a, const LeafEntry& e, int frame,
+                                                   float* __restrict__ s_ctrl, int lane, int nl = 32)
+{
+    const uint32_t* __restrict__ pw = a.payload;
+    const uint64_t base = 4ull * e.word_off;
+    const uint32_t cres = (e.header >> 6) & 7u, fres = (e.header >> 9) & 7u;
+    const int total = (int)a.g.frames;
+    const uint32_t bin8 = time_bin(frame, 8u, total);
+    StreamRef cs{base + 8u, cres * cres * cres, 8u, e.kf & 0xFFFFu, (e.header >> 2) & 3u};
+    for (uint32_t c = lane; c < cs.controls; c += nl) s_ctrl[c] = decode_control(pw, cs, c, frame, bin8);
+    if (e.info & kFlagFine) {
+        StreamRef fs{base + 8u + e.coarse_bytes, fres * fres * fres, 8u, e.kf >> 16, (e.header >> 4) & 3u};
+        for (uint32_t c = lane; c < fs.controls; c += nl) s_ctrl[343 + c] = decode_control(pw, fs, c, frame, bin8);
+    } else if (e.info & kFlagShell) {
+        const uint32_t bin4 = time_bin(frame, 4u, total);
+        StreamRef ss{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
+        for (uint32_t c = lane; c < ss.controls; c += nl) s_ctrl[343 + c] = decode_control(pw, ss, c, frame, bin4);
+    }
+}
+
+// Reconstruct one row (ly, lz) of 8 voxels from the decoded controls.  Voxels outside the leaf
+// extent come out as 0 (they are not part of the frame; in the cache they are defined as 0).
+__device__ __forceinline__ void rt_row(const DeviceAsset& a, const LeafEntry& e, const float* __restrict__ s_ctrl,
+                                       int w, int h, int d, int ly, int lz, float out[8])
+{
+    const uint32_t cres = (e.header >> 6) & 7u, fres = (e.header >> 9) & 7u;
+    const AxisWeight ay = g_axis[axis_index(cres, h, ly)], az = g_axis[axis_index(cres, d, lz)];
+    AxisWeight fy{}, fz{};
+    const bool fine = (e.info & kFlagFine) != 0u;
+    if (fine) {
+        fy = g_axis[axis_index(fres, h, ly)];
+        fz = g_axis[axis_index(fres, d, lz)];
+    }
+    uint64_t mask = 0;
+    uint32_t pref = 0;
+    const bool occ = (e.info & kFlagOccClamp) != 0u;
+    if (occ) {
+        const uint64_t ob = 4ull * e.word_off + 8u + e.coarse_bytes;
+        const uint32_t g = (uint32_t)lz;   // 64 voxels per group = one z layer
+        const uint32_t m0 = ldw(a.payload, (uint32_t)((ob + 8u * g) >> 2));
+        const uint32_t m1 = ldw(a.payload, (uint32_t)((ob + 8u * g + 4u) >> 2));
+        mask = ((uint64_t)m1 << 32) | m0;
+        pref = (ldw(a.payload, (uint32_t)((ob + 64u + 2u * g) >> 2)) >> ((g & 1u) * 16u)) & 0xFFFFu;
+    }
+    const bool shell = (e.info & kFlagShell) != 0u;
+#pragma unroll
+    for (int lx = 0; lx < 8; ++lx) {
+        float v = 0.0f;
+        if (lx < w && ly < h && lz < d) {
+            v = trilinear_rt(s_ctrl, (int)cres, c_axis[axis_index(cres, w, lx)], ay, az);
+            const uint32_t bit = (uint32_t)(ly * 8 + lx);
+            const bool in_occ = occ && ((mask >> bit) & 1ull);
+            if (fine) {
+                v = __fadd_rn(v, trilinear_rt(s_ctrl + 343, (int)fres, c_axis[axis_index(fres, w, lx)], fy, fz));
+            } else if (shell && in_occ) {
+                const uint32_t di = (pref + __popcll(mask & ((1ull << bit) - 1ull))) & 0xFFFFu;
+                v = __fadd_rn(v, s_ctrl[343 + di]);
+            }
+            if (occ && !in_occ && v < 0.0f) v = 0.0f;
+        }
+        out[lx] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// (b') scientific leaf decode (one warp): render/src/scientific_decode.cpp:82-359
+
+struct SciReader {
+    const uint32_t* __restrict__ pw;
+    uint64_t words;
+    bool oob;
+    __device__ __forceinline__ uint32_t byte(uint64_t b)
+    {
+        const uint64_t w = b >> 2;
+        if (w >= words) {
+            oob = true;
+            return 0u;
+        }
+        return (ldw(pw, (uint32_t)w) >> ((uint32_t)(b & 3u) * 8u)) & 0xFFu;
+    }
+    __device__ __forceinline__ uint32_t u16(uint64_t b) { return byte(b) | (byte(b + 1) << 8); }
+    __device__ __forceinline__ uint32_t u32(uint64_t b)
+    {
+        if ((b & 3u) == 0u) {
+            const uint64_t w = b >> 2;
+            if (w >= words) {
+                oob = true;
+                return 0u;
+            }
+            return ldw(pw, (uint32_t)w);
+        }
+        return u16(b) | (u16(b + 2) << 16);
+    }
+};
+
+// Error-free transforms for the compensated sum.
+__device__ __forceinline__ void two_prod(float a, float b, float& p, float& e)
+{
+    p = __fmul_rn(a, b);
+    e = __fmaf_rn(a, b, -p);
+}
+__device__ __forceinline__ void ff_add(float& hi, float& lo, float ph, float pl)
+{
+    const float s = __fadd_rn(hi, ph);
+    const float bb = __fsub_rn(s, hi);
+    const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(ph, bb));
+    const float t = __fadd_rn(__fadd_rn(err, lo), pl);
+    hi = __fadd_rn(s, t);
+    lo = __fsub_rn(t, __fsub_rn(hi, s));
+}
+
+// Coarse control ci at frame t: DC * b0(t) + sum_k (i8 * acScale[k-1]) * bk(t).
+__device__ __forceinline__ float sci_control(const DeviceAsset& a, SciReader& rd, uint64_t base, int keep, int ci,
+                                             const float* __restrict__ brow)
+{
+    const uint64_t cb = base + 4u + (uint64_t)ci * (keep + 1);
+    float hi, lo;
+    two_prod(half_bits_to_float(rd.u16(cb)), __ldg(brow), hi, lo);
+    for (int k = 1; k < keep; ++k) {
+        const float coeff = __fmul_rn((float)(int8_t)rd.byte(cb + 2u + (k - 1)), __ldg(a.scales + k - 1));
+        float ph, pl;
+        two_prod(coeff, __ldg(brow + k), ph, pl);
+        ff_add(hi, lo, ph, pl);
+    }
+    return __fadd_rn(hi, lo);
+}
+
+__device__ __forceinline__ float decode_bfp(uint32_t q, float scale, int bits)
+{
+    if (bits <= 2) {
+        const float lv = q == 0u ? -1.0f : q == 1u ? -0.3333333f : q == 2u ? 0.3333333f : 1.0f;
+        return __fmul_rn(lv, scale);
+    }
+    const int levels = (1 << bits) - 1;
+    const float norm = __fsub_rn(__fmul_rn(__fdiv_rn((float)q, (float)levels), 2.0f), 1.0f);
+    return __fmul_rn(norm, scale);
+}
+
+__device__ __forceinline__ float bfp_sample(SciReader& rd, uint64_t data, int res, int bits, float scale, int ci)
+{
+    const int bo = ci * bits;
+    const uint64_t bi = data + (uint64_t)(bo / 8);
+    const int sh = bo % 8;
+    uint32_t packed = rd.byte(bi);
+    if (sh + bits > 8) packed |= rd.byte(bi + 1) << 8;
+    return decode_bfp((packed >> sh) & ((1u << bits) - 1u), scale, bits);
+}
+
+__device__ __forceinline__ float tri_small(const float* __restrict__ g, int r, const AxisWeight& ax,
+                                           const AxisWeight& ay, const AxisWeight& az)
+{
+    const float* gz0 = g + (az.i0 * r) * r;
+    const float* gz1 = g + (az.i1 * r) * r;
+    const float c00 = lerp_ref(gz0[ay.i0 * r + ax.i0], gz0[ay.i0 * r + ax.i1], ax.t, ax.omt);
+    const float c01 = lerp_ref(gz1[ay.i0 * r + ax.i0], gz1[ay.i0 * r + ax.i1], ax.t, ax.omt);
+    const float c10 = lerp_ref(gz0[ay.i1 * r + ax.i0], gz0[ay.i1 * r + ax.i1], ax.t, ax.omt);
+    const float c11 = lerp_ref(gz1[ay.i1 * r + ax.i0], gz1[ay.i1 * r + ax.i1], ax.t, ax.omt);
+    return lerp_ref(lerp_ref(c00, c10, ay.t, ay.omt), lerp_ref(c01, c11, ay.t, ay.omt), az.t, az.omt);
+}
+
+// Sparse-event residual for local voxel li at frame t (render/src/scientific_decode.cpp:235-295).
+__device__ float sci_sparse(SciReader& rd, uint64_t base, uint32_t hdr, int keep, uint32_t li, uint32_t t)
+{
+    const uint32_t count = (hdr >> 16) & 0x0FFFu;
+    if (count == 0u) return 0.0f;
+    const uint32_t tier = (hdr >> 8) & 3u;
+    const uint32_t cap = tier == 0u ? 64u : tier == 1u ? 256u : tier == 2u ? 768u : 1024u;
+    const uint32_t fpb = ((hdr >> 10) & 0xFu) + 1u;
+    const uint32_t bin = t / fpb < 15u ? t / fpb : 15u;
+    const uint32_t lt = (t - bin * fpb) & 0xFFu;
+    const uint64_t sb = base + 4u + (uint64_t)(64 * (keep + 1));
+    const float es = __uint_as_float(rd.u32(sb));
+    if (!(es > 0.0f)) return 0.0f;
+    const uint32_t mw = rd.u32(sb + 4u + (li >> 5) * 4u);
+    if ((mw & (1u << (li & 31u))) == 0u) return 0.0f;
+    const uint64_t bb = sb + 68u;
+    const uint32_t start = rd.u16(bb + bin * 2u);
+    const uint32_t end = bin + 1u < 16u ? rd.u16(bb + (bin + 1u) * 2u) : (count & 0xFFFFu);
+    if (start >= end) return 0.0f;
+    const uint64_t cb = bb + 32u, rb = cb + cap * 2u;
+    const uint32_t target = ((lt << 9) | (li & 0x1FFu)) & 0xFFFFu;
+    int left = (int)start, right = (int)end - 1;
+    while (left <= right) {
+        const int mid = (left + right) >> 1;
+        const uint32_t key = rd.u16(cb + (uint32_t)mid * 2u);
+        if (key == target) {
+            const uint32_t byte = rd.byte(rb + (uint32_t)(mid >> 1));
+            int q = (int)((mid & 1) == 0 ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
+            if (q & 8) q -= 16;
+            return __fmul_rn((float)q, es);
+        }
+        if (key < target) left = mid + 1;
+        else right = mid - 1;
+    }
+    return 0.0f;
+}
+
+// Warp-cooperative scientific leaf decode at frame t: controls into s_ctrl[0..64), the dense
+// residual grid(s) into s_ctrl[64..) (per-frame grid, or tkeep basis grids), then row values.
+__device__ void sci_decode_controls(const DeviceAsset& a, const LeafEntry& e, uint32_t t, float* __restrict__ s_ctrl,
+                                    int lane, bool& oob, int nl = 32)
+{
+    SciReader rd{a.payload, a.g.payload_words, false};
+    const uint64_t base = 4ull * e.word_off;
+    const uint32_t hdr = e.header;
+    const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
+    const float* brow = a.basis + (uint64_t)t * 64u;
+    for (int c = lane; c < 64; c += nl) s_ctrl[c] = sci_control(a, rd, base, keep, c, brow);
+    const uint32_t mode = hdr & 3u;
+    if (mode >= 2u) {
+        const int res = mode == 2u ? 3 : 4;
+        const int bits = (int)((hdr >> 8) & 0xFu);
+        const uint32_t sub = (hdr >> 12) & 7u;
+        const int per = res * res * res;
+        const uint64_t scales = base + 4u + (uint64_t)(64 * (keep + 1));
+        if (sub == 1u) {
+            const int tkeep = (int)((hdr >> 15) & 0xFu) + 1;
+            const int bbytes = (per * bits + 7) / 8;
+            const uint64_t data = scales + (uint64_t)(tkeep * 2);
+            if (bits > 0) {
+                for (int i = lane; i < tkeep * per; i += nl) {
+                    const int k = i / per, ci = i % per;
+                    const float sc = half_bits_to_float(rd.u16(scales + (uint64_t)(k * 2)));
+                    s_ctrl[64 + i] = bfp_sample(rd, data + (uint64_t)(k * bbytes), res, bits, sc, ci);
+                }
+            }
+        } else {
+            const int fbytes = (per * bits + 7) / 8;
+            const uint64_t data = scales + (uint64_t)a.g.frames * 2u + (uint64_t)t * fbytes;
+            const float sc = half_bits_to_float(rd.u16(scales + t * 2u));
+            for (int ci = lane; ci < per; ci += nl) s_ctrl[64 + ci] = bfp_sample(rd, data, res, bits, sc, ci);
+        }
+    }
+    oob = rd.oob;
+}
+
+__device__ __forceinline__ void sci_row(const DeviceAsset& a, const LeafEntry& e, const float* __restrict__ s_ctrl,
+                                        uint32_t t, int w, int h, int d, int ly, int lz, float out[8], bool& oob)
+{
+    SciReader rd{a.payload, a.g.payload_words, false};
+    const uint64_t base = 4ull * e.word_off;
+    const uint32_t hdr = e.header;
+    const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
+    const uint32_t mode = hdr & 3u;
+    const AxisWeight ay = c_sci_axis[0][ly], az = c_sci_axis[0][lz];
+    const int res = mode == 2u ? 3 : 4;
+    const AxisWeight dy = c_sci_axis[mode == 2u ? 1 : 2][ly], dz = c_sci_axis[mode == 2u ? 1 : 2][lz];
+    const int bits = (int)((hdr >> 8) & 0xFu);
+    const uint32_t sub = (hdr >> 12) & 7u;
+    const int tkeep = (int)((hdr >> 15) & 0xFu) + 1;
+    const float* brow = a.basis + (uint64_t)t * 64u;
+#pragma unroll 1
+    for (int lx = 0; lx < 8; ++lx) {
+        float v = 0.0f;
+        if (lx < w && ly < h && lz < d) {
+            const float coarse = tri_small(s_ctrl, 4, c_sci_axis[0][lx], ay, az);
+            float r = 0.0f;
+            if (mode == 1u) {
+                r = sci_sparse(rd, base, hdr, keep, (uint32_t)((lz * 8 + ly) * 8 + lx), t);
+            } else if (mode >= 2u) {
+                const AxisWeight dx = c_sci_axis[mode == 2u ? 1 : 2][lx];
+                const int per = res * res * res;
+                if (sub == 1u) {
+                    if (bits > 0) {
+                        for (int k = 0; k < tkeep; ++k) {
+                            const float tri = tri_small(s_ctrl + 64 + k * per, res, dx, dy, dz);
+                            r = __fadd_rn(r, __fmul_rn(tri, __ldg(brow + k)));
+                        }
+                    }
+                } else {
+                    r = tri_small(s_ctrl + 64, res, dx, dy, dz);
+                }
+            }
+            v = __fadd_rn(coarse, r);
+        }
+        out[lx] = v;
+    }
+    oob |= rd.oob;
+}
+
+// ---------------------------------------------------------------------------------------------
+// (b) decode kernels: warp-per-(leaf, frame) over the active list; frames in the launch are
+// walked innermost so a warp re-reads its leaf's bytes from L1/L2.
+
+struct FrameList {
+    int n;
+    int f[64];
+};
+
+template <bool DENSE>
+__global__ void __launch_bounds__(kDecodeWarps * 32) decode_kernel(DeviceAsset a, FrameList fl, float* __restrict__ out,
+                                                                  uint64_t frame_stride)
+{
+    __shared__ __align__(16) float s_ctrl_all[kDecodeWarps][kWarpSlots];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* s_ctrl = s_ctrl_all[warp];
+    const uint32_t n_items = DENSE ? a.g.leaf_count : *(volatile const uint32_t*)a.counters;
+    const uint32_t warps_total = gridDim.x * kDecodeWarps;
+    for (uint32_t item = blockIdx.x * kDecodeWarps + warp; item < n_items; item += warps_total) {
+        const uint32_t leaf = DENSE ? item : __ldg(a.active_list + item);
+        const LeafEntry e = a.entries[leaf];
+        uint32_t bx, by, bz;
+        int w, h, d;
+        leaf_extent(a.g, leaf, bx, by, bz, w, h, d);
+        const bool empty = a.g.profile != 2u && (e.header & 3u) == kModeEmpty;
+        const uint32_t st = entry_status(e);
+        if (st != kOk && lane == 0) record_error(a.err, leaf, st);
+        for (int fi = 0; fi < fl.n; ++fi) {
+            const int frame = clamp_frame(fl.f[fi], (int)a.g.frames);
+            bool oob = false;
+            if (!empty && st == kOk) {
+                if (a.g.profile == 2u) sci_decode_controls(a, e, (uint32_t)fl.f[fi], s_ctrl, lane, oob);
+                else rt_decode_controls(a, e, frame, s_ctrl, lane);
+            }
+            __syncwarp();
+            for (int r = lane; r < 64; r += 32) {
+                const int ly = r & 7, lz = r >> 3;
+                float v[8];
+                if (empty || st != kOk) {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) v[i] = 0.0f;
+                } else if (a.g.profile == 2u) {
+                    sci_row(a, e, s_ctrl, (uint32_t)fl.f[fi], w, h, d, ly, lz, v, oob);
+                } else {
+                    rt_row(a, e, s_ctrl, w, h, d, ly, lz, v);
+                }
+                if (DENSE) {
+                    if (ly < h && lz < d) {
+                        float* dst = out + (uint64_t)fi * frame_stride +
+                                     ((uint64_t)(bz * 8 + lz) * a.g.height + (by * 8 + ly)) * a.g.width + bx * 8;
+                        if (w == 8 && (((uintptr_t)dst) & 15u) == 0u) {
+                            reinterpret_cast<float4*>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+                            reinterpret_cast<float4*>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
+                        } else {
+                            for (int i = 0; i < w; ++i) dst[i] = v[i];
+                        }
+                    }
+                } else {
+                    float4* dst = reinterpret_cast<float4*>(out + (uint64_t)fi * frame_stride + (uint64_t)item * 512u + r * 8);
+                    dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+                    dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+                }
+            }
+            if (__any_sync(0xFFFFFFFFu, oob) && lane == 0) record_error(a.err, leaf, kErrDecodeOob);
+            __syncwarp();
+        }
+    }
+}
+
+static int default_grid()
+{
+    static int g = 0;
+    if (!g) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_kernel<false>, kDecodeWarps * 32, 0);
+        g = sms * (per > 0 ? per : 1);
+    }
+    return g;
+}
+
+void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, float* out, uint64_t stride, int grid,
+                         cudaStream_t s)
+{
+    FrameList fl{};
+    fl.n = nframes;
+    for (int i = 0; i < nframes; ++i) fl.f[i] = frames[i];
+    decode_kernel<false><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+}
+
+void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, float* out, int grid, cudaStream_t s)
+{
+    FrameList fl{};
+    fl.n = nframes;
+    for (int i = 0; i < nframes; ++i) fl.f[i] = frames[i];
+    const uint64_t stride = (uint64_t)a.g.width * a.g.height * a.g.depth;
+    decode_kernel<true><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+}
+
+// Plain per-leaf launch: grid = the whole leaf grid, one 64-thread CTA per leaf (EMPTY leaves
+// return at once), controls decoded by both warps' lanes, one frame.  This is the reference
+// Studio's cache dispatch shape and serves as the baseline the batched path is measured against.
+__global__ void __launch_bounds__(64) decode_plain_kernel(DeviceAsset a, int frame_index, float* __restrict__ out)
+{
+    __shared__ __align__(16) float s_ctrl[kWarpSlots];
+    const uint32_t leaf = blockIdx.x;
+    if (leaf >= a.g.leaf_count) return;
+    const uint32_t rank = a.compact[leaf];
+    if (rank == kNoRank) return;
+    const LeafEntry e = a.entries[leaf];
+    const uint32_t st = entry_status(e);
+    uint32_t bx, by, bz;
+    int w, h, d;
+    leaf_extent(a.g, leaf, bx, by, bz, w, h, d);
+    bool oob = false;
+    if (st == kOk) {
+        if (a.g.profile == 2u) sci_decode_controls(a, e, (uint32_t)frame_index, s_ctrl, threadIdx.x, oob, 64);
+        else rt_decode_controls(a, e, clamp_frame(frame_index, (int)a.g.frames), s_ctrl, threadIdx.x, 64);
+    }
+    __syncthreads();
+    const int r = threadIdx.x;
+    float v[8];
+    if (st != kOk) {
+        for (int i = 0; i < 8; ++i) v[i] = 0.0f;
+        if (threadIdx.x == 0) record_error(a.err, leaf, st);
+    } else if (a.g.profile == 2u) {
+        sci_row(a, e, s_ctrl, (uint32_t)frame_index, w, h, d, r & 7, r >> 3, v, oob);
+    } else {
+        rt_row(a, e, s_ctrl, w, h, d, r & 7, r >> 3, v);
+    }
+    float4* dst = reinterpret_cast<float4*>(out + (uint64_t)rank * 512u + r * 8);
+    dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+    dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+    if (oob) record_error(a.err, leaf, kErrDecodeOob);
+}
+
+void launch_decode_cache_plain(const DeviceAsset& a, int frame, float* out, cudaStream_t s)
+{
+    decode_plain_kernel<<<a.g.leaf_count, 64, 0, s>>>(a, frame, out);
+}
+
+// ---------------------------------------------------------------------------------------------
+// (c) point queries: one thread per query, decoding only the corner controls it needs.
+
+__device__ float rt_point(const DeviceAsset& a, const LeafEntry& e, int w, int h, int d, int lx, int ly, int lz,
+                          int frame)
+{
+    const uint32_t* __restrict__ pw = a.payload;
+    const uint64_t base = 4ull * e.word_off;
+    const int total = (int)a.g.frames;
+    const uint32_t cres = (e.header >> 6) & 7u, fres = (e.header >> 9) & 7u;
+    const uint32_t bin8 = time_bin(frame, 8u, total);
+    auto sample = [&](const StreamRef& s, uint32_t res) -> float {
+        if (res == 0u) return 0.0f;
+        if (res == 1u) return decode_control(pw, s, 0, frame, bin8);
+        const AxisWeight ax = g_axis[axis_index(res, w, lx)], ay = g_axis[axis_index(res, h, ly)],
+                         az = g_axis[axis_index(res, d, lz)];
+        const uint32_t r = res;
+        auto at = [&](uint32_t ix, uint32_t iy, uint32_t iz) { return decode_control(pw, s, (iz * r + iy) * r + ix, frame, bin8); };
+        const float c00 = lerp_ref(at(ax.i0, ay.i0, az.i0), at(ax.i1, ay.i0, az.i0), ax.t, ax.omt);
+        const float c01 = lerp_ref(at(ax.i0, ay.i0, az.i1), at(ax.i1, ay.i0, az.i1), ax.t, ax.omt);
+        const float c10 = lerp_ref(at(ax.i0, ay.i1, az.i0), at(ax.i1, ay.i1, az.i0), ax.t, ax.omt);
+        const float c11 = lerp_ref(at(ax.i0, ay.i1, az.i1), at(ax.i1, ay.i1, az.i1), ax.t, ax.omt);
+        return lerp_ref(lerp_ref(c00, c10, ay.t, ay.omt), lerp_ref(c01, c11, ay.t, ay.omt), az.t, az.omt);
+    };
+    StreamRef cs{base + 8u, cres * cres * cres, 8u, e.kf & 0xFFFFu, (e.header >> 2) & 3u};
+    float v = sample(cs, cres);
+    const uint32_t vox = (uint32_t)((lz * 8 + ly) * 8 + lx);
+    bool in_occ = false;
+    uint64_t mask = 0;
+    uint32_t pref = 0;
+    if (e.info & kFlagOccClamp) {
+        const uint64_t ob = base + 8u + e.coarse_bytes;
+        const uint32_t g = vox >> 6;
+        mask = ((uint64_t)ldw(pw, (uint32_t)((ob + 8u * g + 4u) >> 2)) << 32) | ldw(pw, (uint32_t)((ob + 8u * g) >> 2));
+        pref = (ldw(pw, (uint32_t)((ob + 64u + 2u * g) >> 2)) >> ((g & 1u) * 16u)) & 0xFFFFu;
+        in_occ = (mask >> (vox & 63u)) & 1ull;
+    }
+    if (e.info & kFlagFine) {
+        StreamRef fs{base + 8u + e.coarse_bytes, fres * fres * fres, 8u, e.kf >> 16, (e.header >> 4) & 3u};
+        v = __fadd_rn(v, sample(fs, fres));
+    } else if ((e.info & kFlagShell) && in_occ) {
+        StreamRef ss{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
+        const uint32_t di = (pref + __popcll(mask & ((1ull << (vox & 63u)) - 1ull))) & 0xFFFFu;
+        v = __fadd_rn(v, decode_control(pw, ss, di, frame, time_bin(frame, 4u, total)));
+    }
+    if ((e.info & kFlagOccClamp) && !in_occ && v < 0.0f) v = 0.0f;
+    return v;
+}
+
+__device__ float sci_point(const DeviceAsset& a, const LeafEntry& e, uint32_t lx, uint32_t ly, uint32_t lz, uint32_t t,
+                           bool& oob)
+{
+    SciReader rd{a.payload, a.g.payload_words, false};
+    const uint64_t base = 4ull * e.word_off;
+    const uint32_t hdr = e.header;
+    const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
+    const float* brow = a.basis + (uint64_t)t * 64u;
+    const AxisWeight ax = c_sci_axis[0][lx], ay = c_sci_axis[0][ly], az = c_sci_axis[0][lz];
+    auto at = [&](int cx, int cy, int cz) { return sci_control(a, rd, base, keep, (cz * 4 + cy) * 4 + cx, brow); };
+    const float c00 = lerp_ref(at(ax.i0, ay.i0, az.i0), at(ax.i1, ay.i0, az.i0), ax.t, ax.omt);
+    const float c01 = lerp_ref(at(ax.i0, ay.i0, az.i1), at(ax.i1, ay.i0, az.i1), ax.t, ax.omt);
+    const float c10 = lerp_ref(at(ax.i0, ay.i1, az.i0), at(ax.i1, ay.i1, az.i0), ax.t, ax.omt);
+    const float c11 = lerp_ref(at(ax.i0, ay.i1, az.i1), at(ax.i1, ay.i1, az.i1), ax.t, ax.omt);
+    const float coarse = lerp_ref(lerp_ref(c00, c10, ay.t, ay.omt), lerp_ref(c01, c11, ay.t, ay.omt), az.t, az.omt);
+    const uint32_t mode = hdr & 3u;
+    float r = 0.0f;
+    if (mode == 1u) {
+        r = sci_sparse(rd, base, hdr, keep, (lz * 8u + ly) * 8u + lx, t);
+    } else if (mode >= 2u) {
+        const int res = mode == 2u ? 3 : 4;
+        const int bits = (int)((hdr >> 8) & 0xFu);
+        const uint32_t sub = (hdr >> 12) & 7u;
+        const int per = res * res * res;
+        const uint64_t scales = base + 4u + (uint64_t)(64 * (keep + 1));
+        const int gi = mode == 2u ? 1 : 2;
+        const AxisWeight dx = c_sci_axis[gi][lx], dy = c_sci_axis[gi][ly], dz = c_sci_axis[gi][lz];
+        auto tri = [&](uint64_t data, float sc) {
+            auto S = [&](int cx, int cy, int cz) { return bfp_sample(rd, data, res, bits, sc, (cz * res + cy) * res + cx); };
+            const float d00 = lerp_ref(S(dx.i0, dy.i0, dz.i0), S(dx.i1, dy.i0, dz.i0), dx.t, dx.omt);
+            const float d01 = lerp_ref(S(dx.i0, dy.i0, dz.i1), S(dx.i1, dy.i0, dz.i1), dx.t, dx.omt);
+            const float d10 = lerp_ref(S(dx.i0, dy.i1, dz.i0), S(dx.i1, dy.i1, dz.i0), dx.t, dx.omt);
+            const float d11 = lerp_ref(S(dx.i0, dy.i1, dz.i1), S(dx.i1, dy.i1, dz.i1), dx.t, dx.omt);
+            return lerp_ref(lerp_ref(d00, d10, dy.t, dy.omt), lerp_ref(d01, d11, dy.t, dy.omt), dz.t, dz.omt);
+        };
+        if (sub == 1u) {
+            const int tkeep = (int)((hdr >> 15) & 0xFu) + 1;
+            if (bits > 0) {
+                const int bbytes = (per * bits + 7) / 8;
+                const uint64_t data = scales + (uint64_t)(tkeep * 2);
+                for (int k = 0; k < tkeep; ++k) {
+                    const float sc = half_bits_to_float(rd.u16(scales + (uint64_t)(k * 2)));
+                    r = __fadd_rn(r, __fmul_rn(tri(data + (uint64_t)(k * bbytes), sc), __ldg(brow + k)));
+                }
+            }
+        } else {
+            const int fbytes = (per * bits + 7) / 8;
+            const float sc = half_bits_to_float(rd.u16(scales + t * 2u));
+            r = tri(scales + (uint64_t)a.g.frames * 2u + (uint64_t)t * fbytes, sc);
+        }
+    }
+    oob |= rd.oob;
+    return __fadd_rn(coarse, r);
+}
+
+__global__ void __launch_bounds__(128) query_points_kernel(DeviceAsset a, const uint32_t* __restrict__ q, uint64_t n,
+                                                           float* __restrict__ out)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4 qq = reinterpret_cast<const uint4*>(q)[i];
+    const uint32_t x = qq.x, y = qq.y, z = qq.z, t = qq.w;
+    // leaf lookup as render/src/vbt_file.cpp:250-262 leafIndexForVoxel (clamped leaf coordinates)
+    const uint32_t bx = min(a.g.lcx - 1u, x >> 3), by = min(a.g.lcy - 1u, y >> 3), bz = min(a.g.lcz - 1u, z >> 3);
+    const uint32_t leaf = (bz * a.g.lcy + by) * a.g.lcx + bx;
+    const LeafEntry e = a.entries[leaf];
+    const uint32_t st = entry_status(e);
+    if (st != kOk) {
+        record_error(a.err, leaf, st);
+        out[i] = 0.0f;
+        return;
+    }
+    if (a.g.profile == 2u) {
+        if (t >= a.g.frames) {   // the reference indexes its per-frame tables out of range here
+            record_error(a.err, leaf, kErrDecodeOob);
+            out[i] = 0.0f;
+            return;
+        }
+        bool oob = false;
+        out[i] = sci_point(a, e, x & 7u, y & 7u, z & 7u, t, oob);
+        if (oob) record_error(a.err, leaf, kErrDecodeOob);
+        return;
+    }
+    if ((e.header & 3u) == kModeEmpty) {
+        out[i] = 0.0f;
+        return;
+    }
+    uint32_t gx, gy, gz;
+    int w, h, d;
+    leaf_extent(a.g, leaf, gx, gy, gz, w, h, d);
+    const int lx = (int)(x - bx * 8u), ly = (int)(y - by * 8u), lz = (int)(z - bz * 8u);
+    if (lx >= w || ly >= h || lz >= d) {   // outside the volume: no such voxel in any frame
+        out[i] = 0.0f;
+        return;
+    }
+    out[i] = rt_point(a, e, w, h, d, lx, ly, lz, clamp_frame((int)t, (int)a.g.frames));
+}
+
+void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, cudaStream_t s)
+{
+    if (n == 0) return;
+    query_points_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, q, n, out);
+}
+
+// Z-slice over [t0, t1): one warp per (leaf of the z layer, frame); lanes 0..7 produce rows.
+__global__ void __launch_bounds__(kDecodeWarps * 32) query_slice_kernel(DeviceAsset a, uint32_t z, int t0, int t1,
+                                                                        float* __restrict__ out)
+{
+    __shared__ __align__(16) float s_ctrl_all[kDecodeWarps][kWarpSlots];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* s_ctrl = s_ctrl_all[warp];
+    const uint32_t bz = min(a.g.lcz - 1u, z >> 3);
+    const int lz = (int)(z - bz * 8u);
+    const uint32_t layer = a.g.lcx * a.g.lcy;
+    const uint32_t n_items = layer * (uint32_t)(t1 - t0);
+    for (uint32_t item = blockIdx.x * kDecodeWarps + warp; item < n_items; item += gridDim.x * kDecodeWarps) {
+        const uint32_t li = item % layer;
+        const int t = t0 + (int)(item / layer);
+        const uint32_t leaf = bz * layer + li;
+        const LeafEntry e = a.entries[leaf];
+        uint32_t bx, by, bzz;
+        int w, h, d;
+        leaf_extent(a.g, leaf, bx, by, bzz, w, h, d);
+        const uint32_t st = entry_status(e);
+        const bool empty = a.g.profile != 2u && (e.header & 3u) == kModeEmpty;
+        bool oob = false;
+        const bool in_range = lz < d && (a.g.profile != 2u || (uint32_t)t < a.g.frames);
+        if (st != kOk && lane == 0) record_error(a.err, leaf, st);
+        if (in_range && !empty && st == kOk) {
+            if (a.g.profile == 2u) sci_decode_controls(a, e, (uint32_t)t, s_ctrl, lane, oob);
+            else rt_decode_controls(a, e, clamp_frame(t, (int)a.g.frames), s_ctrl, lane);
+        }
+        __syncwarp();
+        if (lane < 8 && lane < h) {
+            float v[8];
+            if (!in_range || empty || st != kOk) {
+                for (int i = 0; i < 8; ++i) v[i] = 0.0f;
+            } else if (a.g.profile == 2u) {
+                sci_row(a, e, s_ctrl, (uint32_t)t, w, h, d, lane, lz, v, oob);
+            } else {
+                rt_row(a, e, s_ctrl, w, h, d, lane, lz, v);
+            }
+            float* dst = out + (uint64_t)(t - t0) * a.g.width * a.g.height + (uint64_t)(by * 8 + lane) * a.g.width + bx * 8;
+            for (int i = 0; i < w; ++i) dst[i] = v[i];
+        }
+        if (__any_sync(0xFFFFFFFFu, oob) && lane == 0) record_error(a.err, leaf, kErrDecodeOob);
+        __syncwarp();
+    }
+}
+
+void launch_query_slice(const DeviceAsset& a, uint32_t z, int t0, int t1, float* out, cudaStream_t s)
+{
+    if (t1 <= t0) return;
+    query_slice_kernel<<<default_grid(), kDecodeWarps * 32, 0, s>>>(a, z, t0, t1, out);
+}
+
+}  // namespace vbtb

@@ -1,0 +1,59 @@
+// kernels.cuh -- launch-argument structs and launchers shared between the kernel and C-ABI units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "vbt_format.cuh"
+
+namespace vbtb {
+
+struct AssetGeom {
+    uint32_t width, height, depth, frames;
+    uint32_t lcx, lcy, lcz, leaf_count;
+    uint32_t profile;       // 2 = scientific, otherwise render-temporal
+    uint32_t scale_count;
+    uint64_t payload_words;
+};
+
+struct DeviceAsset {
+    AssetGeom g;
+    const uint32_t* offsets;     // leaf_count + 1 words
+    const uint32_t* payload;     // payload words
+    const float* scales;         // coarse AC scales (scientific)
+    const float* basis;          // scientific DCT basis table [frames][64]
+    LeafEntry* entries;          // leaf table (kernel a)
+    uint32_t* compact;           // page table: leaf -> rank or kNoRank
+    uint32_t* active_list;       // rank -> leaf
+    uint32_t* counters;          // [0] active count, [1] walk error flags
+    unsigned long long* err;     // first failing (leaf << 8 | status), ~0 when none
+    unsigned long long* tile_state;  // look-back tile descriptors
+};
+
+constexpr int kWalkThreads = 256;
+constexpr int kWalkTile = 256;   // leaves per walker CTA (one scan element per thread)
+
+// Decode work is done one leaf per warp; kDecodeWarps warps per CTA.
+constexpr int kDecodeWarps = 8;
+constexpr int kCtrlSlots = 343 + 512;   // coarse (<= 7^3) + fine (<= 7^3) or shell (<= 512) values
+// per-warp shared slots: max(render controls, scientific 64 controls + 16 basis grids of 4^3)
+constexpr int kWarpSlots = 64 + 16 * 64 > kCtrlSlots ? 64 + 16 * 64 : kCtrlSlots;
+
+void launch_walk(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);
+// Decode `nframes` frames (frames[] on the host, <= 64) of every active leaf into the cache:
+// out[f * cache_frame_stride + rank * 512 + voxel].
+void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, float* out,
+                         uint64_t cache_frame_stride, int grid, cudaStream_t s);
+// Dense frames: out[f * X*Y*Z + (z*Y + y)*X + x]; every leaf (EMPTY ones write zeros).
+void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, float* out, int grid,
+                         cudaStream_t s);
+// Plain path: one CTA per leaf of the whole leaf grid, one frame per launch (the reference
+// Studio dispatch shape, VBTStudio/frontend/src/volume_renderer.cpp:704-735).
+void launch_decode_cache_plain(const DeviceAsset& a, int frame, float* out, cudaStream_t s);
+// Point queries: q[4*i..] = (x, y, z, t); out[i].
+void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, cudaStream_t s);
+// Z-slice over a frame range: out[(t - t0) * X*Y + y*X + x] for t in [t0, t1).
+void launch_query_slice(const DeviceAsset& a, uint32_t z, int t0, int t1, float* out, cudaStream_t s);
+
+void upload_axis_tables();
+
+}  // namespace vbtb
