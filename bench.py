@@ -1,0 +1,385 @@
+#!/usr/bin/env python3
+"""Benchmark: decoded voxels/s of the VBTPACK4 temporal decode path on B200.
+
+Workload (the sparse-smoke configuration): a seeded 256^3 x 96 density plume (fBm inside a
+rising cone, ~12% of 8^3 leaves non-EMPTY), encoded by the reference encoder
+(tests/golden/make_assets.py cfg2_plume).  One step = one pass over the whole 96-frame timeline:
+the payload walker rebuilds the leaf table and active-leaf page table (kernel a), then the
+current-frame voxel cache (512 FP32 per active leaf) is decoded for every frame (kernel b,
+48 frames per launch), into a 96-frame cache ring larger than L2.  L2 is flushed (256 MiB
+write) before every timed step.  `value` counts decoded cache voxels (active leaves x 512 x
+frames) per second of device time, max over ranks; `e2e` is the same through the C-ABI with host
+buffers: the file image is re-uploaded from pinned memory and the whole cache ring is read back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun); the decode path has no
+exchange step, so there is no data-path collective.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DEFAULT_ASSET = os.path.join(ROOT, "assets", "cfg2_plume.vbtp")
+WORKLOAD = "sparse smoke plume 256^3 x 96 (cfg2): page table + current-frame cache for all 96 frames per step"
+METRIC = "decoded voxels/s"
+CHUNK = 48
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--asset", default=DEFAULT_ASSET)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+# ------------------------------------------------------------------------------ helpers
+def algorithmic_bytes_per_frame(rows):
+    """Algorithmic bytes of one frame of cache decode for the active leaves of a leaf table:
+    8 (header + prefix) + per decoded control 4 desc + 2 bin bytes + 2 keyframes x stride
+    + 80 occupancy bytes for Mode2 + 2048 bytes of cache written (512 FP32)."""
+    hdr = rows[:, 1]
+    info = rows[:, 7]
+    active = (info & (1 << 10)) != 0
+    hdr, info = hdr[active], info[active]
+    mode = hdr & 3
+    cc, fcd = (hdr >> 2) & 3, (hdr >> 4) & 3
+    cres, fres = (hdr >> 6) & 7, (hdr >> 9) & 7
+    cstride = np.where(cc == 1, 8, 3)
+    fstride = np.where(fcd == 1, 8, 3)
+    fine = (info & (1 << 11)) != 0
+    shell = (info & (1 << 12)) != 0
+    b = 8 + cres.astype(np.int64) ** 3 * (6 + 2 * cstride)
+    b += np.where(fine, fres.astype(np.int64) ** 3 * (6 + 2 * fstride), 0)
+    b += np.where(shell, (info & 0x3FF).astype(np.int64) * (6 + 2 * fstride), 0)
+    b += np.where(mode == 2, 80, 0)
+    b += 2048
+    return int(b.sum()), int(active.sum())
+
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="vbt_clocks_", suffix=".csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, STREAM-style copy)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the decode kernel from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "decode_cache_cfg2.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("dram_bytes_per_launch_full")
+    return None
+
+
+# ------------------------------------------------------------------------------ CPU baseline
+class CpuDecoder:
+    """The cache workload on the host cores: the reference decoder compiled from its sources
+    (oracle/_ref, kind "reference") when present, else the C restatement (kind "port")."""
+
+    def __init__(self, asset_path, threads=None):
+        import ctypes as C
+        from oracle import oracle as orc
+        self.cores = threads or os.cpu_count() or 1
+        self.f = orc.Oracle().load(asset_path)
+        self.compact, self.n_active = self.f.page_table()
+        self.frames = self.f.frames
+        self.cache = np.zeros(max(self.n_active, 1) * 512, np.float32)
+        if os.path.exists(orc.REF_SO):
+            self.ref = orc.Reference()
+            self.ref.lib.vr_decode_cache.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+            self.h = self.ref.load(asset_path)
+            self.kind = "reference"
+        else:
+            self.ref = None
+            self.kind = "port"
+        self._C, self._orc = C, orc
+
+    def frame(self, t):
+        if self.ref is not None:
+            if self.ref.lib.vr_decode_cache(self.h, t, self.cache.ctypes.data, self.cores) != 0:
+                raise RuntimeError(self.ref.error())
+        else:
+            C, orc = self._C, self._orc
+            self.f.o.lib.vo_decode_cache(C.byref(self.f.f), t, self.compact.ctypes.data_as(orc.u32p),
+                                         self.cache.ctypes.data_as(orc.f32p), self.cores)
+
+    def rate(self, seconds):
+        """Decode consecutive frames until `seconds` elapse; (voxels/s, sample description)."""
+        self.frame(0)
+        done, t0 = 0, time.perf_counter()
+        while True:
+            self.frame(done % self.frames)
+            done += 1
+            el = time.perf_counter() - t0
+            if el >= seconds or done >= 4 * self.frames:
+                break
+        return (self.n_active * 512 * done / el,
+                f"{done} frames of the {self.frames}-frame cache decode ({self.n_active} active leaves), {el:.1f} s")
+
+
+# ------------------------------------------------------------------------------ arms
+def run_reference(args, rank, world):
+    """The reference's own CPU decoder on the host cores, same metric and workload; each step is
+    a bounded sample of the 96-frame timeline (the frames that fit in about 3 s)."""
+    if rank != 0:
+        return 0
+    cpu = CpuDecoder(args.asset)
+    per_frame_s = cpu.n_active * 512 / cpu.rate(1.0)[0]
+    fps = max(1, min(cpu.frames, int(3.0 / max(per_frame_s, 1e-9))))
+    times, t_next = [], 0
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for _ in range(fps):
+            cpu.frame(t_next % cpu.frames)
+            t_next += 1
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = cpu.n_active * 512 * fps * len(times) / sum(times)
+    sample = f"{fps} of {cpu.frames} frames per step ({cpu.n_active} active leaves), {cpu.cores} threads"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "asset": os.path.basename(args.asset), "active_leaves": cpu.n_active,
+                       "frames_per_step": fps},
+            "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cpu.cores, "kind": cpu.kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, local_rank, world):
+    import torch
+    import vbt_b200 as vbt
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    stream = torch.cuda.Stream(device=dev)
+    a = vbt.Asset(args.asset, device=local_rank)
+    T, n_active = a.frames, a.active_count
+    frames = list(range(T))
+    chunks = [frames[i:i + CHUNK] for i in range(0, T, CHUNK)]
+    stride = n_active * 512
+    cache = torch.empty((T, max(n_active, 1), 512), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    rows = a.leaf_table()
+    bytes_per_frame, n_act2 = algorithmic_bytes_per_frame(rows)
+    assert n_act2 == n_active
+
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2 + len(chunks))] for _ in range(args.steps)]
+
+    def step(evs=None):
+        with torch.cuda.stream(stream):
+            if evs:
+                evs[0].record(stream)
+            a.build_page_table(stream)
+            if evs:
+                evs[1].record(stream)
+            for i, ch in enumerate(chunks):
+                a.decode_cache(ch, cache[ch[0]], frame_stride=stride, stream=stream)
+                if evs:
+                    evs[2 + i].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    a.sync_status(stream)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.4)
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        step(ev[k])
+    stream.synchronize()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop() if sampler else None
+    a.sync_status(stream)
+    step_ms = [e[0].elapsed_time(e[-1]) for e in ev]
+    walk_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    dec_ms = [e[1 + i].elapsed_time(e[2 + i]) for e in ev for i in range(len(chunks))]
+    total_ms = float(sum(step_ms))
+    if pg:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    voxels_per_step = n_active * 512 * T
+    value = world * voxels_per_step * args.steps / (total_ms * 1e-3)
+
+    # roofline of the dominant kernel (decode_kernel<cache>), per launch
+    peak, peak_src = measured_peak()
+    mean_launch_s = statistics.mean(dec_ms) * 1e-3
+    alg_per_launch = [bytes_per_frame * len(ch) for ch in chunks]
+    achieved = statistics.mean(alg_per_launch) / mean_launch_s / 1e9
+    traffic = ncu_traffic()
+
+    # plain path: per frame, page table + one-CTA-per-leaf launch (no batching, no persistence)
+    plain_ms = None
+    plain_out = torch.empty((max(n_active, 1), 512), dtype=torch.float32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        for rep in range(2):
+            flush.zero_()
+            e0.record(stream)
+            for t in frames:
+                a.build_page_table(stream)
+                a.decode_cache_plain(t, plain_out, stream)
+            e1.record(stream)
+    stream.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    a.sync_status(stream)
+    plain_value = voxels_per_step / (plain_ms * 1e-3)
+
+    # end-to-end through the C-ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        image = np.fromfile(args.asset, dtype=np.uint8)
+        h_img = torch.from_numpy(image).pin_memory()
+        h_out = torch.empty((T, max(n_active, 1), 512), dtype=torch.float32).pin_memory()
+        ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2e_steps = max(3, min(args.steps, 8))
+        with torch.cuda.stream(stream):
+            for k in range(2 + e2e_steps):
+                if k == 2:
+                    ee0.record(stream)
+                a.upload(h_img, stream)
+                a.build_page_table(stream)
+                for ch in chunks:
+                    a.decode_cache(ch, cache[ch[0]], frame_stride=stride, stream=stream)
+                h_out.copy_(cache, non_blocking=True)
+            ee1.record(stream)
+        stream.synchronize()
+        a.sync_status(stream)
+        e2e_ms = ee0.elapsed_time(ee1) / e2e_steps
+        if pg:
+            t = torch.tensor([e2e_ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * voxels_per_step / (e2e_ms * 1e-3), "unit": "voxels/s",
+               "h2d_bytes_per_step": int(image.nbytes), "d2h_bytes_per_step": int(cache.numel() * 4),
+               "ms_per_step": e2e_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        dec = CpuDecoder(args.asset)
+        v, sample = dec.rate(args.cpu_seconds)
+        cpu = {"value": v, "unit": "voxels/s", "cores": dec.cores, "kind": dec.kind, "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "asset": os.path.basename(args.asset), "leaves": a.leaf_count,
+                           "active_leaves": n_active, "frames_per_step": T, "frames_per_launch": CHUNK,
+                           "l2": "flushed before every timed step (256 MiB write)",
+                           "cache_ring_bytes": int(cache.numel() * 4), "parallelism": f"replicas x{world}"},
+                "roofline": {"bound": "hbm", "kernel": "decode_kernel<cache>", "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                             "algorithmic_bytes_per_launch": int(statistics.mean(alg_per_launch)),
+                             "launch_ms": statistics.mean(dec_ms), "peak_source": peak_src},
+                "kernels_ms": {"walk": statistics.mean(walk_ms), "decode_per_launch": statistics.mean(dec_ms)},
+                "plain": {"value": plain_value, "unit": "voxels/s", "ms_per_step": plain_ms,
+                          "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
+                "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": args.steps * (1 + len(chunks)),
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    a.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    rank, local_rank, world = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, local_rank, world)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

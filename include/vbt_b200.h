@@ -72,6 +72,10 @@ int vbt_validate_file_image(const void* bytes, uint64_t len, vbt_header* out_hea
 int vbt_asset_open(const char* path, int device, vbt_asset** out_asset);
 int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset** out_asset);
 int vbt_asset_destroy(vbt_asset* asset);
+/* Re-upload a file image with the same header and sizes into the asset's resident buffers,
+ * asynchronously on `stream` (host memory should be pinned).  Leaf offsets are re-checked on the
+ * device by the next vbt_build_page_table, which must follow before decoding. */
+int vbt_asset_upload(vbt_asset* asset, const void* file_bytes, uint64_t len, void* stream);
 int vbt_asset_get_info(vbt_asset* asset, vbt_asset_info* out_info);
 
 /* Kernel (a): payload walker + active-leaf page table (compact[leaf] = ascending rank among

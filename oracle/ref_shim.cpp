@@ -44,10 +44,22 @@ std::vector<float> controlCoords(int resolution)
     return coords;
 }
 
+// render/src/render_smoke_vbt_bench_main.cpp:212-219 coordsForResolution caches the coordinates per
+// resolution; here they are built once for every 3-bit resolution (thread-safe static init).
+const std::vector<float>& coordsForResolution(int resolution)
+{
+    static const std::array<std::vector<float>, 8> cache = [] {
+        std::array<std::vector<float>, 8> c;
+        for (int r = 0; r < 8; ++r) c[size_t(r)] = controlCoords(r);
+        return c;
+    }();
+    return cache[size_t(resolution & 7)];
+}
+
 // render/src/render_smoke_vbt_bench_main.cpp:221-234 locateCoord
 std::array<float, 3> locateCoord(float p, int extent, int resolution)
 {
-    const auto coords = controlCoords(resolution);
+    const auto& coords = coordsForResolution(resolution);
     const float maxP = static_cast<float>(std::max(0, extent - 1));
     p = std::clamp(p, 0.0f, maxP);
     int i1 = 1;
@@ -184,6 +196,46 @@ int vr_decode_frame(void* hp, int frame, float* out, int threads)
             for (int ly = 0; ly < h; ++ly)
                 std::memcpy(out + (size_t(bz * 8 + lz) * file.header.height + size_t(by * 8 + ly)) * file.header.width + bx * 8,
                             vals.data() + size_t(lz * h + ly) * w, sizeof(float) * size_t(w));
+    }
+    return failed;
+}
+
+// Current-frame cache over the same composition: only non-EMPTY leaves (route tag != 0) are
+// decoded, into cache[rank * 512 + (lz*8 + ly)*8 + lx] with rank the ascending active rank.
+int vr_decode_cache(void* hp, int frame, float* cache, int threads)
+{
+    const VbtFile& file = static_cast<Handle*>(hp)->file;
+    const int lcx = (int(file.header.width) + 7) / 8, lcy = (int(file.header.height) + 7) / 8,
+              lcz = (int(file.header.depth) + 7) / 8;
+    const uint8_t* payload = reinterpret_cast<const uint8_t*>(file.payloadWords.data());
+    const int64_t L = int64_t(lcx) * lcy * lcz;
+    std::vector<uint32_t> rank(size_t(L), 0xFFFFFFFFu);
+    uint32_t n = 0;
+    for (int64_t li = 0; li < L; ++li)
+        if ((file.payloadWords[file.offsetsWords[li]] & 3u) != 0u) rank[li] = n++;
+    int failed = 0;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 4)
+#endif
+    for (int64_t li = 0; li < L; ++li) {
+        if (rank[li] == 0xFFFFFFFFu) continue;
+        const int bx = int(li % lcx), by = int((li / lcx) % lcy), bz = int(li / (int64_t(lcx) * lcy));
+        const uint32_t wb = file.offsetsWords[li], we = file.offsetsWords[li + 1];
+        const int w = std::min(8, int(file.header.width) - bx * 8), h = std::min(8, int(file.header.height) - by * 8),
+                  d = std::min(8, int(file.header.depth) - bz * 8);
+        std::vector<float> vals(size_t(w) * h * d, 0.0f);
+        try {
+            decodeLeafFrameValues(payload + size_t(wb) * 4, size_t(we - wb) * 4, int(file.header.frames), frame, w, h,
+                                  d, vals);
+        } catch (const std::exception& e) {
+            failed = 1;
+            continue;
+        }
+        float* dst = cache + size_t(rank[li]) * 512u;
+        for (int lz = 0; lz < d; ++lz)
+            for (int ly = 0; ly < h; ++ly)
+                for (int lx = 0; lx < w; ++lx) dst[(lz * 8 + ly) * 8 + lx] = vals[size_t(lz * h + ly) * w + lx];
     }
     return failed;
 }

@@ -87,7 +87,7 @@ def plume(size, frames, seed):
     out = np.empty((frames, S, S, S), np.float32)
     for t in range(frames):
         top = z0 + S * 0.25 + 1.5 * t                      # front of the rising plume
-        radius = 0.12 * S * 0.25 + 0.14 * (zz - z0)        # cone opening upward
+        radius = 0.06 * S + 0.30 * (zz - z0)               # cone opening upward (~12% of leaves)
         inside = (zz >= z0) & (zz <= top) & (r_xy <= radius)
         idx = 2 * zz - 3 * t + zpad                        # z - 1.5 t in half-voxel units
         n = noise[idx, yy, xx]

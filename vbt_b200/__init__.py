@@ -48,6 +48,7 @@ _sig = {
     "vbt_asset_open": ([C.c_char_p, C.c_int, C.POINTER(_vp)], C.c_int),
     "vbt_asset_create": ([_vp, C.c_uint64, C.c_int, C.POINTER(_vp)], C.c_int),
     "vbt_asset_destroy": ([_vp], C.c_int),
+    "vbt_asset_upload": ([_vp, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_asset_get_info": ([_vp, C.POINTER(VbtAssetInfo)], C.c_int),
     "vbt_build_page_table": ([_vp, _vp], C.c_int),
     "vbt_page_table_device": ([_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)], C.c_int),
@@ -165,6 +166,12 @@ class Asset:
     @property
     def handle(self):
         return self._h
+
+    def upload(self, host_image, stream=None):
+        """Re-upload a file image (pinned torch uint8 tensor or numpy array) into this asset."""
+        ptr = host_image.data_ptr() if hasattr(host_image, "data_ptr") else host_image.ctypes.data
+        n = host_image.numel() if hasattr(host_image, "numel") else host_image.nbytes
+        _check(_lib.vbt_asset_upload(self._h, ptr, n, _stream(stream)))
 
     # kernel (a)
     def build_page_table(self, stream=None):

@@ -322,6 +322,30 @@ int vbt_asset_open(const char* path, int device, vbt_asset** out)
     return vbt_asset_create(bytes.data(), bytes.size(), device, out);
 }
 
+int vbt_asset_upload(vbt_asset* a, const void* file_bytes, uint64_t len, void* stream)
+{
+    if (!a || !file_bytes) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    const uint8_t* b = static_cast<const uint8_t*>(file_bytes);
+    if (len < 52 || std::memcmp(b, &"VBTPACK4"[0], 8) != 0) return fail(VBT_STATUS_FILE, "Unsupported magic. Expected VBTPACK4.");
+    uint32_t f[11];
+    for (int i = 0; i < 11; ++i) f[i] = rd32(b + 8 + 4 * i);
+    const vbt_header& h = a->hdr;
+    const uint32_t want[11] = {h.version, h.width, h.height, h.depth, h.frames, h.leaf_size, h.coarse_resolution,
+                               h.max_coarse_keep, h.leaf_count, h.profile_type, h.coarse_ac_scale_count};
+    if (std::memcmp(f, want, sizeof f) != 0) return fail(VBT_STATUS_INVALID_ARGUMENT, "image header differs from the asset's");
+    const uint64_t off_off = 52 + 4ull * h.coarse_ac_scale_count;
+    const uint64_t pay_off = off_off + 4ull * ((uint64_t)h.leaf_count + 1u);
+    if (len != pay_off + 4ull * a->dev.g.payload_words)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "image size differs from the asset's");
+    DeviceGuard guard(a->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (h.coarse_ac_scale_count)
+        CUDA_TRY(cudaMemcpyAsync((void*)a->dev.scales, b + 52, 4ull * h.coarse_ac_scale_count, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync((void*)a->dev.offsets, b + off_off, 4ull * ((uint64_t)h.leaf_count + 1u), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync((void*)a->dev.payload, b + pay_off, 4ull * a->dev.g.payload_words, cudaMemcpyHostToDevice, s));
+    return VBT_STATUS_OK;
+}
+
 int vbt_asset_destroy(vbt_asset* a)
 {
     if (!a) return VBT_STATUS_OK;

@@ -103,8 +103,12 @@ __device__ LeafEntry walk_rt_leaf(const DeviceAsset& a, uint32_t leaf, int lane)
     const uint32_t* __restrict__ pw = a.payload;
     LeafEntry e{};
     const uint32_t wb = __ldg(a.offsets + leaf), we = __ldg(a.offsets + leaf + 1);
-    const uint64_t bytes = 4ull * (we - wb);
     e.word_off = wb;
+    if (we <= wb || we > a.g.payload_words) {   // offsets are re-checked here for re-uploaded images
+        e.info = kErrDecodeOob << 16;
+        return e;
+    }
+    const uint64_t bytes = 4ull * (we - wb);
     e.header = ldw(pw, wb);
     const uint32_t mode = e.header & 3u;
     if (mode == kModeEmpty) return e;
@@ -631,9 +635,9 @@ struct FrameList {
     int f[64];
 };
 
-template <bool DENSE>
-__global__ void __launch_bounds__(kDecodeWarps * 32) decode_kernel(DeviceAsset a, FrameList fl, float* __restrict__ out,
-                                                                  uint64_t frame_stride)
+template <bool DENSE, bool SCI>
+__global__ void __launch_bounds__(kDecodeWarps * 32, 2) decode_kernel(DeviceAsset a, FrameList fl, float* __restrict__ out,
+                                                                     uint64_t frame_stride)
 {
     __shared__ __align__(16) float s_ctrl_all[kDecodeWarps][kWarpSlots];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -646,14 +650,14 @@ __global__ void __launch_bounds__(kDecodeWarps * 32) decode_kernel(DeviceAsset a
         uint32_t bx, by, bz;
         int w, h, d;
         leaf_extent(a.g, leaf, bx, by, bz, w, h, d);
-        const bool empty = a.g.profile != 2u && (e.header & 3u) == kModeEmpty;
+        const bool empty = !SCI && (e.header & 3u) == kModeEmpty;
         const uint32_t st = entry_status(e);
         if (st != kOk && lane == 0) record_error(a.err, leaf, st);
         for (int fi = 0; fi < fl.n; ++fi) {
             const int frame = clamp_frame(fl.f[fi], (int)a.g.frames);
             bool oob = false;
             if (!empty && st == kOk) {
-                if (a.g.profile == 2u) sci_decode_controls(a, e, (uint32_t)fl.f[fi], s_ctrl, lane, oob);
+                if (SCI) sci_decode_controls(a, e, (uint32_t)fl.f[fi], s_ctrl, lane, oob);
                 else rt_decode_controls(a, e, frame, s_ctrl, lane);
             }
             __syncwarp();
@@ -663,7 +667,7 @@ __global__ void __launch_bounds__(kDecodeWarps * 32) decode_kernel(DeviceAsset a
                 if (empty || st != kOk) {
 #pragma unroll
                     for (int i = 0; i < 8; ++i) v[i] = 0.0f;
-                } else if (a.g.profile == 2u) {
+                } else if (SCI) {
                     sci_row(a, e, s_ctrl, (uint32_t)fl.f[fi], w, h, d, ly, lz, v, oob);
                 } else {
                     rt_row(a, e, s_ctrl, w, h, d, ly, lz, v);
@@ -698,7 +702,7 @@ static int default_grid()
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_kernel<false>, kDecodeWarps * 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_kernel<false, false>, kDecodeWarps * 32, 0);
         g = sms * (per > 0 ? per : 1);
     }
     return g;
@@ -710,7 +714,9 @@ void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, f
     FrameList fl{};
     fl.n = nframes;
     for (int i = 0; i < nframes; ++i) fl.f[i] = frames[i];
-    decode_kernel<false><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    const int g = grid > 0 ? grid : default_grid();
+    if (a.g.profile == 2u) decode_kernel<false, true><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    else decode_kernel<false, false><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
 }
 
 void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, float* out, int grid, cudaStream_t s)
@@ -719,7 +725,9 @@ void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, f
     fl.n = nframes;
     for (int i = 0; i < nframes; ++i) fl.f[i] = frames[i];
     const uint64_t stride = (uint64_t)a.g.width * a.g.height * a.g.depth;
-    decode_kernel<true><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    const int g = grid > 0 ? grid : default_grid();
+    if (a.g.profile == 2u) decode_kernel<true, true><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    else decode_kernel<true, false><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
 }
 
 // Plain per-leaf launch: grid = the whole leaf grid, one 64-thread CTA per leaf (EMPTY leaves
