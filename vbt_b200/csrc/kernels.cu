@@ -24,6 +24,14 @@ __device__ AxisWeight g_axis[kAxisRes * kAxisExt * kAxisPos];
 // Scientific trilinear axes: [0] coarse 4^3 grid (f = x/7*3, clamp 0..2), [1] dense 3^3, [2] dense 4^3.
 __constant__ AxisWeight c_sci_axis[3][8];
 
+}  // namespace vbtb
+
+#include <cuda_fp16.h>
+
+#include "rt_decode_v2.cuh"
+
+namespace vbtb {
+
 // ---------------------------------------------------------------------------------------------
 // host: axis tables, computed with the same float expressions as the reference
 // (render/src/render_smoke_vbt_bench_main.cpp:201-234; render/src/scientific_decode.cpp:99-123,
@@ -695,6 +703,137 @@ __global__ void __launch_bounds__(kDecodeWarps * 32, 2) decode_kernel(DeviceAsse
     }
 }
 
+// Render-temporal decode, v2: one warp per (leaf, chunk of up to 16 frames); controls decoded in
+// frame batches, voxels by the separable trilinear (rt_decode_v2.cuh).
+template <bool DENSE>
+__global__ void __launch_bounds__(kV2Warps * 32, 5) decode_rt_v2_kernel(DeviceAsset a, FrameList fl,
+                                                                        float* __restrict__ out, uint64_t frame_stride)
+{
+    __shared__ V2WarpSmem smem[kV2Warps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    V2WarpSmem& sm = smem[warp];
+    const uint32_t* __restrict__ pw = a.payload;
+    const uint32_t n_leaves = DENSE ? a.g.leaf_count : *(volatile const uint32_t*)a.counters;
+    const uint32_t n_chunks = (uint32_t)(fl.n + kV2ChunkFrames - 1) / kV2ChunkFrames;
+    const uint64_t n_items = (uint64_t)n_leaves * n_chunks;
+    const int total = (int)a.g.frames;
+    const int ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
+    for (uint64_t item = (uint64_t)blockIdx.x * kV2Warps + warp; item < n_items;
+         item += (uint64_t)gridDim.x * kV2Warps) {
+        const uint32_t li = (uint32_t)(item / n_chunks), chunk = (uint32_t)(item % n_chunks);
+        const uint32_t leaf = DENSE ? li : __ldg(a.active_list + li);
+        const LeafEntry e = a.entries[leaf];
+        uint32_t bx, by, bz;
+        int w, h, d;
+        leaf_extent(a.g, leaf, bx, by, bz, w, h, d);
+        const uint32_t st = entry_status(e);
+        const bool empty = (e.header & 3u) == kModeEmpty;
+        const int f_begin = (int)chunk * kV2ChunkFrames;
+        const int f_end = min(fl.n, f_begin + kV2ChunkFrames);
+        auto store = [&](int fi, int i, float4 v) {
+            const int lz = 2 * i + (lane >> 4);
+            if (DENSE) {
+                if (ly < h && lz < d) {
+                    float* dst = out + (uint64_t)fi * frame_stride +
+                                 ((uint64_t)(bz * 8 + lz) * a.g.height + (by * 8 + ly)) * a.g.width + bx * 8 + lx0;
+                    if (lx0 + 4 <= w && (((uintptr_t)dst) & 15u) == 0u) {
+                        *reinterpret_cast<float4*>(dst) = v;
+                    } else {
+                        const float vv[4] = {v.x, v.y, v.z, v.w};
+                        for (int k = 0; k < 4 && lx0 + k < w; ++k) dst[k] = vv[k];
+                    }
+                }
+            } else {
+                reinterpret_cast<float4*>(out + (uint64_t)fi * frame_stride + (uint64_t)li * 512u)[lane + 32 * i] = v;
+            }
+        };
+        if (st != kOk || empty) {
+            if (st != kOk && lane == 0 && chunk == 0) record_error(a.err, leaf, st);
+            for (int fi = f_begin; fi < f_end; ++fi)
+                for (int i = 0; i < 4; ++i) store(fi, i, make_float4(0.f, 0.f, 0.f, 0.f));
+            continue;
+        }
+        const uint64_t base = 4ull * e.word_off;
+        const int cres = (int)((e.header >> 6) & 7u), fres = (int)((e.header >> 9) & 7u);
+        const bool fine = (e.info & kFlagFine) != 0u, shell = (e.info & kFlagShell) != 0u;
+        const bool occ = (e.info & kFlagOccClamp) != 0u;
+        const StreamRef cs{base + 8u, (uint32_t)(cres * cres * cres), 8u, e.kf & 0xFFFFu, (e.header >> 2) & 3u};
+        const StreamRef fs{base + 8u + e.coarse_bytes, (uint32_t)(fres * fres * fres), 8u, e.kf >> 16,
+                           (e.header >> 4) & 3u};
+        const StreamRef ss{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
+        const int Cc = (int)cs.controls;
+        const int Cf = fine ? (int)fs.controls : (shell ? (int)ss.controls : 0);
+        const int Ctot = Cc + Cf;
+        const int nb_max = min(kV2MaxBatch, kV2CtrlBudget / max(Ctot, 1));
+        load_axis_weights(sm, 0, cres, w, h, d, lane);
+        if (fine) load_axis_weights(sm, 1, fres, w, h, d, lane);
+        // Mode2 occupancy words of the lane's four z layers
+        uint64_t mask[4] = {0, 0, 0, 0};
+        uint32_t pref[4] = {0, 0, 0, 0};
+        if (occ) {
+            const uint64_t ob = base + 8u + e.coarse_bytes;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const uint32_t g = (uint32_t)(2 * i + (lane >> 4));
+                mask[i] = ((uint64_t)ldw(pw, (uint32_t)((ob + 8u * g + 4u) >> 2)) << 32) |
+                          ldw(pw, (uint32_t)((ob + 8u * g) >> 2));
+                pref[i] = (ldw(pw, (uint32_t)((ob + 64u + 2u * g) >> 2)) >> ((g & 1u) * 16u)) & 0xFFFFu;
+            }
+        }
+        for (int fb = f_begin; fb < f_end; fb += nb_max) {
+            const int nb = min(nb_max, f_end - fb);
+            __syncwarp();
+            if (lane < nb) {
+                const int fr = clamp_frame(fl.f[fb + lane], total);
+                sm.fr[lane] = fr;
+                sm.b8[lane] = (uint8_t)time_bin(fr, 8u, total);
+                sm.b4[lane] = (uint8_t)time_bin(fr, 4u, total);
+            }
+            __syncwarp();
+            for (int c = lane; c < Ctot; c += 32) {
+                if (c < Cc) decode_control_batch(pw, cs, (uint32_t)c, sm, nb, sm.ctrl + c, Ctot);
+                else if (fine) decode_control_batch(pw, fs, (uint32_t)(c - Cc), sm, nb, sm.ctrl + c, Ctot);
+                else decode_control_batch(pw, ss, (uint32_t)(c - Cc), sm, nb, sm.ctrl + c, Ctot);
+            }
+            __syncwarp();
+            for (int j = 0; j < nb; ++j) {
+                const float* g = sm.ctrl + j * Ctot;
+                float4 q[4];
+                if (cres >= 2) trilinear_quads(sm, 0, g, cres, lane, q);
+                else constant_quads(g, cres, q);
+                if (fine) {
+                    float4 qf[4];
+                    if (fres >= 2) trilinear_quads(sm, 1, g + Cc, fres, lane, qf);
+                    else constant_quads(g + Cc, fres, qf);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const float2 lo2 = add2_rn(make_float2(q[i].x, q[i].y), make_float2(qf[i].x, qf[i].y));
+                        const float2 hi2 = add2_rn(make_float2(q[i].z, q[i].w), make_float2(qf[i].z, qf[i].w));
+                        q[i] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int lz = 2 * i + (lane >> 4);
+                    float v[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const uint32_t bit = (uint32_t)(ly * 8 + lx0 + k);
+                        const bool in_occ = occ && ((mask[i] >> bit) & 1ull);
+                        if (shell && in_occ) {
+                            const uint32_t di = (pref[i] + __popcll(mask[i] & ((1ull << bit) - 1ull))) & 0xFFFFu;
+                            v[k] = __fadd_rn(v[k], g[Cc + di]);
+                        }
+                        if (occ && !in_occ && v[k] < 0.0f) v[k] = 0.0f;
+                        if (lx0 + k >= w || ly >= h || lz >= d) v[k] = 0.0f;
+                    }
+                    store(fb + j, i, make_float4(v[0], v[1], v[2], v[3]));
+                }
+            }
+        }
+    }
+}
+
 static int default_grid()
 {
     static int g = 0;
@@ -708,15 +847,30 @@ static int default_grid()
     return g;
 }
 
+// One wave of the render-temporal v2 kernel: SMs x resident CTAs per SM.
+static int rt_v2_grid()
+{
+    static int g = 0;
+    if (!g) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_rt_v2_kernel<false>, kV2Warps * 32, 0);
+        g = sms * (per > 0 ? per : 1);
+    }
+    return g;
+}
+
 void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, float* out, uint64_t stride, int grid,
                          cudaStream_t s)
 {
     FrameList fl{};
     fl.n = nframes;
     for (int i = 0; i < nframes; ++i) fl.f[i] = frames[i];
-    const int g = grid > 0 ? grid : default_grid();
-    if (a.g.profile == 2u) decode_kernel<false, true><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
-    else decode_kernel<false, false><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    if (a.g.profile == 2u)
+        decode_kernel<false, true><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    else
+        decode_rt_v2_kernel<false><<<grid > 0 ? grid : rt_v2_grid(), kV2Warps * 32, 0, s>>>(a, fl, out, stride);
 }
 
 void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, float* out, int grid, cudaStream_t s)
@@ -725,9 +879,10 @@ void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, f
     fl.n = nframes;
     for (int i = 0; i < nframes; ++i) fl.f[i] = frames[i];
     const uint64_t stride = (uint64_t)a.g.width * a.g.height * a.g.depth;
-    const int g = grid > 0 ? grid : default_grid();
-    if (a.g.profile == 2u) decode_kernel<true, true><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
-    else decode_kernel<true, false><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    if (a.g.profile == 2u)
+        decode_kernel<true, true><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    else
+        decode_rt_v2_kernel<true><<<grid > 0 ? grid : rt_v2_grid(), kV2Warps * 32, 0, s>>>(a, fl, out, stride);
 }
 
 // Plain per-leaf launch: grid = the whole leaf grid, one 64-thread CTA per leaf (EMPTY leaves
