@@ -73,8 +73,9 @@ int vbt_asset_open(const char* path, int device, vbt_asset** out_asset);
 int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset** out_asset);
 int vbt_asset_destroy(vbt_asset* asset);
 /* Re-upload a file image with the same header and sizes into the asset's resident buffers,
- * asynchronously on `stream` (host memory should be pinned).  Leaf offsets are re-checked on the
- * device by the next vbt_build_page_table, which must follow before decoding. */
+ * asynchronously on `stream` (host memory should be pinned), then re-walk the leaves and redo the
+ * per-asset key-order analysis on the same stream.  Leaf offsets are checked on the device by the
+ * walker (a leaf whose offsets leave the payload gets VBT_STATUS_DECODE_OOB). */
 int vbt_asset_upload(vbt_asset* asset, const void* file_bytes, uint64_t len, void* stream);
 int vbt_asset_get_info(vbt_asset* asset, vbt_asset_info* out_info);
 

@@ -277,3 +277,41 @@ def test_corrupted_asset_reports_leaf_status(vbt, cuda, oracle):
     assert same_bits(got[m], want[m])
     a.sync_status()   # error was cleared
     a.close()
+
+
+def test_unsorted_keys_and_descending_frames(vbt, cuda, oracle):
+    """Leaves whose key frames are not strictly increasing (here: one key frame byte rewritten)
+    lose the sorted flag and take the reference-search path; descending frame lists take it too.
+    Both must stay bit-exact with the oracle."""
+    path = golden_asset("tiny_density")
+    raw = bytearray(open(path, "rb").read())
+    f = oracle.load(path)
+    off, pay = f.offsets(), f.payload()
+    hdr_bytes = 52 + 4 * (f.leaf_count + 1)
+    leaf = int(np.flatnonzero((pay[off[:-1]] & 3) != 0)[0])
+    st, v = f.o.parse_leaf(pay.view(np.uint8)[4 * off[leaf]:4 * off[leaf + 1]])
+    leaf0 = hdr_bytes + 4 * int(off[leaf])
+    desc = np.frombuffer(bytes(raw[leaf0 + 8:leaf0 + 8 + 4 * 64]), np.uint32)
+    c = int(np.flatnonzero(((desc >> 16) & 0xFF) >= 2)[0])
+    ks = int(desc[c] & 0xFFFF)
+    kb = leaf0 + v.coarse.key_off
+    raw[kb + 3 * (ks + 1)] = raw[kb + 3 * ks]          # duplicate the first key's frame
+    path2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "_work", "unsorted_tiny.vbtp")
+    os.makedirs(os.path.dirname(path2), exist_ok=True)
+    open(path2, "wb").write(raw)
+    a = vbt.Asset(data=bytes(raw))
+    f2 = oracle.load(path2)
+    rows = a.leaf_table()
+    assert (rows[leaf, 7] & (1 << 14)) == 0                 # not flagged sorted
+    others = (rows[:, 7] & (1 << 10)) != 0
+    others[leaf] = False
+    assert np.all((rows[others, 7] & (1 << 14)) != 0)      # every other active leaf is
+    X, Y, Z = a.dims
+    for ts in (list(range(-1, a.frames + 1)), list(range(a.frames, -2, -1))):
+        out = cuda.empty((len(ts), Z, Y, X), dtype=cuda.float32, device="cuda")
+        a.decode_frames(ts, out)
+        a.sync_status()
+        got = out.cpu().numpy()
+        for i, t in enumerate(ts):
+            assert same_bits(got[i], f2.frame(t)), t
+    a.close()

@@ -244,14 +244,14 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     g.payload_words = words;
     const uint32_t L = h.leaf_count;
     const uint32_t tiles = (L + kWalkTile - 1) / kWalkTile;
-    void *d_off, *d_pay, *d_scales, *d_basis, *d_entries, *d_compact, *d_list, *d_counters, *d_err, *d_tiles;
+    void *d_off, *d_pay, *d_scales, *d_basis, *d_entries, *d_compact, *d_list, *d_counters, *d_err, *d_tiles, *d_sorted;
     // payload gets 16 bytes of tail padding so vector reads near the end stay inside the allocation
     if ((st = alloc(a, &d_off, 4ull * (L + 1))) || (st = alloc(a, &d_pay, 4ull * words + 16)) ||
         (st = alloc(a, &d_scales, 4ull * (h.coarse_ac_scale_count + 1))) ||
         (st = alloc(a, &d_basis, h.profile_type == 2u ? 4ull * h.frames * 64u : 16u)) ||
         (st = alloc(a, &d_entries, sizeof(LeafEntry) * (uint64_t)L)) || (st = alloc(a, &d_compact, 4ull * L)) ||
         (st = alloc(a, &d_list, 4ull * L)) || (st = alloc(a, &d_counters, 16)) || (st = alloc(a, &d_err, 8)) ||
-        (st = alloc(a, &d_tiles, 8ull * tiles))) {
+        (st = alloc(a, &d_tiles, 8ull * tiles)) || (st = alloc(a, &d_sorted, L))) {
         free_all(a);
         delete a;
         return st;
@@ -278,6 +278,7 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     cudaMemset(d_counters, 0, 16);
     cudaMemset(d_err, 0xFF, 8);
     cudaMemset(d_tiles, 0, 8ull * tiles);
+    cudaMemset(d_sorted, 0, L);
     const cudaError_t ce = cudaGetLastError();
     if (ce != cudaSuccess) {
         free_all(a);
@@ -295,8 +296,11 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     d.counters = static_cast<uint32_t*>(d_counters);
     d.err = static_cast<unsigned long long*>(d_err);
     d.tile_state = static_cast<unsigned long long*>(d_tiles);
-    // first page-table build, synchronously, so that a returned asset is ready to decode
+    d.key_sorted = static_cast<uint8_t*>(d_sorted);
+    // first page-table build and key-order analysis, synchronously, so that a returned asset is
+    // ready to decode
     launch_walk(d, ++a->epoch, 0);
+    launch_key_order(d, 0);
     const cudaError_t we = cudaDeviceSynchronize();
     if (we != cudaSuccess) {
         free_all(a);
@@ -343,7 +347,10 @@ int vbt_asset_upload(vbt_asset* a, const void* file_bytes, uint64_t len, void* s
         CUDA_TRY(cudaMemcpyAsync((void*)a->dev.scales, b + 52, 4ull * h.coarse_ac_scale_count, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync((void*)a->dev.offsets, b + off_off, 4ull * ((uint64_t)h.leaf_count + 1u), cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync((void*)a->dev.payload, b + pay_off, 4ull * a->dev.g.payload_words, cudaMemcpyHostToDevice, s));
-    return VBT_STATUS_OK;
+    // the key-order analysis belongs to the payload: redo it (it needs a walked leaf table)
+    launch_walk(a->dev, ++a->epoch, s);
+    launch_key_order(a->dev, s);
+    return check_launch("key_order_kernel");
 }
 
 int vbt_asset_destroy(vbt_asset* a)

@@ -230,8 +230,60 @@ __device__ LeafEntry walk_rt_leaf(const DeviceAsset& a, uint32_t leaf, int lane)
         }
         if (__any_sync(0xFFFFFFFFu, bad)) status = kErrKeyRangeOob;
     }
+    if (status == kOk && a.key_sorted[leaf]) flags |= kFlagSorted;
     e.info = (active & 0x3FFu) | flags | (status << 16);
     return e;
+}
+
+// Key-order analysis of one leaf (one warp): are the key frames of every control the decoders
+// read strictly increasing?  Controls with an out-of-pool key range are never decoded (see
+// decode_control) and are skipped.
+__global__ void __launch_bounds__(256) key_order_kernel(DeviceAsset a)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t leaf = blockIdx.x * 8u + (threadIdx.x >> 5);
+    if (leaf >= a.g.leaf_count) return;
+    LeafEntry& e = a.entries[leaf];
+    const uint32_t info = e.info;
+    bool sorted = entry_status(e) == kOk && (info & kFlagActive) && a.g.profile != 2u;
+    if (sorted) {
+        const uint32_t* __restrict__ pw = a.payload;
+        const uint64_t base = 4ull * e.word_off;
+        const uint32_t cres = (e.header >> 6) & 7u, fres = (e.header >> 9) & 7u;
+        StreamRef st[3];
+        int ns = 0;
+        st[ns++] = StreamRef{base + 8u, cres * cres * cres, 8u, e.kf & 0xFFFFu, (e.header >> 2) & 3u};
+        if (info & kFlagFine)
+            st[ns++] = StreamRef{base + 8u + e.coarse_bytes, fres * fres * fres, 8u, e.kf >> 16, (e.header >> 4) & 3u};
+        if (info & kFlagShell)
+            st[ns++] = StreamRef{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
+        bool ok = true;
+        for (int si = 0; si < ns; ++si) {
+            const StreamRef& s = st[si];
+            const uint64_t kb = stream_key_base(s);
+            for (uint32_t c = lane; c < s.controls; c += 32) {
+                const uint32_t desc = ldw(pw, (uint32_t)((s.base + 4ull * c) >> 2));
+                const uint32_t ks = desc & 0xFFFFu, kc = (desc >> 16) & 0xFFu;
+                if (kc < 2u || ks + kc > s.kf) continue;
+                int prev = key_frame(pw, kb, s.codec, ks);
+                for (uint32_t i = 1; i < kc; ++i) {
+                    const int f = key_frame(pw, kb, s.codec, ks + i);
+                    ok &= f > prev;
+                    prev = f;
+                }
+            }
+        }
+        sorted = __all_sync(0xFFFFFFFFu, ok);
+    }
+    if (lane == 0) {
+        a.key_sorted[leaf] = sorted ? 1 : 0;
+        if (sorted) e.info = info | kFlagSorted;
+    }
+}
+
+void launch_key_order(const DeviceAsset& a, cudaStream_t s)
+{
+    key_order_kernel<<<(a.g.leaf_count + 7) / 8, 256, 0, s>>>(a);
 }
 
 // Scientific leaves: every leaf is active.  The decoder reads through bounds-checked accessors
@@ -790,10 +842,13 @@ __global__ void __launch_bounds__(kV2Warps * 32, 5) decode_rt_v2_kernel(DeviceAs
                 sm.b4[lane] = (uint8_t)time_bin(fr, 4u, total);
             }
             __syncwarp();
+            const bool cursor = (e.info & kFlagSorted) &&
+                                __all_sync(0xFFFFFFFFu, lane == 0 || lane >= nb || sm.fr[lane] >= sm.fr[lane - 1]);
             for (int c = lane; c < Ctot; c += 32) {
-                if (c < Cc) decode_control_batch(pw, cs, (uint32_t)c, sm, nb, sm.ctrl + c, Ctot);
-                else if (fine) decode_control_batch(pw, fs, (uint32_t)(c - Cc), sm, nb, sm.ctrl + c, Ctot);
-                else decode_control_batch(pw, ss, (uint32_t)(c - Cc), sm, nb, sm.ctrl + c, Ctot);
+                const StreamRef& s = c < Cc ? cs : (fine ? fs : ss);
+                const uint32_t ci = (uint32_t)(c < Cc ? c : c - Cc);
+                if (cursor) decode_control_cursor(pw, s, ci, sm, nb, sm.ctrl + c, Ctot);
+                else decode_control_batch(pw, s, ci, sm, nb, sm.ctrl + c, Ctot);
             }
             __syncwarp();
             for (int j = 0; j < nb; ++j) {

@@ -27,6 +27,7 @@ struct DeviceAsset {
     uint32_t* counters;          // [0] active count, [1] walk error flags
     unsigned long long* err;     // first failing (leaf << 8 | status), ~0 when none
     unsigned long long* tile_state;  // look-back tile descriptors
+    uint8_t* key_sorted;         // per leaf: 1 when its decoded controls' key frames strictly increase
 };
 
 constexpr int kWalkThreads = 256;
@@ -39,6 +40,9 @@ constexpr int kCtrlSlots = 343 + 512;   // coarse (<= 7^3) + fine (<= 7^3) or sh
 constexpr int kWarpSlots = 64 + 16 * 64 > kCtrlSlots ? 64 + 16 * 64 : kCtrlSlots;
 
 void launch_walk(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);
+// Per-asset key-order analysis (after a walk): sets key_sorted[] and the kFlagSorted bit of the
+// leaf table.  Runs at load and after every re-upload; later walks copy the bit from key_sorted.
+void launch_key_order(const DeviceAsset& a, cudaStream_t s);
 // Decode `nframes` frames (frames[] on the host, <= 64) of every active leaf into the cache:
 // out[f * cache_frame_stride + rank * 512 + voxel].
 void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, float* out,

@@ -104,7 +104,10 @@ __device__ __forceinline__ float decode_control(const uint32_t* __restrict__ pw,
     // bin row: bins bytes at base + 4C + c*bins (4-byte aligned for bins = 4 or 8)
     const uint64_t row = s.base + 4ull * s.controls + (uint64_t)c * s.bins;
     const uint32_t w0 = ldw(pw, (uint32_t)((row + (bin & ~3u)) >> 2));
-    if (kc == 0u) return 0.0f;
+    // keyCount 0 decodes to 0; a key range past the pool only occurs for Mode2 shell controls of
+    // voxels outside a boundary leaf's extent, which are never sampled (the walker validated all
+    // others), so it is not read either.
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) return 0.0f;
     const uint32_t ks = desc & 0xFFFFu;
     const uint32_t last = kc - 1u;
     const uint64_t kb = stream_key_base(s) ;

@@ -1,8 +1,10 @@
 // rt_decode_v2.cuh -- render-temporal leaf decode, one warp per (leaf, frame chunk).
 //
-// Controls: every control of the leaf is decoded for a batch of frames at once; the descriptor
-// and the bin-hint row are loaded once per control and the keyframes of later frames come from
-// L1.  Each decode is the reference's bracket search (rt_decode.cuh), so values are bit-equal.
+// Controls: every control of the leaf is decoded for a batch of frames at once.  Leaves whose key
+// frames are strictly increasing (checked once per asset) use a forward cursor that reads each
+// key once; other leaves, and frame lists that go backwards, use the reference's bracket search
+// with the descriptor and bin-hint row hoisted out of the frame loop.  Both give the reference's
+// bits (rt_decode.cuh).
 //
 // Voxels: the reference's trilinear (render/src/render_smoke_vbt_bench_main.cpp:236-267) lerps
 // along x first, then y, then z:  c00 = lerp_x(g[z0][y0][x0], g[z0][y0][x1]), c0 = lerp_y(c00,
@@ -10,8 +12,6 @@
 // the y-lerp only on (lx, ly, control row z), so they are computed once per leaf and frame
 // (R*R*8 and R*64 lerps) and shared by every voxel that uses them: the same operations on the
 // same operands in the same order, hence the same bits, with 4-6x fewer lerps than per voxel.
-// Pairs of lerps run as packed FP32x2 instructions (__fmul2_rn / __fadd2_rn round each half
-// exactly like the scalar _rn operations).
 #pragma once
 #include "rt_decode.cuh"
 
@@ -84,7 +84,7 @@ __device__ __forceinline__ void decode_control_batch(const uint32_t* __restrict_
     const uint32_t r0 = ldw(pw, (uint32_t)(row >> 2));
     const uint32_t r1 = s.bins == 8u ? ldw(pw, (uint32_t)(row >> 2) + 1u) : 0u;
     const uint32_t kc = (desc >> 16) & 0xFFu;
-    if (kc == 0u) {
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {   // see decode_control (rt_decode.cuh)
         for (int j = 0; j < nb; ++j) dst[j * stride] = 0.0f;
         return;
     }
@@ -143,6 +143,68 @@ __device__ __forceinline__ void decode_control_batch(const uint32_t* __restrict_
                     out = __fadd_rn(v0, __fmul_rn(alpha, __fsub_rn(v1, v0)));
                 }
             }
+        }
+        dst[j * stride] = out;
+    }
+}
+
+// Cursor decode of control c for a batch of non-decreasing frames, valid when the control's key
+// frames are strictly increasing (checked once per asset, kFlagSorted).  For such keys the
+// reference's hinted bracket search returns: the first key's value before it, the last key's
+// value after it, the key's value on an exact hit, else v0 + a*(v1 - v0) with a = (t-f0)/(f1-f0)
+// for the adjacent pair around t -- so a cursor k = "first key with frame > t" that only moves
+// forward, reading each key once, yields the same bits.
+__device__ __forceinline__ void decode_control_cursor(const uint32_t* __restrict__ pw, const StreamRef& s, uint32_t c,
+                                                      const V2WarpSmem& sm, int nb, float* dst, int stride)
+{
+    const uint32_t desc = ldw(pw, (uint32_t)((s.base + 4ull * c) >> 2));
+    const uint32_t kc = (desc >> 16) & 0xFFu;
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {   // see decode_control (rt_decode.cuh)
+        for (int j = 0; j < nb; ++j) dst[j * stride] = 0.0f;
+        return;
+    }
+    const uint32_t ks = desc & 0xFFFFu;
+    const uint64_t kb = stream_key_base(s);
+    // initial cursor for the first frame: start from the bin hint (a predecessor candidate)
+    const int t0 = sm.fr[0];
+    const uint32_t bin = s.bins == 8u ? sm.b8[0] : sm.b4[0];
+    const uint64_t row = s.base + 4ull * s.controls + (uint64_t)c * s.bins;
+    const uint32_t hb = (ldw(pw, (uint32_t)((row + (bin & ~3u)) >> 2)) >> ((bin & 3u) * 8u)) & 0xFFu;
+    uint32_t k = hb < kc - 1u ? hb : kc - 1u;
+    int fk;
+    float vk;
+    key_read_v2(pw, kb, s.codec, ks + k, fk, vk);
+    if (fk > t0) {   // hint overshoots: binary search for the first key > t0 in [0, k]
+        uint32_t lo = 0, hi = k;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (key_frame(pw, kb, s.codec, ks + mid) > t0) hi = mid;
+            else lo = mid + 1u;
+        }
+        k = lo;
+    } else {          // step forward from the hint
+        ++k;
+        while (k < kc && key_frame(pw, kb, s.codec, ks + k) <= t0) ++k;
+    }
+    // prev = key k-1, next = key k (when they exist)
+    int fp = 0, fn = 0;
+    float vp = 0.0f, vn = 0.0f;
+    if (k > 0u) key_read_v2(pw, kb, s.codec, ks + k - 1u, fp, vp);
+    if (k < kc) key_read_v2(pw, kb, s.codec, ks + k, fn, vn);
+    for (int j = 0; j < nb; ++j) {
+        const int t = sm.fr[j];
+        while (k < kc && fn <= t) {
+            fp = fn;
+            vp = vn;
+            ++k;
+            if (k < kc) key_read_v2(pw, kb, s.codec, ks + k, fn, vn);
+        }
+        float out;
+        if (k == 0u) out = vn;               // before the first key
+        else if (k == kc || fp == t) out = vp;   // after the last key, or an exact hit
+        else {
+            const float alpha = __fdiv_rn((float)(t - fp), (float)(fn - fp));
+            out = __fadd_rn(vp, __fmul_rn(alpha, __fsub_rn(vn, vp)));
         }
         dst[j * stride] = out;
     }
