@@ -13,6 +13,7 @@ struct AssetGeom {
     uint32_t profile;       // 2 = scientific, otherwise render-temporal
     uint32_t scale_count;
     uint64_t payload_words;
+    uint32_t stage_bytes;   // shared-memory leaf stage of the render decode kernel (0 = none)
 };
 
 struct DeviceAsset {

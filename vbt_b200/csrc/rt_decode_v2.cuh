@@ -213,31 +213,33 @@ __device__ __forceinline__ void decode_control_cursor(const uint32_t* __restrict
 // Separable trilinear of one control grid (resolution R >= 2) for one frame.  On return each
 // lane holds its 4 voxel quads: quad i covers voxels 4*(lane + 32 i) .. +3, i.e. lz = 2i +
 // (lane >> 4), ly = (lane >> 1) & 7, lx = 4*(lane & 1) .. +3.
-__device__ __forceinline__ void trilinear_quads(V2WarpSmem& sm, int ws, const float* __restrict__ g, int R, int lane,
-                                                float4 q[4])
+// w[axis][p] are the axis weights of this grid; x2 (R*R*4 float2) and y4 (R*16 float4) are the
+// warp's scratch rows in shared memory.
+__device__ __forceinline__ void trilinear_quads_ptr(const AxisWeight (*w)[8], float2* x2, float4* y4,
+                                                    const float* __restrict__ g, int R, int lane, float4 q[4])
 {
     // x-lerps: X[z*R + y][pair] for lx pair (2p, 2p+1)
     const int nx = R * R * 4;
     for (int it = lane; it < nx; it += 32) {
         const int row = it >> 2, p = it & 3;
-        const AxisWeight wa = sm.w[ws][0][2 * p], wb = sm.w[ws][0][2 * p + 1];
+        const AxisWeight wa = w[0][2 * p], wb = w[0][2 * p + 1];
         const float* gr = g + row * R;
         const float2 A = make_float2(gr[wa.i0], gr[wb.i0]);
         const float2 B = make_float2(gr[wa.i1], gr[wb.i1]);
-        sm.x2[it] = lerp2(A, B, make_float2(wa.t, wb.t), make_float2(wa.omt, wb.omt));
+        x2[it] = lerp2(A, B, make_float2(wa.t, wb.t), make_float2(wa.omt, wb.omt));
     }
     __syncwarp();
     // y-lerps: Y[z][ly][quad] for lx quad (4k .. 4k+3), two float2 lerps each
     const int ny = R * 16;
     for (int it = lane; it < ny; it += 32) {
         const int z = it >> 4, ly = (it >> 1) & 7, k = it & 1;
-        const AxisWeight wy = sm.w[ws][1][ly];
-        const float2* xa = sm.x2 + (z * R + wy.i0) * 4 + 2 * k;
-        const float2* xb = sm.x2 + (z * R + wy.i1) * 4 + 2 * k;
+        const AxisWeight wy = w[1][ly];
+        const float2* xa = x2 + (z * R + wy.i0) * 4 + 2 * k;
+        const float2* xb = x2 + (z * R + wy.i1) * 4 + 2 * k;
         const float2 t = make_float2(wy.t, wy.t), omt = make_float2(wy.omt, wy.omt);
         const float2 lo2 = lerp2(xa[0], xb[0], t, omt);
         const float2 hi2 = lerp2(xa[1], xb[1], t, omt);
-        sm.y4[it] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
+        y4[it] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
     }
     __syncwarp();
     // z-lerps: the lane's four voxel quads
@@ -245,15 +247,21 @@ __device__ __forceinline__ void trilinear_quads(V2WarpSmem& sm, int ws, const fl
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int lz = 2 * i + (lane >> 4);
-        const AxisWeight wz = sm.w[ws][2][lz];
-        const float4 A = sm.y4[(wz.i0 * 8 + ly) * 2 + k];
-        const float4 B = sm.y4[(wz.i1 * 8 + ly) * 2 + k];
+        const AxisWeight wz = w[2][lz];
+        const float4 A = y4[(wz.i0 * 8 + ly) * 2 + k];
+        const float4 B = y4[(wz.i1 * 8 + ly) * 2 + k];
         const float2 t = make_float2(wz.t, wz.t), omt = make_float2(wz.omt, wz.omt);
         const float2 lo2 = lerp2(make_float2(A.x, A.y), make_float2(B.x, B.y), t, omt);
         const float2 hi2 = lerp2(make_float2(A.z, A.w), make_float2(B.z, B.w), t, omt);
         q[i] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
     }
     __syncwarp();
+}
+
+__device__ __forceinline__ void trilinear_quads(V2WarpSmem& sm, int ws, const float* __restrict__ g, int R, int lane,
+                                                float4 q[4])
+{
+    trilinear_quads_ptr(sm.w[ws], sm.x2, sm.y4, g, R, lane, q);
 }
 
 __device__ __forceinline__ void load_axis_weights(V2WarpSmem& sm, int ws, int R, int w, int h, int d, int lane)

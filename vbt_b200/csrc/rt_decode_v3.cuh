@@ -1,0 +1,239 @@
+// rt_decode_v3.cuh -- render-temporal decode from a shared-memory copy of the leaf.
+//
+// One CTA decodes one leaf for every frame of the launch.  The leaf's bytes are brought into
+// shared memory by a single TMA bulk copy (cp.async.bulk, completion on an mbarrier), so the
+// per-control keyframe walks -- chains of dependent 3-byte reads -- run at shared-memory latency
+// instead of L2 latency.  The copied window is the leaf rounded out to 16-byte boundaries (the
+// payload allocation is 16-byte aligned and padded by 16 bytes, so the window never leaves it).
+// Leaves larger than the stage are decoded the same way straight from global memory.
+//
+// All decode arithmetic is shared with rt_decode_v2.cuh: cursor walks for leaves whose key frames
+// strictly increase, the reference's hinted bracket search otherwise, and the separable trilinear.
+#pragma once
+#include "rt_decode_v2.cuh"
+
+namespace vbtb {
+
+// Word readers: global (read-only path) or a shared-memory window that starts at word `w0`.
+struct GlobalWords {
+    const uint32_t* __restrict__ pw;
+    __device__ __forceinline__ uint32_t operator()(uint32_t i) const { return __ldg(pw + i); }
+};
+struct SharedWords {
+    const uint32_t* s;
+    uint32_t w0;
+    __device__ __forceinline__ uint32_t operator()(uint32_t i) const { return s[i - w0]; }
+};
+
+template <class M>
+__device__ __forceinline__ uint32_t m_key24(const M& m, uint64_t b)
+{
+    const uint32_t w = (uint32_t)(b >> 2);
+    const uint32_t sh = (uint32_t)(b & 3u) * 8u;
+    const uint32_t lo = m(w);
+    if (sh <= 8u) return (lo >> sh) & 0xFFFFFFu;
+    return __funnelshift_r(lo, m(w + 1u), sh) & 0xFFFFFFu;
+}
+
+template <class M>
+__device__ __forceinline__ int m_key_frame(const M& m, uint64_t kb, uint32_t codec, uint32_t i)
+{
+    if (codec == 1u) return (int)(m((uint32_t)((kb + 8ull * i) >> 2)) & 0xFFFFu);
+    const uint64_t b = kb + 3ull * i;
+    return (int)((m((uint32_t)(b >> 2)) >> ((uint32_t)(b & 3u) * 8u)) & 0xFFu);
+}
+
+template <class M>
+__device__ __forceinline__ void m_key_read(const M& m, uint64_t kb, uint32_t codec, uint32_t i, int& frame,
+                                           float& value)
+{
+    if (codec == 1u) {
+        const uint32_t w = (uint32_t)((kb + 8ull * i) >> 2);
+        frame = (int)(m(w) & 0xFFFFu);
+        value = __uint_as_float(m(w + 1u));
+    } else {
+        const uint32_t k = m_key24(m, kb + 3ull * i);
+        frame = (int)(k & 0xFFu);
+        value = half_to_float_exact(k >> 8);
+    }
+}
+
+struct FrameBatch {
+    const int* fr;          // clamped frames
+    const uint8_t* b8;      // time bins for 8-bin streams
+    const uint8_t* b4;      // time bins for 4-bin streams
+    int nb;
+};
+
+// Cursor walk (strictly increasing key frames, non-decreasing frames); see
+// decode_control_cursor in rt_decode_v2.cuh for why it equals the reference's search.
+template <class M>
+__device__ __forceinline__ void m_control_cursor(const M& m, const StreamRef& s, uint32_t c, const FrameBatch& fb,
+                                                 float* dst, int stride)
+{
+    const uint32_t desc = m((uint32_t)((s.base + 4ull * c) >> 2));
+    const uint32_t kc = (desc >> 16) & 0xFFu;
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {   // see decode_control (rt_decode.cuh)
+        for (int j = 0; j < fb.nb; ++j) dst[j * stride] = 0.0f;
+        return;
+    }
+    const uint32_t ks = desc & 0xFFFFu;
+    const uint64_t kb = stream_key_base(s);
+    const int t0 = fb.fr[0];
+    const uint32_t bin = s.bins == 8u ? fb.b8[0] : fb.b4[0];
+    const uint64_t row = s.base + 4ull * s.controls + (uint64_t)c * s.bins;
+    const uint32_t hb = (m((uint32_t)((row + (bin & ~3u)) >> 2)) >> ((bin & 3u) * 8u)) & 0xFFu;
+    uint32_t k = hb < kc - 1u ? hb : kc - 1u;
+    if (m_key_frame(m, kb, s.codec, ks + k) > t0) {
+        uint32_t lo = 0, hi = k;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (m_key_frame(m, kb, s.codec, ks + mid) > t0) hi = mid;
+            else lo = mid + 1u;
+        }
+        k = lo;
+    } else {
+        ++k;
+        while (k < kc && m_key_frame(m, kb, s.codec, ks + k) <= t0) ++k;
+    }
+    int fp = 0, fn = 0;
+    float vp = 0.0f, vn = 0.0f;
+    if (k > 0u) m_key_read(m, kb, s.codec, ks + k - 1u, fp, vp);
+    if (k < kc) m_key_read(m, kb, s.codec, ks + k, fn, vn);
+    for (int j = 0; j < fb.nb; ++j) {
+        const int t = fb.fr[j];
+        while (k < kc && fn <= t) {
+            fp = fn;
+            vp = vn;
+            ++k;
+            if (k < kc) m_key_read(m, kb, s.codec, ks + k, fn, vn);
+        }
+        float out;
+        if (k == 0u) out = vn;
+        else if (k == kc || fp == t) out = vp;
+        else {
+            const float alpha = __fdiv_rn((float)(t - fp), (float)(fn - fp));
+            out = __fadd_rn(vp, __fmul_rn(alpha, __fsub_rn(vn, vp)));
+        }
+        dst[j * stride] = out;
+    }
+}
+
+// The reference's hinted bracket search per frame (src/render_temporal_decode.cpp:79-131).
+template <class M>
+__device__ __forceinline__ void m_control_search(const M& m, const StreamRef& s, uint32_t c, const FrameBatch& fb,
+                                                 float* dst, int stride)
+{
+    const uint32_t desc = m((uint32_t)((s.base + 4ull * c) >> 2));
+    const uint64_t row = s.base + 4ull * s.controls + (uint64_t)c * s.bins;
+    const uint32_t r0 = m((uint32_t)(row >> 2));
+    const uint32_t r1 = s.bins == 8u ? m((uint32_t)(row >> 2) + 1u) : 0u;
+    const uint32_t kc = (desc >> 16) & 0xFFu;
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {
+        for (int j = 0; j < fb.nb; ++j) dst[j * stride] = 0.0f;
+        return;
+    }
+    const uint32_t ks = desc & 0xFFFFu, last = kc - 1u;
+    const uint64_t kb = stream_key_base(s);
+    const uint8_t* bins_of_frame = s.bins == 8u ? fb.b8 : fb.b4;
+    for (int j = 0; j < fb.nb; ++j) {
+        const int frame = fb.fr[j];
+        const uint32_t bin = bins_of_frame[j];
+        const uint32_t hb = row_byte(r0, r1, bin);
+        uint32_t lo = hb < last ? hb : last;
+        int f0, f1;
+        float v0, v1, out;
+        m_key_read(m, kb, s.codec, ks + lo, f0, v0);
+        if (f0 > frame) {
+            lo = 0u;
+            m_key_read(m, kb, s.codec, ks, f0, v0);
+        }
+        if (f0 >= frame || lo == last) {
+            out = v0;
+        } else {
+            uint32_t hi = last;
+            if (bin + 1u < s.bins) {
+                const uint32_t h = row_byte(r0, r1, bin + 1u) + 1u;
+                hi = h < last ? h : last;
+            }
+            if (hi < lo + 1u) hi = lo + 1u;
+            m_key_read(m, kb, s.codec, ks + hi, f1, v1);
+            if (f1 < frame) {
+                hi = last;
+                m_key_read(m, kb, s.codec, ks + hi, f1, v1);
+            }
+            if (f1 <= frame) {
+                out = v1;
+            } else {
+                bool moved_lo = false, moved_hi = false;
+                while (hi > lo + 1u) {
+                    const uint32_t mid = lo + (hi - lo) / 2u;
+                    const int fm = m_key_frame(m, kb, s.codec, ks + mid);
+                    if (fm < frame) {
+                        lo = mid;
+                        f0 = fm;
+                        moved_lo = true;
+                    } else {
+                        hi = mid;
+                        f1 = fm;
+                        moved_hi = true;
+                    }
+                }
+                if (moved_hi) m_key_read(m, kb, s.codec, ks + hi, f1, v1);
+                if (f1 == frame) {
+                    out = v1;
+                } else {
+                    if (moved_lo) m_key_read(m, kb, s.codec, ks + lo, f0, v0);
+                    const float alpha = __fdiv_rn((float)(frame - f0), (float)(f1 - f0));
+                    out = __fadd_rn(v0, __fmul_rn(alpha, __fsub_rn(v1, v0)));
+                }
+            }
+        }
+        dst[j * stride] = out;
+    }
+}
+
+// ---- TMA bulk copy global -> shared with mbarrier completion (sm_90+ PTX, no multicast) ----
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Issue one bulk copy of `bytes` (multiple of 16; both addresses 16-byte aligned) and arm the
+// barrier with the byte count.  The proxy fence orders this CTA's earlier generic-proxy reads of
+// the destination before the async-proxy writes.
+__device__ __forceinline__ void mbar_expect_and_copy(uint64_t* bar, void* dst, const void* src, uint32_t bytes)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Bounded wait for phase `parity` of the mbarrier: returns false if it did not complete within
+// the iteration limit (the caller records a timeout status instead of hanging).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+}  // namespace vbtb
