@@ -243,23 +243,22 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     g.profile = h.profile_type;
     g.scale_count = h.coarse_ac_scale_count;
     g.payload_words = words;
-    // Shared-memory leaf stage of the render decode kernel: large enough for 98% of the non-EMPTY
-    // leaves' 16-byte-aligned windows, between 4 and 96 KiB (bigger leaves decode from global).
+    // Shared-memory leaf stage of the render decode kernel: the largest 16-byte-aligned window of a
+    // non-EMPTY leaf, capped so that two CTAs fit on an SM (232,448 B of shared memory per SM
+    // less 1 KiB per CTA); an asset with bigger leaves gets the kernel variant that decodes those
+    // from global memory.
     if (h.profile_type != 2u) {
         const uint8_t* off = b + off_off;
-        std::vector<uint32_t> win;
+        uint64_t maxw = 0;
         for (uint32_t i = 0; i < h.leaf_count; ++i) {
             const uint64_t w0 = rd32(off + 4ull * i), w1 = rd32(off + 4ull * (i + 1));
             if ((rd32(b + pay_off + 4ull * w0) & 3u) == 0u) continue;
             const uint64_t a0 = (4ull * w0) & ~15ull, a1 = (4ull * w1 + 15u) & ~15ull;
-            win.push_back((uint32_t)std::min<uint64_t>(a1 - a0, 1u << 30));
+            maxw = std::max(maxw, a1 - a0);
         }
-        uint32_t stage = 4096;
-        if (!win.empty()) {
-            std::sort(win.begin(), win.end());
-            stage = std::max(stage, win[(size_t)((win.size() - 1) * 0.98)]);
-        }
-        g.stage_bytes = std::min<uint32_t>((stage + 1023u) & ~1023u, 96u * 1024u);
+        g.max_window = (uint32_t)std::min<uint64_t>(maxw, 0xFFFFFFFFull);
+        const uint32_t cap = ((233472u / 2u - 1024u - kLeafFixedBytes) / 1024u) * 1024u;
+        g.stage_bytes = std::min<uint32_t>(std::max<uint32_t>((g.max_window + 1023u) & ~1023u, 4096u), cap);
     }
     const uint32_t L = h.leaf_count;
     const uint32_t tiles = (L + kWalkTile - 1) / kWalkTile;

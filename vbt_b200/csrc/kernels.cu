@@ -889,239 +889,10 @@ __global__ void __launch_bounds__(kV2Warps * 32, 5) decode_rt_v2_kernel(DeviceAs
     }
 }
 
-// ---------------------------------------------------------------------------------------------
-// Render-temporal decode, v3: one CTA (4 warps) per leaf and all frames of the launch; the leaf
-// is staged in shared memory by one TMA bulk copy (rt_decode_v3.cuh).
-
-constexpr int kV3Threads = 128;
-constexpr int kV3CtrlBudget = 4096;   // floats: frames x controls of one batch
-constexpr uint32_t kV3Fixed = 16 + 256 + 128 + 576 + 4 * 196 * 8 + 4 * 112 * 16 + kV3CtrlBudget * 4;
-
-struct V3Smem {
-    uint64_t* bar;
-    int* fr;
-    uint8_t *b8, *b4;
-    AxisWeight (*w)[3][8];
-    float2* x2;      // [warp][196]
-    float4* y4;      // [warp][112]
-    float* ctrl;     // [kV3CtrlBudget]
-    uint8_t* stage;  // leaf window
-};
-
-__device__ __forceinline__ V3Smem v3_layout(uint8_t* dyn)
-{
-    V3Smem s;
-    s.bar = reinterpret_cast<uint64_t*>(dyn);
-    s.fr = reinterpret_cast<int*>(dyn + 16);
-    s.b8 = dyn + 16 + 256;
-    s.b4 = s.b8 + 64;
-    s.w = reinterpret_cast<AxisWeight(*)[3][8]>(dyn + 16 + 256 + 128);
-    s.x2 = reinterpret_cast<float2*>(dyn + 16 + 256 + 128 + 576);
-    s.y4 = reinterpret_cast<float4*>(reinterpret_cast<uint8_t*>(s.x2) + 4 * 196 * 8);
-    s.ctrl = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(s.y4) + 4 * 112 * 16);
-    s.stage = reinterpret_cast<uint8_t*>(s.ctrl) + kV3CtrlBudget * 4;
-    return s;
-}
-
-// Decode one (validated, non-EMPTY) leaf for all frames of the launch with word reader `m`.
-template <bool DENSE, class M>
-__device__ __forceinline__ void v3_decode_leaf(const DeviceAsset& a, const M& m, const V3Smem& s, const LeafEntry& e,
-                                               int nframes, bool mono, uint32_t li, uint32_t bx, uint32_t by,
-                                               uint32_t bz, int w, int h, int d, float* __restrict__ out,
-                                               uint64_t frame_stride)
-{
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint64_t base = 4ull * e.word_off;
-    const int cres = (int)((e.header >> 6) & 7u), fres = (int)((e.header >> 9) & 7u);
-    const bool fine = (e.info & kFlagFine) != 0u, shell = (e.info & kFlagShell) != 0u;
-    const bool occ = (e.info & kFlagOccClamp) != 0u;
-    const StreamRef cs{base + 8u, (uint32_t)(cres * cres * cres), 8u, e.kf & 0xFFFFu, (e.header >> 2) & 3u};
-    const StreamRef fs{base + 8u + e.coarse_bytes, (uint32_t)(fres * fres * fres), 8u, e.kf >> 16,
-                       (e.header >> 4) & 3u};
-    const StreamRef ss{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
-    const int Cc = (int)cs.controls;
-    const int Cf = fine ? (int)fs.controls : (shell ? (int)ss.controls : 0);
-    const int Ctot = Cc + Cf;
-    const int nb_max = min(nframes, kV3CtrlBudget / max(Ctot, 1));
-    const bool cursor = mono && (e.info & kFlagSorted) != 0u;
-    const int ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
-    uint64_t mask[4] = {0, 0, 0, 0};
-    uint32_t pref[4] = {0, 0, 0, 0};
-    if (occ) {
-        const uint64_t ob = base + 8u + e.coarse_bytes;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const uint32_t g = (uint32_t)(2 * i + (lane >> 4));
-            mask[i] = ((uint64_t)m((uint32_t)((ob + 8u * g + 4u) >> 2)) << 32) | m((uint32_t)((ob + 8u * g) >> 2));
-            pref[i] = (m((uint32_t)((ob + 64u + 2u * g) >> 2)) >> ((g & 1u) * 16u)) & 0xFFFFu;
-        }
-    }
-    float2* x2 = s.x2 + warp * 196;
-    float4* y4 = s.y4 + warp * 112;
-    for (int fb0 = 0; fb0 < nframes; fb0 += nb_max) {
-        const int nb = min(nb_max, nframes - fb0);
-        const FrameBatch fb{s.fr + fb0, s.b8 + fb0, s.b4 + fb0, nb};
-        for (int c = tid; c < Ctot; c += kV3Threads) {
-            const StreamRef& st = c < Cc ? cs : (fine ? fs : ss);
-            const uint32_t ci = (uint32_t)(c < Cc ? c : c - Cc);
-            if (cursor) m_control_cursor(m, st, ci, fb, s.ctrl + c, Ctot);
-            else m_control_search(m, st, ci, fb, s.ctrl + c, Ctot);
-        }
-        __syncthreads();
-        for (int j = warp; j < nb; j += kV3Threads / 32) {
-            const float* g = s.ctrl + j * Ctot;
-            float4 q[4];
-            if (cres >= 2) trilinear_quads_ptr(s.w[0], x2, y4, g, cres, lane, q);
-            else constant_quads(g, cres, q);
-            if (fine) {
-                float4 qf[4];
-                if (fres >= 2) trilinear_quads_ptr(s.w[1], x2, y4, g + Cc, fres, lane, qf);
-                else constant_quads(g + Cc, fres, qf);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const float2 lo2 = add2_rn(make_float2(q[i].x, q[i].y), make_float2(qf[i].x, qf[i].y));
-                    const float2 hi2 = add2_rn(make_float2(q[i].z, q[i].w), make_float2(qf[i].z, qf[i].w));
-                    q[i] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
-                }
-            }
-            const int fi = fb0 + j;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int lz = 2 * i + (lane >> 4);
-                float v[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const uint32_t bit = (uint32_t)(ly * 8 + lx0 + k);
-                    const bool in_occ = occ && ((mask[i] >> bit) & 1ull);
-                    if (shell && in_occ) {
-                        const uint32_t di = (pref[i] + __popcll(mask[i] & ((1ull << bit) - 1ull))) & 0xFFFFu;
-                        v[k] = __fadd_rn(v[k], g[Cc + di]);
-                    }
-                    if (occ && !in_occ && v[k] < 0.0f) v[k] = 0.0f;
-                    if (lx0 + k >= w || ly >= h || lz >= d) v[k] = 0.0f;
-                }
-                if (DENSE) {
-                    if (ly < h && lz < d) {
-                        float* dst = out + (uint64_t)fi * frame_stride +
-                                     ((uint64_t)(bz * 8 + lz) * a.g.height + (by * 8 + ly)) * a.g.width + bx * 8 + lx0;
-                        if (lx0 + 4 <= w && (((uintptr_t)dst) & 15u) == 0u) {
-                            *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
-                        } else {
-                            for (int k = 0; k < 4 && lx0 + k < w; ++k) dst[k] = v[k];
-                        }
-                    }
-                } else {
-                    reinterpret_cast<float4*>(out + (uint64_t)fi * frame_stride + (uint64_t)li * 512u)[lane + 32 * i] =
-                        make_float4(v[0], v[1], v[2], v[3]);
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
-template <bool DENSE>
-__global__ void __launch_bounds__(kV3Threads, 2) decode_rt_v3_kernel(DeviceAsset a, FrameList fl,
-                                                                     float* __restrict__ out, uint64_t frame_stride)
-{
-    extern __shared__ __align__(128) uint8_t dyn[];
-    const V3Smem s = v3_layout(dyn);
-    const int tid = threadIdx.x;
-    const int total = (int)a.g.frames;
-    if (tid == 0) {
-        mbar_init(s.bar, 1);
-        mbar_init_fence();
-    }
-    if (tid < fl.n) {
-        const int fr = clamp_frame(fl.f[tid], total);
-        s.fr[tid] = fr;
-        s.b8[tid] = (uint8_t)time_bin(fr, 8u, total);
-        s.b4[tid] = (uint8_t)time_bin(fr, 4u, total);
-    }
-    __syncthreads();
-    const bool mono = __syncthreads_and(tid == 0 || tid >= fl.n || s.fr[tid] >= s.fr[tid - 1]) != 0;
-    const uint32_t n_leaves = DENSE ? a.g.leaf_count : *(volatile const uint32_t*)a.counters;
-    const uint8_t* pay_bytes = reinterpret_cast<const uint8_t*>(a.payload);
-    uint32_t phase = 0;
-    for (uint32_t li = blockIdx.x; li < n_leaves; li += gridDim.x) {
-        const uint32_t leaf = DENSE ? li : __ldg(a.active_list + li);
-        const LeafEntry e = a.entries[leaf];
-        uint32_t bx, by, bz;
-        int w, h, d;
-        leaf_extent(a.g, leaf, bx, by, bz, w, h, d);
-        const uint32_t st = entry_status(e);
-        if (st != kOk || (e.header & 3u) == kModeEmpty) {
-            if (st != kOk && tid == 0) record_error(a.err, leaf, st);
-            // zeros for every frame: thread -> (frame, voxel quad)
-            for (int idx = tid; idx < fl.n * 128; idx += kV3Threads) {
-                const int fi = idx >> 7, qd = idx & 127;
-                const int lz = qd >> 4, ly = (qd >> 1) & 7, lx0 = 4 * (qd & 1);
-                if (DENSE) {
-                    if (ly < h && lz < d)
-                        for (int k = 0; k < 4 && lx0 + k < w; ++k)
-                            out[(uint64_t)fi * frame_stride +
-                                ((uint64_t)(bz * 8 + lz) * a.g.height + (by * 8 + ly)) * a.g.width + bx * 8 + lx0 + k] = 0.0f;
-                } else {
-                    reinterpret_cast<float4*>(out + (uint64_t)fi * frame_stride + (uint64_t)li * 512u)[qd] =
-                        make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
-            continue;
-        }
-        const uint64_t b0 = 4ull * e.word_off;
-        const uint64_t b1 = 4ull * (uint64_t)__ldg(a.offsets + leaf + 1);
-        const uint64_t a0 = b0 & ~15ull, a1 = (b1 + 15u) & ~15ull;
-        const bool staged = a1 - a0 <= a.g.stage_bytes;
-        __syncthreads();   // the previous leaf's shared-memory reads are complete
-        if (staged && tid == 0) mbar_expect_and_copy(s.bar, s.stage, pay_bytes + a0, (uint32_t)(a1 - a0));
-        if (tid < 48) {
-            const int ws = tid / 24, axis = (tid % 24) >> 3, p = tid & 7;
-            const int R = ws == 0 ? (int)((e.header >> 6) & 7u) : (int)((e.header >> 9) & 7u);
-            const int ext = axis == 0 ? w : (axis == 1 ? h : d);
-            s.w[ws][axis][p] = g_axis[axis_index(R, ext, p)];
-        }
-        if (staged) {
-            if (!mbar_wait(s.bar, phase)) {
-                if (tid == 0) record_error(a.err, leaf, kErrWaitTimeout);
-                mbar_wait(s.bar, phase);   // a second bounded wait for the copy in flight, then stop
-                return;
-            }
-            phase ^= 1u;
-        }
-        __syncthreads();
-        if (staged) {
-            const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
-            v3_decode_leaf<DENSE>(a, m, s, e, fl.n, mono, li, bx, by, bz, w, h, d, out, frame_stride);
-        } else {
-            const GlobalWords m{a.payload};
-            v3_decode_leaf<DENSE>(a, m, s, e, fl.n, mono, li, bx, by, bz, w, h, d, out, frame_stride);
-        }
-    }
-}
-
-static int v3_grid(uint32_t smem_bytes)
-{
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_rt_v3_kernel<false>, kV3Threads, smem_bytes);
-    return sms * (per > 0 ? per : 1);
-}
-
-static void launch_rt_v3(const DeviceAsset& a, const FrameList& fl, float* out, uint64_t stride, int grid, bool dense,
-                         cudaStream_t s)
-{
-    const uint32_t smem = kV3Fixed + a.g.stage_bytes;
-    static uint32_t configured = 0;
-    if (smem > configured) {
-        cudaFuncSetAttribute(decode_rt_v3_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(decode_rt_v3_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = smem;
-    }
-    const int g = grid > 0 ? grid : v3_grid(smem);
-    if (dense) decode_rt_v3_kernel<true><<<g, kV3Threads, smem, s>>>(a, fl, out, stride);
-    else decode_rt_v3_kernel<false><<<g, kV3Threads, smem, s>>>(a, fl, out, stride);
-}
+// Render-temporal decode kernel (TMA-staged leaf, one CTA per leaf): rt_kernel_leaf.cuh
+}  // namespace vbtb
+#include "rt_kernel_leaf.cuh"
+namespace vbtb {
 
 static int default_grid()
 {
@@ -1159,7 +930,7 @@ void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, f
     if (a.g.profile == 2u)
         decode_kernel<false, true><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
     else
-        launch_rt_v3(a, fl, out, stride, grid, false, s);
+        launch_rt_leaf(a, fl, out, stride, grid, false, s);
 }
 
 void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, float* out, int grid, cudaStream_t s)
@@ -1171,7 +942,7 @@ void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, f
     if (a.g.profile == 2u)
         decode_kernel<true, true><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
     else
-        launch_rt_v3(a, fl, out, stride, grid, true, s);
+        launch_rt_leaf(a, fl, out, stride, grid, true, s);
 }
 
 // Plain per-leaf launch: grid = the whole leaf grid, one 64-thread CTA per leaf (EMPTY leaves

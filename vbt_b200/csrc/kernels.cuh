@@ -14,6 +14,7 @@ struct AssetGeom {
     uint32_t scale_count;
     uint64_t payload_words;
     uint32_t stage_bytes;   // shared-memory leaf stage of the render decode kernel (0 = none)
+    uint32_t max_window;    // largest 16-byte-aligned window of a non-EMPTY leaf
 };
 
 struct DeviceAsset {
@@ -30,6 +31,10 @@ struct DeviceAsset {
     unsigned long long* tile_state;  // look-back tile descriptors
     uint8_t* key_sorted;         // per leaf: 1 when its decoded controls' key frames strictly increase
 };
+
+// Fixed shared memory of the render decode kernel besides its leaf stage (rt_kernel_leaf.cuh:
+// barrier, frame tables, axis weights, 8 warps x (x-lerp + y-lerp rows), 3072-float controls).
+constexpr uint32_t kLeafFixedBytes = 16 + 256 + 128 + 576 + 8 * 196 * 8 + 8 * 112 * 16 + 3072 * 4;
 
 constexpr int kWalkThreads = 256;
 constexpr int kWalkTile = 256;   // leaves per walker CTA (one scan element per thread)

@@ -119,6 +119,66 @@ __device__ __forceinline__ void m_control_cursor(const M& m, const StreamRef& s,
     }
 }
 
+// Streaming cursor over frames t0, t1, ... with t(j+1) - t(j) in {0, 1} (a clamped timeline
+// window), for a control whose key frames strictly increase.  The cursor k (first key with
+// frame > t) then advances at most once per frame, so the key after next is prefetched one
+// advance ahead and no frame waits on a load: the per-frame work is a compare, a register
+// shift and the value, independent across frames.  Values equal the reference's (see
+// decode_control_cursor in rt_decode_v2.cuh).
+template <class M>
+__device__ __forceinline__ void m_control_stream(const M& m, const StreamRef& s, uint32_t c, const int* fr,
+                                                 uint32_t bin0, int n, float* dst, int stride)
+{
+    const uint32_t desc = m((uint32_t)((s.base + 4ull * c) >> 2));
+    const uint32_t kc = (desc >> 16) & 0xFFu;
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {   // see decode_control (rt_decode.cuh)
+        for (int j = 0; j < n; ++j) dst[j * stride] = 0.0f;
+        return;
+    }
+    const uint32_t ks = desc & 0xFFFFu;
+    const uint64_t kb = stream_key_base(s);
+    const int t0 = fr[0];
+    const uint64_t row = s.base + 4ull * s.controls + (uint64_t)c * s.bins;
+    const uint32_t hb = (m((uint32_t)((row + (bin0 & ~3u)) >> 2)) >> ((bin0 & 3u) * 8u)) & 0xFFu;
+    uint32_t k = hb < kc - 1u ? hb : kc - 1u;
+    if (m_key_frame(m, kb, s.codec, ks + k) > t0) {
+        uint32_t lo = 0, hi = k;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (m_key_frame(m, kb, s.codec, ks + mid) > t0) hi = mid;
+            else lo = mid + 1u;
+        }
+        k = lo;
+    } else {
+        ++k;
+        while (k < kc && m_key_frame(m, kb, s.codec, ks + k) <= t0) ++k;
+    }
+    int fp = 0, fn = 0, fnn = 0;
+    float vp = 0.0f, vn = 0.0f, vnn = 0.0f;
+    if (k > 0u) m_key_read(m, kb, s.codec, ks + k - 1u, fp, vp);
+    if (k < kc) m_key_read(m, kb, s.codec, ks + k, fn, vn);
+    if (k + 1u < kc) m_key_read(m, kb, s.codec, ks + k + 1u, fnn, vnn);
+    for (int j = 0; j < n; ++j) {
+        const int t = fr[j];
+        if (k < kc && fn <= t) {
+            fp = fn;
+            vp = vn;
+            fn = fnn;
+            vn = vnn;
+            ++k;
+            if (k + 1u < kc) m_key_read(m, kb, s.codec, ks + k + 1u, fnn, vnn);
+        }
+        float out;
+        if (k == 0u) out = vn;
+        else if (k == kc || fp == t) out = vp;
+        else {
+            const float alpha = __fdiv_rn((float)(t - fp), (float)(fn - fp));
+            out = __fadd_rn(vp, __fmul_rn(alpha, __fsub_rn(vn, vp)));
+        }
+        dst[j * stride] = out;
+    }
+}
+
 // The reference's hinted bracket search per frame (src/render_temporal_decode.cpp:79-131).
 template <class M>
 __device__ __forceinline__ void m_control_search(const M& m, const StreamRef& s, uint32_t c, const FrameBatch& fb,

@@ -1,0 +1,284 @@
+// rt_kernel_leaf.cuh -- the render-temporal decode kernel: one CTA per leaf, all frames of the
+// launch, leaf bytes staged in shared memory by a TMA bulk copy.  Included by kernels.cu (it uses
+// that file's axis table g_axis and helpers).
+//
+// Per leaf, frames are processed in batches that fit the control buffer.  For each batch:
+//  1. controls: every (control, frame range) unit decodes its values into ctrl[frame][control].
+//     A leaf with few controls splits each control's frames over several threads, so all 256
+//     threads work.  Timeline batches (frame steps of 0 or 1) on leaves with strictly increasing
+//     key frames use the streaming cursor; anything else uses the reference's bracket search.
+//  2. voxels: each warp reconstructs whole frames with the separable trilinear and stores them.
+#pragma once
+
+namespace vbtb {
+
+constexpr int kLeafThreads = 256;
+constexpr int kLeafWarps = kLeafThreads / 32;
+constexpr int kLeafCtrlBudget = 3072;   // floats: frames x controls of one batch
+constexpr uint32_t kLeafFixed = 16 + 256 + 128 + 576 + kLeafWarps * 196 * 8 + kLeafWarps * 112 * 16 + kLeafCtrlBudget * 4;
+static_assert(kLeafFixed == kLeafFixedBytes, "host stage sizing must match the kernel's shared-memory layout");
+
+struct LeafSmem {
+    uint64_t* bar;
+    int* fr;
+    uint8_t *b8, *b4;
+    AxisWeight (*w)[3][8];
+    float2* x2;      // [warp][196]
+    float4* y4;      // [warp][112]
+    float* ctrl;     // [kLeafCtrlBudget]
+    uint8_t* stage;  // leaf window (16-byte aligned)
+};
+
+__device__ __forceinline__ LeafSmem leaf_layout(uint8_t* dyn)
+{
+    LeafSmem s;
+    s.bar = reinterpret_cast<uint64_t*>(dyn);
+    s.fr = reinterpret_cast<int*>(dyn + 16);
+    s.b8 = dyn + 16 + 256;
+    s.b4 = s.b8 + 64;
+    s.w = reinterpret_cast<AxisWeight(*)[3][8]>(dyn + 16 + 256 + 128);
+    s.x2 = reinterpret_cast<float2*>(dyn + 16 + 256 + 128 + 576);
+    s.y4 = reinterpret_cast<float4*>(reinterpret_cast<uint8_t*>(s.x2) + kLeafWarps * 196 * 8);
+    s.ctrl = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(s.y4) + kLeafWarps * 112 * 16);
+    s.stage = reinterpret_cast<uint8_t*>(s.ctrl) + kLeafCtrlBudget * 4;
+    return s;
+}
+
+struct LeafGeom {
+    uint32_t li, bx, by, bz;
+    int w, h, d;
+};
+
+template <bool DENSE>
+__device__ __forceinline__ void store_quad(const DeviceAsset& a, const LeafGeom& G, float* __restrict__ out,
+                                           uint64_t frame_stride, int fi, int lane, int i, float4 v)
+{
+    const int lz = 2 * i + (lane >> 4), ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
+    if (DENSE) {
+        if (ly < G.h && lz < G.d) {
+            float* dst = out + (uint64_t)fi * frame_stride +
+                         ((uint64_t)(G.bz * 8 + lz) * a.g.height + (G.by * 8 + ly)) * a.g.width + G.bx * 8 + lx0;
+            if (lx0 + 4 <= G.w && (((uintptr_t)dst) & 15u) == 0u) {
+                *reinterpret_cast<float4*>(dst) = v;
+            } else {
+                const float vv[4] = {v.x, v.y, v.z, v.w};
+                for (int k = 0; k < 4 && lx0 + k < G.w; ++k) dst[k] = vv[k];
+            }
+        }
+    } else {
+        reinterpret_cast<float4*>(out + (uint64_t)fi * frame_stride + (uint64_t)G.li * 512u)[lane + 32 * i] = v;
+    }
+}
+
+// Decode one validated, non-EMPTY leaf for all frames of the launch with word reader `m`.
+template <bool DENSE, class M>
+__device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, const LeafSmem& s, const LeafEntry& e,
+                                            int nframes, bool steps01, const LeafGeom& G, float* __restrict__ out,
+                                            uint64_t frame_stride)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t base = 4ull * e.word_off;
+    const int cres = (int)((e.header >> 6) & 7u), fres = (int)((e.header >> 9) & 7u);
+    const bool fine = (e.info & kFlagFine) != 0u, shell = (e.info & kFlagShell) != 0u;
+    const bool occ = (e.info & kFlagOccClamp) != 0u;
+    const StreamRef cs{base + 8u, (uint32_t)(cres * cres * cres), 8u, e.kf & 0xFFFFu, (e.header >> 2) & 3u};
+    const StreamRef fs{base + 8u + e.coarse_bytes, (uint32_t)(fres * fres * fres), 8u, e.kf >> 16,
+                       (e.header >> 4) & 3u};
+    const StreamRef ss{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
+    const int Cc = (int)cs.controls;
+    const int Cf = fine ? (int)fs.controls : (shell ? (int)ss.controls : 0);
+    const int Ctot = Cc + Cf;
+    const int nb_max = min(nframes, kLeafCtrlBudget / max(Ctot, 1));
+    const bool stream = steps01 && (e.info & kFlagSorted) != 0u;
+    // threads per control: split a control's frames when the leaf has few controls
+    int tpc = 1;
+    while (tpc < 8 && Ctot * tpc * 2 <= kLeafThreads) tpc *= 2;
+    const bool plain = !occ && G.w == 8 && G.h == 8 && G.d == 8;
+    const int ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
+    uint64_t mask[4] = {0, 0, 0, 0};
+    uint32_t pref[4] = {0, 0, 0, 0};
+    if (occ) {
+        const uint64_t ob = base + 8u + e.coarse_bytes;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t g = (uint32_t)(2 * i + (lane >> 4));
+            mask[i] = ((uint64_t)m((uint32_t)((ob + 8u * g + 4u) >> 2)) << 32) | m((uint32_t)((ob + 8u * g) >> 2));
+            pref[i] = (m((uint32_t)((ob + 64u + 2u * g) >> 2)) >> ((g & 1u) * 16u)) & 0xFFFFu;
+        }
+    }
+    float2* x2 = s.x2 + warp * 196;
+    float4* y4 = s.y4 + warp * 112;
+    for (int fb0 = 0; fb0 < nframes; fb0 += nb_max) {
+        const int nb = min(nb_max, nframes - fb0);
+        // 1. controls
+        const int part_len = (nb + tpc - 1) / tpc;
+        for (int unit = tid; unit < Ctot * tpc; unit += kLeafThreads) {
+            const int c = unit / tpc, q = unit % tpc;
+            const int j0 = q * part_len, j1 = min(nb, j0 + part_len);
+            if (j0 >= j1) continue;
+            const StreamRef& st = c < Cc ? cs : (fine ? fs : ss);
+            const uint32_t ci = (uint32_t)(c < Cc ? c : c - Cc);
+            float* dst = s.ctrl + j0 * Ctot + c;
+            if (stream) {
+                const uint32_t bin0 = st.bins == 8u ? s.b8[fb0 + j0] : s.b4[fb0 + j0];
+                m_control_stream(m, st, ci, s.fr + fb0 + j0, bin0, j1 - j0, dst, Ctot);
+            } else {
+                const FrameBatch fb{s.fr + fb0 + j0, s.b8 + fb0 + j0, s.b4 + fb0 + j0, j1 - j0};
+                m_control_search(m, st, ci, fb, dst, Ctot);
+            }
+        }
+        __syncthreads();
+        // 2. voxels
+        for (int j = warp; j < nb; j += kLeafWarps) {
+            const float* g = s.ctrl + j * Ctot;
+            float4 q[4];
+            if (cres >= 2) trilinear_quads_ptr(s.w[0], x2, y4, g, cres, lane, q);
+            else constant_quads(g, cres, q);
+            if (fine) {
+                float4 qf[4];
+                if (fres >= 2) trilinear_quads_ptr(s.w[1], x2, y4, g + Cc, fres, lane, qf);
+                else constant_quads(g + Cc, fres, qf);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float2 lo2 = add2_rn(make_float2(q[i].x, q[i].y), make_float2(qf[i].x, qf[i].y));
+                    const float2 hi2 = add2_rn(make_float2(q[i].z, q[i].w), make_float2(qf[i].z, qf[i].w));
+                    q[i] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
+                }
+            }
+            const int fi = fb0 + j;
+            if (plain) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) store_quad<DENSE>(a, G, out, frame_stride, fi, lane, i, q[i]);
+                continue;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int lz = 2 * i + (lane >> 4);
+                float v[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const uint32_t bit = (uint32_t)(ly * 8 + lx0 + k);
+                    const bool in_occ = occ && ((mask[i] >> bit) & 1ull);
+                    if (shell && in_occ) {
+                        const uint32_t di = (pref[i] + __popcll(mask[i] & ((1ull << bit) - 1ull))) & 0xFFFFu;
+                        v[k] = __fadd_rn(v[k], g[Cc + di]);
+                    }
+                    if (occ && !in_occ && v[k] < 0.0f) v[k] = 0.0f;
+                    if (lx0 + k >= G.w || ly >= G.h || lz >= G.d) v[k] = 0.0f;
+                }
+                store_quad<DENSE>(a, G, out, frame_stride, fi, lane, i, make_float4(v[0], v[1], v[2], v[3]));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// GLOBAL_FALLBACK: leaves whose window exceeds the stage are decoded from global memory (only
+// instantiated for assets that have such leaves; it costs registers).
+template <bool DENSE, bool GLOBAL_FALLBACK>
+__global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsset a, FrameList fl,
+                                                                      float* __restrict__ out, uint64_t frame_stride)
+{
+    extern __shared__ __align__(128) uint8_t dyn[];
+    const LeafSmem s = leaf_layout(dyn);
+    const int tid = threadIdx.x;
+    const int total = (int)a.g.frames;
+    if (tid == 0) {
+        mbar_init(s.bar, 1);
+        mbar_init_fence();
+    }
+    if (tid < fl.n) {
+        const int fr = clamp_frame(fl.f[tid], total);
+        s.fr[tid] = fr;
+        s.b8[tid] = (uint8_t)time_bin(fr, 8u, total);
+        s.b4[tid] = (uint8_t)time_bin(fr, 4u, total);
+    }
+    __syncthreads();
+    const bool steps01 =
+        __syncthreads_and(tid == 0 || tid >= fl.n || (unsigned)(s.fr[tid] - s.fr[tid - 1]) <= 1u) != 0;
+    const uint32_t n_leaves = DENSE ? a.g.leaf_count : *(volatile const uint32_t*)a.counters;
+    const uint8_t* pay_bytes = reinterpret_cast<const uint8_t*>(a.payload);
+    uint32_t phase = 0;
+    for (uint32_t li = blockIdx.x; li < n_leaves; li += gridDim.x) {
+        const uint32_t leaf = DENSE ? li : __ldg(a.active_list + li);
+        const LeafEntry e = a.entries[leaf];
+        LeafGeom G;
+        G.li = li;
+        leaf_extent(a.g, leaf, G.bx, G.by, G.bz, G.w, G.h, G.d);
+        const uint32_t st = entry_status(e);
+        if (st != kOk || (e.header & 3u) == kModeEmpty) {
+            if (st != kOk && tid == 0) record_error(a.err, leaf, st);
+            for (int idx = tid; idx < fl.n * 128; idx += kLeafThreads)
+                store_quad<DENSE>(a, G, out, frame_stride, idx >> 7, (idx & 127) & 31, (idx & 127) >> 5,
+                                  make_float4(0.f, 0.f, 0.f, 0.f));
+            continue;
+        }
+        const uint64_t b0 = 4ull * e.word_off;
+        const uint64_t b1 = 4ull * (uint64_t)__ldg(a.offsets + leaf + 1);
+        const uint64_t a0 = b0 & ~15ull, a1 = (b1 + 15u) & ~15ull;
+        const bool staged = a1 - a0 <= a.g.stage_bytes;
+        if (!GLOBAL_FALLBACK && !staged) {   // the launcher never lets this happen
+            if (tid == 0) record_error(a.err, leaf, kErrDecodeOob);
+            continue;
+        }
+        __syncthreads();   // the previous leaf's shared-memory reads are complete
+        if (staged && tid == 0) mbar_expect_and_copy(s.bar, s.stage, pay_bytes + a0, (uint32_t)(a1 - a0));
+        if (tid < 48) {
+            const int ws = tid / 24, axis = (tid % 24) >> 3, p = tid & 7;
+            const int R = ws == 0 ? (int)((e.header >> 6) & 7u) : (int)((e.header >> 9) & 7u);
+            const int ext = axis == 0 ? G.w : (axis == 1 ? G.h : G.d);
+            s.w[ws][axis][p] = g_axis[axis_index(R, ext, p)];
+        }
+        if (staged) {
+            if (!mbar_wait(s.bar, phase)) {
+                if (tid == 0) record_error(a.err, leaf, kErrWaitTimeout);
+                mbar_wait(s.bar, phase);   // a second bounded wait for the copy in flight, then stop
+                return;
+            }
+            phase ^= 1u;
+        }
+        __syncthreads();
+        if (staged) {
+            const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
+            leaf_decode<DENSE>(a, m, s, e, fl.n, steps01, G, out, frame_stride);
+        } else if (GLOBAL_FALLBACK) {
+            const GlobalWords m{a.payload};
+            leaf_decode<DENSE>(a, m, s, e, fl.n, steps01, G, out, frame_stride);
+        }
+    }
+}
+
+template <bool DENSE, bool GF>
+static int leaf_grid(uint32_t smem_bytes)
+{
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_leaf_kernel<DENSE, GF>, kLeafThreads, smem_bytes);
+    return sms * (per > 0 ? per : 1);
+}
+
+template <bool DENSE, bool GF>
+static void launch_leaf_variant(const DeviceAsset& a, const FrameList& fl, float* out, uint64_t stride, int grid,
+                                cudaStream_t s)
+{
+    const uint32_t smem = kLeafFixed + a.g.stage_bytes;
+    cudaFuncSetAttribute(decode_leaf_kernel<DENSE, GF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int g = grid > 0 ? grid : leaf_grid<DENSE, GF>(smem);
+    decode_leaf_kernel<DENSE, GF><<<g, kLeafThreads, smem, s>>>(a, fl, out, stride);
+}
+
+static void launch_rt_leaf(const DeviceAsset& a, const FrameList& fl, float* out, uint64_t stride, int grid, bool dense,
+                           cudaStream_t s)
+{
+    const bool gf = a.g.max_window > a.g.stage_bytes;
+    if (dense) {
+        if (gf) launch_leaf_variant<true, true>(a, fl, out, stride, grid, s);
+        else launch_leaf_variant<true, false>(a, fl, out, stride, grid, s);
+    } else {
+        if (gf) launch_leaf_variant<false, true>(a, fl, out, stride, grid, s);
+        else launch_leaf_variant<false, false>(a, fl, out, stride, grid, s);
+    }
+}
+
+}  // namespace vbtb
