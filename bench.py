@@ -22,7 +22,6 @@ import os
 import statistics
 import subprocess
 import sys
-import tempfile
 import threading
 import time
 
@@ -40,7 +39,7 @@ CHUNK = 48
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=300)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--asset", default=DEFAULT_ASSET)
@@ -86,29 +85,42 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = tempfile.mktemp(prefix="vbt_clocks_", suffix=".csv")
+        self.lines = []
 
     def start(self):
+        """nvidia-smi every 50 ms; each line is stamped with the host clock when it arrives."""
         try:
-            self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
-                                         stderr=subprocess.DEVNULL)
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True, bufsize=1)
         except Exception:
             self.proc = None
+            return
 
-    def stop(self):
+        def reader():
+            for line in self.proc.stdout:
+                self.lines.append((time.time(), line))
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 10.0:   # nvidia-smi takes a moment to start
+            time.sleep(0.05)
+
+    def stop(self, t0, t1):
+        """Samples that arrived inside the host-clock window [t0, t1] of the timed region."""
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        self.fh.close()
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for ts, line in list(self.lines):
+            if ts < t0 or ts > t1:
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 7:
                 continue
@@ -120,7 +132,6 @@ class ClockSampler:
             for n, v in zip(names, parts[3:7]):
                 if v.lower() == "active":
                     reasons.add(n)
-        os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "samples": len(sm), "reasons": sorted(reasons)}
 
@@ -134,11 +145,13 @@ def measured_peak():
 
 
 def ncu_traffic():
-    """Per-launch DRAM bytes of the decode kernel from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "decode_cache_cfg2.json")
+    """Per-launch DRAM bytes (read + write) of the decode kernel from the committed ncu summary
+    (profiles/decode_leaf_cfg2.md, line `traffic_bytes_per_launch: N`), if present."""
+    p = os.path.join(ROOT, "profiles", "decode_leaf_cfg2.md")
     if os.path.exists(p):
-        d = json.load(open(p))
-        return d.get("dram_bytes_per_launch_full")
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1])
     return None
 
 
@@ -267,16 +280,17 @@ def run_ours(args, rank, local_rank, world):
     sampler = ClockSampler(local_rank) if rank == 0 else None
     if sampler:
         sampler.start()
-        time.sleep(0.4)
+    t_begin = time.time()
     for k in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
         step(ev[k])
     stream.synchronize()
     torch.cuda.synchronize()
+    t_end = time.time()
     if pg:
         pg.barrier()
-    clocks = sampler.stop() if sampler else None
+    clocks = sampler.stop(t_begin, t_end) if sampler else None
     a.sync_status(stream)
     step_ms = [e[0].elapsed_time(e[-1]) for e in ev]
     walk_ms = [e[0].elapsed_time(e[1]) for e in ev]
@@ -356,7 +370,7 @@ def run_ours(args, rank, local_rank, world):
                            "active_leaves": n_active, "frames_per_step": T, "frames_per_launch": CHUNK,
                            "l2": "flushed before every timed step (256 MiB write)",
                            "cache_ring_bytes": int(cache.numel() * 4), "parallelism": f"replicas x{world}"},
-                "roofline": {"bound": "hbm", "kernel": "decode_kernel<cache>", "achieved": achieved, "peak": peak,
+                "roofline": {"bound": "hbm", "kernel": "decode_leaf_kernel<cache>", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                              "algorithmic_bytes_per_launch": int(statistics.mean(alg_per_launch)),
                              "launch_ms": statistics.mean(dec_ms), "peak_source": peak_src},

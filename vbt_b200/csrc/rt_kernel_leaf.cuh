@@ -110,7 +110,8 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
     float4* y4 = s.y4 + warp * 112;
     for (int fb0 = 0; fb0 < nframes; fb0 += nb_max) {
         const int nb = min(nb_max, nframes - fb0);
-        // 1. controls
+        // 1. controls: (control, frame range) units; a leaf with few controls splits each
+        //    control's frames over tpc threads so that all threads work
         const int part_len = (nb + tpc - 1) / tpc;
         for (int unit = tid; unit < Ctot * tpc; unit += kLeafThreads) {
             const int c = unit / tpc, q = unit % tpc;
