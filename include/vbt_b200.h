@@ -129,6 +129,20 @@ int vbt_decode_control_values(const uint8_t* d_stream, uint32_t stream_bytes, ui
                               const uint32_t* d_control_index, const int32_t* d_frame, uint64_t n, float* d_out,
                               int32_t* d_status, void* stream);
 
+/* Active-leaf page table with no allocation of any kind, for callers that must not have a library
+ * allocate device memory (a renderer or plugin host that hands out all buffers from its own pool;
+ * a frame loop that cannot afford cudaMalloc's device synchronisation).  No counterpart in the
+ * reference.  Inputs are the asset's offsets (leaf_count + 1 words) and payload words already in
+ * device memory; outputs are compact[leaf_count], active_list[leaf_count] and *active_count, with
+ * the same values as vbt_build_page_table / vbt_get_page_table (0xFFFFFFFF in *active_count means a
+ * bounded device-side wait gave up).  Scratch is a fixed 512 KiB array inside the library, held by
+ * every GPU that loads it, so leaf_count is limited to 16,777,216 (VBT_STATUS_LIMIT beyond).  The
+ * first call on a device looks up that array's device address and should come before any stream
+ * capture.  All calls share the array: calls whose kernels overlap on the GPU race. */
+int vbt_build_page_table_noalloc(const uint32_t* d_offsets, const uint32_t* d_payload, uint64_t payload_words,
+                                 uint32_t leaf_count, uint32_t profile_type, uint32_t* d_compact,
+                                 uint32_t* d_active_list, uint32_t* d_active_count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

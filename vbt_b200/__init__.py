@@ -64,6 +64,7 @@ _sig = {
     "vbt_decode_frames_host": ([_vp, _i32p, C.c_int, _vp, _vp], C.c_int),
     "vbt_decode_control_values": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
                                    C.c_int, _vp, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
+    "vbt_build_page_table_noalloc": ([_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp], C.c_int),
 }
 for _name, (_args, _res) in _sig.items():
     _f = getattr(_lib, _name)
@@ -232,6 +233,15 @@ class Asset:
     def decode_frames_host(self, frames, out, stream=None):
         fr = (C.c_int32 * len(frames))(*frames)
         _check(_lib.vbt_decode_frames_host(self._h, fr, len(frames), out.ctypes.data, _stream(stream)))
+
+
+def build_page_table_noalloc(d_offsets, d_payload, payload_words, leaf_count, profile_type, d_compact,
+                             d_active_list, d_active_count, stream=None):
+    """Page table from caller-owned device buffers; the library allocates nothing (see the C
+    declaration in include/vbt_b200.h for the scratch array and its limit)."""
+    _check(_lib.vbt_build_page_table_noalloc(_addr(d_offsets), _addr(d_payload), payload_words, leaf_count,
+                                             profile_type, _addr(d_compact), _addr(d_active_list),
+                                             _addr(d_active_count), _stream(stream)))
 
 
 def decode_control_values(d_stream, stream_bytes, codec, control_count, bins, kf, total_frames, d_ci, d_frames, n,

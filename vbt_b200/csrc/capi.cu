@@ -169,6 +169,11 @@ int check_launch(const char* what)
 
 }  // namespace
 
+namespace vbtb {
+// Message for vbt_last_error() from other translation units of the library.
+int set_last_error(int status, const std::string& msg) { return fail(status, msg); }
+}  // namespace vbtb
+
 extern "C" {
 
 const char* vbt_status_string(int s)
