@@ -23,7 +23,6 @@ __constant__ AxisWeight c_axis[kAxisRes * kAxisExt * kAxisPos];
 __device__ AxisWeight g_axis[kAxisRes * kAxisExt * kAxisPos];
 // Scientific trilinear axes: [0] coarse 4^3 grid (f = x/7*3, clamp 0..2), [1] dense 3^3, [2] dense 4^3.
 __constant__ AxisWeight c_sci_axis[3][8];
-
 }  // namespace vbtb
 
 #include <cuda_fp16.h>

@@ -90,9 +90,6 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
     const int Ctot = Cc + Cf;
     const int nb_max = min(nframes, kLeafCtrlBudget / max(Ctot, 1));
     const bool stream = steps01 && (e.info & kFlagSorted) != 0u;
-    // threads per control: split a control's frames when the leaf has few controls
-    int tpc = 1;
-    while (tpc < 8 && Ctot * tpc * 2 <= kLeafThreads) tpc *= 2;
     const bool plain = !occ && G.w == 8 && G.h == 8 && G.d == 8;
     const int ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
     uint64_t mask[4] = {0, 0, 0, 0};
@@ -110,14 +107,12 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
     float4* y4 = s.y4 + warp * 112;
     for (int fb0 = 0; fb0 < nframes; fb0 += nb_max) {
         const int nb = min(nb_max, nframes - fb0);
-        // 1. controls: (control, frame range) units; a leaf with few controls splits each
-        //    control's frames over tpc threads so that all threads work
-        const int part_len = (nb + tpc - 1) / tpc;
-        for (int unit = tid; unit < Ctot * tpc; unit += kLeafThreads) {
-            const int c = unit / tpc, q = unit % tpc;
-            const int j0 = q * part_len, j1 = min(nb, j0 + part_len);
-            if (j0 >= j1) continue;
-            const StreamRef& st = c < Cc ? cs : (fine ? fs : ss);
+        // 1. controls, as (control, frame range) units.  With at most one control per thread, each
+        //    control's frames are split over tpc threads so that all threads work; with more, each
+        //    thread owns one whole control and the remaining controls are cut into short frame
+        //    ranges spread over all threads (each thread starts at most one extra range).
+        auto run_unit = [&](int c, int j0, int j1) {
+            const StreamRef st = c < Cc ? cs : (fine ? fs : ss);
             const uint32_t ci = (uint32_t)(c < Cc ? c : c - Cc);
             float* dst = s.ctrl + j0 * Ctot + c;
             if (stream) {
@@ -127,6 +122,16 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
                 const FrameBatch fb{s.fr + fb0 + j0, s.b8 + fb0 + j0, s.b4 + fb0 + j0, j1 - j0};
                 m_control_search(m, st, ci, fb, dst, Ctot);
             }
+        };
+        const int c0 = Ctot > kLeafThreads ? kLeafThreads : 0;   // controls [0, c0) are owned whole
+        if (c0) run_unit(tid, 0, nb);
+        const int rest = Ctot - c0;
+        const int tpc = min(8, max(1, kLeafThreads / rest));
+        const int part_len = (nb + tpc - 1) / tpc;
+        for (int unit = tid; unit < rest * tpc; unit += kLeafThreads) {
+            const int c = c0 + unit / tpc, q = unit % tpc;
+            const int j0 = q * part_len, j1 = min(nb, j0 + part_len);
+            if (j0 < j1) run_unit(c, j0, j1);
         }
         __syncthreads();
         // 2. voxels
