@@ -201,6 +201,25 @@ class Reference:
         L.vr_build_leaf.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u8p, C.c_size_t, u8p, C.c_size_t, u8p,
                                     C.c_size_t, C.c_int, u8p, C.c_size_t]
         L.vr_build_leaf.restype = C.c_long
+        L.vr_generate_queries.argtypes = [C.c_uint32] * 4 + [C.c_int, C.c_uint32, C.c_uint32, u32p, u32p]
+        L.vr_dct.argtypes = [f32p, f32p, C.c_int, C.c_int, f32p, f32p]
+
+    def generate_queries(self, dims, pattern, count, seed):
+        """(generated, sorted) as [count, 5] arrays of (x, y, z, t, leafIndex)."""
+        out = np.zeros((count, 5), np.uint32)
+        srt = np.zeros((count, 5), np.uint32)
+        self.lib.vr_generate_queries(*dims, pattern, count, seed, _ptr(out, u32p), _ptr(srt, u32p))
+        return out, srt
+
+    def dct(self, series, keep, weights=None):
+        """(coeffs, decoded) of dctEncodeKeep[Weighted] and dctDecodeAt."""
+        s = np.ascontiguousarray(series, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        coeffs = np.zeros(max(1, s.size), np.float32)
+        dec = np.zeros(s.size, np.float32)
+        k = self.lib.vr_dct(_ptr(s, f32p), None if w is None else _ptr(w, f32p), s.size, keep, _ptr(coeffs, f32p),
+                            _ptr(dec, f32p))
+        return coeffs[:k], dec
 
     def error(self):
         return self.lib.vr_last_error().decode()

@@ -7,6 +7,7 @@
 // full-frame composition lives in a Vulkan translation unit of the reference
 // (render/src/render_smoke_vbt_bench_main.cpp:201-452, anonymous namespace), so it is restated
 // here over the same public calls, in the same order.
+#include "dct_codec.h"
 #include "render_temporal_decode.h"
 #include "render_temporal_payload.h"
 #include "scientific_decode.h"
@@ -380,6 +381,47 @@ long vr_build_leaf(uint32_t packedHeader, uint32_t coarseKf, uint32_t fineKf, co
         fail(e);
         return -1;
     }
+}
+
+// generateQueries + fillLeafIndices (render/src/query_patterns.cpp:29-90) into out[count][5]
+// (x, y, z, t, leafIndex); sorted[count][5] receives the same queries after sortQueriesByLeaf.
+int vr_generate_queries(uint32_t w, uint32_t h, uint32_t d, uint32_t frames, int pattern, uint32_t count,
+                        uint32_t seed, uint32_t* out, uint32_t* sorted)
+{
+    vbt::render::VbtFileHeader hdr{};
+    hdr.width = w;
+    hdr.height = h;
+    hdr.depth = d;
+    hdr.frames = frames;
+    hdr.leafSize = 8;
+    auto q = vbt::render::generateQueries(hdr, vbt::render::QueryPattern(pattern), count, seed);
+    vbt::render::fillLeafIndices(hdr, q);
+    auto put = [&](const std::vector<vbt::render::Query4D>& v, uint32_t* dst) {
+        for (size_t i = 0; i < v.size(); ++i) {
+            dst[5 * i] = v[i].x;
+            dst[5 * i + 1] = v[i].y;
+            dst[5 * i + 2] = v[i].z;
+            dst[5 * i + 3] = v[i].t;
+            dst[5 * i + 4] = v[i].leafIndex;
+        }
+    };
+    put(q, out);
+    vbt::render::sortQueriesByLeaf(q);
+    put(q, sorted);
+    return 0;
+}
+
+// dctEncodeKeep / dctEncodeKeepWeighted (weights == nullptr selects the former) and dctDecodeAt
+// (src/dct_codec.cpp:63-122): coeffs[keep'] and decoded[n] = dctDecodeAt(coeffs, n, i).
+int vr_dct(const float* series, const float* weights, int n, int keep, float* coeffs, float* decoded)
+{
+    const std::vector<float> s(series, series + n);
+    std::vector<float> c;
+    if (weights) c = dctEncodeKeepWeighted(s, std::vector<float>(weights, weights + n), keep);
+    else c = dctEncodeKeep(s, keep);
+    std::memcpy(coeffs, c.data(), 4 * c.size());
+    for (int i = 0; i < n; ++i) decoded[i] = dctDecodeAt(c, n, i);
+    return static_cast<int>(c.size());
 }
 
 } // extern "C"

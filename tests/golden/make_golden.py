@@ -227,10 +227,55 @@ def gen_assets(ref):
         print(name, os.path.getsize(dst), "bytes;", frames.shape)
 
 
+QUERY_DIMS = [(20, 12, 17, 9), (256, 256, 256, 96), (1, 1, 1, 1), (8, 8, 8, 4), (100, 37, 64, 33)]
+QUERY_SEEDS = [0, 7, 12345]
+QUERY_COUNT = 513
+DCT_LENGTHS = [1, 2, 3, 7, 24, 96, 128]
+
+
+def gen_host_api(ref):
+    """host_api.npz: the reference's generateQueries/fillLeafIndices/sortQueriesByLeaf
+    (render/src/query_patterns.cpp:29-101) and dctEncodeKeep[Weighted]/dctDecodeAt
+    (src/dct_codec.cpp:63-122) on seeded inputs."""
+    qmeta, qgen, qsorted = [], [], []
+    for dims in QUERY_DIMS:
+        for pattern in range(4):
+            for seed in QUERY_SEEDS:
+                g, s = ref.generate_queries(dims, pattern, QUERY_COUNT, seed)
+                qmeta.append(list(dims) + [pattern, seed, QUERY_COUNT])
+                qgen.append(g)
+                qsorted.append(s)
+    rng = np.random.default_rng(5)
+    dmeta, series, weights, coeffs, decoded = [], [], [], [], []
+    for n in DCT_LENGTHS:
+        for keep in sorted({1, 3, n, n + 2}):
+            for weighted in (0, 1):
+                s = (rng.standard_normal(n) * 3.0 + 1.0).astype(np.float32)
+                w = rng.uniform(0.0, 2.0, n).astype(np.float32)
+                w[rng.uniform(size=n) < 0.2] = 0.0
+                c, d = ref.dct(s, keep, w if weighted else None)
+                dmeta.append([n, keep, weighted, c.size])
+                series.append(s)
+                weights.append(w)
+                coeffs.append(c)
+                decoded.append(d)
+    np.savez_compressed(os.path.join(HERE, "host_api.npz"), qmeta=np.array(qmeta, np.uint32),
+                        qgen=np.concatenate(qgen), qsorted=np.concatenate(qsorted),
+                        dmeta=np.array(dmeta, np.int32), series=np.concatenate(series),
+                        weights=np.concatenate(weights), coeffs=np.concatenate(coeffs),
+                        decoded=np.concatenate(decoded))
+    print("host api cases:", len(qmeta), "query sets,", len(dmeta), "dct cases")
+
+
 if __name__ == "__main__":
     r = Reference()
+    if len(sys.argv) > 1:
+        for name in sys.argv[1:]:
+            globals()["gen_" + name](r) if name != "reader_cases" else gen_reader_cases()
+        sys.exit(0)
     gen_streams(r)
     gen_shell(r)
     gen_payload_cases(r)
     gen_reader_cases()
     gen_assets(r)
+    gen_host_api(r)
