@@ -79,10 +79,12 @@ int vbt_asset_destroy(vbt_asset* asset);
 int vbt_asset_upload(vbt_asset* asset, const void* file_bytes, uint64_t len, void* stream);
 int vbt_asset_get_info(vbt_asset* asset, vbt_asset_info* out_info);
 
-/* Kernel (a): payload walker + active-leaf page table (compact[leaf] = ascending rank among
- * non-EMPTY leaves, 0xFFFFFFFF for EMPTY).  Replaces parseRenderTemporalPackedLeaf
- * (src/render_temporal_payload.cpp:234-311) per leaf and the Studio's page-table shader
- * (VBTStudio/frontend/shaders/vbt_active_index.comp:28-57). Asynchronous on `stream`. */
+/* Kernel (a): active-leaf page table (compact[leaf] = ascending rank among non-EMPTY leaves,
+ * 0xFFFFFFFF for EMPTY), the Studio's page-table shader
+ * (VBTStudio/frontend/shaders/vbt_active_index.comp:28-57).  The payload walker, which replaces
+ * parseRenderTemporalPackedLeaf (src/render_temporal_payload.cpp:234-311) per leaf, runs when the
+ * payload is uploaded (vbt_asset_create / vbt_asset_upload) and leaves a per-leaf table; this
+ * call compacts that table's active flags.  Asynchronous on `stream`. */
 int vbt_build_page_table(vbt_asset* asset, void* stream);
 /* Device views of the page table: compact[leaf_count], active_list[rank] = leaf, and the
  * device-resident active count (one uint32). */

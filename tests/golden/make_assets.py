@@ -98,6 +98,42 @@ def plume(size, frames, seed):
     return out
 
 
+_FIRE = {}
+
+
+def fire(shape_xyz, frames, seed):
+    """Three aligned fields (density, flames, temperature) of an expanding fireball: fBm inside a
+    sphere of radius 20 + 2.5 t at the volume's lower centre, the noise advected upward at one
+    voxel per frame; flames = the fBm of a second seed in the sphere's outer band; temperature
+    = 300 + 1500 * flames + N(0, 20).  Cached, so the three encodes share one generation."""
+    key = (tuple(shape_xyz), frames, seed)
+    if key in _FIRE:
+        return _FIRE[key]
+    rng = np.random.default_rng(seed + 1000)
+    X, Y, Z = shape_xyz
+    n1 = fbm_volume((Z + frames, Y, X), 4, 32, seed)
+    n2 = fbm_volume((Z + frames, Y, X), 4, 16, seed + 1)
+    zz, yy, xx = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(X), indexing="ij")
+    r = np.sqrt((xx - X / 2.0) ** 2 + (yy - Y / 2.0) ** 2 + (zz - Z * 0.3) ** 2)
+    den = np.empty((frames, Z, Y, X), np.float32)
+    fl = np.empty((frames, Z, Y, X), np.float32)
+    tmp = np.empty((frames, Z, Y, X), np.float32)
+    for t in range(frames):
+        R = 20.0 + 2.5 * t
+        inside = r <= R
+        sl = slice(frames - t, frames - t + Z)           # advect upward one voxel per frame
+        d = np.clip((n1[sl] - 0.3) * 2.0, 0.0, 1.0) * np.clip((R - r) / 4.0, 0.0, 1.0)
+        band = np.clip(1.0 - np.abs(r - 0.8 * R) / (0.25 * R + 1e-6), 0.0, 1.0)
+        f = np.clip((n2[sl] - 0.4) * 3.0, 0.0, 1.0) * band
+        d[~inside] = 0.0
+        f[~inside] = 0.0
+        den[t] = d
+        fl[t] = f
+        tmp[t] = (300.0 + 1500.0 * f + rng.normal(0.0, 20.0, f.shape)).astype(np.float32)
+    _FIRE[key] = (den, fl, tmp)
+    return _FIRE[key]
+
+
 def sdf_scene(shape_xyz, frames, plane_z, plane_amp, kx, n_spheres, rmin, rmax, seed, g=0.05):
     rng = np.random.default_rng(seed)
     X, Y, Z = shape_xyz
@@ -183,7 +219,22 @@ RECIPES = {
     "sci_64": lambda: encode("sci_64", grf_scientific((64, 64, 64), 32, 6), (64, 64, 64, 32), "generic",
                              time_fastest=True),
     "cfg2_plume": lambda: encode("cfg2_plume", plume(256, 96, 2), (256, 256, 256, 96), "density"),
+    # serving-mix assets: the config-3/4/5 scenes at reduced sizes (the full sizes need 36-64 GB
+    # of raw float32 input per field, more than this machine's memory), plus a second plume
+    "mix_plume_b": lambda: encode("mix_plume_b", plume(256, 96, 3), (256, 256, 256, 96), "density"),
+    "mix_fire_density": lambda: encode("mix_fire_density", fire((192, 192, 256), 60, 7)[0], (192, 192, 256, 60),
+                                       "density"),
+    "mix_fire_flames": lambda: encode("mix_fire_flames", fire((192, 192, 256), 60, 7)[1], (192, 192, 256, 60),
+                                      "density"),
+    "mix_fire_temperature": lambda: encode("mix_fire_temperature", fire((192, 192, 256), 60, 7)[2],
+                                           (192, 192, 256, 60), "density"),
+    "mix_sdf": lambda: encode("mix_sdf", sdf_scene((256, 256, 256), 48, 100.0, 12.0, 0.05, 40, 3.0, 12.0, 9),
+                              (256, 256, 256, 48), "density", LEVELSET),
+    "mix_sci": lambda: encode("mix_sci", grf_scientific((128, 128, 128), 64, 8), (128, 128, 128, 64), "generic",
+                              time_fastest=True),
 }
+MIX = ["cfg2_plume", "mix_plume_b", "mix_fire_density", "mix_fire_flames", "mix_fire_temperature", "mix_sdf",
+       "cfg1_blobs", "cfg4_sdf_small", "mix_sci"]
 DEFAULT = ["tiny_density", "tiny_levelset", "sci_small", "cfg1_blobs", "cfg4_sdf_small", "sci_64", "cfg2_plume"]
 
 if __name__ == "__main__":

@@ -10,11 +10,13 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/vbt_b200.h"
+#include "asset.h"
 #include "kernels.cuh"
 
 namespace vbtb {
@@ -25,20 +27,6 @@ void launch_checked_decode(const uint8_t* stream, uint32_t bytes, uint32_t codec
 
 using namespace vbtb;
 
-struct vbt_asset {
-    int device = 0;
-    vbt_header hdr{};
-    DeviceAsset dev{};
-    uint32_t epoch = 0;
-    uint64_t device_bytes = 0;
-    std::vector<void*> allocations;
-    // staging for the host-buffer calls (grow-only)
-    void* stage_in = nullptr;
-    size_t stage_in_bytes = 0;
-    void* stage_out = nullptr;
-    size_t stage_out_bytes = 0;
-    std::mutex mu;
-};
 
 namespace {
 
@@ -267,14 +255,16 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     }
     const uint32_t L = h.leaf_count;
     const uint32_t tiles = (L + kWalkTile - 1) / kWalkTile;
-    void *d_off, *d_pay, *d_scales, *d_basis, *d_entries, *d_compact, *d_list, *d_counters, *d_err, *d_tiles, *d_sorted;
+    void *d_off, *d_pay, *d_scales, *d_basis, *d_entries, *d_compact, *d_list, *d_counters, *d_err, *d_tiles, *d_sorted,
+        *d_work;
     // payload gets 16 bytes of tail padding so vector reads near the end stay inside the allocation
     if ((st = alloc(a, &d_off, 4ull * (L + 1))) || (st = alloc(a, &d_pay, 4ull * words + 16)) ||
         (st = alloc(a, &d_scales, 4ull * (h.coarse_ac_scale_count + 1))) ||
         (st = alloc(a, &d_basis, h.profile_type == 2u ? 4ull * h.frames * 64u : 16u)) ||
         (st = alloc(a, &d_entries, sizeof(LeafEntry) * (uint64_t)L)) || (st = alloc(a, &d_compact, 4ull * L)) ||
         (st = alloc(a, &d_list, 4ull * L)) || (st = alloc(a, &d_counters, 16)) || (st = alloc(a, &d_err, 8)) ||
-        (st = alloc(a, &d_tiles, 8ull * tiles)) || (st = alloc(a, &d_sorted, L))) {
+        (st = alloc(a, &d_tiles, 8ull * tiles)) || (st = alloc(a, &d_sorted, L)) ||
+        (st = alloc(a, &d_work, 8ull * kWorkSlots))) {
         free_all(a);
         delete a;
         return st;
@@ -302,6 +292,7 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     cudaMemset(d_err, 0xFF, 8);
     cudaMemset(d_tiles, 0, 8ull * tiles);
     cudaMemset(d_sorted, 0, L);
+    cudaMemset(d_work, 0, 8ull * kWorkSlots);
     const cudaError_t ce = cudaGetLastError();
     if (ce != cudaSuccess) {
         free_all(a);
@@ -320,6 +311,7 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     d.err = static_cast<unsigned long long*>(d_err);
     d.tile_state = static_cast<unsigned long long*>(d_tiles);
     d.key_sorted = static_cast<uint8_t*>(d_sorted);
+    d.work = static_cast<unsigned long long*>(d_work);
     // first page-table build and key-order analysis, synchronously, so that a returned asset is
     // ready to decode
     launch_walk(d, ++a->epoch, 0);
@@ -407,8 +399,10 @@ int vbt_build_page_table(vbt_asset* a, void* stream)
 {
     if (!a) return fail(VBT_STATUS_INVALID_ARGUMENT, "null asset");
     DeviceGuard guard(a->device);
-    launch_walk(a->dev, ++a->epoch, static_cast<cudaStream_t>(stream));
-    return check_launch("walk_kernel");
+    // the leaf table was built by the walker when the payload was uploaded; a page table needs
+    // only each row's active flag
+    launch_page_table(a->dev, ++a->epoch, static_cast<cudaStream_t>(stream));
+    return check_launch("page_table_kernel");
 }
 
 int vbt_page_table_device(vbt_asset* a, const uint32_t** c, const uint32_t** l, const uint32_t** n)
@@ -455,7 +449,7 @@ int vbt_decode_cache(vbt_asset* a, const int* frames, int nframes, float* out, u
     int st = check_frames(a, frames, nframes);
     if (st) return st;
     DeviceGuard guard(a->device);
-    launch_decode_cache(a->dev, frames, nframes, out, stride, grid, static_cast<cudaStream_t>(stream));
+    launch_decode_cache(a->dev, a->launch_seq.fetch_add(1), frames, nframes, out, stride, grid, static_cast<cudaStream_t>(stream));
     return check_launch("decode_kernel<cache>");
 }
 
@@ -475,7 +469,7 @@ int vbt_decode_frames(vbt_asset* a, const int* frames, int nframes, float* out, 
     int st = check_frames(a, frames, nframes);
     if (st) return st;
     DeviceGuard guard(a->device);
-    launch_decode_dense(a->dev, frames, nframes, out, grid, static_cast<cudaStream_t>(stream));
+    launch_decode_dense(a->dev, a->launch_seq.fetch_add(1), frames, nframes, out, grid, static_cast<cudaStream_t>(stream));
     return check_launch("decode_kernel<dense>");
 }
 
@@ -543,7 +537,7 @@ int vbt_decode_frames_host(vbt_asset* a, const int* frames, int nframes, float* 
     const uint64_t vox = (uint64_t)a->hdr.width * a->hdr.height * a->hdr.depth;
     if ((st = grow(&a->stage_out, &a->stage_out_bytes, 4ull * vox * nframes))) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    launch_decode_dense(a->dev, frames, nframes, static_cast<float*>(a->stage_out), 0, s);
+    launch_decode_dense(a->dev, a->launch_seq.fetch_add(1), frames, nframes, static_cast<float*>(a->stage_out), 0, s);
     if ((st = check_launch("decode_kernel<dense>"))) return st;
     CUDA_TRY(cudaMemcpyAsync(out, a->stage_out, 4ull * vox * nframes, cudaMemcpyDeviceToHost, s));
     return vbt_asset_sync_status(a, stream, nullptr);

@@ -1,8 +1,9 @@
 // kernels.cu -- the hand-written sm_100a kernels of the decode path.
 //
-//  (a) walk_kernel          payload walker: validates every leaf once, writes the 32-byte leaf
-//                           table, and builds the active-leaf page table by warp-ballot/popc
-//                           compaction with a single-pass decoupled look-back across CTAs.
+//  (a) walk_kernel          payload walker: validates every leaf once per upload, writes the
+//                           32-byte leaf table, and builds the active-leaf page table by
+//                           warp-ballot/popc compaction with a single-pass decoupled look-back.
+//      page_table_kernel    the per-frame page table from the leaf table's active flags.
 //  (b) decode_*_kernel      warp-per-leaf decode into the current-frame voxel cache (512 FP32
 //                           per active leaf) or into dense frames, several frames per launch.
 //  (c) query_*_kernel       batched (x, y, z, t) point queries and z-slice queries.
@@ -301,32 +302,17 @@ __device__ LeafEntry walk_sci_leaf(const DeviceAsset& a, uint32_t leaf)
     return e;
 }
 
-__global__ void __launch_bounds__(kWalkThreads) walk_kernel(DeviceAsset a, uint32_t epoch)
+// Page-table compaction of one tile of kWalkTile leaves (one flag per thread): ballot/popc within
+// warps, a serial scan over the tile's warps, and a single-pass decoupled look-back across tiles
+// (epoch-tagged descriptors, bounded spin).  Writes compact[], active_list[] and, from the last
+// tile, the active count.
+__device__ __forceinline__ void compact_tile(const DeviceAsset& a, uint32_t epoch, uint32_t tile, bool flag,
+                                             uint32_t* s_warp, uint32_t& s_base)
 {
-    __shared__ uint8_t s_flag[kWalkTile];
-    __shared__ uint32_t s_warp[kWalkThreads / 32];
-    __shared__ uint32_t s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile = blockIdx.x;
     const uint32_t leaf0 = tile * kWalkTile;
     const uint32_t L = a.g.leaf_count;
-
-    // phase 1: one warp per leaf, 32 leaves per warp
-    for (int j = 0; j < kWalkTile / (kWalkThreads / 32); ++j) {
-        const uint32_t local = warp * (kWalkTile / (kWalkThreads / 32)) + j;
-        const uint32_t leaf = leaf0 + local;
-        if (leaf >= L) break;
-        const LeafEntry e = a.g.profile == 2u ? walk_sci_leaf(a, leaf) : walk_rt_leaf(a, leaf, lane);
-        if (lane == 0) {
-            a.entries[leaf] = e;
-            s_flag[local] = (e.info & kFlagActive) ? 1 : 0;
-        }
-    }
-    __syncthreads();
-
-    // phase 2: ballot/popc compaction of the tile's active flags
     const uint32_t leaf = leaf0 + threadIdx.x;
-    const bool flag = leaf < L && s_flag[threadIdx.x] != 0;
     const unsigned bal = __ballot_sync(0xFFFFFFFFu, flag);
     const uint32_t in_warp = __popc(bal & ((1u << lane) - 1u));
     if (lane == 0) s_warp[warp] = __popc(bal);
@@ -377,10 +363,57 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(DeviceAsset a, uint3
     }
 }
 
+__global__ void __launch_bounds__(kWalkThreads) walk_kernel(DeviceAsset a, uint32_t epoch)
+{
+    __shared__ uint8_t s_flag[kWalkTile];
+    __shared__ uint32_t s_warp[kWalkThreads / 32];
+    __shared__ uint32_t s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t leaf0 = tile * kWalkTile;
+    const uint32_t L = a.g.leaf_count;
+
+    // phase 1: one warp per leaf, 32 leaves per warp
+    for (int j = 0; j < kWalkTile / (kWalkThreads / 32); ++j) {
+        const uint32_t local = warp * (kWalkTile / (kWalkThreads / 32)) + j;
+        const uint32_t leaf = leaf0 + local;
+        if (leaf >= L) break;
+        const LeafEntry e = a.g.profile == 2u ? walk_sci_leaf(a, leaf) : walk_rt_leaf(a, leaf, lane);
+        if (lane == 0) {
+            a.entries[leaf] = e;
+            s_flag[local] = (e.info & kFlagActive) ? 1 : 0;
+        }
+    }
+    __syncthreads();
+
+    // phase 2: compaction of the tile's active flags
+    const uint32_t leaf = leaf0 + threadIdx.x;
+    compact_tile(a, epoch, tile, leaf < L && s_flag[threadIdx.x] != 0, s_warp, s_base);
+}
+
+// Per-frame page table of an asset whose leaf table is already built: the active flag of each
+// leaf's 32-byte row (the walker's predicate: offsets inside the payload, route tag not EMPTY, or
+// any scientific leaf), compacted as the walker compacts it.
+__global__ void __launch_bounds__(kWalkThreads) page_table_kernel(DeviceAsset a, uint32_t epoch)
+{
+    __shared__ uint32_t s_warp[kWalkThreads / 32];
+    __shared__ uint32_t s_base;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t leaf = tile * kWalkTile + threadIdx.x;
+    const bool flag = leaf < a.g.leaf_count && (__ldg(&a.entries[leaf].info) & kFlagActive) != 0u;
+    compact_tile(a, epoch, tile, flag, s_warp, s_base);
+}
+
 void launch_walk(const DeviceAsset& a, uint32_t epoch, cudaStream_t s)
 {
     const uint32_t tiles = (a.g.leaf_count + kWalkTile - 1) / kWalkTile;
     walk_kernel<<<tiles, kWalkThreads, 0, s>>>(a, epoch);
+}
+
+void launch_page_table(const DeviceAsset& a, uint32_t epoch, cudaStream_t s)
+{
+    const uint32_t tiles = (a.g.leaf_count + kWalkTile - 1) / kWalkTile;
+    page_table_kernel<<<tiles, kWalkThreads, 0, s>>>(a, epoch);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -754,140 +787,6 @@ __global__ void __launch_bounds__(kDecodeWarps * 32, 2) decode_kernel(DeviceAsse
     }
 }
 
-// Render-temporal decode, v2: one warp per (leaf, chunk of up to 16 frames); controls decoded in
-// frame batches, voxels by the separable trilinear (rt_decode_v2.cuh).
-template <bool DENSE>
-__global__ void __launch_bounds__(kV2Warps * 32, 5) decode_rt_v2_kernel(DeviceAsset a, FrameList fl,
-                                                                        float* __restrict__ out, uint64_t frame_stride)
-{
-    __shared__ V2WarpSmem smem[kV2Warps];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    V2WarpSmem& sm = smem[warp];
-    const uint32_t* __restrict__ pw = a.payload;
-    const uint32_t n_leaves = DENSE ? a.g.leaf_count : *(volatile const uint32_t*)a.counters;
-    const uint32_t n_chunks = (uint32_t)(fl.n + kV2ChunkFrames - 1) / kV2ChunkFrames;
-    const uint64_t n_items = (uint64_t)n_leaves * n_chunks;
-    const int total = (int)a.g.frames;
-    const int ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
-    for (uint64_t item = (uint64_t)blockIdx.x * kV2Warps + warp; item < n_items;
-         item += (uint64_t)gridDim.x * kV2Warps) {
-        const uint32_t li = (uint32_t)(item / n_chunks), chunk = (uint32_t)(item % n_chunks);
-        const uint32_t leaf = DENSE ? li : __ldg(a.active_list + li);
-        const LeafEntry e = a.entries[leaf];
-        uint32_t bx, by, bz;
-        int w, h, d;
-        leaf_extent(a.g, leaf, bx, by, bz, w, h, d);
-        const uint32_t st = entry_status(e);
-        const bool empty = (e.header & 3u) == kModeEmpty;
-        const int f_begin = (int)chunk * kV2ChunkFrames;
-        const int f_end = min(fl.n, f_begin + kV2ChunkFrames);
-        auto store = [&](int fi, int i, float4 v) {
-            const int lz = 2 * i + (lane >> 4);
-            if (DENSE) {
-                if (ly < h && lz < d) {
-                    float* dst = out + (uint64_t)fi * frame_stride +
-                                 ((uint64_t)(bz * 8 + lz) * a.g.height + (by * 8 + ly)) * a.g.width + bx * 8 + lx0;
-                    if (lx0 + 4 <= w && (((uintptr_t)dst) & 15u) == 0u) {
-                        *reinterpret_cast<float4*>(dst) = v;
-                    } else {
-                        const float vv[4] = {v.x, v.y, v.z, v.w};
-                        for (int k = 0; k < 4 && lx0 + k < w; ++k) dst[k] = vv[k];
-                    }
-                }
-            } else {
-                reinterpret_cast<float4*>(out + (uint64_t)fi * frame_stride + (uint64_t)li * 512u)[lane + 32 * i] = v;
-            }
-        };
-        if (st != kOk || empty) {
-            if (st != kOk && lane == 0 && chunk == 0) record_error(a.err, leaf, st);
-            for (int fi = f_begin; fi < f_end; ++fi)
-                for (int i = 0; i < 4; ++i) store(fi, i, make_float4(0.f, 0.f, 0.f, 0.f));
-            continue;
-        }
-        const uint64_t base = 4ull * e.word_off;
-        const int cres = (int)((e.header >> 6) & 7u), fres = (int)((e.header >> 9) & 7u);
-        const bool fine = (e.info & kFlagFine) != 0u, shell = (e.info & kFlagShell) != 0u;
-        const bool occ = (e.info & kFlagOccClamp) != 0u;
-        const StreamRef cs{base + 8u, (uint32_t)(cres * cres * cres), 8u, e.kf & 0xFFFFu, (e.header >> 2) & 3u};
-        const StreamRef fs{base + 8u + e.coarse_bytes, (uint32_t)(fres * fres * fres), 8u, e.kf >> 16,
-                           (e.header >> 4) & 3u};
-        const StreamRef ss{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
-        const int Cc = (int)cs.controls;
-        const int Cf = fine ? (int)fs.controls : (shell ? (int)ss.controls : 0);
-        const int Ctot = Cc + Cf;
-        const int nb_max = min(kV2MaxBatch, kV2CtrlBudget / max(Ctot, 1));
-        load_axis_weights(sm, 0, cres, w, h, d, lane);
-        if (fine) load_axis_weights(sm, 1, fres, w, h, d, lane);
-        // Mode2 occupancy words of the lane's four z layers
-        uint64_t mask[4] = {0, 0, 0, 0};
-        uint32_t pref[4] = {0, 0, 0, 0};
-        if (occ) {
-            const uint64_t ob = base + 8u + e.coarse_bytes;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const uint32_t g = (uint32_t)(2 * i + (lane >> 4));
-                mask[i] = ((uint64_t)ldw(pw, (uint32_t)((ob + 8u * g + 4u) >> 2)) << 32) |
-                          ldw(pw, (uint32_t)((ob + 8u * g) >> 2));
-                pref[i] = (ldw(pw, (uint32_t)((ob + 64u + 2u * g) >> 2)) >> ((g & 1u) * 16u)) & 0xFFFFu;
-            }
-        }
-        for (int fb = f_begin; fb < f_end; fb += nb_max) {
-            const int nb = min(nb_max, f_end - fb);
-            __syncwarp();
-            if (lane < nb) {
-                const int fr = clamp_frame(fl.f[fb + lane], total);
-                sm.fr[lane] = fr;
-                sm.b8[lane] = (uint8_t)time_bin(fr, 8u, total);
-                sm.b4[lane] = (uint8_t)time_bin(fr, 4u, total);
-            }
-            __syncwarp();
-            const bool cursor = (e.info & kFlagSorted) &&
-                                __all_sync(0xFFFFFFFFu, lane == 0 || lane >= nb || sm.fr[lane] >= sm.fr[lane - 1]);
-            for (int c = lane; c < Ctot; c += 32) {
-                const StreamRef& s = c < Cc ? cs : (fine ? fs : ss);
-                const uint32_t ci = (uint32_t)(c < Cc ? c : c - Cc);
-                if (cursor) decode_control_cursor(pw, s, ci, sm, nb, sm.ctrl + c, Ctot);
-                else decode_control_batch(pw, s, ci, sm, nb, sm.ctrl + c, Ctot);
-            }
-            __syncwarp();
-            for (int j = 0; j < nb; ++j) {
-                const float* g = sm.ctrl + j * Ctot;
-                float4 q[4];
-                if (cres >= 2) trilinear_quads(sm, 0, g, cres, lane, q);
-                else constant_quads(g, cres, q);
-                if (fine) {
-                    float4 qf[4];
-                    if (fres >= 2) trilinear_quads(sm, 1, g + Cc, fres, lane, qf);
-                    else constant_quads(g + Cc, fres, qf);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const float2 lo2 = add2_rn(make_float2(q[i].x, q[i].y), make_float2(qf[i].x, qf[i].y));
-                        const float2 hi2 = add2_rn(make_float2(q[i].z, q[i].w), make_float2(qf[i].z, qf[i].w));
-                        q[i] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int lz = 2 * i + (lane >> 4);
-                    float v[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const uint32_t bit = (uint32_t)(ly * 8 + lx0 + k);
-                        const bool in_occ = occ && ((mask[i] >> bit) & 1ull);
-                        if (shell && in_occ) {
-                            const uint32_t di = (pref[i] + __popcll(mask[i] & ((1ull << bit) - 1ull))) & 0xFFFFu;
-                            v[k] = __fadd_rn(v[k], g[Cc + di]);
-                        }
-                        if (occ && !in_occ && v[k] < 0.0f) v[k] = 0.0f;
-                        if (lx0 + k >= w || ly >= h || lz >= d) v[k] = 0.0f;
-                    }
-                    store(fb + j, i, make_float4(v[0], v[1], v[2], v[3]));
-                }
-            }
-        }
-    }
-}
-
 // Render-temporal decode kernel (TMA-staged leaf, one CTA per leaf): rt_kernel_leaf.cuh
 }  // namespace vbtb
 #include "rt_kernel_leaf.cuh"
@@ -906,22 +805,8 @@ static int default_grid()
     return g;
 }
 
-// One wave of the render-temporal v2 kernel: SMs x resident CTAs per SM.
-static int rt_v2_grid()
-{
-    static int g = 0;
-    if (!g) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_rt_v2_kernel<false>, kV2Warps * 32, 0);
-        g = sms * (per > 0 ? per : 1);
-    }
-    return g;
-}
-
-void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, float* out, uint64_t stride, int grid,
-                         cudaStream_t s)
+void launch_decode_cache(const DeviceAsset& a, uint32_t seq, const int* frames, int nframes, float* out,
+                         uint64_t stride, int grid, cudaStream_t s)
 {
     FrameList fl{};
     fl.n = nframes;
@@ -929,10 +814,11 @@ void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, f
     if (a.g.profile == 2u)
         decode_kernel<false, true><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
     else
-        launch_rt_leaf(a, fl, out, stride, grid, false, s);
+        launch_rt_leaf(a, seq, fl, out, stride, grid, false, s);
 }
 
-void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, float* out, int grid, cudaStream_t s)
+void launch_decode_dense(const DeviceAsset& a, uint32_t seq, const int* frames, int nframes, float* out, int grid,
+                         cudaStream_t s)
 {
     FrameList fl{};
     fl.n = nframes;
@@ -941,7 +827,7 @@ void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, f
     if (a.g.profile == 2u)
         decode_kernel<true, true><<<grid > 0 ? grid : default_grid(), kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
     else
-        launch_rt_leaf(a, fl, out, stride, grid, true, s);
+        launch_rt_leaf(a, seq, fl, out, stride, grid, true, s);
 }
 
 // Plain per-leaf launch: grid = the whole leaf grid, one 64-thread CTA per leaf (EMPTY leaves
@@ -1090,12 +976,9 @@ __device__ float sci_point(const DeviceAsset& a, const LeafEntry& e, uint32_t lx
     return __fadd_rn(coarse, r);
 }
 
-__global__ void __launch_bounds__(128) query_points_kernel(DeviceAsset a, const uint32_t* __restrict__ q, uint64_t n,
-                                                           float* __restrict__ out)
+// One point query (x, y, z, t) of one asset; decode errors go to `err`.
+__device__ __forceinline__ float point_value(const DeviceAsset& a, uint4 qq, unsigned long long* err)
 {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint4 qq = reinterpret_cast<const uint4*>(q)[i];
     const uint32_t x = qq.x, y = qq.y, z = qq.z, t = qq.w;
     // leaf lookup as render/src/vbt_file.cpp:250-262 leafIndexForVoxel (clamped leaf coordinates)
     const uint32_t bx = min(a.g.lcx - 1u, x >> 3), by = min(a.g.lcy - 1u, y >> 3), bz = min(a.g.lcz - 1u, z >> 3);
@@ -1103,34 +986,53 @@ __global__ void __launch_bounds__(128) query_points_kernel(DeviceAsset a, const 
     const LeafEntry e = a.entries[leaf];
     const uint32_t st = entry_status(e);
     if (st != kOk) {
-        record_error(a.err, leaf, st);
-        out[i] = 0.0f;
-        return;
+        record_error(err, leaf, st);
+        return 0.0f;
     }
     if (a.g.profile == 2u) {
         if (t >= a.g.frames) {   // the reference indexes its per-frame tables out of range here
-            record_error(a.err, leaf, kErrDecodeOob);
-            out[i] = 0.0f;
-            return;
+            record_error(err, leaf, kErrDecodeOob);
+            return 0.0f;
         }
         bool oob = false;
-        out[i] = sci_point(a, e, x & 7u, y & 7u, z & 7u, t, oob);
-        if (oob) record_error(a.err, leaf, kErrDecodeOob);
-        return;
+        const float v = sci_point(a, e, x & 7u, y & 7u, z & 7u, t, oob);
+        if (oob) record_error(err, leaf, kErrDecodeOob);
+        return v;
     }
-    if ((e.header & 3u) == kModeEmpty) {
-        out[i] = 0.0f;
-        return;
-    }
+    if ((e.header & 3u) == kModeEmpty) return 0.0f;
     uint32_t gx, gy, gz;
     int w, h, d;
     leaf_extent(a.g, leaf, gx, gy, gz, w, h, d);
     const int lx = (int)(x - bx * 8u), ly = (int)(y - by * 8u), lz = (int)(z - bz * 8u);
-    if (lx >= w || ly >= h || lz >= d) {   // outside the volume: no such voxel in any frame
-        out[i] = 0.0f;
-        return;
-    }
-    out[i] = rt_point(a, e, w, h, d, lx, ly, lz, clamp_frame((int)t, (int)a.g.frames));
+    if (lx >= w || ly >= h || lz >= d) return 0.0f;   // outside the volume: no such voxel in any frame
+    return rt_point(a, e, w, h, d, lx, ly, lz, clamp_frame((int)t, (int)a.g.frames));
+}
+
+__global__ void __launch_bounds__(128) query_points_kernel(DeviceAsset a, const uint32_t* __restrict__ q, uint64_t n,
+                                                           float* __restrict__ out)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = point_value(a, reinterpret_cast<const uint4*>(q)[i], a.err);
+}
+
+// Point queries of several resident assets in one launch: query i belongs to assets[which[i]].
+// Decode errors of the whole launch go to one error word.
+__global__ void __launch_bounds__(128) query_points_multi_kernel(const DeviceAsset* __restrict__ assets,
+                                                                 const uint4* __restrict__ q,
+                                                                 const uint8_t* __restrict__ which, uint64_t n,
+                                                                 float* __restrict__ out, unsigned long long* err)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = point_value(assets[__ldg(which + i)], q[i], err);
+}
+
+void launch_query_points_multi(const DeviceAsset* assets, const uint4* q, const uint8_t* which, uint64_t n, float* out,
+                               unsigned long long* err, cudaStream_t s)
+{
+    if (n == 0) return;
+    query_points_multi_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(assets, q, which, n, out, err);
 }
 
 void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, cudaStream_t s)

@@ -30,7 +30,13 @@ struct DeviceAsset {
     unsigned long long* err;     // first failing (leaf << 8 | status), ~0 when none
     unsigned long long* tile_state;  // look-back tile descriptors
     uint8_t* key_sorted;         // per leaf: 1 when its decoded controls' key frames strictly increase
+    unsigned long long* work;    // kWorkSlots leaf-work counters [epoch:32 | next index:32]
 };
+
+// Decode launches of one asset take their leaves from a work counter; launch number n uses slot
+// n % kWorkSlots tagged with epoch n + 1, so up to kWorkSlots launches of one asset may run at
+// the same time.
+constexpr uint32_t kWorkSlots = 64;
 
 // Fixed shared memory of the render decode kernel besides its leaf stage (rt_kernel_leaf.cuh:
 // barrier, frame tables, axis weights, 8 warps x (x-lerp + y-lerp rows), 3072-float controls).
@@ -46,21 +52,27 @@ constexpr int kCtrlSlots = 343 + 512;   // coarse (<= 7^3) + fine (<= 7^3) or sh
 constexpr int kWarpSlots = 64 + 16 * 64 > kCtrlSlots ? 64 + 16 * 64 : kCtrlSlots;
 
 void launch_walk(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);
+// page table only, from the leaf table the walker built (same predicate, same ranks)
+void launch_page_table(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);
 // Per-asset key-order analysis (after a walk): sets key_sorted[] and the kFlagSorted bit of the
 // leaf table.  Runs at load and after every re-upload; later walks copy the bit from key_sorted.
 void launch_key_order(const DeviceAsset& a, cudaStream_t s);
 // Decode `nframes` frames (frames[] on the host, <= 64) of every active leaf into the cache:
 // out[f * cache_frame_stride + rank * 512 + voxel].
-void launch_decode_cache(const DeviceAsset& a, const int* frames, int nframes, float* out,
+void launch_decode_cache(const DeviceAsset& a, uint32_t seq, const int* frames, int nframes, float* out,
                          uint64_t cache_frame_stride, int grid, cudaStream_t s);
 // Dense frames: out[f * X*Y*Z + (z*Y + y)*X + x]; every leaf (EMPTY ones write zeros).
-void launch_decode_dense(const DeviceAsset& a, const int* frames, int nframes, float* out, int grid,
+void launch_decode_dense(const DeviceAsset& a, uint32_t seq, const int* frames, int nframes, float* out, int grid,
                          cudaStream_t s);
 // Plain path: one CTA per leaf of the whole leaf grid, one frame per launch (the reference
 // Studio dispatch shape, VBTStudio/frontend/src/volume_renderer.cpp:704-735).
 void launch_decode_cache_plain(const DeviceAsset& a, int frame, float* out, cudaStream_t s);
 // Point queries: q[4*i..] = (x, y, z, t); out[i].
 void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, cudaStream_t s);
+// Point queries over several assets (a device array of DeviceAsset): query i reads assets[which[i]];
+// decode errors are recorded in *err (first failing leaf, as DeviceAsset::err).
+void launch_query_points_multi(const DeviceAsset* assets, const uint4* q, const uint8_t* which, uint64_t n, float* out,
+                               unsigned long long* err, cudaStream_t s);
 // Z-slice over a frame range: out[(t - t0) * X*Y + y*X + x] for t in [t0, t1).
 void launch_query_slice(const DeviceAsset& a, uint32_t z, int t0, int t1, float* out, cudaStream_t s);
 

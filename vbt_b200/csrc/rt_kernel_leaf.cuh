@@ -179,19 +179,51 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
     }
 }
 
+// Next leaf index of this launch from its work counter ([epoch:32 | next index:32]).  The slot
+// still carries an older launch's epoch until the first CTA of this launch installs its own
+// (taking index 0); from then on a grab is one atomicAdd.  Every failed compare-and-swap means
+// another CTA changed the slot, so the loop ends; the bound only guards against a corrupt slot.
+__device__ __forceinline__ uint32_t grab_leaf(unsigned long long* slot, uint32_t epoch, bool& timed_out)
+{
+    unsigned long long v = atomicAdd(slot, 1ull);
+    if ((uint32_t)(v >> 32) == epoch) return (uint32_t)v;
+    unsigned long long expect = v + 1ull;
+    const unsigned long long mine = ((unsigned long long)epoch << 32) | 1ull;
+    for (int it = 0; it < (1 << 20); ++it) {
+        const unsigned long long seen = atomicCAS(slot, expect, mine);
+        if (seen == expect) return 0u;
+        if ((uint32_t)(seen >> 32) == epoch) {
+            v = atomicAdd(slot, 1ull);
+            return (uint32_t)v;
+        }
+        expect = seen;
+    }
+    timed_out = true;
+    return 0xFFFFFFFFu;
+}
+
 // GLOBAL_FALLBACK: leaves whose window exceeds the stage are decoded from global memory (only
 // instantiated for assets that have such leaves; it costs registers).
+// Leaves are handed out dynamically (grab_leaf), one at a time per CTA, so that CTAs that drew
+// cheap leaves (few controls, few keys) take more of them.
 template <bool DENSE, bool GLOBAL_FALLBACK>
 __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsset a, FrameList fl,
-                                                                      float* __restrict__ out, uint64_t frame_stride)
+                                                                      float* __restrict__ out, uint64_t frame_stride,
+                                                                      unsigned long long* work, uint32_t epoch)
 {
     extern __shared__ __align__(128) uint8_t dyn[];
     const LeafSmem s = leaf_layout(dyn);
+    uint32_t* const s_next = reinterpret_cast<uint32_t*>(dyn + 8);   // beside the 8-byte barrier
     const int tid = threadIdx.x;
     const int total = (int)a.g.frames;
+    const uint32_t n_leaves = DENSE ? a.g.leaf_count : *(volatile const uint32_t*)a.counters;
     if (tid == 0) {
         mbar_init(s.bar, 1);
         mbar_init_fence();
+        bool to = false;
+        const uint32_t first = grab_leaf(work, epoch, to);
+        if (to) record_error(a.err, 0u, kErrWaitTimeout);
+        *s_next = first;
     }
     if (tid < fl.n) {
         const int fr = clamp_frame(fl.f[tid], total);
@@ -202,55 +234,61 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
     __syncthreads();
     const bool steps01 =
         __syncthreads_and(tid == 0 || tid >= fl.n || (unsigned)(s.fr[tid] - s.fr[tid - 1]) <= 1u) != 0;
-    const uint32_t n_leaves = DENSE ? a.g.leaf_count : *(volatile const uint32_t*)a.counters;
     const uint8_t* pay_bytes = reinterpret_cast<const uint8_t*>(a.payload);
     uint32_t phase = 0;
-    for (uint32_t li = blockIdx.x; li < n_leaves; li += gridDim.x) {
+    uint32_t li = *s_next;
+    while (li < n_leaves) {
+        // every thread has read li, and the previous leaf's shared-memory reads are complete
+        __syncthreads();
         const uint32_t leaf = DENSE ? li : __ldg(a.active_list + li);
         const LeafEntry e = a.entries[leaf];
         LeafGeom G;
         G.li = li;
         leaf_extent(a.g, leaf, G.bx, G.by, G.bz, G.w, G.h, G.d);
         const uint32_t st = entry_status(e);
-        if (st != kOk || (e.header & 3u) == kModeEmpty) {
+        const uint64_t b0 = 4ull * e.word_off;
+        const uint64_t b1 = 4ull * (uint64_t)__ldg(a.offsets + leaf + 1);
+        const uint64_t a0 = b0 & ~15ull, a1 = (b1 + 15u) & ~15ull;
+        const bool skip = st != kOk || (e.header & 3u) == kModeEmpty;
+        const bool staged = !skip && a1 - a0 <= a.g.stage_bytes;
+        if (tid == 0) {
+            if (staged) mbar_expect_and_copy(s.bar, s.stage, pay_bytes + a0, (uint32_t)(a1 - a0));
+            bool to = false;
+            const uint32_t nx = grab_leaf(work, epoch, to);
+            if (to) record_error(a.err, leaf, kErrWaitTimeout);
+            *s_next = nx;
+        }
+        if (skip) {
             if (st != kOk && tid == 0) record_error(a.err, leaf, st);
             for (int idx = tid; idx < fl.n * 128; idx += kLeafThreads)
                 store_quad<DENSE>(a, G, out, frame_stride, idx >> 7, (idx & 127) & 31, (idx & 127) >> 5,
                                   make_float4(0.f, 0.f, 0.f, 0.f));
-            continue;
-        }
-        const uint64_t b0 = 4ull * e.word_off;
-        const uint64_t b1 = 4ull * (uint64_t)__ldg(a.offsets + leaf + 1);
-        const uint64_t a0 = b0 & ~15ull, a1 = (b1 + 15u) & ~15ull;
-        const bool staged = a1 - a0 <= a.g.stage_bytes;
-        if (!GLOBAL_FALLBACK && !staged) {   // the launcher never lets this happen
+        } else if (!GLOBAL_FALLBACK && !staged) {   // the launcher never lets this happen
             if (tid == 0) record_error(a.err, leaf, kErrDecodeOob);
-            continue;
-        }
-        __syncthreads();   // the previous leaf's shared-memory reads are complete
-        if (staged && tid == 0) mbar_expect_and_copy(s.bar, s.stage, pay_bytes + a0, (uint32_t)(a1 - a0));
-        if (tid < 48) {
-            const int ws = tid / 24, axis = (tid % 24) >> 3, p = tid & 7;
-            const int R = ws == 0 ? (int)((e.header >> 6) & 7u) : (int)((e.header >> 9) & 7u);
-            const int ext = axis == 0 ? G.w : (axis == 1 ? G.h : G.d);
-            s.w[ws][axis][p] = g_axis[axis_index(R, ext, p)];
-        }
-        if (staged) {
-            if (!mbar_wait(s.bar, phase)) {
+        } else {
+            if (tid < 48) {
+                const int ws = tid / 24, axis = (tid % 24) >> 3, p = tid & 7;
+                const int R = ws == 0 ? (int)((e.header >> 6) & 7u) : (int)((e.header >> 9) & 7u);
+                const int ext = axis == 0 ? G.w : (axis == 1 ? G.h : G.d);
+                s.w[ws][axis][p] = g_axis[axis_index(R, ext, p)];
+            }
+            const bool ok = !staged || mbar_wait(s.bar, phase);
+            if (__syncthreads_or(!ok)) {   // any thread gave up: the whole CTA stops, together
                 if (tid == 0) record_error(a.err, leaf, kErrWaitTimeout);
-                mbar_wait(s.bar, phase);   // a second bounded wait for the copy in flight, then stop
+                if (staged) mbar_wait(s.bar, phase);   // a second bounded wait for the copy in flight
                 return;
             }
-            phase ^= 1u;
+            if (staged) phase ^= 1u;
+            if (staged) {
+                const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
+                leaf_decode<DENSE>(a, m, s, e, fl.n, steps01, G, out, frame_stride);
+            } else if (GLOBAL_FALLBACK) {
+                const GlobalWords m{a.payload};
+                leaf_decode<DENSE>(a, m, s, e, fl.n, steps01, G, out, frame_stride);
+            }
         }
-        __syncthreads();
-        if (staged) {
-            const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
-            leaf_decode<DENSE>(a, m, s, e, fl.n, steps01, G, out, frame_stride);
-        } else if (GLOBAL_FALLBACK) {
-            const GlobalWords m{a.payload};
-            leaf_decode<DENSE>(a, m, s, e, fl.n, steps01, G, out, frame_stride);
-        }
+        __syncthreads();   // the next index is visible
+        li = *s_next;
     }
 }
 
@@ -265,25 +303,26 @@ static int leaf_grid(uint32_t smem_bytes)
 }
 
 template <bool DENSE, bool GF>
-static void launch_leaf_variant(const DeviceAsset& a, const FrameList& fl, float* out, uint64_t stride, int grid,
-                                cudaStream_t s)
+static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameList& fl, float* out, uint64_t stride,
+                                int grid, cudaStream_t s)
 {
     const uint32_t smem = kLeafFixed + a.g.stage_bytes;
     cudaFuncSetAttribute(decode_leaf_kernel<DENSE, GF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int g = grid > 0 ? grid : leaf_grid<DENSE, GF>(smem);
-    decode_leaf_kernel<DENSE, GF><<<g, kLeafThreads, smem, s>>>(a, fl, out, stride);
+    decode_leaf_kernel<DENSE, GF><<<g, kLeafThreads, smem, s>>>(a, fl, out, stride, a.work + seq % kWorkSlots,
+                                                                seq + 1u);
 }
 
-static void launch_rt_leaf(const DeviceAsset& a, const FrameList& fl, float* out, uint64_t stride, int grid, bool dense,
-                           cudaStream_t s)
+static void launch_rt_leaf(const DeviceAsset& a, uint32_t seq, const FrameList& fl, float* out, uint64_t stride,
+                           int grid, bool dense, cudaStream_t s)
 {
     const bool gf = a.g.max_window > a.g.stage_bytes;
     if (dense) {
-        if (gf) launch_leaf_variant<true, true>(a, fl, out, stride, grid, s);
-        else launch_leaf_variant<true, false>(a, fl, out, stride, grid, s);
+        if (gf) launch_leaf_variant<true, true>(a, seq, fl, out, stride, grid, s);
+        else launch_leaf_variant<true, false>(a, seq, fl, out, stride, grid, s);
     } else {
-        if (gf) launch_leaf_variant<false, true>(a, fl, out, stride, grid, s);
-        else launch_leaf_variant<false, false>(a, fl, out, stride, grid, s);
+        if (gf) launch_leaf_variant<false, true>(a, seq, fl, out, stride, grid, s);
+        else launch_leaf_variant<false, false>(a, seq, fl, out, stride, grid, s);
     }
 }
 
