@@ -18,6 +18,12 @@ Field recipes (shapes are X x Y x Z x T):
   tiny_*          small, odd-sized fields (boundary leaves with cropped extents).
   sci_*           scientific (generic profile, time-fastest RAW) Gaussian random fields with a
                   k^-5/3 spectrum, phase drift, and 0.1% spikes of 10 sigma.
+  mix_fire_*      the config-3 fire (density, flames, temperature = 300 + 1500 flames + N(0, 20))
+                  at 128 x 128 x 192 x 40: fBm inside a sphere of radius 20 + 2.5 t.
+  mix_sdf         the config-4 liquid level set at 128^3 x 48 (sloshing plane, 20 ballistic spheres
+                  under gravity 0.05 voxels/frame^2); Mode2 shell.
+  mix_sci         the config-5 scientific field at 128^3 x 64, time fastest.
+  The mix_* assets, cfg2_plume, cfg1_blobs and cfg4_sdf_small are the serving mix (MIX).
 
 Usage: python tests/golden/make_assets.py [names...]   (default: the small set + cfg1 + cfg2)
 """
@@ -220,20 +226,20 @@ RECIPES = {
                              time_fastest=True),
     "cfg2_plume": lambda: encode("cfg2_plume", plume(256, 96, 2), (256, 256, 256, 96), "density"),
     # serving-mix assets: the config-3/4/5 scenes at reduced sizes (the full sizes need 36-64 GB
-    # of raw float32 input per field, more than this machine's memory), plus a second plume
-    "mix_plume_b": lambda: encode("mix_plume_b", plume(256, 96, 3), (256, 256, 256, 96), "density"),
-    "mix_fire_density": lambda: encode("mix_fire_density", fire((192, 192, 256), 60, 7)[0], (192, 192, 256, 60),
+    # of raw float32 input per field, more than this machine's memory, and the encoded fields
+    # must stay small enough to travel with the working tree)
+    "mix_fire_density": lambda: encode("mix_fire_density", fire((128, 128, 192), 40, 7)[0], (128, 128, 192, 40),
                                        "density"),
-    "mix_fire_flames": lambda: encode("mix_fire_flames", fire((192, 192, 256), 60, 7)[1], (192, 192, 256, 60),
+    "mix_fire_flames": lambda: encode("mix_fire_flames", fire((128, 128, 192), 40, 7)[1], (128, 128, 192, 40),
                                       "density"),
-    "mix_fire_temperature": lambda: encode("mix_fire_temperature", fire((192, 192, 256), 60, 7)[2],
-                                           (192, 192, 256, 60), "density"),
-    "mix_sdf": lambda: encode("mix_sdf", sdf_scene((256, 256, 256), 48, 100.0, 12.0, 0.05, 40, 3.0, 12.0, 9),
-                              (256, 256, 256, 48), "density", LEVELSET),
+    "mix_fire_temperature": lambda: encode("mix_fire_temperature", fire((128, 128, 192), 40, 7)[2],
+                                           (128, 128, 192, 40), "density"),
+    "mix_sdf": lambda: encode("mix_sdf", sdf_scene((128, 128, 128), 48, 50.0, 12.0, 0.05, 20, 3.0, 12.0, 9),
+                              (128, 128, 128, 48), "density", LEVELSET),
     "mix_sci": lambda: encode("mix_sci", grf_scientific((128, 128, 128), 64, 8), (128, 128, 128, 64), "generic",
                               time_fastest=True),
 }
-MIX = ["cfg2_plume", "mix_plume_b", "mix_fire_density", "mix_fire_flames", "mix_fire_temperature", "mix_sdf",
+MIX = ["cfg2_plume", "mix_fire_density", "mix_fire_flames", "mix_fire_temperature", "mix_sdf",
        "cfg1_blobs", "cfg4_sdf_small", "mix_sci"]
 DEFAULT = ["tiny_density", "tiny_levelset", "sci_small", "cfg1_blobs", "cfg4_sdf_small", "sci_64", "cfg2_plume"]
 

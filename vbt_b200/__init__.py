@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libvbt_b200.so")
 
 if not os.path.exists(LIB_PATH):
-    raise ImportError(f"vbt_b200: {LIB_PATH} is missing; build it with `python -m vbt_b200.build`")
+    raise ImportError(f"vbt_b200: {LIB_PATH} is missing; build it with `python vbt_b200/build.py`")
 
 _lib = C.CDLL(LIB_PATH)
 
