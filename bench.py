@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=300)
     return p.parse_args()
 
 
@@ -199,6 +201,131 @@ class CpuDecoder:
                 break
         return (self.n_active * 512 * done / el,
                 f"{done} frames of the {self.frames}-frame cache decode ({self.n_active} active leaves), {el:.1f} s")
+
+
+# ------------------------------------------------------------------------------ serving
+SERVE_ASSETS = ["cfg2_plume", "mix_fire_density", "mix_fire_flames", "mix_fire_temperature", "mix_sdf",
+                "cfg1_blobs", "cfg4_sdf_small", "mix_sci"]
+SERVE_BUDGET = 8 << 30
+
+
+def serving_requests(assets, n, seed=11):
+    """The serving mix: 70% point batches of 1e3..1e6 uniform (x, y, z, t) (log-uniform sizes),
+    20% z-slices over 1..16 frames, 10% single dense frames, each on a uniformly drawn asset."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for _ in range(n):
+        i = int(rng.integers(len(assets)))
+        X, Y, Z = assets[i].dims
+        T = assets[i].frames
+        u = rng.random()
+        if u < 0.7:
+            m = int(10 ** rng.uniform(3.0, 6.0))
+            q = np.empty((m, 4), np.uint32)
+            q[:, 0] = rng.integers(0, X, m)
+            q[:, 1] = rng.integers(0, Y, m)
+            q[:, 2] = rng.integers(0, Z, m)
+            q[:, 3] = rng.integers(0, T, m)
+            reqs.append(("points", i, q))
+        elif u < 0.9:
+            t0 = int(rng.integers(0, T))
+            reqs.append(("slice", i, (int(rng.integers(0, Z)), t0, min(T, t0 + int(rng.integers(1, 17))))))
+        else:
+            reqs.append(("frames", i, [int(rng.integers(0, T))]))
+    return reqs
+
+
+def serve_once(vbt, assets, reqs, pinned, plain, arrivals):
+    """Run the request list through one server; arrivals=None submits everything at once.
+    Latency = done - submit on the server's clock."""
+    srv = vbt.Server(hbm_budget_bytes=SERVE_BUDGET, slots=4, plain=plain, host_staging_bytes=256 << 20)
+    ids = [srv.add_asset(a) for a in assets]
+    tickets = [None] * len(reqs)
+    t0 = time.perf_counter()
+    for j, (kind, i, arg) in enumerate(reqs):
+        if arrivals is not None:
+            while time.perf_counter() - t0 < arrivals[j]:
+                pass
+        if kind == "points":
+            tickets[j] = srv.submit_points(ids[i], pinned[j][0], pinned[j][1])
+        elif kind == "slice":
+            tickets[j] = srv.submit_slice(ids[i], *arg)
+        else:
+            tickets[j] = srv.submit_frames(ids[i], arg)
+    lat, first, last, bad = [], None, 0.0, 0
+    for t in tickets:
+        r = srv.wait(t)
+        bad += int(r.status != 0)
+        lat.append(r.done_ms - r.submit_ms)
+        first = r.submit_ms if first is None else min(first, r.submit_ms)
+        last = max(last, r.done_ms)
+        srv.release(t)
+    st = srv.stats()
+    srv.close()
+    dims = [a.dims for a in assets]
+    pts = sum(x[2].shape[0] for x in reqs if x[0] == "points")
+    vox = sum((x[2][2] - x[2][1]) * dims[x[1]][0] * dims[x[1]][1] for x in reqs if x[0] == "slice")
+    vox += sum(len(x[2]) * dims[x[1]][0] * dims[x[1]][1] * dims[x[1]][2] for x in reqs if x[0] == "frames")
+    span_s = (last - first) * 1e-3
+    lat = np.array(lat)
+    return {"errors": bad, "makespan_ms": last - first, "requests_per_s": len(reqs) / span_s,
+            "decoded_values_per_s": (pts + vox) / span_s, "queries_per_s": pts / span_s, "voxels_per_s": vox / span_s,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "launches": int(st.launches), "units": int(st.units), "arena_peak_bytes": int(st.arena_peak_bytes)}
+
+
+def run_serving(args, local_rank):
+    """The serving mix over the resident assets: served (4 streams, HBM-budget admission, point
+    requests merged across assets) against plain (one request per launch, one launch in flight),
+    closed loop (all requests at once) and open loop (Poisson arrivals at a common rate)."""
+    import torch
+    import vbt_b200 as vbt
+    assets, names, skipped = [], [], []
+    for n in SERVE_ASSETS:
+        p = os.path.join(ROOT, "assets", n + ".vbtp")
+        if not os.path.exists(p):
+            skipped.append(f"{n}: not generated")
+            continue
+        try:
+            assets.append(vbt.Asset(p, device=local_rank))
+            names.append(n)
+        except vbt.VbtError as e:
+            skipped.append(f"{n}: {e}")
+    if len(assets) < 2:
+        return {"skipped": "serving-mix assets not generated (tests/golden/make_assets.py)"}
+    reqs = serving_requests(assets, args.serve_requests)
+    pinned = {}
+    for j, (kind, i, arg) in enumerate(reqs):
+        if kind == "points":
+            q = torch.from_numpy(arg).pin_memory()
+            o = torch.empty(arg.shape[0], dtype=torch.float32).pin_memory()
+            pinned[j] = (q.numpy(), o.numpy(), q, o)
+    serve_once(vbt, assets, reqs[:20], pinned, False, None)   # warm-up
+    closed_s = serve_once(vbt, assets, reqs, pinned, False, None)
+    closed_p = serve_once(vbt, assets, reqs, pinned, True, None)
+    gaps = np.random.default_rng(5).exponential(1.0, len(reqs))
+
+    def at_rate(rate):
+        return np.cumsum(gaps / rate) - gaps[0] / rate
+
+    lam_p = 0.8 * closed_p["requests_per_s"]
+    lam_s = 0.8 * closed_s["requests_per_s"]
+    open_s_p = serve_once(vbt, assets, reqs, pinned, False, at_rate(lam_p))
+    open_p_p = serve_once(vbt, assets, reqs, pinned, True, at_rate(lam_p))
+    open_s_s = serve_once(vbt, assets, reqs, pinned, False, at_rate(lam_s))
+    for a in assets:
+        a.close()
+    return {"workload": "serving mix: 70% point batches of 1e3-1e6 uniform (x,y,z,t), 20% z-slices over 1-16 "
+                        "frames, 10% dense frames, uniform over the assets; point inputs and outputs in pinned host "
+                        "memory, slice and frame results device-resident (released when done)",
+            "assets": names, "assets_skipped": skipped, "requests": len(reqs),
+            "kinds": {k: sum(1 for r in reqs if r[0] == k) for k in ("points", "slice", "frames")},
+            "server": {"hbm_budget_bytes": SERVE_BUDGET, "slots": 4},
+            "served": {"closed_loop": closed_s, "poisson_at_0.8x_plain_capacity": open_s_p,
+                       "poisson_at_0.8x_served_capacity": open_s_s},
+            "plain": {"closed_loop": closed_p, "poisson_at_0.8x_plain_capacity": open_p_p},
+            "throughput_ratio_closed_loop": closed_s["decoded_values_per_s"] / closed_p["decoded_values_per_s"],
+            "arrival_rates_req_per_s": {"0.8x_plain": lam_p, "0.8x_served": lam_s}}
 
 
 # ------------------------------------------------------------------------------ arms
@@ -356,6 +483,10 @@ def run_ours(args, rank, local_rank, world):
                "h2d_bytes_per_step": int(image.nbytes), "d2h_bytes_per_step": int(cache.numel() * 4),
                "ms_per_step": e2e_ms}
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        serving = run_serving(args, local_rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         dec = CpuDecoder(args.asset)
@@ -377,7 +508,7 @@ def run_ours(args, rank, local_rank, world):
                 "kernels_ms": {"page_table": statistics.mean(pt_ms), "decode_per_launch": statistics.mean(dec_ms)},
                 "plain": {"value": plain_value, "unit": "voxels/s", "ms_per_step": plain_ms,
                           "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
-                "cpu_baseline": cpu, "e2e": e2e,
+                "cpu_baseline": cpu, "e2e": e2e, "serving": serving,
                 "gpu_launches": args.steps * (1 + len(chunks)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)

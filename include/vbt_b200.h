@@ -145,6 +145,73 @@ int vbt_build_page_table_noalloc(const uint32_t* d_offsets, const uint32_t* d_pa
                                  uint32_t leaf_count, uint32_t profile_type, uint32_t* d_compact,
                                  uint32_t* d_active_list, uint32_t* d_active_count, void* stream);
 
+/* ---- Serving loop -----------------------------------------------------------------------------
+ * No counterpart in the reference (its decoders are one call per value or per frame).  A server
+ * keeps several resident assets, accepts point, slice and frame requests from any thread, admits
+ * them while an HBM budget for their inputs and results has room, merges the point requests that
+ * are admitted together into one multi-asset launch, and runs launches on `slots` streams so
+ * that requests arriving while others are on the GPU overlap with them (continuous batching).
+ * One scheduler thread per server issues all GPU work.  Results are identical to the one-asset
+ * calls above (the same kernels; tested alone versus in a mix). */
+typedef struct vbt_server vbt_server;
+
+typedef struct {
+    int device;                  /* CUDA device of the server and of every asset added to it */
+    uint64_t hbm_budget_bytes;   /* device memory for in-flight inputs and not yet released results */
+    uint64_t host_staging_bytes; /* pinned host memory for requests with pageable host buffers */
+    uint32_t slots;              /* launch streams, 1 .. 32 (units in flight at once) */
+    uint32_t max_batch_queries;  /* point queries merged into one launch, 0 = 4,194,304 */
+    uint32_t plain;              /* 1: one request per launch, one launch in flight, FIFO (baseline) */
+} vbt_server_config;
+
+#define VBT_REQ_POINTS 1u   /* points[n_points] = (x, y, z, t) quads -> n_points floats */
+#define VBT_REQ_SLICE 2u    /* z layer over frames [t0, t1) -> (t1 - t0) * X * Y floats */
+#define VBT_REQ_FRAMES 3u   /* frames[n_frames] -> n_frames * X * Y * Z floats (dense, clamped) */
+
+typedef struct {
+    uint32_t kind;               /* VBT_REQ_* */
+    uint32_t asset;              /* id returned by vbt_server_add_asset */
+    const uint32_t* points;      /* POINTS: host array; must stay valid until the request is done */
+    uint64_t n_points;
+    uint32_t z;                  /* SLICE */
+    int32_t t0, t1;
+    const int32_t* frames;       /* FRAMES: host array (copied at submit) */
+    uint32_t n_frames;
+    float* host_out;             /* result destination on the host, or NULL to keep the result in
+                                  * device memory until vbt_serve_release */
+} vbt_request;
+
+typedef struct {
+    int status;                  /* VBT_STATUS_* of the request (decode errors included) */
+    uint32_t bad_leaf;           /* first failing leaf when status is a decode status */
+    uint64_t result_floats;
+    const float* device_result;  /* when host_out was NULL: the result, valid until release */
+    double submit_ms, start_ms, done_ms;   /* server clock: submitted, launched, seen complete */
+} vbt_request_result;
+
+typedef struct {
+    uint64_t requests_done, points_done, voxels_done;   /* voxels: slice and frame outputs */
+    uint64_t launches, units;          /* kernel launches; launch groups */
+    uint64_t arena_peak_bytes, arena_bytes, resident_asset_bytes;
+    double p50_ms, p99_ms, max_ms;     /* submit -> done, over requests done since the last reset */
+    double busy_ms;                    /* wall time with at least one unit in flight */
+} vbt_server_stats;
+
+int vbt_server_create(const vbt_server_config* config, vbt_server** out);
+/* The asset stays owned by the caller and must outlive the server; at most 64 assets, all on the
+ * server's device. */
+int vbt_server_add_asset(vbt_server* server, vbt_asset* asset, uint32_t* asset_id);
+/* VBT_STATUS_LIMIT when the request alone needs more than the budget. */
+int vbt_serve_submit(vbt_server* server, const vbt_request* request, uint64_t* ticket);
+int vbt_serve_poll(vbt_server* server, uint64_t ticket, int* done, vbt_request_result* result);
+int vbt_serve_wait(vbt_server* server, uint64_t ticket, vbt_request_result* result);
+/* Frees the ticket and a device-resident result; every ticket must be released once done. */
+int vbt_serve_release(vbt_server* server, uint64_t ticket);
+int vbt_server_get_stats(vbt_server* server, vbt_server_stats* out);
+int vbt_server_reset_stats(vbt_server* server);
+/* Waits for all submitted requests, then frees the server's streams and memory. */
+int vbt_server_destroy(vbt_server* server);
+
 #ifdef __cplusplus
 }
 #endif

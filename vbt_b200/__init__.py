@@ -39,6 +39,32 @@ class VbtAssetInfo(C.Structure):
                 ("device_bytes", C.c_uint64), ("device", C.c_int)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_uint64), ("host_staging_bytes", C.c_uint64),
+                ("slots", C.c_uint32), ("max_batch_queries", C.c_uint32), ("plain", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("asset", C.c_uint32), ("points", C.c_void_p), ("n_points", C.c_uint64),
+                ("z", C.c_uint32), ("t0", C.c_int32), ("t1", C.c_int32), ("frames", C.c_void_p),
+                ("n_frames", C.c_uint32), ("host_out", C.c_void_p)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("bad_leaf", C.c_uint32), ("result_floats", C.c_uint64),
+                ("device_result", C.c_void_p), ("submit_ms", C.c_double), ("start_ms", C.c_double),
+                ("done_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests_done", C.c_uint64), ("points_done", C.c_uint64), ("voxels_done", C.c_uint64),
+                ("launches", C.c_uint64), ("units", C.c_uint64), ("arena_peak_bytes", C.c_uint64),
+                ("arena_bytes", C.c_uint64), ("resident_asset_bytes", C.c_uint64), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("max_ms", C.c_double), ("busy_ms", C.c_double)]
+
+
+REQ_POINTS, REQ_SLICE, REQ_FRAMES = 1, 2, 3
+
 _vp, _u32p, _i32p, _f32p = C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.c_void_p
 _sig = {
     "vbt_status_string": ([C.c_int], C.c_char_p),
@@ -65,6 +91,15 @@ _sig = {
     "vbt_decode_control_values": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
                                    C.c_int, _vp, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
     "vbt_build_page_table_noalloc": ([_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_server_create": ([C.POINTER(ServerConfig), C.POINTER(_vp)], C.c_int),
+    "vbt_server_add_asset": ([_vp, _vp, _u32p], C.c_int),
+    "vbt_serve_submit": ([_vp, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
+    "vbt_serve_poll": ([_vp, C.c_uint64, C.POINTER(C.c_int), C.POINTER(RequestResult)], C.c_int),
+    "vbt_serve_wait": ([_vp, C.c_uint64, C.POINTER(RequestResult)], C.c_int),
+    "vbt_serve_release": ([_vp, C.c_uint64], C.c_int),
+    "vbt_server_get_stats": ([_vp, C.POINTER(ServerStats)], C.c_int),
+    "vbt_server_reset_stats": ([_vp], C.c_int),
+    "vbt_server_destroy": ([_vp], C.c_int),
 }
 for _name, (_args, _res) in _sig.items():
     _f = getattr(_lib, _name)
@@ -249,3 +284,82 @@ def decode_control_values(d_stream, stream_bytes, codec, control_count, bins, kf
     _check(_lib.vbt_decode_control_values(_addr(d_stream), stream_bytes, codec, control_count, bins, kf, int(align),
                                           total_frames, _addr(d_ci), _addr(d_frames), n, _addr(d_out),
                                           _addr(d_status), _stream(stream)))
+
+
+class Server:
+    """The serving loop (vbt_server_* in include/vbt_b200.h): resident assets, requests admitted
+    by an HBM budget, point requests merged across assets, launches overlapped on `slots` streams.
+
+    Host buffers handed to submit_*() (numpy arrays) must stay alive until the request is done;
+    the object keeps references to them until release()."""
+
+    def __init__(self, hbm_budget_bytes=1 << 30, slots=4, max_batch_queries=0, plain=False, device=0,
+                 host_staging_bytes=256 << 20):
+        cfg = ServerConfig(device, hbm_budget_bytes, host_staging_bytes, slots, max_batch_queries, int(plain))
+        self._h = _vp()
+        _check(_lib.vbt_server_create(C.byref(cfg), C.byref(self._h)))
+        self._keep = {}
+
+    def add_asset(self, asset):
+        i = C.c_uint32()
+        _check(_lib.vbt_server_add_asset(self._h, asset.handle, C.byref(i)))
+        return i.value
+
+    def _submit(self, req, keep):
+        t = C.c_uint64()
+        _check(_lib.vbt_serve_submit(self._h, C.byref(req), C.byref(t)))
+        self._keep[t.value] = keep
+        return t.value
+
+    def submit_points(self, asset_id, xyzt, host_out=None):
+        """xyzt: contiguous uint32 numpy array [n, 4]; host_out: float32 numpy array [n], or None to
+        keep the result in device memory until release()."""
+        req = Request(kind=REQ_POINTS, asset=asset_id, points=xyzt.ctypes.data, n_points=xyzt.shape[0],
+                      host_out=None if host_out is None else host_out.ctypes.data)
+        return self._submit(req, (xyzt, host_out))
+
+    def submit_slice(self, asset_id, z, t0, t1, host_out=None):
+        req = Request(kind=REQ_SLICE, asset=asset_id, z=z, t0=t0, t1=t1,
+                      host_out=None if host_out is None else host_out.ctypes.data)
+        return self._submit(req, (host_out,))
+
+    def submit_frames(self, asset_id, frames, host_out=None):
+        fr = (C.c_int32 * len(frames))(*frames)
+        req = Request(kind=REQ_FRAMES, asset=asset_id, frames=C.cast(fr, C.c_void_p), n_frames=len(frames),
+                      host_out=None if host_out is None else host_out.ctypes.data)
+        return self._submit(req, (fr, host_out))
+
+    def poll(self, ticket):
+        done = C.c_int()
+        res = RequestResult()
+        _check(_lib.vbt_serve_poll(self._h, ticket, C.byref(done), C.byref(res)))
+        return bool(done.value), res
+
+    def wait(self, ticket):
+        res = RequestResult()
+        _check(_lib.vbt_serve_wait(self._h, ticket, C.byref(res)))
+        return res
+
+    def release(self, ticket):
+        _check(_lib.vbt_serve_release(self._h, ticket))
+        self._keep.pop(ticket, None)
+
+    def stats(self):
+        st = ServerStats()
+        _check(_lib.vbt_server_get_stats(self._h, C.byref(st)))
+        return st
+
+    def reset_stats(self):
+        _check(_lib.vbt_server_reset_stats(self._h))
+
+    def close(self):
+        if self._h:
+            _lib.vbt_server_destroy(self._h)
+            self._h = _vp()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

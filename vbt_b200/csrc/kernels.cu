@@ -1016,23 +1016,33 @@ __global__ void __launch_bounds__(128) query_points_kernel(DeviceAsset a, const 
     out[i] = point_value(a, reinterpret_cast<const uint4*>(q)[i], a.err);
 }
 
-// Point queries of several resident assets in one launch: query i belongs to assets[which[i]].
-// Decode errors of the whole launch go to one error word.
-__global__ void __launch_bounds__(128) query_points_multi_kernel(const DeviceAsset* __restrict__ assets,
-                                                                 const uint4* __restrict__ q,
-                                                                 const uint8_t* __restrict__ which, uint64_t n,
-                                                                 float* __restrict__ out, unsigned long long* err)
+// Point queries of several requests over several resident assets in one launch.  The segment
+// table holds starts[0..k] (each request's first query; starts[k] = n), asset[k] (request r reads
+// assets[asset[r]]) and, 8-byte aligned after them, outs[k] (request r's result array).  Request
+// r's decode errors go to errs[r].
+__global__ void __launch_bounds__(128) query_points_batch_kernel(const DeviceAsset* __restrict__ assets,
+                                                                 const uint32_t* __restrict__ seg, uint32_t k,
+                                                                 const uint4* __restrict__ q, uint64_t n,
+                                                                 unsigned long long* errs)
 {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    out[i] = point_value(assets[__ldg(which + i)], q[i], err);
+    int lo = 0, hi = (int)k - 1;
+    while (lo < hi) {   // the last request whose first query is at or before i
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(seg + mid) <= (uint32_t)i) lo = mid;
+        else hi = mid - 1;
+    }
+    const unsigned long long* outs = reinterpret_cast<const unsigned long long*>(seg + ((2u * k + 2u) & ~1u));
+    float* o = reinterpret_cast<float*>(__ldg(outs + lo));
+    o[i - __ldg(seg + lo)] = point_value(assets[__ldg(seg + k + 1 + lo)], q[i], errs + lo);
 }
 
-void launch_query_points_multi(const DeviceAsset* assets, const uint4* q, const uint8_t* which, uint64_t n, float* out,
-                               unsigned long long* err, cudaStream_t s)
+void launch_query_points_batch(const DeviceAsset* assets, const uint32_t* seg, uint32_t k, const uint4* q, uint64_t n,
+                               unsigned long long* errs, cudaStream_t s)
 {
-    if (n == 0) return;
-    query_points_multi_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(assets, q, which, n, out, err);
+    if (n == 0 || k == 0) return;
+    query_points_batch_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(assets, seg, k, q, n, errs);
 }
 
 void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, cudaStream_t s)

@@ -69,10 +69,11 @@ void launch_decode_dense(const DeviceAsset& a, uint32_t seq, const int* frames, 
 void launch_decode_cache_plain(const DeviceAsset& a, int frame, float* out, cudaStream_t s);
 // Point queries: q[4*i..] = (x, y, z, t); out[i].
 void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, cudaStream_t s);
-// Point queries over several assets (a device array of DeviceAsset): query i reads assets[which[i]];
-// decode errors are recorded in *err (first failing leaf, as DeviceAsset::err).
-void launch_query_points_multi(const DeviceAsset* assets, const uint4* q, const uint8_t* which, uint64_t n, float* out,
-                               unsigned long long* err, cudaStream_t s);
+// Point queries of k requests over several assets in one launch (a device array of DeviceAsset).
+// seg: starts[0..k] (first query of each request, starts[k] = n), asset[k], then 8-byte aligned
+// outs[k] (result arrays, as 64-bit addresses); decode errors of request r are recorded in errs[r].
+void launch_query_points_batch(const DeviceAsset* assets, const uint32_t* seg, uint32_t k, const uint4* q, uint64_t n,
+                               unsigned long long* errs, cudaStream_t s);
 // Z-slice over a frame range: out[(t - t0) * X*Y + y*X + x] for t in [t0, t1).
 void launch_query_slice(const DeviceAsset& a, uint32_t z, int t0, int t1, float* out, cudaStream_t s);
 
