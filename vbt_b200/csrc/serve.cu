@@ -141,8 +141,11 @@ bool is_pinned(const void* p)
 
 // Segment table of a k-request point unit: starts[k+1], asset[k], 8-byte aligned outs[k].
 uint64_t seg_bytes(uint32_t k) { return ((4ull * (2 * k + 1) + 7) & ~7ull) + 8ull * k; }
-// Device input block of a point unit: [errs 8k][segment table, 16-aligned][queries 16N].
-uint64_t points_in_bytes(uint32_t k, uint64_t n) { return 8ull * k + ((seg_bytes(k) + 15) & ~15ull) + 16ull * n; }
+// Error words of a unit, padded so that what follows starts on a 16-byte boundary.
+uint64_t err_bytes(uint32_t k) { return (8ull * k + 15) & ~15ull; }
+// Device input block of a point unit: [errs][segment table][queries 16N], each part 16-byte
+// aligned (the queries are read as uint4, the output addresses as 64-bit words).
+uint64_t points_in_bytes(uint32_t k, uint64_t n) { return err_bytes(k) + ((seg_bytes(k) + 15) & ~15ull) + 16ull * n; }
 
 }  // namespace
 
@@ -170,6 +173,7 @@ struct vbt_server {
     std::vector<Block> to_free;   // device results released by clients
     uint64_t next_ticket = 1;
     bool stop = false;
+    bool dead = false;   // the device reported a fault; no further work is launched
     std::thread worker;
     // stats (guarded by mu)
     std::vector<double> latencies;
@@ -345,7 +349,7 @@ void vbt_server::launch(Unit* u, int slot)
             run += u->reqs[i]->r.n_points;
         }
         starts[k] = (uint32_t)run;
-        uint8_t* dseg = din + 8ull * k;
+        uint8_t* dseg = din + err_bytes(k);
         uint8_t* dq = dseg + ((seg_bytes(k) + 15) & ~15ull);
         cudaMemcpyAsync(dseg, hseg, seg_bytes(k), cudaMemcpyHostToDevice, st);
         uint8_t* hpage = hseg + seg_bytes(k);
@@ -448,12 +452,19 @@ void vbt_server::run()
         int in_flight = 0;
         for (uint32_t s = 0; s < cfg.slots; ++s) {
             if (!busy[s]) continue;
-            if (cudaEventQuery(events[s]) == cudaSuccess) {
+            const cudaError_t q = cudaEventQuery(events[s]);
+            if (q == cudaSuccess) {
                 finalize(busy[s], (int)s);
                 progressed = true;
-            } else {
-                cudaGetLastError();   // cudaErrorNotReady is not sticky; clear it
+            } else if (q == cudaErrorNotReady) {
+                cudaGetLastError();   // not sticky; clear it
                 ++in_flight;
+            } else {
+                // the device reported a fault: the unit's requests fail, and so does all later work
+                dead = true;
+                for (Req* r : busy[s]->reqs) r->status = VBT_STATUS_CUDA;
+                finalize(busy[s], (int)s);
+                progressed = true;
             }
         }
         std::vector<Unit*> ready;
@@ -461,6 +472,16 @@ void vbt_server::run()
             std::unique_lock<std::mutex> lk(mu);
             for (const Block& b : to_free) arena.release(b.off, b.bytes);
             to_free.clear();
+            if (dead) {   // complete everything pending with the device error
+                const double t = now_ms();
+                for (Req* r : pending) {
+                    r->status = VBT_STATUS_CUDA;
+                    r->t_done = t;
+                    r->state = 2;
+                }
+                pending.clear();
+                cv_done.notify_all();
+            }
             int free_slots = 0;
             for (uint32_t s = 0; s < cfg.slots; ++s) free_slots += busy[s] ? 0 : 1;
             if (cfg.plain && in_flight > 0) free_slots = 0;
