@@ -56,6 +56,17 @@ def dist_env():
 
 
 # ------------------------------------------------------------------------------ helpers
+def max_over_ranks(value, dist, device):
+    """The largest `value` over all ranks of the process group (every rank gets it); the plain
+    value when there is no group.  Device timings of a multi-GPU step are reported this way."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def algorithmic_bytes_per_frame(rows):
     """Algorithmic bytes of one frame of cache decode for the active leaves of a leaf table:
     8 (header + prefix) + per decoded control 4 desc + 2 bin bytes + 2 keyframes x stride
@@ -423,10 +434,7 @@ def run_ours(args, rank, local_rank, world):
     pt_ms = [e[0].elapsed_time(e[1]) for e in ev]
     dec_ms = [e[1 + i].elapsed_time(e[2 + i]) for e in ev for i in range(len(chunks))]
     total_ms = float(sum(step_ms))
-    if pg:
-        t = torch.tensor([total_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, pg, dev)
     voxels_per_step = n_active * 512 * T
     value = world * voxels_per_step * args.steps / (total_ms * 1e-3)
 
@@ -475,10 +483,7 @@ def run_ours(args, rank, local_rank, world):
         stream.synchronize()
         a.sync_status(stream)
         e2e_ms = ee0.elapsed_time(ee1) / e2e_steps
-        if pg:
-            t = torch.tensor([e2e_ms], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e2e_ms, pg, dev)
         e2e = {"value": world * voxels_per_step / (e2e_ms * 1e-3), "unit": "voxels/s",
                "h2d_bytes_per_step": int(image.nbytes), "d2h_bytes_per_step": int(cache.numel() * 4),
                "ms_per_step": e2e_ms}
