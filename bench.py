@@ -386,9 +386,13 @@ def run_ours(args, rank, local_rank, world):
     a = vbt.Asset(args.asset, device=local_rank)
     T, n_active = a.frames, a.active_count
     frames = list(range(T))
-    chunks = [frames[i:i + CHUNK] for i in range(0, T, CHUNK)]
     stride = n_active * 512
     cache = torch.empty((T, max(n_active, 1), 512), dtype=torch.float32, device=dev)
+    # launch shape chosen by the library's autotuner on this asset and output
+    tuning = a.autotune(T, cache, stream=stream)
+    stream.synchronize()
+    fpl = tuning.frames_per_launch if tuning.variant == 0 else CHUNK
+    chunks = [frames[i:i + fpl] for i in range(0, T, fpl)]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     rows = a.leaf_table()
     bytes_per_frame, n_act2 = algorithmic_bytes_per_frame(rows)
@@ -444,6 +448,20 @@ def run_ours(args, rank, local_rank, world):
     alg_per_launch = [bytes_per_frame * len(ch) for ch in chunks]
     achieved = statistics.mean(alg_per_launch) / mean_launch_s / 1e9
     traffic = ncu_traffic()
+
+    # the same step replayed from a captured CUDA graph (page table + all decode launches, one
+    # cudaGraphLaunch), timed the same way
+    a.decode_cache_timeline(0, T, cache, frame_stride=stride, graph=True, stream=stream)
+    gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            gev[k][0].record(stream)
+            a.decode_cache_timeline(0, T, cache, frame_stride=stride, graph=True, stream=stream)
+            gev[k][1].record(stream)
+    stream.synchronize()
+    a.sync_status(stream)
+    graph_ms = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in gev), pg, dev) / args.steps
 
     # plain path: per frame, page table + one-CTA-per-leaf launch (no batching, no persistence)
     plain_ms = None
@@ -503,7 +521,7 @@ def run_ours(args, rank, local_rank, world):
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "asset": os.path.basename(args.asset), "leaves": a.leaf_count,
-                           "active_leaves": n_active, "frames_per_step": T, "frames_per_launch": CHUNK,
+                           "active_leaves": n_active, "frames_per_step": T, "frames_per_launch": fpl,
                            "l2": "flushed before every timed step (256 MiB write)",
                            "cache_ring_bytes": int(cache.numel() * 4), "parallelism": f"replicas x{world}"},
                 "roofline": {"bound": "hbm", "kernel": "decode_leaf_kernel<cache>", "achieved": achieved, "peak": peak,
@@ -511,6 +529,11 @@ def run_ours(args, rank, local_rank, world):
                              "algorithmic_bytes_per_launch": int(statistics.mean(alg_per_launch)),
                              "launch_ms": statistics.mean(dec_ms), "peak_source": peak_src},
                 "kernels_ms": {"page_table": statistics.mean(pt_ms), "decode_per_launch": statistics.mean(dec_ms)},
+                "graph": {"value": world * voxels_per_step / (graph_ms * 1e-3), "unit": "voxels/s",
+                          "ms_per_step": graph_ms, "launches_per_step": 1},
+                "tuning": {"variant": ["leaf per CTA", "leaf per warp"][tuning.variant],
+                           "frames_per_launch": tuning.frames_per_launch, "grid": tuning.grid,
+                           "ms_per_frame": tuning.ms_per_frame, "ms_per_frame_untuned": tuning.ms_per_frame_default},
                 "plain": {"value": plain_value, "unit": "voxels/s", "ms_per_step": plain_ms,
                           "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
                 "cpu_baseline": cpu, "e2e": e2e, "serving": serving,

@@ -145,6 +145,35 @@ int vbt_build_page_table_noalloc(const uint32_t* d_offsets, const uint32_t* d_pa
                                  uint32_t leaf_count, uint32_t profile_type, uint32_t* d_compact,
                                  uint32_t* d_active_list, uint32_t* d_active_count, void* stream);
 
+/* ---- Batched timeline: autotuned, graph-captured ---------------------------------------------
+ * No counterpart in the reference.  The current-frame cache of a frame range is a page-table build
+ * plus one decode launch per `frames_per_launch` frames.  The launch shape (leaf per CTA: the
+ * TMA-staged kernel; leaf per warp: eight leaves per CTA), the frames per launch and the grid are
+ * chosen per asset by timing the candidates on the caller's output (vbt_autotune_cache), or set
+ * directly (vbt_set_tuning).  vbt_decode_cache_timeline then runs the whole range; with use_graph
+ * it is captured once into a CUDA graph per (first frame, count, output, stride) and replayed with
+ * one cudaGraphLaunch.  Output as vbt_decode_cache: d_out[f * frame_stride + rank * 512 + voxel]. */
+typedef struct {
+    uint32_t variant;            /* 0: leaf per CTA; 1: leaf per warp */
+    uint32_t frames_per_launch;  /* 1 .. 64 */
+    int grid;                    /* CTAs per launch, 0 = one wave */
+    float ms_per_frame;          /* measured by vbt_autotune_cache (0 when set by hand) */
+    float ms_per_frame_default;  /* the untuned configuration (leaf per CTA, 48 frames, one wave) */
+} vbt_tuning;
+
+/* Times every candidate over frames [0, nframes) into d_out (frame_stride floats per frame),
+ * keeps the fastest for the asset and returns it.  Synchronises `stream`. */
+int vbt_autotune_cache(vbt_asset* asset, int nframes, float* d_out, uint64_t frame_stride, vbt_tuning* out,
+                       void* stream);
+int vbt_set_tuning(vbt_asset* asset, const vbt_tuning* tuning);
+int vbt_get_tuning(vbt_asset* asset, vbt_tuning* out);
+/* Page table + cache of frames [t0, t0 + n) with the asset's tuning.  The first call with
+ * use_graph for a given (t0, n, d_out, frame_stride) captures the graph on `stream` (which must not
+ * be the legacy default stream); a graph is never replayed concurrently with itself, and changing
+ * the tuning drops the captured graphs. */
+int vbt_decode_cache_timeline(vbt_asset* asset, int t0, int n, float* d_out, uint64_t frame_stride, int use_graph,
+                              void* stream);
+
 /* ---- Serving loop -----------------------------------------------------------------------------
  * No counterpart in the reference (its decoders are one call per value or per frame).  A server
  * keeps several resident assets, accepts point, slice and frame requests from any thread, admits

@@ -63,6 +63,11 @@ class ServerStats(C.Structure):
                 ("p99_ms", C.c_double), ("max_ms", C.c_double), ("busy_ms", C.c_double)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("variant", C.c_uint32), ("frames_per_launch", C.c_uint32), ("grid", C.c_int),
+                ("ms_per_frame", C.c_float), ("ms_per_frame_default", C.c_float)]
+
+
 REQ_POINTS, REQ_SLICE, REQ_FRAMES = 1, 2, 3
 
 _vp, _u32p, _i32p, _f32p = C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.c_void_p
@@ -91,6 +96,10 @@ _sig = {
     "vbt_decode_control_values": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
                                    C.c_int, _vp, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
     "vbt_build_page_table_noalloc": ([_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_autotune_cache": ([_vp, C.c_int, _vp, C.c_uint64, C.POINTER(Tuning), _vp], C.c_int),
+    "vbt_set_tuning": ([_vp, C.POINTER(Tuning)], C.c_int),
+    "vbt_get_tuning": ([_vp, C.POINTER(Tuning)], C.c_int),
+    "vbt_decode_cache_timeline": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, C.c_int, _vp], C.c_int),
     "vbt_server_create": ([C.POINTER(ServerConfig), C.POINTER(_vp)], C.c_int),
     "vbt_server_add_asset": ([_vp, _vp, _u32p], C.c_int),
     "vbt_serve_submit": ([_vp, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
@@ -237,6 +246,28 @@ class Asset:
         if frame_stride is None:
             frame_stride = self.active_count * 512
         _check(_lib.vbt_decode_cache(self._h, fr, len(frames), _addr(out), frame_stride, grid, _stream(stream)))
+
+    def autotune(self, nframes, out, frame_stride=None, stream=None):
+        """Time the cache-timeline launch shapes on `out` and keep the fastest (returns Tuning)."""
+        t = Tuning()
+        stride = self.active_count * 512 if frame_stride is None else frame_stride
+        _check(_lib.vbt_autotune_cache(self._h, nframes, _addr(out), stride, C.byref(t), _stream(stream)))
+        return t
+
+    def set_tuning(self, variant, frames_per_launch, grid=0):
+        t = Tuning(variant, frames_per_launch, grid, 0.0, 0.0)
+        _check(_lib.vbt_set_tuning(self._h, C.byref(t)))
+
+    def tuning(self):
+        t = Tuning()
+        _check(_lib.vbt_get_tuning(self._h, C.byref(t)))
+        return t
+
+    def decode_cache_timeline(self, t0, n, out, frame_stride=None, graph=True, stream=None):
+        """Page table + cache of frames [t0, t0 + n) with the asset's tuning; graph=True replays a
+        CUDA graph captured on the first call for this (t0, n, out, stride)."""
+        stride = self.active_count * 512 if frame_stride is None else frame_stride
+        _check(_lib.vbt_decode_cache_timeline(self._h, t0, n, _addr(out), stride, int(graph), _stream(stream)))
 
     def decode_cache_plain(self, frame, out, stream=None):
         _check(_lib.vbt_decode_cache_plain(self._h, frame, _addr(out), _stream(stream)))

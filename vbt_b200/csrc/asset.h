@@ -4,8 +4,12 @@
 
 #include <atomic>
 #include <cstdint>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "../../include/vbt_b200.h"
 #include "kernels.cuh"
@@ -24,4 +28,14 @@ struct vbt_asset {
     void* stage_out = nullptr;
     size_t stage_out_bytes = 0;
     std::mutex mu;
+    // cache-timeline configuration (vbt_autotune_cache / vbt_set_tuning) and its captured graphs,
+    // keyed by (first frame, frame count, output, frame stride)
+    vbt_tuning tuning{0u, 48u, 0, 0.0f, 0.0f};
+    std::mutex graph_mu;
+    std::map<std::tuple<int, int, uintptr_t, uint64_t>, cudaGraphExec_t> graphs;
 };
+
+namespace vbtb {
+// Destroys the asset's captured timeline graphs (tune.cu).
+void release_timeline_graphs(vbt_asset* a);
+}

@@ -373,6 +373,7 @@ int vbt_asset_destroy(vbt_asset* a)
     if (!a) return VBT_STATUS_OK;
     {
         DeviceGuard guard(a->device);
+        release_timeline_graphs(a);
         free_all(a);
     }
     delete a;

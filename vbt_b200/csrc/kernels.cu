@@ -413,6 +413,11 @@ void launch_walk(const DeviceAsset& a, uint32_t epoch, cudaStream_t s)
 void launch_page_table(const DeviceAsset& a, uint32_t epoch, cudaStream_t s)
 {
     const uint32_t tiles = (a.g.leaf_count + kWalkTile - 1) / kWalkTile;
+    // Inside a stream capture the epoch is frozen into the graph, so every replay would find the
+    // previous replay's descriptors carrying its own tag: clear them first in the graph.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+        cudaMemsetAsync(a.tile_state, 0, 8ull * tiles, s);
     page_table_kernel<<<tiles, kWalkThreads, 0, s>>>(a, epoch);
 }
 
@@ -829,6 +834,21 @@ void launch_decode_dense(const DeviceAsset& a, uint32_t seq, const int* frames, 
     else
         launch_rt_leaf(a, seq, fl, out, stride, grid, true, s);
 }
+
+// Leaf-per-warp cache decode (8 warps per CTA, each warp one leaf at a time, frames in turn):
+// the alternative shape the autotuner weighs against the leaf-per-CTA kernel.
+void launch_decode_cache_warp(const DeviceAsset& a, const int* frames, int nframes, float* out, uint64_t stride,
+                              int grid, cudaStream_t s)
+{
+    FrameList fl{};
+    fl.n = nframes;
+    for (int i = 0; i < nframes; ++i) fl.f[i] = frames[i];
+    const int g = grid > 0 ? grid : default_grid();
+    if (a.g.profile == 2u) decode_kernel<false, true><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+    else decode_kernel<false, false><<<g, kDecodeWarps * 32, 0, s>>>(a, fl, out, stride);
+}
+
+int decode_warp_grid() { return default_grid(); }
 
 // Plain per-leaf launch: grid = the whole leaf grid, one 64-thread CTA per leaf (EMPTY leaves
 // return at once), controls decoded by both warps' lanes, one frame.  This is the reference

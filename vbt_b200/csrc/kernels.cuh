@@ -64,6 +64,10 @@ void launch_decode_cache(const DeviceAsset& a, uint32_t seq, const int* frames, 
 // Dense frames: out[f * X*Y*Z + (z*Y + y)*X + x]; every leaf (EMPTY ones write zeros).
 void launch_decode_dense(const DeviceAsset& a, uint32_t seq, const int* frames, int nframes, float* out, int grid,
                          cudaStream_t s);
+// Leaf-per-warp cache decode (same output as launch_decode_cache); grid 0 = one wave.
+void launch_decode_cache_warp(const DeviceAsset& a, const int* frames, int nframes, float* out, uint64_t stride,
+                              int grid, cudaStream_t s);
+int decode_warp_grid();
 // Plain path: one CTA per leaf of the whole leaf grid, one frame per launch (the reference
 // Studio dispatch shape, VBTStudio/frontend/src/volume_renderer.cpp:704-735).
 void launch_decode_cache_plain(const DeviceAsset& a, int frame, float* out, cudaStream_t s);

@@ -309,8 +309,13 @@ static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameL
     const uint32_t smem = kLeafFixed + a.g.stage_bytes;
     cudaFuncSetAttribute(decode_leaf_kernel<DENSE, GF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int g = grid > 0 ? grid : leaf_grid<DENSE, GF>(smem);
-    decode_leaf_kernel<DENSE, GF><<<g, kLeafThreads, smem, s>>>(a, fl, out, stride, a.work + seq % kWorkSlots,
-                                                                seq + 1u);
+    unsigned long long* slot = a.work + seq % kWorkSlots;
+    // Inside a stream capture the epoch is frozen into the graph: every replay starts from a
+    // cleared slot instead (a graph is never replayed concurrently with itself).
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+        cudaMemsetAsync(slot, 0, sizeof(unsigned long long), s);
+    decode_leaf_kernel<DENSE, GF><<<g, kLeafThreads, smem, s>>>(a, fl, out, stride, slot, seq + 1u);
 }
 
 static void launch_rt_leaf(const DeviceAsset& a, uint32_t seq, const FrameList& fl, float* out, uint64_t stride,
