@@ -39,6 +39,7 @@ extern "C" {
 #define VBT_STATUS_FILE 41                /* the VBTPACK4 reader rejected the file (message set) */
 #define VBT_STATUS_CUDA 42                /* CUDA runtime error or no usable device (message set) */
 #define VBT_STATUS_LIMIT 43               /* request exceeds a fixed capacity of the call */
+#define VBT_STATUS_UNSUPPORTED 44         /* a leaf mode the call does not cover (recorded per leaf) */
 
 typedef struct vbt_asset vbt_asset;
 
@@ -144,6 +145,25 @@ int vbt_decode_control_values(const uint8_t* d_stream, uint32_t stream_bytes, ui
 int vbt_build_page_table_noalloc(const uint32_t* d_offsets, const uint32_t* d_payload, uint64_t payload_words,
                                  uint32_t leaf_count, uint32_t profile_type, uint32_t* d_compact,
                                  uint32_t* d_active_list, uint32_t* d_active_count, void* stream);
+
+/* ---- (d) Window decode on the tensor cores -----------------------------------------------------
+ * No counterpart in the reference.  Scientific assets (profile 2): the current-frame cache of
+ * frames [t0, t0 + n), n <= 64, d_out[f * frame_stride + leaf * 512 + voxel] as vbt_decode_cache,
+ * computed per leaf as one contraction S(512 x 64) . C(64 x n) on tcgen05 tensor cores: S = the
+ * coarse trilinear weights (343 S is an integer matrix, exact in BF16), C = the coarse controls at
+ * the window's frames (the DCT-II sum of scientific_decode.cpp:82-97, in FP32) split into three
+ * BF16 terms; FP32 accumulation in tensor memory; the sparse-event residual is added exactly as
+ * the per-frame path does.  Values are not bit-identical to the reference; vbt_window_error gives
+ * their error.  CoarseOnly and SparseEvents leaves are covered; DenseGrid leaves record
+ * VBT_STATUS_UNSUPPORTED (read by vbt_asset_sync_status) and are written as zeros. */
+int vbt_decode_window(vbt_asset* asset, int t0, int n, float* d_out, uint64_t frame_stride, void* stream);
+/* FP64 error oracle on the GPU for any scientific cache of frames [t0, t0 + n) (from
+ * vbt_decode_window or vbt_decode_cache): the reference model evaluated in double without
+ * intermediate rounding (same FP32 coefficients, basis values and trilinear weights) and reduced in
+ * double.  stats[0] = max |value - oracle|, stats[1] = rms, stats[2] / stats[3] = oracle min / max.
+ * Synchronises `stream`. */
+int vbt_window_error(vbt_asset* asset, int t0, int n, const float* d_values, uint64_t frame_stride, double* stats,
+                     void* stream);
 
 /* ---- Batched timeline: autotuned, graph-captured ---------------------------------------------
  * No counterpart in the reference.  The current-frame cache of a frame range is a page-table build

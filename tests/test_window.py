@@ -1,0 +1,94 @@
+"""(d) Window decode of scientific leaves on the tensor cores (vbt_decode_window) and its FP64
+error oracle (vbt_window_error).
+
+The window path is not bit-exact by design (split-BF16 products, FP32 accumulation); the bar is
+1e-6 of the field range against the FP64 oracle and against the exact per-frame decode.  The
+oracle is checked to report a planted deviation of known size.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ASSETS, golden_asset
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-6   # relative to the field range
+
+
+def sci_paths():
+    out = [golden_asset("sci_small")]
+    for n in ("sci_64", "mix_sci"):
+        p = os.path.join(ASSETS, n + ".vbtp")
+        if os.path.exists(p):
+            out.append(p)
+    return out
+
+
+def windows(T):
+    w = [(0, min(T, 16)), (max(0, T - 7), min(T, 7)), (0, min(T, 64))]
+    if T > 40:
+        w.append((T // 2 - 20, 40))
+    return w
+
+
+@pytest.mark.parametrize("path", sci_paths(), ids=os.path.basename)
+def test_window_matches_per_frame_and_oracle(vbt, cuda, path):
+    a = vbt.Asset(path)
+    T, L = a.frames, a.leaf_count
+    assert a.active_count == L
+    for t0, n in windows(T):
+        exact = cuda.empty((n, L, 512), dtype=cuda.float32, device="cuda")
+        a.decode_cache(list(range(t0, t0 + n)), exact, frame_stride=L * 512)
+        win = cuda.full((n, L, 512), float("nan"), dtype=cuda.float32, device="cuda")
+        a.decode_window(t0, n, win)
+        a.sync_status()
+        e = exact.cpu().numpy().astype(np.float64)
+        w = win.cpu().numpy().astype(np.float64)
+        assert np.isfinite(w).all()
+        mx, rms, lo, hi = a.window_error(t0, n, win)
+        mx_e, rms_e, lo_e, hi_e = a.window_error(t0, n, exact)
+        assert (lo, hi) == (lo_e, hi_e)
+        orng = hi - lo
+        assert orng > 0
+        diff = np.abs(w - e).max()
+        assert diff <= TOL * orng, (t0, n, diff, orng)
+        assert mx <= TOL * orng and mx_e <= TOL * orng, (mx, mx_e, orng)
+    a.close()
+
+
+def test_oracle_sees_a_perturbation(vbt, cuda):
+    """The oracle's max error of the exact per-frame output is tiny; after moving one value by a
+    known amount it reports that amount."""
+    a = vbt.Asset(golden_asset("sci_small"))
+    T, L = a.frames, a.leaf_count
+    n = min(T, 16)
+    exact = cuda.empty((n, L, 512), dtype=cuda.float32, device="cuda")
+    a.decode_cache(list(range(n)), exact, frame_stride=L * 512)
+    a.sync_status()
+    mx, rms, lo, hi = a.window_error(0, n, exact)
+    rng = hi - lo
+    assert mx <= TOL * rng and rms <= mx
+    bump = 1e-3 * rng
+    exact[3, L // 2, 77] += bump
+    mx2, _, lo2, hi2 = a.window_error(0, n, exact)
+    assert (lo2, hi2) == (lo, hi)
+    assert abs(mx2 - bump) <= 1e-6 * rng, (mx2, bump)
+    a.close()
+
+
+def test_window_rejects_render_assets_and_long_windows(vbt, cuda):
+    a = vbt.Asset(golden_asset("tiny_density"))
+    out = cuda.empty(a.frames * a.leaf_count * 512, dtype=cuda.float32, device="cuda")
+    with pytest.raises(vbt.VbtError) as ei:
+        a.decode_window(0, 4, out)
+    assert ei.value.status == 40
+    a.close()
+    s = vbt.Asset(golden_asset("sci_small"))
+    out = cuda.empty(65 * s.leaf_count * 512, dtype=cuda.float32, device="cuda")
+    with pytest.raises(vbt.VbtError):
+        s.decode_window(0, 65, out)
+    with pytest.raises(vbt.VbtError):
+        s.decode_window(s.frames - 2, 4, out)
+    s.close()

@@ -23,7 +23,7 @@ STATUS = {
     0: "OK", 1: "LEAF_TOO_SMALL", 2: "PREFIX_MISSING", 3: "LEAF_SHORT", 4: "SHELL_OCC_OOB",
     5: "SHELL_GROUP_PREFIX", 6: "SHELL_NO_ACTIVE", 7: "SHELL_RESIDUAL_OOB", 8: "SHELL_TRAILING",
     9: "CONTROL_INDEX", 10: "STREAM_OOB", 11: "DECODE_OOB", 12: "KEY_RANGE_OOB", 13: "KEY_INDEX",
-    30: "WAIT_TIMEOUT", 40: "INVALID_ARGUMENT", 41: "FILE", 42: "CUDA", 43: "LIMIT",
+    30: "WAIT_TIMEOUT", 40: "INVALID_ARGUMENT", 41: "FILE", 42: "CUDA", 43: "LIMIT", 44: "UNSUPPORTED",
 }
 
 
@@ -96,6 +96,8 @@ _sig = {
     "vbt_decode_control_values": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
                                    C.c_int, _vp, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
     "vbt_build_page_table_noalloc": ([_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
+    "vbt_window_error": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, C.POINTER(C.c_double), _vp], C.c_int),
     "vbt_autotune_cache": ([_vp, C.c_int, _vp, C.c_uint64, C.POINTER(Tuning), _vp], C.c_int),
     "vbt_set_tuning": ([_vp, C.POINTER(Tuning)], C.c_int),
     "vbt_get_tuning": ([_vp, C.POINTER(Tuning)], C.c_int),
@@ -246,6 +248,20 @@ class Asset:
         if frame_stride is None:
             frame_stride = self.active_count * 512
         _check(_lib.vbt_decode_cache(self._h, fr, len(frames), _addr(out), frame_stride, grid, _stream(stream)))
+
+    def decode_window(self, t0, n, out, frame_stride=None, stream=None):
+        """(d) scientific window decode on the tensor cores (frames [t0, t0 + n), n <= 64) into
+        `out` in the cache layout."""
+        stride = self.leaf_count * 512 if frame_stride is None else frame_stride
+        _check(_lib.vbt_decode_window(self._h, t0, n, _addr(out), stride, _stream(stream)))
+
+    def window_error(self, t0, n, values, frame_stride=None, stream=None):
+        """FP64 oracle error of a scientific cache of frames [t0, t0 + n):
+        (max_abs, rms, oracle_min, oracle_max)."""
+        stride = self.leaf_count * 512 if frame_stride is None else frame_stride
+        st = (C.c_double * 4)()
+        _check(_lib.vbt_window_error(self._h, t0, n, _addr(values), stride, st, _stream(stream)))
+        return tuple(st)
 
     def autotune(self, nframes, out, frame_stride=None, stream=None):
         """Time the cache-timeline launch shapes on `out` and keep the fastest (returns Tuning)."""

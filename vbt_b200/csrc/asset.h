@@ -28,6 +28,7 @@ struct vbt_asset {
     void* stage_out = nullptr;
     size_t stage_out_bytes = 0;
     std::mutex mu;
+    unsigned long long* d_stats = nullptr;   // 4 words for the window error oracle's reduction
     // cache-timeline configuration (vbt_autotune_cache / vbt_set_tuning) and its captured graphs,
     // keyed by (first frame, frame count, output, frame stride)
     vbt_tuning tuning{0u, 48u, 0, 0.0f, 0.0f};

@@ -186,6 +186,7 @@ const char* vbt_status_string(int s)
     case VBT_STATUS_FILE: return "invalid VBTPACK4 file";
     case VBT_STATUS_CUDA: return "CUDA error";
     case VBT_STATUS_LIMIT: return "request exceeds a fixed capacity";
+    case VBT_STATUS_UNSUPPORTED: return "leaf mode not covered by this call";
     default: return "unknown status";
     }
 }
@@ -264,7 +265,7 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
         (st = alloc(a, &d_entries, sizeof(LeafEntry) * (uint64_t)L)) || (st = alloc(a, &d_compact, 4ull * L)) ||
         (st = alloc(a, &d_list, 4ull * L)) || (st = alloc(a, &d_counters, 16)) || (st = alloc(a, &d_err, 8)) ||
         (st = alloc(a, &d_tiles, 8ull * tiles)) || (st = alloc(a, &d_sorted, L)) ||
-        (st = alloc(a, &d_work, 8ull * kWorkSlots))) {
+        (st = alloc(a, &d_work, 8ull * kWorkSlots)) || (st = alloc(a, reinterpret_cast<void**>(&a->d_stats), 32))) {
         free_all(a);
         delete a;
         return st;
@@ -542,6 +543,53 @@ int vbt_decode_frames_host(vbt_asset* a, const int* frames, int nframes, float* 
     if ((st = check_launch("decode_kernel<dense>"))) return st;
     CUDA_TRY(cudaMemcpyAsync(out, a->stage_out, 4ull * vox * nframes, cudaMemcpyDeviceToHost, s));
     return vbt_asset_sync_status(a, stream, nullptr);
+}
+
+int vbt_decode_window(vbt_asset* a, int t0, int n, float* d_out, uint64_t frame_stride, void* stream)
+{
+    if (!a || !d_out) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    if (a->hdr.profile_type != 2u)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "window decode covers scientific (profile 2) assets");
+    if (n < 1 || n > 64 || t0 < 0 || (uint64_t)t0 + (uint64_t)n > a->hdr.frames)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "window must be 1..64 frames inside [0, frames)");
+    if (frame_stride < 512ull * a->hdr.leaf_count)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "frame_stride below leaf_count * 512");
+    DeviceGuard guard(a->device);
+    launch_sci_window(a->dev, t0, n, d_out, frame_stride, static_cast<cudaStream_t>(stream));
+    return check_launch("sci_window_kernel");
+}
+
+int vbt_window_error(vbt_asset* a, int t0, int n, const float* d_values, uint64_t frame_stride, double* stats,
+                     void* stream)
+{
+    if (!a || !d_values || !stats) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    if (a->hdr.profile_type != 2u)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "the window oracle covers scientific (profile 2) assets");
+    if (n < 1 || t0 < 0 || (uint64_t)t0 + (uint64_t)n > a->hdr.frames)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "frames outside [0, frames)");
+    DeviceGuard guard(a->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    launch_sci_window_oracle(a->dev, t0, n, d_values, frame_stride, a->d_stats, s);
+    int st;
+    if ((st = check_launch("sci_window_oracle_kernel"))) return st;
+    unsigned long long raw[4];
+    CUDA_TRY(cudaMemcpyAsync(raw, a->d_stats, sizeof(raw), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    auto unorder = [](unsigned long long o) {
+        const unsigned long long b = (o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o;
+        double d;
+        std::memcpy(&d, &b, 8);
+        return d;
+    };
+    double mx, sum;
+    std::memcpy(&mx, &raw[0], 8);
+    std::memcpy(&sum, &raw[1], 8);
+    const double count = (double)a->hdr.leaf_count * 512.0 * (double)n;
+    stats[0] = mx;
+    stats[1] = std::sqrt(sum / count);
+    stats[2] = unorder(raw[2]);
+    stats[3] = unorder(raw[3]);
+    return VBT_STATUS_OK;
 }
 
 int vbt_decode_control_values(const uint8_t* d_stream, uint32_t bytes, uint32_t codec, uint32_t cc, uint32_t bins,

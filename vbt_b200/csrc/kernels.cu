@@ -1124,3 +1124,8 @@ void launch_query_slice(const DeviceAsset& a, uint32_t z, int t0, int t1, float*
 }
 
 }  // namespace vbtb
+
+// (d) window decode of scientific leaves on the tensor cores: sci_window.cuh
+#include <cuda_bf16.h>
+
+#include "sci_window.cuh"

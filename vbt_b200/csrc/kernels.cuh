@@ -68,6 +68,12 @@ void launch_decode_dense(const DeviceAsset& a, uint32_t seq, const int* frames, 
 void launch_decode_cache_warp(const DeviceAsset& a, const int* frames, int nframes, float* out, uint64_t stride,
                               int grid, cudaStream_t s);
 int decode_warp_grid();
+// (d) scientific window decode on the tensor cores, frames [t0, t0 + n), n <= 64, cache layout.
+void launch_sci_window(const DeviceAsset& a, int t0, int n, float* out, uint64_t frame_stride, cudaStream_t s);
+// FP64 oracle of a scientific window: stats[0] max |err| (double bits), stats[1] sum err^2
+// (double), stats[2] / stats[3] oracle min / max (order-preserving bits).
+void launch_sci_window_oracle(const DeviceAsset& a, int t0, int n, const float* vals, uint64_t frame_stride,
+                              unsigned long long* stats, cudaStream_t s);
 // Plain path: one CTA per leaf of the whole leaf grid, one frame per launch (the reference
 // Studio dispatch shape, VBTStudio/frontend/src/volume_renderer.cpp:704-735).
 void launch_decode_cache_plain(const DeviceAsset& a, int frame, float* out, cudaStream_t s);

@@ -1,0 +1,399 @@
+// sci_window.cuh -- (d) multi-frame window decode of scientific leaves on the tensor cores, and
+// its FP64 error oracle.  Included by kernels.cu (it uses that file's scientific helpers).
+//
+// For one leaf and a window of n <= 64 frames starting at t0, the voxels are
+//     V(512 x n) = S(512 x 64) . C(64 x n) + residual,
+// C = the 64 coarse controls at the window's frames (DC b0(t) + sum_k q_k b_k(t), the DCT-II
+// contraction of render/src/scientific_decode.cpp:82-97) and S = the trilinear weights of
+// sampleCoarseAt (:99-123).  Those weights are products of three axis weights that are multiples
+// of 1/7, so S' = 343 S is an integer matrix with entries <= 343.  Every entry but 343 (the eight
+// voxels that sit on a control point, weight 1) is exact in one BF16; the A operand holds S' with
+// 343 entered as 342, and the missing 1 x C term of those eight voxels is added on the CUDA cores.
+// C is computed in FP32 (compensated sum) and split into three BF16 terms c = c_hi + c_mid + c_lo
+// (residual below 2^-26 |c|).  The contraction is 3 tcgen05.mma products per 16-wide K step
+// (S'.c_hi + S'.c_mid + S'.c_lo), accumulated in FP32 in tensor memory: 4 M tiles (128 voxels)
+// x 4 K steps x 3 terms = 48 MMAs of 128 x N x 16 per leaf-window, N = n rounded up to 16.
+// The epilogue reads D from tensor memory, adds the corner terms, scales by 1/343, adds the
+// sparse-event residual (CUDA cores, as the per-frame path) and writes the cache layout.
+//
+// Shared-memory operand layout (canonical K-major, no swizzle): per K step, core matrices of
+// 8 rows x 16 bytes; the two 8-element K halves 128 bytes apart (leading byte offset), 8-row
+// groups 256 bytes apart (stride byte offset).
+#pragma once
+
+namespace vbtb {
+
+constexpr int kWinThreads = 256;
+constexpr int kWinMaxN = 64;
+constexpr uint32_t kWinTmemCols = 256;                  // 4 M tiles x 64 columns of FP32
+constexpr uint32_t kWinA = 4u * 4u * 4096u;             // 4 M tiles x 4 K steps x (128 rows x 32 B)
+constexpr uint32_t kWinB = 4u * 3u * (kWinMaxN * 32u);  // 4 K steps x 3 terms x (64 rows x 32 B)
+constexpr uint32_t kWinCorner = 8u * kWinMaxN * 4u;     // corner controls x frames, FP32
+constexpr uint32_t kWinQ = 64u * 64u * 4u;              // 64 controls x keep (<= 64) coefficients
+constexpr uint32_t kWinSmem = kWinA + kWinB + kWinCorner + kWinQ + 64u;
+
+__device__ __forceinline__ uint32_t win_smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: start >> 4 [0,14), LBO >> 4 [16,30), SBO >> 4 [32,46),
+// version 1 [46,48), no swizzle [61,64).
+__device__ __forceinline__ uint64_t win_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(256u >> 4) << 32) |
+           (1ull << 46);
+}
+
+// Byte offset of (row, k) inside one K step of a K-major operand tile.
+__device__ __forceinline__ uint32_t win_off(uint32_t row, uint32_t k)
+{
+    return (row >> 3) * 256u + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// 7 x the trilinear weight of control coordinate c (0..3) for voxel coordinate x (0..7): the
+// sample position is 3x/7 control spacings (scientific_decode.cpp:99-123, f = x/7*3 clamped to
+// cell 0..2).
+__device__ __forceinline__ uint32_t win_w7(uint32_t x, uint32_t c)
+{
+    const uint32_t f7 = 3u * x;
+    const uint32_t i0 = min(2u, f7 / 7u);
+    const uint32_t t7 = f7 - 7u * i0;
+    return c == i0 ? 7u - t7 : (c == i0 + 1u ? t7 : 0u);
+}
+
+// Index 0..7 of a corner control ((cx, cy, cz) in {0, 3}^3), or -1.
+__device__ __forceinline__ int win_corner_of_control(uint32_t ci)
+{
+    const uint32_t cx = ci & 3u, cy = (ci >> 2) & 3u, cz = ci >> 4;
+    if ((cx != 0u && cx != 3u) || (cy != 0u && cy != 3u) || (cz != 0u && cz != 3u)) return -1;
+    return (int)((cx ? 1u : 0u) | (cy ? 2u : 0u) | (cz ? 4u : 0u));
+}
+// Index 0..7 of a voxel on a control point ((lx, ly, lz) in {0, 7}^3), or -1.
+__device__ __forceinline__ int win_corner_of_voxel(uint32_t v)
+{
+    const uint32_t lx = v & 7u, ly = (v >> 3) & 7u, lz = v >> 6;
+    if ((lx != 0u && lx != 7u) || (ly != 0u && ly != 7u) || (lz != 0u && lz != 7u)) return -1;
+    return (int)((lx ? 1u : 0u) | (ly ? 2u : 0u) | (lz ? 4u : 0u));
+}
+
+__device__ __forceinline__ uint16_t win_bf16_bits(float x)
+{
+    const __nv_bfloat16 b = __float2bfloat16_rn(x);
+    return *reinterpret_cast<const uint16_t*>(&b);
+}
+__device__ __forceinline__ float win_bf16_val(uint16_t bits)
+{
+    return __uint_as_float((uint32_t)bits << 16);
+}
+
+__device__ __forceinline__ void win_tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void win_tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// D[tmem] (+)= A[desc] x B[desc], kind::f16 (BF16 inputs, FP32 accumulate).
+__device__ __forceinline__ void win_mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void win_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(win_smem_u32(bar))
+                 : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void win_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// One CTA per leaf at a time (grid-stride), 256 threads, 2 CTAs per SM (shared memory and the
+// 256 tensor-memory columns each).  out[f * frame_stride + leaf * 512 + voxel] for f < n.
+__global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset a, int t0, int n,
+                                                                    float* __restrict__ out, uint64_t frame_stride)
+{
+    extern __shared__ __align__(1024) uint8_t wdyn[];
+    uint8_t* sA = wdyn;
+    uint8_t* sB = wdyn + kWinA;
+    float* sCorner = reinterpret_cast<float*>(wdyn + kWinA + kWinB);
+    float* sQ = reinterpret_cast<float*>(wdyn + kWinA + kWinB + kWinCorner);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wdyn + kWinA + kWinB + kWinCorner + kWinQ);
+    uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int N = (n + 15) & ~15;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(win_smem_u32(s_taddr)),
+                     "r"(kWinTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init_fence();
+    }
+    // A = S' (343 entered as 342), one exact BF16 per entry
+    for (uint32_t idx = tid; idx < 512u * 64u; idx += kWinThreads) {
+        const uint32_t v = idx >> 6, ci = idx & 63u;
+        uint32_t w = win_w7(v & 7u, ci & 3u) * win_w7((v >> 3) & 7u, (ci >> 2) & 3u) * win_w7(v >> 6, ci >> 4);
+        if (w == 343u) w = 342u;
+        const uint32_t m = v >> 7, s = ci >> 4;
+        *reinterpret_cast<uint16_t*>(sA + (m * 4u + s) * 4096u + win_off(v & 127u, ci & 15u)) = win_bf16_bits((float)w);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    win_tc_fence_before();
+    __syncthreads();
+    win_tc_fence_after();
+    const uint32_t taddr = *s_taddr;
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    uint32_t phase = 0;
+
+    for (uint32_t leaf = blockIdx.x; leaf < a.g.leaf_count; leaf += gridDim.x) {
+        const LeafEntry e = a.entries[leaf];
+        const uint32_t st = entry_status(e);
+        const uint32_t hdr = e.header, mode = hdr & 3u;
+        const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
+        if (st != kOk || mode >= 2u) {   // uniform over the CTA
+            if (tid == 0) record_error(a.err, leaf, st != kOk ? st : kErrUnsupported);
+            for (int i = tid; i < n * 512; i += kWinThreads)
+                out[(uint64_t)(i >> 9) * frame_stride + (uint64_t)leaf * 512u + (i & 511)] = 0.0f;
+            continue;
+        }
+        const uint64_t base = 4ull * e.word_off;
+        // 1. coefficients q[ci][k]: DC (fp16) for k = 0, int8 x acScale[k-1] otherwise
+        SciReader rd{a.payload, a.g.payload_words, false};
+        for (int i = tid; i < 64 * keep; i += kWinThreads) {
+            const int ci = i / keep, k = i % keep;
+            const uint64_t cb = base + 4u + (uint64_t)ci * (keep + 1);
+            sQ[i] = k == 0 ? half_bits_to_float(rd.u16(cb))
+                           : __fmul_rn((float)(int8_t)rd.byte(cb + 2u + (k - 1)), __ldg(a.scales + k - 1));
+        }
+        if (rd.oob) record_error(a.err, leaf, kErrDecodeOob);
+        __syncthreads();
+        // 2. C[f][ci] (compensated FP32 sum), split into three BF16 terms, B tiles and corners
+        for (int i = tid; i < 64 * N; i += kWinThreads) {
+            const int ci = i & 63, f = i >> 6;
+            float c = 0.0f;
+            if (f < n) {
+                const float* brow = a.basis + (uint64_t)(t0 + f) * 64u;
+                float hi, lo;
+                two_prod(sQ[ci * keep], __ldg(brow), hi, lo);
+                for (int k = 1; k < keep; ++k) {
+                    float ph, pl;
+                    two_prod(sQ[ci * keep + k], __ldg(brow + k), ph, pl);
+                    ff_add(hi, lo, ph, pl);
+                }
+                c = __fadd_rn(hi, lo);
+            }
+            const uint16_t b0 = win_bf16_bits(c);
+            const float r1 = __fsub_rn(c, win_bf16_val(b0));
+            const uint16_t b1 = win_bf16_bits(r1);
+            const uint16_t b2 = win_bf16_bits(__fsub_rn(r1, win_bf16_val(b1)));
+            const uint32_t s = (uint32_t)ci >> 4, off = win_off((uint32_t)f, (uint32_t)ci & 15u);
+            *reinterpret_cast<uint16_t*>(sB + (s * 3u + 0u) * (uint32_t)(N * 32) + off) = b0;
+            *reinterpret_cast<uint16_t*>(sB + (s * 3u + 1u) * (uint32_t)(N * 32) + off) = b1;
+            *reinterpret_cast<uint16_t*>(sB + (s * 3u + 2u) * (uint32_t)(N * 32) + off) = b2;
+            const int corner = win_corner_of_control((uint32_t)ci);
+            if (corner >= 0) sCorner[corner * kWinMaxN + f] = c;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        win_tc_fence_before();
+        __syncthreads();
+        win_tc_fence_after();
+        // 3. one thread issues the 48 MMAs and commits them to the barrier
+        if (tid == 0) {
+            for (uint32_t m = 0; m < 4u; ++m)
+                for (uint32_t s = 0; s < 4u; ++s) {
+                    const uint64_t ad = win_desc(win_smem_u32(sA + (m * 4u + s) * 4096u));
+                    for (uint32_t p = 0; p < 3u; ++p) {
+                        const uint64_t bd = win_desc(win_smem_u32(sB + (s * 3u + p) * (uint32_t)(N * 32)));
+                        win_mma(taddr + m * (uint32_t)N, ad, bd, idesc, (s | p) != 0u ? 1u : 0u);
+                    }
+                }
+            win_commit(bar);
+        }
+        // 4. wait for the products (bounded); a timeout stops the whole CTA after a second wait
+        const bool ok = mbar_wait(bar, phase);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) record_error(a.err, leaf, kErrWaitTimeout);
+            mbar_wait(bar, phase);
+            break;
+        }
+        phase ^= 1u;
+        win_tc_fence_after();
+        // 5. epilogue: warp w reads lanes 32 (w % 4) .. +31 (voxel rows), half of the columns;
+        //    voxels outside a boundary leaf's extent are 0, as in the per-frame cache
+        uint32_t gx, gy, gz;
+        int ew, eh, ed;
+        leaf_extent(a.g, leaf, gx, gy, gz, ew, eh, ed);
+        const uint32_t quarter = (uint32_t)(warp & 3), half = (uint32_t)(warp >> 2);
+        const uint32_t row = quarter * 32u + (uint32_t)lane;
+        const int cols_per_half = N / 2;
+        for (uint32_t m = 0; m < 4u; ++m) {
+            const uint32_t v = m * 128u + row;
+            const int corner = win_corner_of_voxel(v);
+            const bool inside = (int)(v & 7u) < ew && (int)((v >> 3) & 7u) < eh && (int)(v >> 6) < ed;
+            for (int c0 = (int)half * cols_per_half; c0 < (int)(half + 1) * cols_per_half; c0 += 16) {
+                float d[16];
+                win_ld16(taddr + ((quarter * 32u) << 16) + m * (uint32_t)N + (uint32_t)c0, d);
+#pragma unroll 4
+                for (int j = 0; j < 16; ++j) {
+                    const int f = c0 + j;
+                    if (f >= n) break;
+                    float val = d[j];
+                    if (corner >= 0) val = __fadd_rn(val, sCorner[corner * kWinMaxN + f]);
+                    val = __fmul_rn(val, 1.0f / 343.0f);
+                    if (mode == 1u) val = __fadd_rn(val, sci_sparse(rd, base, hdr, keep, v, (uint32_t)(t0 + f)));
+                    out[(uint64_t)f * frame_stride + (uint64_t)leaf * 512u + v] = inside ? val : 0.0f;
+                }
+            }
+        }
+        if (rd.oob) record_error(a.err, leaf, kErrDecodeOob);
+        win_tc_fence_before();
+        __syncthreads();   // D and the B tiles are free for the next leaf
+        win_tc_fence_after();
+    }
+    win_tc_fence_before();
+    __syncthreads();
+    win_tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kWinTmemCols) : "memory");
+}
+
+// FP64 error oracle of a window (any scientific output of frames [t0, t0 + n) in the cache
+// layout; voxels outside a boundary leaf's extent must be 0): per voxel and frame the reference
+// model evaluated in double -- the coarse controls
+// as sum_k q_k b_k(t) over the same FP32 coefficients and basis values, the trilinear weights as
+// the reference's FP32 t and 1 - t, both without rounding, plus the FP32 sparse residual -- and
+// the reduction stats[0] = max |value - oracle| (as ordered bits), stats[1] = sum of squares,
+// stats[2] / stats[3] = oracle min / max (as ordered bits), in double.
+__device__ __forceinline__ unsigned long long win_ordered(double x)
+{
+    const unsigned long long b = __double_as_longlong(x);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__global__ void __launch_bounds__(256) sci_window_oracle_kernel(DeviceAsset a, int t0, int n,
+                                                                const float* __restrict__ vals, uint64_t frame_stride,
+                                                                unsigned long long* stats)
+{
+    __shared__ double s_max[8], s_sum[8];
+    __shared__ unsigned long long s_lo[8], s_hi[8];
+    double my_max = 0.0, my_sum = 0.0;
+    unsigned long long my_lo = ~0ull, my_hi = 0ull;
+    const uint64_t items = (uint64_t)a.g.leaf_count * 512u;
+    for (uint64_t it = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+         it += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t leaf = (uint32_t)(it >> 9), v = (uint32_t)(it & 511u);
+        const LeafEntry e = a.entries[leaf];
+        const uint32_t hdr = e.header, mode = hdr & 3u;
+        if (entry_status(e) != kOk || mode >= 2u) continue;
+        const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
+        const uint64_t base = 4ull * e.word_off;
+        SciReader rd{a.payload, a.g.payload_words, false};
+        const uint32_t lx = v & 7u, ly = (v >> 3) & 7u, lz = v >> 6;
+        uint32_t gx, gy, gz;
+        int ew, eh, ed;
+        leaf_extent(a.g, leaf, gx, gy, gz, ew, eh, ed);
+        if ((int)lx >= ew || (int)ly >= eh || (int)lz >= ed) {   // outside the volume: the cache holds 0
+            for (int f = 0; f < n; ++f)
+                my_max = fmax(my_max, fabs((double)vals[(uint64_t)f * frame_stride + (uint64_t)leaf * 512u + v]));
+            continue;
+        }
+        const AxisWeight ax = c_sci_axis[0][lx], ay = c_sci_axis[0][ly], az = c_sci_axis[0][lz];
+        for (int f = 0; f < n; ++f) {
+            const uint32_t t = (uint32_t)(t0 + f);
+            const float* brow = a.basis + (uint64_t)t * 64u;
+            double ref = 0.0;
+            for (int cz = 0; cz < 2; ++cz)
+                for (int cy = 0; cy < 2; ++cy)
+                    for (int cx = 0; cx < 2; ++cx) {
+                        const int ci = ((cz ? az.i1 : az.i0) * 4 + (cy ? ay.i1 : ay.i0)) * 4 + (cx ? ax.i1 : ax.i0);
+                        const double w = (double)(cx ? ax.t : ax.omt) * (double)(cy ? ay.t : ay.omt) *
+                                         (double)(cz ? az.t : az.omt);
+                        const uint64_t cb = base + 4u + (uint64_t)ci * (keep + 1);
+                        double c = (double)half_bits_to_float(rd.u16(cb)) * (double)__ldg(brow);
+                        for (int k = 1; k < keep; ++k) {
+                            const float q = __fmul_rn((float)(int8_t)rd.byte(cb + 2u + (k - 1)), __ldg(a.scales + k - 1));
+                            c += (double)q * (double)__ldg(brow + k);
+                        }
+                        ref += w * c;
+                    }
+            if (mode == 1u) ref += (double)sci_sparse(rd, base, hdr, keep, v, t);
+            const double got = (double)vals[(uint64_t)f * frame_stride + (uint64_t)leaf * 512u + v];
+            const double err = fabs(got - ref);
+            my_max = fmax(my_max, err);
+            my_sum += err * err;
+            const unsigned long long o = win_ordered(ref);
+            my_lo = o < my_lo ? o : my_lo;
+            my_hi = o > my_hi ? o : my_hi;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        my_max = fmax(my_max, __shfl_down_sync(0xFFFFFFFFu, my_max, o));
+        my_sum += __shfl_down_sync(0xFFFFFFFFu, my_sum, o);
+        const unsigned long long lo2 = __shfl_down_sync(0xFFFFFFFFu, my_lo, o);
+        const unsigned long long hi2 = __shfl_down_sync(0xFFFFFFFFu, my_hi, o);
+        my_lo = lo2 < my_lo ? lo2 : my_lo;
+        my_hi = hi2 > my_hi ? hi2 : my_hi;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_max[warp] = my_max;
+        s_sum[warp] = my_sum;
+        s_lo[warp] = my_lo;
+        s_hi[warp] = my_hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0.0, sm = 0.0;
+        unsigned long long lo = ~0ull, hi = 0ull;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            mx = fmax(mx, s_max[w]);
+            sm += s_sum[w];
+            lo = s_lo[w] < lo ? s_lo[w] : lo;
+            hi = s_hi[w] > hi ? s_hi[w] : hi;
+        }
+        atomicMax(stats + 0, (unsigned long long)__double_as_longlong(mx));   // non-negative: bits order
+        atomicAdd(reinterpret_cast<double*>(stats + 1), sm);
+        atomicMin(stats + 2, lo);
+        atomicMax(stats + 3, hi);
+    }
+}
+
+void launch_sci_window(const DeviceAsset& a, int t0, int n, float* out, uint64_t frame_stride, cudaStream_t s)
+{
+    cudaFuncSetAttribute(sci_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWinSmem);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (int)(a.g.leaf_count < (uint32_t)(2 * sms) ? a.g.leaf_count : (uint32_t)(2 * sms));
+    sci_window_kernel<<<grid, kWinThreads, kWinSmem, s>>>(a, t0, n, out, frame_stride);
+}
+
+void launch_sci_window_oracle(const DeviceAsset& a, int t0, int n, const float* vals, uint64_t frame_stride,
+                              unsigned long long* stats, cudaStream_t s)
+{
+    cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), s);       // max, sum (0.0), -, max
+    cudaMemsetAsync(stats + 2, 0xFF, sizeof(unsigned long long), s);   // min starts at the top
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    sci_window_oracle_kernel<<<4 * sms, 256, 0, s>>>(a, t0, n, vals, frame_stride, stats);
+}
+
+}  // namespace vbtb

@@ -43,6 +43,7 @@ enum : uint32_t {
     kErrKeyRangeOob = 12,
     kErrKeyIndex = 13,
     kErrWaitTimeout = 30,
+    kErrUnsupported = 44,   // a leaf mode the call does not cover
 };
 
 // One 32-byte leaf-table row, written by the payload walker (kernel a) and read by every decode
