@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--no-window", action="store_true")
     p.add_argument("--serve-requests", type=int, default=300)
     return p.parse_args()
 
@@ -339,6 +340,58 @@ def run_serving(args, local_rank):
             "arrival_rates_req_per_s": {"0.8x_plain": lam_p, "0.8x_served": lam_s}}
 
 
+# ------------------------------------------------------------------------------ (d) precision
+WINDOW_ASSET = os.path.join(ROOT, "assets", "mix_sci.vbtp")
+
+
+def run_window(args, local_rank, reps=10):
+    """(d) on the scientific field (config-5 scene, 128^3 x 64): the whole 64-frame timeline as
+    one tensor-core window per leaf (vbt_decode_window) against the exact per-frame decode of the
+    same frames (vbt_decode_cache, 64 frames per launch); device time per timeline, and the error
+    of both against the FP64 oracle, relative to the field range."""
+    import torch
+    import vbt_b200 as vbt
+    path = WINDOW_ASSET if os.path.exists(WINDOW_ASSET) else os.path.join(ROOT, "assets", "sci_64.vbtp")
+    if not os.path.exists(path):
+        return {"skipped": "no scientific asset generated"}
+    a = vbt.Asset(path, device=local_rank)
+    T, L = a.frames, a.leaf_count
+    n = min(T, 64)
+    s = torch.cuda.Stream()
+    win = torch.empty((n, L, 512), dtype=torch.float32, device=f"cuda:{local_rank}")
+    ref = torch.empty_like(win)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=win.device)
+
+    def timed(fn):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        with torch.cuda.stream(s):
+            fn()
+            for e0, e1 in ev:
+                flush.zero_()
+                e0.record(s)
+                fn()
+                e1.record(s)
+        s.synchronize()
+        return statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+
+    win_ms = timed(lambda: a.decode_window(0, n, win, stream=s))
+    ref_ms = timed(lambda: a.decode_cache(list(range(n)), ref, frame_stride=L * 512, stream=s))
+    a.sync_status(s)
+    mx_w, rms_w, lo, hi = a.window_error(0, n, win, stream=s)
+    mx_r, rms_r, _, _ = a.window_error(0, n, ref, stream=s)
+    rng = hi - lo
+    vox = L * 512 * n
+    a.close()
+    return {"asset": os.path.basename(path), "frames": n, "leaves": L,
+            "tensor_core_window": {"ms_per_timeline": win_ms, "voxels_per_s": vox / (win_ms * 1e-3),
+                                   "max_abs_err_rel_range": mx_w / rng, "rms_err_rel_range": rms_w / rng,
+                                   "products": "split-BF16: exact S' x three BF16 terms of C, FP32 accumulate"},
+            "fp32_per_frame": {"ms_per_timeline": ref_ms, "voxels_per_s": vox / (ref_ms * 1e-3),
+                               "max_abs_err_rel_range": mx_r / rng, "rms_err_rel_range": rms_r / rng},
+            "oracle": "FP64 on the GPU (reference model without intermediate rounding), range "
+                      f"{lo:.6g} .. {hi:.6g}", "speedup": ref_ms / win_ms}
+
+
 # ------------------------------------------------------------------------------ arms
 def run_reference(args, rank, world):
     """The reference's own CPU decoder on the host cores, same metric and workload; each step is
@@ -506,6 +559,10 @@ def run_ours(args, rank, local_rank, world):
                "h2d_bytes_per_step": int(image.nbytes), "d2h_bytes_per_step": int(cache.numel() * 4),
                "ms_per_step": e2e_ms}
 
+    window = None
+    if rank == 0 and world == 1 and not args.no_window:
+        window = run_window(args, local_rank)
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         serving = run_serving(args, local_rank)
@@ -536,7 +593,7 @@ def run_ours(args, rank, local_rank, world):
                            "ms_per_frame": tuning.ms_per_frame, "ms_per_frame_untuned": tuning.ms_per_frame_default},
                 "plain": {"value": plain_value, "unit": "voxels/s", "ms_per_step": plain_ms,
                           "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
-                "cpu_baseline": cpu, "e2e": e2e, "serving": serving,
+                "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "precision_window": window,
                 "gpu_launches": args.steps * (1 + len(chunks)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)

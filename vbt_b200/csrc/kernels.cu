@@ -640,6 +640,60 @@ __device__ float sci_sparse(SciReader& rd, uint64_t base, uint32_t hdr, int keep
     return 0.0f;
 }
 
+// The frame-independent part of a SparseEvents leaf's residual (the same reads and checks as
+// sci_sparse, split so that a caller decoding many frames of one voxel reads them once).
+struct SparseLeaf {
+    uint64_t sb, bb;        // section base, bin table
+    float es;               // event scale (residuals are 0 unless es > 0)
+    uint32_t count, cap, fpb;
+};
+
+__device__ __forceinline__ SparseLeaf sparse_leaf(SciReader& rd, uint64_t base, uint32_t hdr, int keep)
+{
+    SparseLeaf s{};
+    s.count = (hdr >> 16) & 0x0FFFu;
+    const uint32_t tier = (hdr >> 8) & 3u;
+    s.cap = tier == 0u ? 64u : tier == 1u ? 256u : tier == 2u ? 768u : 1024u;
+    s.fpb = ((hdr >> 10) & 0xFu) + 1u;
+    s.sb = base + 4u + (uint64_t)(64 * (keep + 1));
+    s.bb = s.sb + 68u;
+    s.es = s.count ? __uint_as_float(rd.u32(s.sb)) : 0.0f;
+    return s;
+}
+
+// Mask word w (voxels 32w .. 32w+31) of a sparse leaf.
+__device__ __forceinline__ uint32_t sparse_mask_word(SciReader& rd, const SparseLeaf& s, uint32_t w)
+{
+    return rd.u32(s.sb + 4u + w * 4u);
+}
+
+// Residual of voxel li at frame t, for a voxel whose mask bit is set in a leaf with count > 0
+// and es > 0 (sci_sparse's remaining steps: bin range, binary search of the 16-bit keys).
+__device__ __forceinline__ float sparse_at(SciReader& rd, const SparseLeaf& s, uint32_t li, uint32_t t)
+{
+    const uint32_t bin = t / s.fpb < 15u ? t / s.fpb : 15u;
+    const uint32_t lt = (t - bin * s.fpb) & 0xFFu;
+    const uint32_t start = rd.u16(s.bb + bin * 2u);
+    const uint32_t end = bin + 1u < 16u ? rd.u16(s.bb + (bin + 1u) * 2u) : (s.count & 0xFFFFu);
+    if (start >= end) return 0.0f;
+    const uint64_t cb = s.bb + 32u, rb = cb + s.cap * 2u;
+    const uint32_t target = ((lt << 9) | (li & 0x1FFu)) & 0xFFFFu;
+    int left = (int)start, right = (int)end - 1;
+    while (left <= right) {
+        const int mid = (left + right) >> 1;
+        const uint32_t key = rd.u16(cb + (uint32_t)mid * 2u);
+        if (key == target) {
+            const uint32_t byte = rd.byte(rb + (uint32_t)(mid >> 1));
+            int q = (int)((mid & 1) == 0 ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
+            if (q & 8) q -= 16;
+            return __fmul_rn((float)q, s.es);
+        }
+        if (key < target) left = mid + 1;
+        else right = mid - 1;
+    }
+    return 0.0f;
+}
+
 // Warp-cooperative scientific leaf decode at frame t: controls into s_ctrl[0..64), the dense
 // residual grid(s) into s_ctrl[64..) (per-frame grid, or tkeep basis grids), then row values.
 __device__ void sci_decode_controls(const DeviceAsset& a, const LeafEntry& e, uint32_t t, float* __restrict__ s_ctrl,
@@ -694,6 +748,17 @@ __device__ __forceinline__ void sci_row(const DeviceAsset& a, const LeafEntry& e
     const uint32_t sub = (hdr >> 12) & 7u;
     const int tkeep = (int)((hdr >> 15) & 0xFu) + 1;
     const float* brow = a.basis + (uint64_t)t * 64u;
+    // sparse events: the section header and this row's mask word once (the row's 8 voxels share
+    // one 32-bit mask word); per voxel only the bin range and key search remain
+    SparseLeaf sp{};
+    uint32_t row_mask = 0u;
+    if (mode == 1u) {
+        sp = sparse_leaf(rd, base, hdr, keep);
+        if (sp.count && sp.es > 0.0f) {
+            const uint32_t li0 = (uint32_t)((lz * 8 + ly) * 8);
+            row_mask = (sparse_mask_word(rd, sp, li0 >> 5) >> (li0 & 31u)) & 0xFFu;
+        }
+    }
 #pragma unroll 1
     for (int lx = 0; lx < 8; ++lx) {
         float v = 0.0f;
@@ -701,7 +766,7 @@ __device__ __forceinline__ void sci_row(const DeviceAsset& a, const LeafEntry& e
             const float coarse = tri_small(s_ctrl, 4, c_sci_axis[0][lx], ay, az);
             float r = 0.0f;
             if (mode == 1u) {
-                r = sci_sparse(rd, base, hdr, keep, (uint32_t)((lz * 8 + ly) * 8 + lx), t);
+                if ((row_mask >> lx) & 1u) r = sparse_at(rd, sp, (uint32_t)((lz * 8 + ly) * 8 + lx), t);
             } else if (mode >= 2u) {
                 const AxisWeight dx = c_sci_axis[mode == 2u ? 1 : 2][lx];
                 const int per = res * res * res;

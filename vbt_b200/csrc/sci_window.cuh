@@ -30,7 +30,7 @@ constexpr uint32_t kWinA = 4u * 4u * 4096u;             // 4 M tiles x 4 K steps
 constexpr uint32_t kWinB = 4u * 3u * (kWinMaxN * 32u);  // 4 K steps x 3 terms x (64 rows x 32 B)
 constexpr uint32_t kWinCorner = 8u * kWinMaxN * 4u;     // corner controls x frames, FP32
 constexpr uint32_t kWinQ = 64u * 64u * 4u;              // 64 controls x keep (<= 64) coefficients
-constexpr uint32_t kWinSmem = kWinA + kWinB + kWinCorner + kWinQ + 64u;
+constexpr uint32_t kWinSmem = kWinA + kWinB + kWinCorner + kWinQ + 256u;   // + barrier, TMEM address, sparse header
 
 __device__ __forceinline__ uint32_t win_smem_u32(const void* p)
 {
@@ -133,6 +133,9 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
     float* sQ = reinterpret_cast<float*>(wdyn + kWinA + kWinB + kWinCorner);
     uint64_t* bar = reinterpret_cast<uint64_t*>(wdyn + kWinA + kWinB + kWinCorner + kWinQ);
     uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
+    SparseLeaf* s_sparse = reinterpret_cast<SparseLeaf*>(bar + 2);                 // 40 bytes
+    uint32_t* s_mask = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(bar) + 64);   // 16 words
+    uint32_t* s_bin = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(bar) + 128);   // 16 bin starts
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int N = (n + 15) & ~15;
 
@@ -182,8 +185,34 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
             sQ[i] = k == 0 ? half_bits_to_float(rd.u16(cb))
                            : __fmul_rn((float)(int8_t)rd.byte(cb + 2u + (k - 1)), __ldg(a.scales + k - 1));
         }
+        // the sparse section's header and occupancy mask, once per leaf
+        if (mode == 1u && tid < 16) {
+            const SparseLeaf sp = sparse_leaf(rd, base, hdr, keep);
+            const bool any = sp.count && sp.es > 0.0f;
+            s_mask[tid] = any ? sparse_mask_word(rd, sp, (uint32_t)tid) : 0u;
+            s_bin[tid] = any ? rd.u16(sp.bb + 2u * (uint32_t)tid) : 0u;
+            if (tid == 0) *s_sparse = sp;
+        }
         if (rd.oob) record_error(a.err, leaf, kErrDecodeOob);
         __syncthreads();
+        // Events can be scattered onto their (frame, voxel) when every bin's keys strictly increase
+        // (the reference's binary search then finds a key exactly when it is present); otherwise
+        // each voxel with events searches per frame, as the reference does.
+        bool scatter = false;
+        if (mode == 1u) {
+            const SparseLeaf sp = *s_sparse;
+            bool bad = false;
+            if (sp.count && sp.es > 0.0f) {
+                for (uint32_t b = 0; b < 16u; ++b) {
+                    const uint32_t st0 = s_bin[b], en = b < 15u ? s_bin[b + 1] : (sp.count & 0xFFFFu);
+                    if (st0 >= en) continue;
+                    if (en > sp.cap) bad = true;
+                    for (uint32_t e = st0 + (uint32_t)tid; e + 1u < en && !bad; e += kWinThreads)
+                        bad = rd.u16(sp.bb + 32u + 2u * e) >= rd.u16(sp.bb + 32u + 2u * (e + 1u));
+                }
+            }
+            scatter = !__syncthreads_or(bad) && sp.count && sp.es > 0.0f;
+        }
         // 2. C[f][ci] (compensated FP32 sum), split into three BF16 terms, B tiles and corners
         for (int i = tid; i < 64 * N; i += kWinThreads) {
             const int ci = i & 63, f = i >> 6;
@@ -247,18 +276,48 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
             const uint32_t v = m * 128u + row;
             const int corner = win_corner_of_voxel(v);
             const bool inside = (int)(v & 7u) < ew && (int)((v >> 3) & 7u) < eh && (int)(v >> 6) < ed;
+            const bool events = mode == 1u && !scatter && ((s_mask[v >> 5] >> (v & 31u)) & 1u) != 0u;
             for (int c0 = (int)half * cols_per_half; c0 < (int)(half + 1) * cols_per_half; c0 += 16) {
                 float d[16];
                 win_ld16(taddr + ((quarter * 32u) << 16) + m * (uint32_t)N + (uint32_t)c0, d);
-#pragma unroll 4
+#pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const int f = c0 + j;
-                    if (f >= n) break;
-                    float val = d[j];
-                    if (corner >= 0) val = __fadd_rn(val, sCorner[corner * kWinMaxN + f]);
-                    val = __fmul_rn(val, 1.0f / 343.0f);
-                    if (mode == 1u) val = __fadd_rn(val, sci_sparse(rd, base, hdr, keep, v, (uint32_t)(t0 + f)));
-                    out[(uint64_t)f * frame_stride + (uint64_t)leaf * 512u + v] = inside ? val : 0.0f;
+                    if (f < n) {
+                        float val = d[j];
+                        if (corner >= 0) val = __fadd_rn(val, sCorner[corner * kWinMaxN + f]);
+                        val = __fmul_rn(val, 1.0f / 343.0f);
+                        if (mode == 1u)
+                            val = __fadd_rn(val, events ? sparse_at(rd, *s_sparse, v, (uint32_t)(t0 + f)) : 0.0f);
+                        out[(uint64_t)f * frame_stride + (uint64_t)leaf * 512u + v] = inside ? val : 0.0f;
+                    }
+                }
+            }
+        }
+        // 6. scattered events: each event key (lt << 9 | voxel) of bin b adds q * es to the frames
+        //    whose search would find it -- b * fpb + lt for b < 15 (lt < fpb), and for the last
+        //    bin every frame 15 * fpb + lt + 128 j (the search key keeps 7 bits of the local time)
+        if (scatter) {
+            __syncthreads();   // this leaf's coarse values are written
+            const SparseLeaf sp = *s_sparse;
+            const uint64_t cb = sp.bb + 32u, rb = cb + sp.cap * 2u;
+            for (uint32_t b = 0; b < 16u; ++b) {
+                const uint32_t st0 = s_bin[b], en = b < 15u ? s_bin[b + 1] : (sp.count & 0xFFFFu);
+                for (uint32_t e = st0 + (uint32_t)tid; e < en; e += kWinThreads) {
+                    const uint32_t key = rd.u16(cb + 2u * e);
+                    const uint32_t lt = key >> 9, li = key & 511u;
+                    if ((int)(li & 7u) >= ew || (int)((li >> 3) & 7u) >= eh || (int)(li >> 6) >= ed) continue;
+                    const uint32_t byte = rd.byte(rb + (e >> 1));
+                    int q = (int)((e & 1u) == 0u ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
+                    if (q & 8) q -= 16;
+                    const float r = __fmul_rn((float)q, sp.es);
+                    uint32_t t = b * sp.fpb + lt;
+                    if (b < 15u && lt >= sp.fpb) continue;
+                    for (; t < a.g.frames; t += (b < 15u ? a.g.frames : 128u)) {
+                        if (t < (uint32_t)t0 || t >= (uint32_t)(t0 + n)) continue;
+                        float* o = out + (uint64_t)(t - (uint32_t)t0) * frame_stride + (uint64_t)leaf * 512u + li;
+                        *o = __fadd_rn(*o, r);
+                    }
                 }
             }
         }
