@@ -281,9 +281,12 @@ __global__ void __launch_bounds__(256) key_order_kernel(DeviceAsset a)
     }
 }
 
+static void launch_sci_event_order(const DeviceAsset& a, cudaStream_t s);
+
 void launch_key_order(const DeviceAsset& a, cudaStream_t s)
 {
-    key_order_kernel<<<(a.g.leaf_count + 7) / 8, 256, 0, s>>>(a);
+    if (a.g.profile == 2u) launch_sci_event_order(a, s);
+    else key_order_kernel<<<(a.g.leaf_count + 7) / 8, 256, 0, s>>>(a);
 }
 
 // Scientific leaves: every leaf is active.  The decoder reads through bounds-checked accessors
@@ -694,6 +697,78 @@ __device__ __forceinline__ float sparse_at(SciReader& rd, const SparseLeaf& s, u
     return 0.0f;
 }
 
+// Scientific leaves: kFlagSorted marks a SparseEvents leaf whose event keys strictly increase
+// within every bin range (and whose ranges stay inside the key table).  The reference finds an
+// event by binary search per voxel and frame (render/src/scientific_decode.cpp:235-295); on such a
+// leaf the search finds a key exactly when it is present, so decoders may instead visit the
+// events of a frame's bin and add each to its voxel.  One warp per leaf, at load and upload.
+__global__ void __launch_bounds__(256) sci_event_order_kernel(DeviceAsset a)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t leaf = blockIdx.x * 8u + (threadIdx.x >> 5);
+    if (leaf >= a.g.leaf_count) return;
+    LeafEntry& e = a.entries[leaf];
+    const uint32_t info = e.info, hdr = e.header;
+    bool sorted = entry_status(e) == kOk && (hdr & 3u) == 1u;
+    if (sorted) {
+        SciReader rd{a.payload, a.g.payload_words, false};
+        const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
+        const SparseLeaf sp = sparse_leaf(rd, 4ull * e.word_off, hdr, keep);
+        bool ok = true;
+        if (sp.count && sp.es > 0.0f) {
+            for (uint32_t b = 0; b < 16u; ++b) {
+                const uint32_t st0 = rd.u16(sp.bb + 2u * b);
+                const uint32_t en = b < 15u ? rd.u16(sp.bb + 2u * (b + 1u)) : (sp.count & 0xFFFFu);
+                if (st0 >= en) continue;
+                if (en > sp.cap) ok = false;
+                for (uint32_t i = st0 + (uint32_t)lane; i + 1u < en && ok; i += 32u)
+                    ok = rd.u16(sp.bb + 32u + 2u * i) < rd.u16(sp.bb + 32u + 2u * (i + 1u));
+            }
+        }
+        sorted = __all_sync(0xFFFFFFFFu, ok && !rd.oob);
+    }
+    if (lane == 0) {
+        a.key_sorted[leaf] = sorted ? 1 : 0;
+        if (sorted) e.info = info | kFlagSorted;
+    }
+}
+
+static void launch_sci_event_order(const DeviceAsset& a, cudaStream_t s)
+{
+    sci_event_order_kernel<<<(a.g.leaf_count + 7) / 8, 256, 0, s>>>(a);
+}
+
+// Add the events of frame t to the voxels of one SparseEvents leaf with kFlagSorted (one warp;
+// the voxels' coarse values are already written).  dst(li) is the voxel's output address.
+template <class Dst>
+__device__ __forceinline__ void sci_scatter_frame(const DeviceAsset& a, const LeafEntry& e, uint32_t t, int w, int h,
+                                                  int d, int lane, Dst dst, bool& oob)
+{
+    SciReader rd{a.payload, a.g.payload_words, false};
+    const uint32_t hdr = e.header;
+    const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
+    const SparseLeaf sp = sparse_leaf(rd, 4ull * e.word_off, hdr, keep);
+    if (sp.count && sp.es > 0.0f) {
+        const uint32_t bin = t / sp.fpb < 15u ? t / sp.fpb : 15u;
+        const uint32_t lt7 = (t - bin * sp.fpb) & 0x7Fu;   // the search key keeps 7 bits of it
+        const uint32_t st0 = rd.u16(sp.bb + bin * 2u);
+        const uint32_t en = bin + 1u < 16u ? rd.u16(sp.bb + (bin + 1u) * 2u) : (sp.count & 0xFFFFu);
+        const uint64_t cb = sp.bb + 32u, rb = cb + sp.cap * 2u;
+        for (uint32_t i = st0 + (uint32_t)lane; i < en; i += 32u) {
+            const uint32_t key = rd.u16(cb + 2u * i);
+            if ((key >> 9) != lt7) continue;
+            const uint32_t li = key & 511u;
+            if ((int)(li & 7u) >= w || (int)((li >> 3) & 7u) >= h || (int)(li >> 6) >= d) continue;
+            const uint32_t byte = rd.byte(rb + (i >> 1));
+            int q = (int)((i & 1u) == 0u ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
+            if (q & 8) q -= 16;
+            float* o = dst(li);
+            *o = __fadd_rn(*o, __fmul_rn((float)q, sp.es));
+        }
+    }
+    oob |= rd.oob;
+}
+
 // Warp-cooperative scientific leaf decode at frame t: controls into s_ctrl[0..64), the dense
 // residual grid(s) into s_ctrl[64..) (per-frame grid, or tkeep basis grids), then row values.
 __device__ void sci_decode_controls(const DeviceAsset& a, const LeafEntry& e, uint32_t t, float* __restrict__ s_ctrl,
@@ -733,8 +808,10 @@ __device__ void sci_decode_controls(const DeviceAsset& a, const LeafEntry& e, ui
     oob = rd.oob;
 }
 
+// skip_events: the sparse-event residual is left out (added by sci_scatter_frame afterwards).
 __device__ __forceinline__ void sci_row(const DeviceAsset& a, const LeafEntry& e, const float* __restrict__ s_ctrl,
-                                        uint32_t t, int w, int h, int d, int ly, int lz, float out[8], bool& oob)
+                                        uint32_t t, int w, int h, int d, int ly, int lz, float out[8], bool& oob,
+                                        bool skip_events = false)
 {
     SciReader rd{a.payload, a.g.payload_words, false};
     const uint64_t base = 4ull * e.word_off;
@@ -752,7 +829,7 @@ __device__ __forceinline__ void sci_row(const DeviceAsset& a, const LeafEntry& e
     // one 32-bit mask word); per voxel only the bin range and key search remain
     SparseLeaf sp{};
     uint32_t row_mask = 0u;
-    if (mode == 1u) {
+    if (mode == 1u && !skip_events) {
         sp = sparse_leaf(rd, base, hdr, keep);
         if (sp.count && sp.es > 0.0f) {
             const uint32_t li0 = (uint32_t)((lz * 8 + ly) * 8);
@@ -815,6 +892,9 @@ __global__ void __launch_bounds__(kDecodeWarps * 32, 2) decode_kernel(DeviceAsse
         const bool empty = !SCI && (e.header & 3u) == kModeEmpty;
         const uint32_t st = entry_status(e);
         if (st != kOk && lane == 0) record_error(a.err, leaf, st);
+        // scientific SparseEvents leaves with sorted keys: events are added by visiting the
+        // frame's bin after the rows are written, instead of one search per voxel
+        const bool scatter = SCI && st == kOk && (e.header & 3u) == 1u && (e.info & kFlagSorted) != 0u;
         for (int fi = 0; fi < fl.n; ++fi) {
             const int frame = clamp_frame(fl.f[fi], (int)a.g.frames);
             bool oob = false;
@@ -830,7 +910,7 @@ __global__ void __launch_bounds__(kDecodeWarps * 32, 2) decode_kernel(DeviceAsse
 #pragma unroll
                     for (int i = 0; i < 8; ++i) v[i] = 0.0f;
                 } else if (SCI) {
-                    sci_row(a, e, s_ctrl, (uint32_t)fl.f[fi], w, h, d, ly, lz, v, oob);
+                    sci_row(a, e, s_ctrl, (uint32_t)fl.f[fi], w, h, d, ly, lz, v, oob, scatter);
                 } else {
                     rt_row(a, e, s_ctrl, w, h, d, ly, lz, v);
                 }
@@ -849,6 +929,22 @@ __global__ void __launch_bounds__(kDecodeWarps * 32, 2) decode_kernel(DeviceAsse
                     float4* dst = reinterpret_cast<float4*>(out + (uint64_t)fi * frame_stride + (uint64_t)item * 512u + r * 8);
                     dst[0] = make_float4(v[0], v[1], v[2], v[3]);
                     dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+                }
+            }
+            if (scatter && (uint32_t)fl.f[fi] < a.g.frames) {
+                __syncwarp();   // the rows written by the other lanes are visible
+                if (DENSE) {
+                    float* fb = out + (uint64_t)fi * frame_stride;
+                    sci_scatter_frame(a, e, (uint32_t)fl.f[fi], w, h, d, lane,
+                                      [&](uint32_t li) {
+                                          return fb + ((uint64_t)(bz * 8 + (li >> 6)) * a.g.height +
+                                                       (by * 8 + ((li >> 3) & 7u))) * a.g.width + bx * 8 + (li & 7u);
+                                      },
+                                      oob);
+                } else {
+                    float* fb = out + (uint64_t)fi * frame_stride + (uint64_t)item * 512u;
+                    sci_scatter_frame(a, e, (uint32_t)fl.f[fi], w, h, d, lane, [&](uint32_t li) { return fb + li; },
+                                      oob);
                 }
             }
             if (__any_sync(0xFFFFFFFFu, oob) && lane == 0) record_error(a.err, leaf, kErrDecodeOob);

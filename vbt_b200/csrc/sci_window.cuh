@@ -195,24 +195,10 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
         }
         if (rd.oob) record_error(a.err, leaf, kErrDecodeOob);
         __syncthreads();
-        // Events can be scattered onto their (frame, voxel) when every bin's keys strictly increase
-        // (the reference's binary search then finds a key exactly when it is present); otherwise
-        // each voxel with events searches per frame, as the reference does.
-        bool scatter = false;
-        if (mode == 1u) {
-            const SparseLeaf sp = *s_sparse;
-            bool bad = false;
-            if (sp.count && sp.es > 0.0f) {
-                for (uint32_t b = 0; b < 16u; ++b) {
-                    const uint32_t st0 = s_bin[b], en = b < 15u ? s_bin[b + 1] : (sp.count & 0xFFFFu);
-                    if (st0 >= en) continue;
-                    if (en > sp.cap) bad = true;
-                    for (uint32_t e = st0 + (uint32_t)tid; e + 1u < en && !bad; e += kWinThreads)
-                        bad = rd.u16(sp.bb + 32u + 2u * e) >= rd.u16(sp.bb + 32u + 2u * (e + 1u));
-                }
-            }
-            scatter = !__syncthreads_or(bad) && sp.count && sp.es > 0.0f;
-        }
+        // Events are scattered onto their (frame, voxel) on leaves whose keys strictly increase
+        // within every bin (kFlagSorted, set at load); otherwise each voxel with events searches
+        // per frame, as the reference does.
+        const bool scatter = mode == 1u && (e.info & kFlagSorted) != 0u && s_sparse->count && s_sparse->es > 0.0f;
         // 2. C[f][ci] (compensated FP32 sum), split into three BF16 terms, B tiles and corners
         for (int i = tid; i < 64 * N; i += kWinThreads) {
             const int ci = i & 63, f = i >> 6;
