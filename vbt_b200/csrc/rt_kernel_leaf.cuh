@@ -202,6 +202,57 @@ __device__ __forceinline__ uint32_t grab_leaf(unsigned long long* slot, uint32_t
     return 0xFFFFFFFFu;
 }
 
+// Dense frames, EMPTY leaves: zero their segments of every output row (row = (frame, z, y), y
+// fastest), one row per group of per_row threads, rows grid-strided.  This runs as its own
+// full-occupancy launch before the leaf decode, which then visits only the active leaves: the
+// stores of the zero fill are bandwidth-bound and need many warps in flight, the leaf decode is
+// latency-bound with 16 warps per SM.  An inactive leaf with a walker status records it (once).
+__global__ void __launch_bounds__(256) zero_empty_kernel(DeviceAsset a, float* __restrict__ out,
+                                                         uint64_t frame_stride, uint32_t nframes)
+{
+    const uint32_t X = a.g.width, Y = a.g.height, Z = a.g.depth;
+    const uint64_t rows = (uint64_t)nframes * Z * Y;
+    const bool vec = (X & 3u) == 0u && (reinterpret_cast<uintptr_t>(out) & 15u) == 0u && (frame_stride & 3u) == 0u;
+    const uint32_t per_row = vec ? X >> 2 : X;
+    const uint32_t group = per_row >= 256u ? 1u : 256u / per_row;
+    const uint32_t k = threadIdx.x / per_row;
+    if (k >= group) return;
+    const uint32_t u0 = threadIdx.x - k * per_row, ustep = group == 1u ? 256u : per_row;
+    // a contiguous block of rows per CTA: one division to place the thread's first row, then the
+    // (frame, z, y) coordinates are carried forward
+    const uint64_t per_cta = (rows + gridDim.x - 1) / gridDim.x;
+    const uint64_t rb = (uint64_t)blockIdx.x * per_cta;
+    const uint64_t re = rows < rb + per_cta ? rows : rb + per_cta;
+    if (rb + k >= re) return;
+    const uint64_t zy_n = (uint64_t)Z * Y;
+    uint32_t fi = (uint32_t)((rb + k) / zy_n);
+    const uint32_t zy = (uint32_t)(rb + k - (uint64_t)fi * zy_n);
+    uint32_t z = zy / Y, y = zy - z * Y;
+    for (uint64_t r = rb + k; r < re; r += group) {
+        const uint32_t lrow = ((z >> 3) * a.g.lcy + (y >> 3)) * a.g.lcx;
+        float* row = out + (uint64_t)fi * frame_stride + ((uint64_t)z * Y + y) * X;
+        for (uint32_t u = u0; u < per_row; u += ustep) {
+            const uint32_t x = vec ? 4u * u : u;
+            const uint32_t leaf = lrow + (x >> 3);
+            if (__ldg(a.compact + leaf) != kNoRank) continue;
+            if (fi == 0u && ((x | y | z) & 7u) == 0u) {
+                const uint32_t st = entry_status(a.entries[leaf]);
+                if (st != kOk) record_error(a.err, leaf, st);
+            }
+            if (vec) *reinterpret_cast<float4*>(row + x) = make_float4(0.f, 0.f, 0.f, 0.f);
+            else row[x] = 0.0f;
+        }
+        y += group;
+        while (y >= Y) {
+            y -= Y;
+            if (++z == Z) {
+                z = 0;
+                ++fi;
+            }
+        }
+    }
+}
+
 // GLOBAL_FALLBACK: leaves whose window exceeds the stage are decoded from global memory (only
 // instantiated for assets that have such leaves; it costs registers).
 // Leaves are handed out dynamically (grab_leaf), one at a time per CTA, so that CTAs that drew
@@ -216,7 +267,8 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
     uint32_t* const s_next = reinterpret_cast<uint32_t*>(dyn + 8);   // beside the 8-byte barrier
     const int tid = threadIdx.x;
     const int total = (int)a.g.frames;
-    const uint32_t n_leaves = DENSE ? a.g.leaf_count : *(volatile const uint32_t*)a.counters;
+    // the active leaves by rank (dense frames: EMPTY leaves are zeroed by zero_empty_kernel)
+    const uint32_t n_leaves = *(volatile const uint32_t*)a.counters;
     if (tid == 0) {
         mbar_init(s.bar, 1);
         mbar_init_fence();
@@ -240,10 +292,11 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
     while (li < n_leaves) {
         // every thread has read li, and the previous leaf's shared-memory reads are complete
         __syncthreads();
-        const uint32_t leaf = DENSE ? li : __ldg(a.active_list + li);
+        const uint32_t rank = li;
+        const uint32_t leaf = __ldg(a.active_list + rank);
         const LeafEntry e = a.entries[leaf];
         LeafGeom G;
-        G.li = li;
+        G.li = rank;
         leaf_extent(a.g, leaf, G.bx, G.by, G.bz, G.w, G.h, G.d);
         const uint32_t st = entry_status(e);
         const uint64_t b0 = 4ull * e.word_off;
@@ -315,6 +368,12 @@ static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameL
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
         cudaMemsetAsync(slot, 0, sizeof(unsigned long long), s);
+    if (DENSE) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        zero_empty_kernel<<<8 * sms, 256, 0, s>>>(a, out, stride, (uint32_t)fl.n);
+    }
     decode_leaf_kernel<DENSE, GF><<<g, kLeafThreads, smem, s>>>(a, fl, out, stride, slot, seq + 1u);
 }
 
