@@ -1,6 +1,6 @@
 """Build libvbt_b200.so in-tree: every CUDA source compiled for sm_100a only.
 
-    python -m vbt_b200.build            # or: python vbt_b200/build.py
+    python vbt_b200/build.py
 
 Device code is compiled with --fmad=false as a safety net (the decode arithmetic already uses
 explicitly rounded _rn intrinsics), IEEE division and square root, and -lineinfo for ncu.

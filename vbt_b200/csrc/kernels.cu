@@ -14,6 +14,8 @@
 // double accumulation (render/src/scientific_decode.cpp:82-97) without FP64 on the device.
 #include <cuda/atomic>
 
+#include <mutex>
+
 #include "kernels.cuh"
 #include "rt_decode.cuh"
 

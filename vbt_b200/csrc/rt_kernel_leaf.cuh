@@ -345,6 +345,16 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
     }
 }
 
+// One non-blocking side stream per device for the dense zero fill (created on first use, with
+// the device current; kept for the process).
+static cudaStream_t dense_side_stream(int dev)
+{
+    static std::once_flag once[64];
+    static cudaStream_t streams[64];
+    std::call_once(once[dev & 63], [&] { cudaStreamCreateWithFlags(&streams[dev & 63], cudaStreamNonBlocking); });
+    return streams[dev & 63];
+}
+
 template <bool DENSE, bool GF>
 static int leaf_grid(uint32_t smem_bytes)
 {
@@ -369,10 +379,26 @@ static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameL
     if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
         cudaMemsetAsync(slot, 0, sizeof(unsigned long long), s);
     if (DENSE) {
+        // The zero fill (bandwidth-bound, small CTAs) runs beside the leaf decode (latency-bound)
+        // on a side stream: fork and join through events on the caller's stream, the decode given
+        // one CTA per SM so that zero-fill CTAs fit beside it.  The two write disjoint segments.
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        zero_empty_kernel<<<8 * sms, 256, 0, s>>>(a, out, stride, (uint32_t)fl.n);
+        cudaStream_t side = dense_side_stream(dev);
+        cudaEvent_t fork = nullptr, join = nullptr;
+        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+        cudaEventRecord(fork, s);
+        cudaStreamWaitEvent(side, fork, 0);
+        zero_empty_kernel<<<8 * sms, 256, 0, side>>>(a, out, stride, (uint32_t)fl.n);
+        cudaEventRecord(join, side);
+        decode_leaf_kernel<DENSE, GF><<<grid > 0 ? grid : sms, kLeafThreads, smem, s>>>(a, fl, out, stride, slot,
+                                                                                         seq + 1u);
+        cudaStreamWaitEvent(s, join, 0);
+        cudaEventDestroy(fork);
+        cudaEventDestroy(join);
+        return;
     }
     decode_leaf_kernel<DENSE, GF><<<g, kLeafThreads, smem, s>>>(a, fl, out, stride, slot, seq + 1u);
 }
