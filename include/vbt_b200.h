@@ -165,6 +165,14 @@ int vbt_decode_window(vbt_asset* asset, int t0, int n, float* d_out, uint64_t fr
 int vbt_window_error(vbt_asset* asset, int t0, int n, const float* d_values, uint64_t frame_stride, double* stats,
                      void* stream);
 
+/* Self-test, no counterpart in the reference.  The render decode forms the interpolation weight
+ * (t - f0) / (f1 - f0) of src/render_temporal_decode.cpp:129-130 without a division: one
+ * reciprocal per key interval and a Markstein correction per frame.  This compares that quotient
+ * with IEEE division on `device` for every integer pair 0 < a < b <= b_max (b_max <= 65535, the
+ * widest key-frame span).  result[0] = mismatches, result[1] = smallest failing (b << 16 | a), or
+ * all ones when there is none.  Synchronous. */
+int vbt_selftest_key_division(uint32_t b_max, uint64_t* result, int device);
+
 /* ---- Batched timeline: autotuned, graph-captured ---------------------------------------------
  * No counterpart in the reference.  The current-frame cache of a frame range is a page-table build
  * plus one decode launch per `frames_per_launch` frames.  The launch shape (leaf per CTA: the

@@ -97,6 +97,7 @@ _sig = {
                                    C.c_int, _vp, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
     "vbt_build_page_table_noalloc": ([_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp], C.c_int),
     "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
+    "vbt_selftest_key_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_window_error": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, C.POINTER(C.c_double), _vp], C.c_int),
     "vbt_autotune_cache": ([_vp, C.c_int, _vp, C.c_uint64, C.POINTER(Tuning), _vp], C.c_int),
     "vbt_set_tuning": ([_vp, C.POINTER(Tuning)], C.c_int),
@@ -315,6 +316,14 @@ class Asset:
     def decode_frames_host(self, frames, out, stream=None):
         fr = (C.c_int32 * len(frames))(*frames)
         _check(_lib.vbt_decode_frames_host(self._h, fr, len(frames), out.ctypes.data, _stream(stream)))
+
+
+def selftest_key_division(b_max=65535, device=0):
+    """(mismatches, smallest failing b << 16 | a) of the render decode's division-free interval
+    quotient against IEEE division, over every 0 < a < b <= b_max."""
+    r = (C.c_uint64 * 2)()
+    _check(_lib.vbt_selftest_key_division(b_max, r, device))
+    return int(r[0]), int(r[1])
 
 
 def build_page_table_noalloc(d_offsets, d_payload, payload_words, leaf_count, profile_type, d_compact,

@@ -251,7 +251,7 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
             maxw = std::max(maxw, a1 - a0);
         }
         g.max_window = (uint32_t)std::min<uint64_t>(maxw, 0xFFFFFFFFull);
-        const uint32_t cap = ((233472u / 2u - 1024u - kLeafFixedBytes) / 1024u) * 1024u;
+        const uint32_t cap = ((233472u / 2u - 1024u - kLeafFixedBytes - 16u) / 1024u) * 1024u;
         g.stage_bytes = std::min<uint32_t>(std::max<uint32_t>((g.max_window + 1023u) & ~1023u, 4096u), cap);
     }
     const uint32_t L = h.leaf_count;
@@ -589,6 +589,32 @@ int vbt_window_error(vbt_asset* a, int t0, int n, const float* d_values, uint64_
     stats[1] = std::sqrt(sum / count);
     stats[2] = unorder(raw[2]);
     stats[3] = unorder(raw[3]);
+    return VBT_STATUS_OK;
+}
+
+int vbt_selftest_key_division(uint32_t b_max, uint64_t* result, int device)
+{
+    if (!result) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    if (b_max < 2u || b_max > 65535u) return fail(VBT_STATUS_INVALID_ARGUMENT, "b_max must lie in [2, 65535]");
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        return fail(VBT_STATUS_CUDA, "no CUDA device");
+    if (device < 0 || device >= dev_count) return fail(VBT_STATUS_INVALID_ARGUMENT, "device out of range");
+    DeviceGuard guard(device);
+    unsigned long long* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+    const unsigned long long init[2] = {0ull, ~0ull};
+    cudaError_t e = cudaMemcpy(d, init, sizeof(init), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        launch_key_division_check(b_max, d, nullptr);
+        e = cudaGetLastError();
+    }
+    unsigned long long h[2] = {0ull, 0ull};
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(VBT_STATUS_CUDA, std::string("key division check: ") + cudaGetErrorString(e));
+    result[0] = h[0];
+    result[1] = h[1];
     return VBT_STATUS_OK;
 }
 

@@ -1286,6 +1286,34 @@ void launch_query_slice(const DeviceAsset& a, uint32_t z, int t0, int t1, float*
     query_slice_kernel<<<default_grid(), kDecodeWarps * 32, 0, s>>>(a, z, t0, t1, out);
 }
 
+// Exhaustive check of div_small_rn (the render decode's interval quotient) against IEEE division:
+// every pair 0 < a < b <= b_max, with RN(1/b) as the decode forms it.  Counts mismatches and keeps
+// the smallest failing (b << 16 | a).
+__global__ void key_division_check_kernel(uint32_t b_max, unsigned long long* bad, unsigned long long* first)
+{
+    unsigned long long local = 0;
+    for (uint32_t b = 2u + blockIdx.x; b <= b_max; b += gridDim.x) {
+        const float bf = (float)b;
+        const float y = __frcp_rn(bf);
+        for (uint32_t a = 1u + threadIdx.x; a < b; a += blockDim.x) {
+            const float q = div_small_rn((float)a, bf, y);
+            if (__float_as_uint(q) != __float_as_uint(__fdiv_rn((float)a, bf))) {
+                ++local;
+                atomicMin(first, ((unsigned long long)b << 16) | a);
+            }
+        }
+    }
+    if (local) atomicAdd(bad, local);
+}
+
+void launch_key_division_check(uint32_t b_max, unsigned long long* d_out, cudaStream_t s)
+{
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    key_division_check_kernel<<<8 * (sms > 0 ? sms : 1), 256, 0, s>>>(b_max, d_out, d_out + 1);
+}
+
 }  // namespace vbtb
 
 // (d) window decode of scientific leaves on the tensor cores: sci_window.cuh

@@ -40,7 +40,7 @@ constexpr uint32_t kWorkSlots = 64;
 
 // Fixed shared memory of the render decode kernel besides its leaf stage (rt_kernel_leaf.cuh:
 // barrier, frame tables, axis weights, 8 warps x (x-lerp + y-lerp rows), 3072-float controls).
-constexpr uint32_t kLeafFixedBytes = 16 + 256 + 128 + 576 + 8 * 196 * 8 + 8 * 112 * 16 + 3072 * 4;
+constexpr uint32_t kLeafFixedBytes = 16 + 256 + 128 + 576 + 8 * 196 * 8 + 8 * 112 * 16 + 3072 * 4 + 256 * 4;
 
 constexpr int kWalkThreads = 256;
 constexpr int kWalkTile = 256;   // leaves per walker CTA (one scan element per thread)
@@ -72,6 +72,7 @@ int decode_warp_grid();
 void launch_sci_window(const DeviceAsset& a, int t0, int n, float* out, uint64_t frame_stride, cudaStream_t s);
 // FP64 oracle of a scientific window: stats[0] max |err| (double bits), stats[1] sum err^2
 // (double), stats[2] / stats[3] oracle min / max (order-preserving bits).
+void launch_key_division_check(uint32_t b_max, unsigned long long* d_out, cudaStream_t s);
 void launch_sci_window_oracle(const DeviceAsset& a, int t0, int n, const float* vals, uint64_t frame_stride,
                               unsigned long long* stats, cudaStream_t s);
 // Plain path: one CTA per leaf of the whole leaf grid, one frame per launch (the reference

@@ -51,9 +51,9 @@ __device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t, float2 omt
 // src/render_temporal_decode.cpp:167-199 maps them.
 __device__ __forceinline__ float half_to_float_exact(uint32_t h)
 {
-    if ((h & 0x7C00u) == 0x7C00u && (h & 0x3FFu) != 0u)
-        return __uint_as_float(((h & 0x8000u) << 16) | 0x7F800000u | ((h & 0x3FFu) << 13));
-    return __half2float(__ushort_as_half((unsigned short)h));
+    const float f = __half2float(__ushort_as_half((unsigned short)h));
+    const bool nan = (h & 0x7C00u) == 0x7C00u && (h & 0x3FFu) != 0u;
+    return nan ? __uint_as_float(((h & 0x8000u) << 16) | 0x7F800000u | ((h & 0x3FFu) << 13)) : f;
 }
 
 __device__ __forceinline__ void key_read_v2(const uint32_t* __restrict__ pw, uint64_t kb, uint32_t codec, uint32_t i,

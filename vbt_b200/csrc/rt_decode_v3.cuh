@@ -119,15 +119,50 @@ __device__ __forceinline__ void m_control_cursor(const M& m, const StreamRef& s,
     }
 }
 
+// Correctly rounded a / b for integers 0 < a < b < 2^16 given y = RN(1/b), without a division:
+// q0 = RN(a y) is within one ulp of a / b, the remainder a - b q0 is exact in one fused
+// multiply-add, and RN(q0 + r y) is the correctly rounded quotient (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990).
+// vbt_selftest_key_division checks it against IEEE division for every such pair.
+__device__ __forceinline__ float div_small_rn(float a, float b, float y)
+{
+    const float q0 = __fmul_rn(a, y);
+    const float r = __fmaf_rn(-q0, b, a);
+    return __fmaf_rn(r, y, q0);
+}
+
+// Key read with no data-dependent branch: a 3-byte key is always taken from two words (the
+// shared-memory stage and the payload both carry 16 bytes of padding past any key).
+template <class M>
+__device__ __forceinline__ void m_key_read_nb(const M& m, uint64_t kb, uint32_t codec, uint32_t i, int& frame,
+                                              float& value)
+{
+    if (codec == 1u) {
+        const uint32_t w = (uint32_t)((kb + 8ull * i) >> 2);
+        frame = (int)(m(w) & 0xFFFFu);
+        value = __uint_as_float(m(w + 1u));
+    } else {
+        const uint64_t b = kb + 3ull * i;
+        const uint32_t w = (uint32_t)(b >> 2);
+        const uint32_t k = __funnelshift_r(m(w), m(w + 1u), (uint32_t)(b & 3u) * 8u) & 0xFFFFFFu;
+        frame = (int)(k & 0xFFu);
+        value = half_to_float_exact(k >> 8);
+    }
+}
+
 // Streaming cursor over frames t0, t1, ... with t(j+1) - t(j) in {0, 1} (a clamped timeline
 // window), for a control whose key frames strictly increase.  The cursor k (first key with
 // frame > t) then advances at most once per frame, so the key after next is prefetched one
-// advance ahead and no frame waits on a load: the per-frame work is a compare, a register
-// shift and the value, independent across frames.  Values equal the reference's (see
-// decode_control_cursor in rt_decode_v2.cuh).
+// advance ahead and no frame waits on a load.  Per key interval the span b = f1 - f0, its
+// reciprocal RN(1/b) (`rcp`, a table of RN(1/i) for i < 256) and the difference v1 - v0 are
+// formed once; per frame the value is v0 + RN(RN((t - f0) / b) * (v1 - v0)), the quotient by
+// div_small_rn, the first key's value before it, the last key's after it and the key's value on
+// an exact hit -- the bits of the reference's search (see decode_control_cursor in
+// rt_decode_v2.cuh), with selects instead of branches.
 template <class M>
 __device__ __forceinline__ void m_control_stream(const M& m, const StreamRef& s, uint32_t c, const int* fr,
-                                                 uint32_t bin0, int n, float* dst, int stride)
+                                                 uint32_t bin0, int n, float* dst, int stride,
+                                                 const float* __restrict__ rcp)
 {
     const uint32_t desc = m((uint32_t)((s.base + 4ull * c) >> 2));
     const uint32_t kc = (desc >> 16) & 0xFFu;
@@ -155,9 +190,18 @@ __device__ __forceinline__ void m_control_stream(const M& m, const StreamRef& s,
     }
     int fp = 0, fn = 0, fnn = 0;
     float vp = 0.0f, vn = 0.0f, vnn = 0.0f;
-    if (k > 0u) m_key_read(m, kb, s.codec, ks + k - 1u, fp, vp);
-    if (k < kc) m_key_read(m, kb, s.codec, ks + k, fn, vn);
-    if (k + 1u < kc) m_key_read(m, kb, s.codec, ks + k + 1u, fnn, vnn);
+    if (k > 0u) m_key_read_nb(m, kb, s.codec, ks + k - 1u, fp, vp);
+    if (k < kc) m_key_read_nb(m, kb, s.codec, ks + k, fn, vn);
+    if (k + 1u < kc) m_key_read_nb(m, kb, s.codec, ks + k + 1u, fnn, vnn);
+    // the interval [fp, fn); outside 0 < k < kc its values are never selected
+    float bf, y, d;
+    auto interval = [&]() {
+        const uint32_t b = (uint32_t)(fn - fp);
+        bf = (float)(int)b;
+        y = b < 256u ? rcp[b] : __frcp_rn(bf);
+        d = __fsub_rn(vn, vp);
+    };
+    interval();
     for (int j = 0; j < n; ++j) {
         const int t = fr[j];
         if (k < kc && fn <= t) {
@@ -166,16 +210,12 @@ __device__ __forceinline__ void m_control_stream(const M& m, const StreamRef& s,
             fn = fnn;
             vn = vnn;
             ++k;
-            if (k + 1u < kc) m_key_read(m, kb, s.codec, ks + k + 1u, fnn, vnn);
+            if (k + 1u < kc) m_key_read_nb(m, kb, s.codec, ks + k + 1u, fnn, vnn);
+            interval();
         }
-        float out;
-        if (k == 0u) out = vn;
-        else if (k == kc || fp == t) out = vp;
-        else {
-            const float alpha = __fdiv_rn((float)(t - fp), (float)(fn - fp));
-            out = __fadd_rn(vp, __fmul_rn(alpha, __fsub_rn(vn, vp)));
-        }
-        dst[j * stride] = out;
+        const int ai = t - fp;
+        const float lerp = __fadd_rn(vp, __fmul_rn(div_small_rn((float)ai, bf, y), d));
+        dst[j * stride] = k == 0u ? vn : ((k == kc || ai == 0) ? vp : lerp);
     }
 }
 

@@ -15,7 +15,9 @@ namespace vbtb {
 constexpr int kLeafThreads = 256;
 constexpr int kLeafWarps = kLeafThreads / 32;
 constexpr int kLeafCtrlBudget = 3072;   // floats: frames x controls of one batch
-constexpr uint32_t kLeafFixed = 16 + 256 + 128 + 576 + kLeafWarps * 196 * 8 + kLeafWarps * 112 * 16 + kLeafCtrlBudget * 4;
+constexpr uint32_t kLeafFixed =
+    16 + 256 + 128 + 576 + kLeafWarps * 196 * 8 + kLeafWarps * 112 * 16 + kLeafCtrlBudget * 4 + 256 * 4;
+constexpr uint32_t kStagePad = 16;   // readable bytes past the largest staged window
 static_assert(kLeafFixed == kLeafFixedBytes, "host stage sizing must match the kernel's shared-memory layout");
 
 struct LeafSmem {
@@ -26,7 +28,8 @@ struct LeafSmem {
     float2* x2;      // [warp][196]
     float4* y4;      // [warp][112]
     float* ctrl;     // [kLeafCtrlBudget]
-    uint8_t* stage;  // leaf window (16-byte aligned)
+    float* rcp;      // [256] RN(1/i)
+    uint8_t* stage;  // leaf window (16-byte aligned), kStagePad bytes of padding after it
 };
 
 __device__ __forceinline__ LeafSmem leaf_layout(uint8_t* dyn)
@@ -40,7 +43,8 @@ __device__ __forceinline__ LeafSmem leaf_layout(uint8_t* dyn)
     s.x2 = reinterpret_cast<float2*>(dyn + 16 + 256 + 128 + 576);
     s.y4 = reinterpret_cast<float4*>(reinterpret_cast<uint8_t*>(s.x2) + kLeafWarps * 196 * 8);
     s.ctrl = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(s.y4) + kLeafWarps * 112 * 16);
-    s.stage = reinterpret_cast<uint8_t*>(s.ctrl) + kLeafCtrlBudget * 4;
+    s.rcp = s.ctrl + kLeafCtrlBudget;
+    s.stage = reinterpret_cast<uint8_t*>(s.rcp + 256);
     return s;
 }
 
@@ -117,7 +121,7 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
             float* dst = s.ctrl + j0 * Ctot + c;
             if (stream) {
                 const uint32_t bin0 = st.bins == 8u ? s.b8[fb0 + j0] : s.b4[fb0 + j0];
-                m_control_stream(m, st, ci, s.fr + fb0 + j0, bin0, j1 - j0, dst, Ctot);
+                m_control_stream(m, st, ci, s.fr + fb0 + j0, bin0, j1 - j0, dst, Ctot, s.rcp);
             } else {
                 const FrameBatch fb{s.fr + fb0 + j0, s.b8 + fb0 + j0, s.b4 + fb0 + j0, j1 - j0};
                 m_control_search(m, st, ci, fb, dst, Ctot);
@@ -277,6 +281,7 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
         if (to) record_error(a.err, 0u, kErrWaitTimeout);
         *s_next = first;
     }
+    s.rcp[tid] = __frcp_rn((float)tid);
     if (tid < fl.n) {
         const int fr = clamp_frame(fl.f[tid], total);
         s.fr[tid] = fr;
@@ -369,7 +374,7 @@ template <bool DENSE, bool GF>
 static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameList& fl, float* out, uint64_t stride,
                                 int grid, cudaStream_t s)
 {
-    const uint32_t smem = kLeafFixed + a.g.stage_bytes;
+    const uint32_t smem = kLeafFixed + a.g.stage_bytes + kStagePad;
     cudaFuncSetAttribute(decode_leaf_kernel<DENSE, GF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int g = grid > 0 ? grid : leaf_grid<DENSE, GF>(smem);
     unsigned long long* slot = a.work + seq % kWorkSlots;
