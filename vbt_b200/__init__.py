@@ -251,14 +251,15 @@ class Asset:
         _check(_lib.vbt_decode_cache(self._h, fr, len(frames), _addr(out), frame_stride, grid, _stream(stream)))
 
     def decode_window(self, t0, n, out, frame_stride=None, stream=None):
-        """(d) scientific window decode on the tensor cores (frames [t0, t0 + n), n <= 64) into
-        `out` in the cache layout."""
+        """(d) window decode on the tensor cores of frames [t0, t0 + n) into `out` in the cache
+        layout: scientific assets n <= 64, every leaf; render assets n <= 16, the active leaves of
+        the current page table (build it first)."""
         stride = self.leaf_count * 512 if frame_stride is None else frame_stride
         _check(_lib.vbt_decode_window(self._h, t0, n, _addr(out), stride, _stream(stream)))
 
     def window_error(self, t0, n, values, frame_stride=None, stream=None):
-        """FP64 oracle error of a scientific cache of frames [t0, t0 + n):
-        (max_abs, rms, oracle_min, oracle_max)."""
+        """FP64 oracle error of a cache of frames [t0, t0 + n) (scientific: every leaf; render:
+        the active leaves of the current page table): (max_abs, rms, oracle_min, oracle_max)."""
         stride = self.leaf_count * 512 if frame_stride is None else frame_stride
         st = (C.c_double * 4)()
         _check(_lib.vbt_window_error(self._h, t0, n, _addr(values), stride, st, _stream(stream)))

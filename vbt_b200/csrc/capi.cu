@@ -548,32 +548,41 @@ int vbt_decode_frames_host(vbt_asset* a, const int* frames, int nframes, float* 
 int vbt_decode_window(vbt_asset* a, int t0, int n, float* d_out, uint64_t frame_stride, void* stream)
 {
     if (!a || !d_out) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");
-    if (a->hdr.profile_type != 2u)
-        return fail(VBT_STATUS_INVALID_ARGUMENT, "window decode covers scientific (profile 2) assets");
-    if (n < 1 || n > 64 || t0 < 0 || (uint64_t)t0 + (uint64_t)n > a->hdr.frames)
-        return fail(VBT_STATUS_INVALID_ARGUMENT, "window must be 1..64 frames inside [0, frames)");
-    if (frame_stride < 512ull * a->hdr.leaf_count)
-        return fail(VBT_STATUS_INVALID_ARGUMENT, "frame_stride below leaf_count * 512");
+    if (a->hdr.profile_type == 2u) {
+        if (n < 1 || n > 64 || t0 < 0 || (uint64_t)t0 + (uint64_t)n > a->hdr.frames)
+            return fail(VBT_STATUS_INVALID_ARGUMENT, "window must be 1..64 frames inside [0, frames)");
+        if (frame_stride < 512ull * a->hdr.leaf_count)
+            return fail(VBT_STATUS_INVALID_ARGUMENT, "frame_stride below leaf_count * 512");
+        DeviceGuard guard(a->device);
+        launch_sci_window(a->dev, t0, n, d_out, frame_stride, static_cast<cudaStream_t>(stream));
+        return check_launch("sci_window_kernel");
+    }
+    if (n < 1 || n > 16 || t0 < 0 || (uint64_t)t0 + (uint64_t)n > a->hdr.frames)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "render window must be 1..16 frames inside [0, frames)");
+    if ((reinterpret_cast<uintptr_t>(d_out) & 3u) != 0u)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "output must be 4-byte aligned");
     DeviceGuard guard(a->device);
-    launch_sci_window(a->dev, t0, n, d_out, frame_stride, static_cast<cudaStream_t>(stream));
-    return check_launch("sci_window_kernel");
+    launch_render_window(a->dev, t0, n, d_out, frame_stride, static_cast<cudaStream_t>(stream));
+    return check_launch("render_window_kernel");
 }
 
 int vbt_window_error(vbt_asset* a, int t0, int n, const float* d_values, uint64_t frame_stride, double* stats,
                      void* stream)
 {
     if (!a || !d_values || !stats) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");
-    if (a->hdr.profile_type != 2u)
-        return fail(VBT_STATUS_INVALID_ARGUMENT, "the window oracle covers scientific (profile 2) assets");
     if (n < 1 || t0 < 0 || (uint64_t)t0 + (uint64_t)n > a->hdr.frames)
         return fail(VBT_STATUS_INVALID_ARGUMENT, "frames outside [0, frames)");
     DeviceGuard guard(a->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    launch_sci_window_oracle(a->dev, t0, n, d_values, frame_stride, a->d_stats, s);
+    const bool sci = a->hdr.profile_type == 2u;
+    if (sci) launch_sci_window_oracle(a->dev, t0, n, d_values, frame_stride, a->d_stats, s);
+    else launch_render_window_oracle(a->dev, t0, n, d_values, frame_stride, a->d_stats, s);
     int st;
-    if ((st = check_launch("sci_window_oracle_kernel"))) return st;
+    if ((st = check_launch(sci ? "sci_window_oracle_kernel" : "render_window_oracle_kernel"))) return st;
     unsigned long long raw[4];
+    uint32_t leaves = a->hdr.leaf_count;
     CUDA_TRY(cudaMemcpyAsync(raw, a->d_stats, sizeof(raw), cudaMemcpyDeviceToHost, s));
+    if (!sci) CUDA_TRY(cudaMemcpyAsync(&leaves, a->dev.counters, sizeof(leaves), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     auto unorder = [](unsigned long long o) {
         const unsigned long long b = (o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o;
@@ -584,7 +593,7 @@ int vbt_window_error(vbt_asset* a, int t0, int n, const float* d_values, uint64_
     double mx, sum;
     std::memcpy(&mx, &raw[0], 8);
     std::memcpy(&sum, &raw[1], 8);
-    const double count = (double)a->hdr.leaf_count * 512.0 * (double)n;
+    const double count = (double)(leaves ? leaves : 1u) * 512.0 * (double)n;
     stats[0] = mx;
     stats[1] = std::sqrt(sum / count);
     stats[2] = unorder(raw[2]);

@@ -1320,3 +1320,4 @@ void launch_key_division_check(uint32_t b_max, unsigned long long* d_out, cudaSt
 #include <cuda_bf16.h>
 
 #include "sci_window.cuh"
+#include "render_window.cuh"

@@ -219,7 +219,68 @@ __device__ __forceinline__ void m_control_stream(const M& m, const StreamRef& s,
     }
 }
 
-// The reference's hinted bracket search per frame (src/render_temporal_decode.cpp:79-131).
+// The reference's hinted bracket search for one frame (src/render_temporal_decode.cpp:79-131) on a
+// control with keys [ks, ks + kc), kc > 0: kind 1 = the value v0, kind 2 = the value v1,
+// kind 3 = v0 + (frame - f0) / (f1 - f0) * (v1 - v0).  r0 / r1 hold the control's bin hint bytes.
+struct Bracket {
+    int kind, f0, f1;
+    float v0, v1;
+};
+
+template <class M>
+__device__ __forceinline__ Bracket m_search_bracket(const M& m, uint64_t kb, uint32_t codec, uint32_t ks, uint32_t kc,
+                                                    uint32_t bins, uint32_t r0, uint32_t r1, int frame, uint32_t bin)
+{
+    const uint32_t last = kc - 1u;
+    const uint32_t hb = row_byte(r0, r1, bin);
+    uint32_t lo = hb < last ? hb : last;
+    Bracket b{1, 0, 0, 0.0f, 0.0f};
+    m_key_read(m, kb, codec, ks + lo, b.f0, b.v0);
+    if (b.f0 > frame) {
+        lo = 0u;
+        m_key_read(m, kb, codec, ks, b.f0, b.v0);
+    }
+    if (b.f0 >= frame || lo == last) return b;
+    uint32_t hi = last;
+    if (bin + 1u < bins) {
+        const uint32_t h = row_byte(r0, r1, bin + 1u) + 1u;
+        hi = h < last ? h : last;
+    }
+    if (hi < lo + 1u) hi = lo + 1u;
+    m_key_read(m, kb, codec, ks + hi, b.f1, b.v1);
+    if (b.f1 < frame) {
+        hi = last;
+        m_key_read(m, kb, codec, ks + hi, b.f1, b.v1);
+    }
+    if (b.f1 <= frame) {
+        b.kind = 2;
+        return b;
+    }
+    bool moved_lo = false, moved_hi = false;
+    while (hi > lo + 1u) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        const int fm = m_key_frame(m, kb, codec, ks + mid);
+        if (fm < frame) {
+            lo = mid;
+            b.f0 = fm;
+            moved_lo = true;
+        } else {
+            hi = mid;
+            b.f1 = fm;
+            moved_hi = true;
+        }
+    }
+    if (moved_hi) m_key_read(m, kb, codec, ks + hi, b.f1, b.v1);
+    if (b.f1 == frame) {
+        b.kind = 2;
+        return b;
+    }
+    if (moved_lo) m_key_read(m, kb, codec, ks + lo, b.f0, b.v0);
+    b.kind = 3;
+    return b;
+}
+
+// The reference's search for every frame of a batch, rounded as the reference rounds.
 template <class M>
 __device__ __forceinline__ void m_control_search(const M& m, const StreamRef& s, uint32_t c, const FrameBatch& fb,
                                                  float* dst, int stride)
@@ -233,64 +294,39 @@ __device__ __forceinline__ void m_control_search(const M& m, const StreamRef& s,
         for (int j = 0; j < fb.nb; ++j) dst[j * stride] = 0.0f;
         return;
     }
-    const uint32_t ks = desc & 0xFFFFu, last = kc - 1u;
+    const uint32_t ks = desc & 0xFFFFu;
     const uint64_t kb = stream_key_base(s);
     const uint8_t* bins_of_frame = s.bins == 8u ? fb.b8 : fb.b4;
     for (int j = 0; j < fb.nb; ++j) {
         const int frame = fb.fr[j];
-        const uint32_t bin = bins_of_frame[j];
-        const uint32_t hb = row_byte(r0, r1, bin);
-        uint32_t lo = hb < last ? hb : last;
-        int f0, f1;
-        float v0, v1, out;
-        m_key_read(m, kb, s.codec, ks + lo, f0, v0);
-        if (f0 > frame) {
-            lo = 0u;
-            m_key_read(m, kb, s.codec, ks, f0, v0);
-        }
-        if (f0 >= frame || lo == last) {
-            out = v0;
-        } else {
-            uint32_t hi = last;
-            if (bin + 1u < s.bins) {
-                const uint32_t h = row_byte(r0, r1, bin + 1u) + 1u;
-                hi = h < last ? h : last;
-            }
-            if (hi < lo + 1u) hi = lo + 1u;
-            m_key_read(m, kb, s.codec, ks + hi, f1, v1);
-            if (f1 < frame) {
-                hi = last;
-                m_key_read(m, kb, s.codec, ks + hi, f1, v1);
-            }
-            if (f1 <= frame) {
-                out = v1;
-            } else {
-                bool moved_lo = false, moved_hi = false;
-                while (hi > lo + 1u) {
-                    const uint32_t mid = lo + (hi - lo) / 2u;
-                    const int fm = m_key_frame(m, kb, s.codec, ks + mid);
-                    if (fm < frame) {
-                        lo = mid;
-                        f0 = fm;
-                        moved_lo = true;
-                    } else {
-                        hi = mid;
-                        f1 = fm;
-                        moved_hi = true;
-                    }
-                }
-                if (moved_hi) m_key_read(m, kb, s.codec, ks + hi, f1, v1);
-                if (f1 == frame) {
-                    out = v1;
-                } else {
-                    if (moved_lo) m_key_read(m, kb, s.codec, ks + lo, f0, v0);
-                    const float alpha = __fdiv_rn((float)(frame - f0), (float)(f1 - f0));
-                    out = __fadd_rn(v0, __fmul_rn(alpha, __fsub_rn(v1, v0)));
-                }
-            }
+        const Bracket b = m_search_bracket(m, kb, s.codec, ks, kc, s.bins, r0, r1, frame, bins_of_frame[j]);
+        float out;
+        if (b.kind == 1) out = b.v0;
+        else if (b.kind == 2) out = b.v1;
+        else {
+            const float alpha = __fdiv_rn((float)(frame - b.f0), (float)(b.f1 - b.f0));
+            out = __fadd_rn(b.v0, __fmul_rn(alpha, __fsub_rn(b.v1, b.v0)));
         }
         dst[j * stride] = out;
     }
+}
+
+// The same control value in double without intermediate rounding (the FP64 error oracle): the
+// bracket the reference's search selects, interpolated exactly.
+template <class M>
+__device__ __forceinline__ double m_control_value_f64(const M& m, const StreamRef& s, uint32_t c, int frame,
+                                                      uint32_t bin)
+{
+    const uint32_t desc = m((uint32_t)((s.base + 4ull * c) >> 2));
+    const uint64_t row = s.base + 4ull * s.controls + (uint64_t)c * s.bins;
+    const uint32_t r0 = m((uint32_t)(row >> 2));
+    const uint32_t r1 = s.bins == 8u ? m((uint32_t)(row >> 2) + 1u) : 0u;
+    const uint32_t kc = (desc >> 16) & 0xFFu;
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) return 0.0;
+    const Bracket b = m_search_bracket(m, stream_key_base(s), s.codec, desc & 0xFFFFu, kc, s.bins, r0, r1, frame, bin);
+    if (b.kind == 1) return (double)b.v0;
+    if (b.kind == 2) return (double)b.v1;
+    return (double)b.v0 + (double)(frame - b.f0) / (double)(b.f1 - b.f0) * ((double)b.v1 - (double)b.v0);
 }
 
 // ---- TMA bulk copy global -> shared with mbarrier completion (sm_90+ PTX, no multicast) ----

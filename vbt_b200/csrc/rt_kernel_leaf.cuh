@@ -74,11 +74,27 @@ __device__ __forceinline__ void store_quad(const DeviceAsset& a, const LeafGeom&
     }
 }
 
-// Decode one validated, non-EMPTY leaf for all frames of the launch with word reader `m`.
-template <bool DENSE, class M>
+// Where leaf_decode puts a finished voxel quad: the current-frame cache or dense frames.
+template <bool DENSE>
+struct FrameSink {
+    const DeviceAsset& a;
+    const LeafGeom& G;
+    float* __restrict__ out;
+    uint64_t frame_stride;
+    __device__ __forceinline__ void operator()(int fi, int lane, int i, float4 v) const
+    {
+        store_quad<DENSE>(a, G, out, frame_stride, fi, lane, i, v);
+    }
+};
+
+// Decode one validated, non-EMPTY leaf for all frames of the launch with word reader `m`; each
+// finished quad of 4 voxels goes to `sink(frame index, lane, quad, values)`.  Frame lists that
+// step by 0 or 1 stream each control's keys; other non-decreasing lists (`monotone`) walk a
+// cursor; anything else, or keys that do not strictly increase, uses the reference's search.
+template <class M, class Sink>
 __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, const LeafSmem& s, const LeafEntry& e,
-                                            int nframes, bool steps01, const LeafGeom& G, float* __restrict__ out,
-                                            uint64_t frame_stride)
+                                            int nframes, bool steps01, bool monotone, const LeafGeom& G,
+                                            const Sink& sink)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t base = 4ull * e.word_off;
@@ -94,6 +110,7 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
     const int Ctot = Cc + Cf;
     const int nb_max = min(nframes, kLeafCtrlBudget / max(Ctot, 1));
     const bool stream = steps01 && (e.info & kFlagSorted) != 0u;
+    const bool cursor = !stream && monotone && (e.info & kFlagSorted) != 0u;
     const bool plain = !occ && G.w == 8 && G.h == 8 && G.d == 8;
     const int ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
     uint64_t mask[4] = {0, 0, 0, 0};
@@ -124,7 +141,8 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
                 m_control_stream(m, st, ci, s.fr + fb0 + j0, bin0, j1 - j0, dst, Ctot, s.rcp);
             } else {
                 const FrameBatch fb{s.fr + fb0 + j0, s.b8 + fb0 + j0, s.b4 + fb0 + j0, j1 - j0};
-                m_control_search(m, st, ci, fb, dst, Ctot);
+                if (cursor) m_control_cursor(m, st, ci, fb, dst, Ctot);
+                else m_control_search(m, st, ci, fb, dst, Ctot);
             }
         };
         const int c0 = Ctot > kLeafThreads ? kLeafThreads : 0;   // controls [0, c0) are owned whole
@@ -158,7 +176,7 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
             const int fi = fb0 + j;
             if (plain) {
 #pragma unroll
-                for (int i = 0; i < 4; ++i) store_quad<DENSE>(a, G, out, frame_stride, fi, lane, i, q[i]);
+                for (int i = 0; i < 4; ++i) sink(fi, lane, i, q[i]);
                 continue;
             }
 #pragma unroll
@@ -176,7 +194,7 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
                     if (occ && !in_occ && v[k] < 0.0f) v[k] = 0.0f;
                     if (lx0 + k >= G.w || ly >= G.h || lz >= G.d) v[k] = 0.0f;
                 }
-                store_quad<DENSE>(a, G, out, frame_stride, fi, lane, i, make_float4(v[0], v[1], v[2], v[3]));
+                sink(fi, lane, i, make_float4(v[0], v[1], v[2], v[3]));
             }
         }
         __syncthreads();
@@ -291,6 +309,7 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
     __syncthreads();
     const bool steps01 =
         __syncthreads_and(tid == 0 || tid >= fl.n || (unsigned)(s.fr[tid] - s.fr[tid - 1]) <= 1u) != 0;
+    const bool monotone = __syncthreads_and(tid == 0 || tid >= fl.n || s.fr[tid] >= s.fr[tid - 1]) != 0;
     const uint8_t* pay_bytes = reinterpret_cast<const uint8_t*>(a.payload);
     uint32_t phase = 0;
     uint32_t li = *s_next;
@@ -339,10 +358,10 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
             if (staged) phase ^= 1u;
             if (staged) {
                 const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
-                leaf_decode<DENSE>(a, m, s, e, fl.n, steps01, G, out, frame_stride);
+                leaf_decode(a, m, s, e, fl.n, steps01, monotone, G, FrameSink<DENSE>{a, G, out, frame_stride});
             } else if (GLOBAL_FALLBACK) {
                 const GlobalWords m{a.payload};
-                leaf_decode<DENSE>(a, m, s, e, fl.n, steps01, G, out, frame_stride);
+                leaf_decode(a, m, s, e, fl.n, steps01, monotone, G, FrameSink<DENSE>{a, G, out, frame_stride});
             }
         }
         __syncthreads();   // the next index is visible
