@@ -156,16 +156,18 @@ int vbt_build_page_table_noalloc(const uint32_t* d_offsets, const uint32_t* d_pa
  * the per-frame path does.  Values are not bit-identical to the reference; vbt_window_error gives
  * their error.  CoarseOnly and SparseEvents leaves are covered; DenseGrid leaves record
  * VBT_STATUS_UNSUPPORTED (read by vbt_asset_sync_status) and are written as zeros.
- * Render-temporal assets (profile 1): frames [t0, t0 + n), n <= 16, d_out[f * frame_stride +
+ * Render-temporal assets (profile 1): frames [t0, t0 + n), n <= 64, d_out[f * frame_stride +
  * rank * 512 + voxel] over the active leaves of the current page table (vbt_build_page_table
- * first), as vbt_decode_cache.  Per leaf, the union U of all controls' key frames inside the
- * window plus its first and last frame are the knots; between knots every voxel is linear in t
+ * first), as vbt_decode_cache, in consecutive windows of 16 frames.  Per leaf and window, the
+ * union U of all controls' key frames inside the window plus its first and last frame are the
+ * knots; between knots every voxel is linear in t
  * (decodeFromSequence, src/render_temporal_decode.cpp:79-131, is piecewise linear in t and the
  * trilinear is linear in the controls).  The voxels at the K = |U| knots are decoded exactly on
  * the CUDA cores and the window is V(512 x n) = Coef(512 x K) . H(K x n) on tcgen05 tensor cores,
  * H the hat functions of U, both split into three BF16 terms, FP32 accumulation.  Knot frames are
  * bit-identical to vbt_decode_cache; Mode2 leaves and leaves whose keys do not strictly increase
- * take every frame as a knot. */
+ * take every frame as a knot, and a window whose every frame is a knot is decoded exactly without
+ * the contraction.  d_out 16-byte aligned, frame_stride a multiple of 4. */
 int vbt_decode_window(vbt_asset* asset, int t0, int n, float* d_out, uint64_t frame_stride, void* stream);
 /* FP64 error oracle on the GPU for any cache of frames [t0, t0 + n) (from vbt_decode_window or
  * vbt_decode_cache; render assets: the active ranks of the current page table): the reference

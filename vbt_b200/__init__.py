@@ -252,8 +252,8 @@ class Asset:
 
     def decode_window(self, t0, n, out, frame_stride=None, stream=None):
         """(d) window decode on the tensor cores of frames [t0, t0 + n) into `out` in the cache
-        layout: scientific assets n <= 64, every leaf; render assets n <= 16, the active leaves of
-        the current page table (build it first)."""
+        layout: scientific assets n <= 64, every leaf; render assets n <= 64 as 16-frame
+        windows, the active leaves of the current page table (build it first)."""
         stride = self.leaf_count * 512 if frame_stride is None else frame_stride
         _check(_lib.vbt_decode_window(self._h, t0, n, _addr(out), stride, _stream(stream)))
 

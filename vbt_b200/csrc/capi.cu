@@ -557,10 +557,10 @@ int vbt_decode_window(vbt_asset* a, int t0, int n, float* d_out, uint64_t frame_
         launch_sci_window(a->dev, t0, n, d_out, frame_stride, static_cast<cudaStream_t>(stream));
         return check_launch("sci_window_kernel");
     }
-    if (n < 1 || n > 16 || t0 < 0 || (uint64_t)t0 + (uint64_t)n > a->hdr.frames)
-        return fail(VBT_STATUS_INVALID_ARGUMENT, "render window must be 1..16 frames inside [0, frames)");
-    if ((reinterpret_cast<uintptr_t>(d_out) & 3u) != 0u)
-        return fail(VBT_STATUS_INVALID_ARGUMENT, "output must be 4-byte aligned");
+    if (n < 1 || n > 64 || t0 < 0 || (uint64_t)t0 + (uint64_t)n > a->hdr.frames)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "render windows must cover 1..64 frames inside [0, frames)");
+    if ((reinterpret_cast<uintptr_t>(d_out) & 15u) != 0u || (frame_stride & 3u) != 0u)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "output must be 16-byte aligned, frame_stride a multiple of 4");
     DeviceGuard guard(a->device);
     launch_render_window(a->dev, t0, n, d_out, frame_stride, static_cast<cudaStream_t>(stream));
     return check_launch("render_window_kernel");

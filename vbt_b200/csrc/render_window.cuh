@@ -15,17 +15,23 @@
 // N = 16 frames, K = 16 knots) accumulated in FP32 in tensor memory: 4 M tiles x 6 = 24 MMAs per
 // leaf-window.  A knot frame's value is the sum of its three exact terms: bit-identical to the
 // per-frame decode.  Leaves whose keys do not strictly increase, and Mode2 leaves (the clamp to
-// zero outside the occupancy is not linear), take every frame as a knot.
+// zero outside the occupancy is not linear), take every frame as a knot; a window whose every
+// frame is a knot is decoded exactly, without the contraction.
+// A launch covers up to 64 frames as consecutive 16-frame windows: each leaf is staged once and
+// its knots are found for all windows in one pass over its keys.
 #pragma once
 
 namespace vbtb {
 
-constexpr int kRwMaxN = 16;
+constexpr int kRwWin = 16;                      // frames per window (the MMA's N)
+constexpr int kRwMaxN = 64;                     // frames per launch
 constexpr uint32_t kRwA = 4u * 3u * 4096u;      // 4 M tiles x 3 terms x (128 voxel rows x 16 knots)
 constexpr uint32_t kRwB = 3u * 512u;            // 3 terms x (16 frame rows x 16 knots)
-constexpr uint32_t kRwCoef = 16u * 512u * 4u;   // FP32 voxels at the knots, [knot][voxel]
 constexpr uint32_t kRwMisc = 128u;              // MMA barrier, TMEM address, knot mask, knot offsets
-constexpr uint32_t kRwHead = kRwA + kRwB + kRwCoef + kRwMisc;   // the leaf-kernel layout follows
+constexpr uint32_t kRwHead = kRwA + kRwB + kRwMisc;   // the leaf-kernel layout follows
+// The FP32 voxels at the knots ([knot][voxel], 32 KiB) live in the first half of the A region
+// until the split into A's BF16 terms overwrites them.
+static_assert(16u * 512u * 4u <= kRwA, "the knot values fit inside the A operand region");
 constexpr uint32_t kRwTmemCols = 64u;           // 4 M tiles x 16 FP32 columns
 static_assert(kRwHead % 128u == 0u, "the leaf-kernel layout after the window head stays aligned");
 
@@ -45,18 +51,21 @@ __device__ __forceinline__ void win_split3(float x, uint16_t& b0, uint16_t& b1, 
     b2 = win_bf16_bits(__fsub_rn(r1, win_bf16_val(b1)));
 }
 
-// One leaf-window.  Returns false when a bounded wait gave up (the CTA then stops).
+// One leaf, every window of the launch.  Returns false when a bounded wait gave up (the CTA then
+// stops).
 template <class M>
 __device__ __forceinline__ bool render_window_leaf(const DeviceAsset& a, const M& m, const LeafSmem& s,
                                                    const LeafEntry& e, const LeafGeom& G, int t0, int n,
-                                                   uint8_t* sA, uint8_t* sB, float* sCoef, uint32_t* s_mask,
+                                                   uint8_t* sA, uint8_t* sB, unsigned long long* s_mask,
                                                    int* s_knot, uint64_t* bar_mma, uint32_t taddr, uint32_t& ph_mma,
                                                    float* __restrict__ out, uint64_t frame_stride, uint32_t leaf)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int total = (int)a.g.frames;
-    // 1. knots: every control's key frames strictly inside the window (the ends are set already)
-    const bool interp = (e.info & kFlagSorted) != 0u && (e.info & (kFlagOccClamp | kFlagShell)) == 0u && n > 2;
+    float* const sCoef = reinterpret_cast<float*>(sA);
+    // 1. knots: every control's key frames strictly inside the launch's frames (each window's
+    //    first and last frame are set already)
+    const bool interp = (e.info & kFlagSorted) != 0u && (e.info & (kFlagOccClamp | kFlagShell)) == 0u;
     if (interp) {
         const uint64_t base = 4ull * e.word_off;
         const int cres = (int)((e.header >> 6) & 7u), fres = (int)((e.header >> 9) & 7u);
@@ -78,128 +87,155 @@ __device__ __forceinline__ bool render_window_leaf(const DeviceAsset& a, const M
                 if (m_key_frame(m, kb, st.codec, ks + mid) > t0) hi = mid;
                 else lo = mid + 1u;
             }
-            uint32_t bits = 0;
+            unsigned long long bits = 0ull;
             for (uint32_t k = lo; k < kc; ++k) {
                 const int f = m_key_frame(m, kb, st.codec, ks + k);
                 if (f >= t0 + n - 1) break;
-                bits |= 1u << (f - t0);
+                bits |= 1ull << (f - t0);
             }
             if (bits) atomicOr(s_mask, bits);
         }
     } else if (tid == 0) {
-        *s_mask = (1u << n) - 1u;
+        *s_mask = n == 64 ? ~0ull : ((1ull << n) - 1ull);
     }
     __syncthreads();
-    const uint32_t mask = *s_mask;
-    const int K = __popc(mask);
-    if (tid < n && ((mask >> tid) & 1u)) {
-        const int k = __popc(mask & ((1u << tid) - 1u));
-        const int fr = t0 + tid;
-        s.fr[k] = fr;
-        s.b8[k] = (uint8_t)time_bin(fr, 8u, total);
-        s.b4[k] = (uint8_t)time_bin(fr, 4u, total);
-        s_knot[k] = tid;
-    }
-    __syncthreads();
-    // 2. exact voxels at the knots (a window with every frame a knot streams its keys)
-    leaf_decode(a, m, s, e, K, K == n, true, G, CoefSink{sCoef});
-    // 3. A = Coef split into three BF16 terms (knot columns >= K are 0); B = H split likewise
-    for (int it = tid; it < 1024; it += kLeafThreads) {
-        const uint32_t v = (uint32_t)it & 511u, g = (uint32_t)it >> 9;
-        uint32_t w[3][4];
+    const unsigned long long mask = *s_mask;
+    for (int w0 = 0; w0 < n; w0 += kRwWin) {
+        const int nw = min(kRwWin, n - w0);
+        const uint32_t sub = (uint32_t)(mask >> w0) & ((1u << nw) - 1u);
+        const int K = __popc(sub);
+        if (tid < nw && ((sub >> tid) & 1u)) {
+            const int k = __popc(sub & ((1u << tid) - 1u));
+            const int fr = t0 + w0 + tid;
+            s.fr[k] = fr;
+            s.b8[k] = (uint8_t)time_bin(fr, 8u, total);
+            s.b4[k] = (uint8_t)time_bin(fr, 4u, total);
+            s_knot[k] = tid;
+        }
+        __syncthreads();
+        // A window whose every frame is a knot has nothing to interpolate: its frames are decoded
+        // exactly, straight into the output.
+        if (K == nw) {
+            leaf_decode(a, m, s, e, nw, true, true, G,
+                        FrameSink<false>{a, G, out + (uint64_t)w0 * frame_stride, frame_stride});
+            continue;
+        }
+        // 2. exact voxels at the knots
+        leaf_decode(a, m, s, e, K, false, true, G, CoefSink{sCoef});
+        // 3. A = Coef split into three BF16 terms (knot columns >= K are 0), through registers
+        //    since A overwrites the knot values; B = H split likewise
+        uint32_t w[4][3][4];
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) {
-            const int k = (int)(8u * g) + kk;
-            uint16_t t[3];
-            win_split3(k < K ? sCoef[k * 512 + (int)v] : 0.0f, t[0], t[1], t[2]);
+        for (int r = 0; r < 4; ++r) {
+            const int it = tid + r * kLeafThreads;
+            const uint32_t v = (uint32_t)it & 511u, g = (uint32_t)it >> 9;
+            if ((int)(8u * g) >= K) {   // a knot group past K: zeros (B's rows there are 0 too)
 #pragma unroll
-            for (int p = 0; p < 3; ++p) {
-                if (kk & 1) w[p][kk >> 1] |= (uint32_t)t[p] << 16;
-                else w[p][kk >> 1] = t[p];
+                for (int p = 0; p < 3; ++p) w[r][p][0] = w[r][p][1] = w[r][p][2] = w[r][p][3] = 0u;
+                continue;
+            }
+#pragma unroll
+            for (int kk = 0; kk < 8; kk += 2) {
+                const int k = (int)(8u * g) + kk;
+                const float x0 = k < K ? sCoef[k * 512 + (int)v] : 0.0f;
+                const float x1 = k + 1 < K ? sCoef[(k + 1) * 512 + (int)v] : 0.0f;
+                uint16_t a0[3], a1[3];
+                win_split3(x0, a0[0], a0[1], a0[2]);
+                win_split3(x1, a1[0], a1[1], a1[2]);
+#pragma unroll
+                for (int p = 0; p < 3; ++p) w[r][p][kk >> 1] = (uint32_t)a0[p] | ((uint32_t)a1[p] << 16);
             }
         }
-        const uint32_t mt = v >> 7, r = v & 127u;
+        __syncthreads();
 #pragma unroll
-        for (int p = 0; p < 3; ++p)
-            *reinterpret_cast<uint4*>(sA + (mt * 3u + (uint32_t)p) * 4096u + win_off(r, 8u * g)) =
-                make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
-    }
-    {
-        const int j = tid >> 4, k = tid & 15;   // 256 threads = 16 frames x 16 knots
-        float h = 0.0f;
-        if (j < n && k < K) {
-            const int u = s_knot[k];
-            if (u == j) h = 1.0f;
-            else if (u < j && k + 1 < K && s_knot[k + 1] > j)
-                h = __fdiv_rn((float)(s_knot[k + 1] - j), (float)(s_knot[k + 1] - u));
-            else if (u > j && k > 0 && s_knot[k - 1] < j)
-                h = __fdiv_rn((float)(j - s_knot[k - 1]), (float)(u - s_knot[k - 1]));
+        for (int r = 0; r < 4; ++r) {
+            const int it = tid + r * kLeafThreads;
+            const uint32_t v = (uint32_t)it & 511u, g = (uint32_t)it >> 9;
+            const uint32_t mt = v >> 7, row = v & 127u;
+#pragma unroll
+            for (int p = 0; p < 3; ++p)
+                *reinterpret_cast<uint4*>(sA + (mt * 3u + (uint32_t)p) * 4096u + win_off(row, 8u * g)) =
+                    make_uint4(w[r][p][0], w[r][p][1], w[r][p][2], w[r][p][3]);
         }
-        uint16_t t[3];
-        win_split3(h, t[0], t[1], t[2]);
+        {
+            const int j = tid >> 4, k = tid & 15;   // 256 threads = 16 frames x 16 knots
+            float h = 0.0f;
+            if (j < nw && k < K) {
+                const int u = s_knot[k];
+                if (u == j) h = 1.0f;
+                else if (u < j && k + 1 < K && s_knot[k + 1] > j)
+                    h = __fdiv_rn((float)(s_knot[k + 1] - j), (float)(s_knot[k + 1] - u));
+                else if (u > j && k > 0 && s_knot[k - 1] < j)
+                    h = __fdiv_rn((float)(j - s_knot[k - 1]), (float)(u - s_knot[k - 1]));
+            }
+            uint16_t t[3];
+            win_split3(h, t[0], t[1], t[2]);
 #pragma unroll
-        for (int p = 0; p < 3; ++p)
-            *reinterpret_cast<uint16_t*>(sB + (uint32_t)p * 512u + win_off((uint32_t)j, (uint32_t)k)) = t[p];
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    win_tc_fence_before();
-    __syncthreads();
-    win_tc_fence_after();
-    // 4. one thread issues the 24 MMAs (term pairs p + q <= 2) and commits them
-    if (tid == 0) {
-        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
-        for (uint32_t mt = 0; mt < 4u; ++mt) {
-            uint32_t acc = 0u;
-            for (uint32_t p = 0; p < 3u; ++p)
-                for (uint32_t q = 0; p + q < 3u; ++q) {
-                    win_mma(taddr + mt * 16u, win_desc(win_smem_u32(sA + (mt * 3u + p) * 4096u)),
-                            win_desc(win_smem_u32(sB + q * 512u)), idesc, acc);
-                    acc = 1u;
-                }
+            for (int p = 0; p < 3; ++p)
+                *reinterpret_cast<uint16_t*>(sB + (uint32_t)p * 512u + win_off((uint32_t)j, (uint32_t)k)) = t[p];
         }
-        win_commit(bar_mma);
-    }
-    const bool ok = mbar_wait(bar_mma, ph_mma);
-    if (__syncthreads_or(!ok)) {
-        if (tid == 0) record_error(a.err, leaf, kErrWaitTimeout);
-        mbar_wait(bar_mma, ph_mma);
-        return false;
-    }
-    ph_mma ^= 1u;
-    win_tc_fence_after();
-    // 5. epilogue: warp w reads voxel rows 32 (w % 4) .. +31 of M tiles 2 (w / 4) and 2 (w / 4) + 1
-    const uint32_t quarter = (uint32_t)(warp & 3), half = (uint32_t)(warp >> 2);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        win_tc_fence_before();
+        __syncthreads();
+        win_tc_fence_after();
+        // 4. one thread issues the 24 MMAs (term pairs p + q <= 2) and commits them
+        if (tid == 0) {
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+            for (uint32_t mt = 0; mt < 4u; ++mt) {
+                uint32_t acc = 0u;
+                for (uint32_t p = 0; p < 3u; ++p)
+                    for (uint32_t q = 0; p + q < 3u; ++q) {
+                        win_mma(taddr + mt * 16u, win_desc(win_smem_u32(sA + (mt * 3u + p) * 4096u)),
+                                win_desc(win_smem_u32(sB + q * 512u)), idesc, acc);
+                        acc = 1u;
+                    }
+            }
+            win_commit(bar_mma);
+        }
+        const bool ok = mbar_wait(bar_mma, ph_mma);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) record_error(a.err, leaf, kErrWaitTimeout);
+            mbar_wait(bar_mma, ph_mma);
+            return false;
+        }
+        ph_mma ^= 1u;
+        win_tc_fence_after();
+        // 5. epilogue: warp w reads voxel rows 32 (w % 4) .. +31 of M tiles 2 (w / 4) and
+        //    2 (w / 4) + 1
+        const uint32_t quarter = (uint32_t)(warp & 3), half = (uint32_t)(warp >> 2);
 #pragma unroll
-    for (uint32_t mm = 0; mm < 2u; ++mm) {
-        const uint32_t mt = half * 2u + mm;
-        float d[16];
-        win_ld16(taddr + ((quarter * 32u) << 16) + mt * 16u, d);
-        const uint32_t v = mt * 128u + quarter * 32u + (uint32_t)lane;
+        for (uint32_t mm = 0; mm < 2u; ++mm) {
+            const uint32_t mt = half * 2u + mm;
+            float d[16];
+            win_ld16(taddr + ((quarter * 32u) << 16) + mt * 16u, d);
+            const uint32_t v = mt * 128u + quarter * 32u + (uint32_t)lane;
+            float* o = out + (uint64_t)w0 * frame_stride + (uint64_t)G.li * 512u + v;
 #pragma unroll
-        for (int j = 0; j < kRwMaxN; ++j)
-            if (j < n) out[(uint64_t)j * frame_stride + (uint64_t)G.li * 512u + v] = d[j];
+            for (int j = 0; j < kRwWin; ++j)
+                if (j < nw) o[(uint64_t)j * frame_stride] = d[j];
+        }
+        win_tc_fence_before();
+        __syncthreads();   // D, A, B and the knot buffers are free for the next window or leaf
+        win_tc_fence_after();
     }
-    win_tc_fence_before();
-    __syncthreads();   // D, A, B and the knot buffers are free for the next leaf
-    win_tc_fence_after();
     return true;
 }
 
-// One CTA per SM over the active leaves (rank-strided), 256 threads.  out[f * frame_stride +
-// rank * 512 + voxel] for f < n, the current-frame cache layout of frames t0 .. t0 + n - 1.
+// Persistent CTAs over the active leaves (rank-strided), 256 threads, as many per SM as shared
+// memory allows.  out[f * frame_stride + rank * 512 + voxel] for f < n, the current-frame cache
+// layout of frames t0 .. t0 + n - 1.
 template <bool GLOBAL_FALLBACK>
-__global__ void __launch_bounds__(kLeafThreads, 1) render_window_kernel(DeviceAsset a, int t0, int n,
+__global__ void __launch_bounds__(kLeafThreads, 2) render_window_kernel(DeviceAsset a, int t0, int n,
                                                                         float* __restrict__ out, uint64_t frame_stride)
 {
     extern __shared__ __align__(1024) uint8_t rdyn[];
     uint8_t* sA = rdyn;
     uint8_t* sB = rdyn + kRwA;
-    float* sCoef = reinterpret_cast<float*>(rdyn + kRwA + kRwB);
-    uint8_t* misc = rdyn + kRwA + kRwB + kRwCoef;
+    uint8_t* misc = rdyn + kRwA + kRwB;
     uint64_t* bar_mma = reinterpret_cast<uint64_t*>(misc);
-    uint32_t* s_taddr = reinterpret_cast<uint32_t*>(misc + 8);
-    uint32_t* s_mask = reinterpret_cast<uint32_t*>(misc + 12);
-    int* s_knot = reinterpret_cast<int*>(misc + 16);   // 16 knot offsets from t0, ascending
+    unsigned long long* s_mask = reinterpret_cast<unsigned long long*>(misc + 8);
+    uint32_t* s_taddr = reinterpret_cast<uint32_t*>(misc + 16);
+    int* s_knot = reinterpret_cast<int*>(misc + 32);   // a window's knot offsets, ascending
     const LeafSmem s = leaf_layout(rdyn + kRwHead);
     const int tid = threadIdx.x, warp = tid >> 5;
 
@@ -243,7 +279,9 @@ __global__ void __launch_bounds__(kLeafThreads, 1) render_window_kernel(DeviceAs
         }
         if (tid == 0) {
             if (staged) mbar_expect_and_copy(s.bar, s.stage, pay_bytes + a0, (uint32_t)(a1 - a0));
-            *s_mask = 1u | (1u << (n - 1));
+            unsigned long long ends = 0ull;
+            for (int w0 = 0; w0 < n; w0 += kRwWin) ends |= (1ull << w0) | (1ull << min(n - 1, w0 + kRwWin - 1));
+            *s_mask = ends;
         }
         if (tid < 48) {
             const int ws = tid / 24, axis = (tid % 24) >> 3, p = tid & 7;
@@ -261,11 +299,11 @@ __global__ void __launch_bounds__(kLeafThreads, 1) render_window_kernel(DeviceAs
         bool done;
         if (staged) {
             const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
-            done = render_window_leaf(a, m, s, e, G, t0, n, sA, sB, sCoef, s_mask, s_knot, bar_mma, taddr, ph_mma, out,
+            done = render_window_leaf(a, m, s, e, G, t0, n, sA, sB, s_mask, s_knot, bar_mma, taddr, ph_mma, out,
                                       frame_stride, leaf);
         } else {
             const GlobalWords m{a.payload};
-            done = render_window_leaf(a, m, s, e, G, t0, n, sA, sB, sCoef, s_mask, s_knot, bar_mma, taddr, ph_mma, out,
+            done = render_window_leaf(a, m, s, e, G, t0, n, sA, sB, s_mask, s_knot, bar_mma, taddr, ph_mma, out,
                                       frame_stride, leaf);
         }
         if (!done) break;
@@ -413,19 +451,31 @@ __global__ void __launch_bounds__(256) render_window_oracle_kernel(DeviceAsset a
     }
 }
 
-void launch_render_window(const DeviceAsset& a, int t0, int n, float* out, uint64_t frame_stride, cudaStream_t s)
+void launch_render_window(const DeviceAsset& asset, int t0, int n, float* out, uint64_t frame_stride, cudaStream_t s)
 {
+    // Two CTAs per SM when the leaf stage allows; leaves whose window exceeds that stage are read
+    // from global memory (the GLOBAL_FALLBACK instantiation).
+    DeviceAsset a = asset;
+    constexpr uint32_t cap2 = ((233472u / 2u - 1024u - kRwHead - kLeafFixed - kStagePad) / 1024u) * 1024u;
+    if (a.g.stage_bytes > cap2) a.g.stage_bytes = cap2;
     const uint32_t smem = kRwHead + kLeafFixed + a.g.stage_bytes + kStagePad;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (a.g.max_window > a.g.stage_bytes) {
-        cudaFuncSetAttribute(render_window_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        render_window_kernel<true><<<sms, kLeafThreads, smem, s>>>(a, t0, n, out, frame_stride);
-    } else {
-        cudaFuncSetAttribute(render_window_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        render_window_kernel<false><<<sms, kLeafThreads, smem, s>>>(a, t0, n, out, frame_stride);
-    }
+    auto go = [&](auto kernel) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        // CTAs per SM from the shared memory per SM and per block (registers allow two: the
+        // kernel's launch bounds)
+        int per_sm = 0, reserved = 0;
+        cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        const int fit = (int)((uint32_t)per_sm / (smem + (uint32_t)reserved));
+        const int per = fit >= 2 ? 2 : 1;
+        kernel<<<sms * per, kLeafThreads, smem, s>>>(a, t0, n, out, frame_stride);
+    };
+    if (a.g.max_window > a.g.stage_bytes) go(render_window_kernel<true>);
+    else go(render_window_kernel<false>);
 }
 
 void launch_render_window_oracle(const DeviceAsset& a, int t0, int n, const float* vals, uint64_t frame_stride,
