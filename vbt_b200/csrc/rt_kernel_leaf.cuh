@@ -108,7 +108,10 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
     const int Cc = (int)cs.controls;
     const int Cf = fine ? (int)fs.controls : (shell ? (int)ss.controls : 0);
     const int Ctot = Cc + Cf;
-    const int nb_max = min(nframes, kLeafCtrlBudget / max(Ctot, 1));
+    // frames per batch: as many as the control buffer holds, rounded down to a multiple of the
+    // warp count when that still leaves a full round (each warp reconstructs whole frames)
+    int nb_max = min(nframes, kLeafCtrlBudget / max(Ctot, 1));
+    if (nb_max < nframes && nb_max > kLeafWarps) nb_max -= nb_max % kLeafWarps;
     const bool stream = steps01 && (e.info & kFlagSorted) != 0u;
     const bool cursor = !stream && monotone && (e.info & kFlagSorted) != 0u;
     const bool plain = !occ && G.w == 8 && G.h == 8 && G.d == 8;
