@@ -562,7 +562,8 @@ int vbt_decode_window(vbt_asset* a, int t0, int n, float* d_out, uint64_t frame_
     if ((reinterpret_cast<uintptr_t>(d_out) & 15u) != 0u || (frame_stride & 3u) != 0u)
         return fail(VBT_STATUS_INVALID_ARGUMENT, "output must be 16-byte aligned, frame_stride a multiple of 4");
     DeviceGuard guard(a->device);
-    launch_render_window(a->dev, t0, n, d_out, frame_stride, static_cast<cudaStream_t>(stream));
+    launch_render_window(a->dev, a->launch_seq.fetch_add(1), t0, n, d_out, frame_stride,
+                         static_cast<cudaStream_t>(stream));
     return check_launch("render_window_kernel");
 }
 

@@ -221,12 +221,14 @@ __device__ __forceinline__ bool render_window_leaf(const DeviceAsset& a, const M
     return true;
 }
 
-// Persistent CTAs over the active leaves (rank-strided), 256 threads, as many per SM as shared
-// memory allows.  out[f * frame_stride + rank * 512 + voxel] for f < n, the current-frame cache
+// Persistent CTAs over the active leaves, 256 threads, as many per SM as shared memory allows;
+// leaves are handed out one at a time by the launch's work counter (grab_leaf), so that CTAs that
+// drew cheap leaves (few knots) take more of them.  out[f * frame_stride + rank * 512 + voxel] for f < n, the current-frame cache
 // layout of frames t0 .. t0 + n - 1.
 template <bool GLOBAL_FALLBACK>
 __global__ void __launch_bounds__(kLeafThreads, 2) render_window_kernel(DeviceAsset a, int t0, int n,
-                                                                        float* __restrict__ out, uint64_t frame_stride)
+                                                                        float* __restrict__ out, uint64_t frame_stride,
+                                                                        unsigned long long* work, uint32_t epoch)
 {
     extern __shared__ __align__(1024) uint8_t rdyn[];
     uint8_t* sA = rdyn;
@@ -236,6 +238,7 @@ __global__ void __launch_bounds__(kLeafThreads, 2) render_window_kernel(DeviceAs
     unsigned long long* s_mask = reinterpret_cast<unsigned long long*>(misc + 8);
     uint32_t* s_taddr = reinterpret_cast<uint32_t*>(misc + 16);
     int* s_knot = reinterpret_cast<int*>(misc + 32);   // a window's knot offsets, ascending
+    uint32_t* s_next = reinterpret_cast<uint32_t*>(misc + 96);   // the next rank from the work counter
     const LeafSmem s = leaf_layout(rdyn + kRwHead);
     const int tid = threadIdx.x, warp = tid >> 5;
 
@@ -249,6 +252,10 @@ __global__ void __launch_bounds__(kLeafThreads, 2) render_window_kernel(DeviceAs
         mbar_init(s.bar, 1);
         mbar_init(bar_mma, 1);
         mbar_init_fence();
+        bool to = false;
+        const uint32_t first = grab_leaf(work, epoch, to);
+        if (to) record_error(a.err, 0u, kErrWaitTimeout);
+        *s_next = first;
     }
     s.rcp[tid] = __frcp_rn((float)tid);
     win_tc_fence_before();
@@ -259,7 +266,15 @@ __global__ void __launch_bounds__(kLeafThreads, 2) render_window_kernel(DeviceAs
     const uint8_t* pay_bytes = reinterpret_cast<const uint8_t*>(a.payload);
     uint32_t ph_tma = 0, ph_mma = 0;
 
-    for (uint32_t rank = blockIdx.x; rank < n_leaves; rank += gridDim.x) {
+    uint32_t rank = *s_next;
+    while (rank < n_leaves) {
+        __syncthreads();   // every thread has read the rank
+        if (tid == 0) {
+            bool to = false;
+            const uint32_t nx = grab_leaf(work, epoch, to);
+            if (to) record_error(a.err, 0u, kErrWaitTimeout);
+            *s_next = nx;
+        }
         const uint32_t leaf = __ldg(a.active_list + rank);
         const LeafEntry e = a.entries[leaf];
         LeafGeom G;
@@ -275,6 +290,8 @@ __global__ void __launch_bounds__(kLeafThreads, 2) render_window_kernel(DeviceAs
             if (tid == 0) record_error(a.err, leaf, st != kOk ? st : kErrDecodeOob);
             for (int i = tid; i < n * 512; i += kLeafThreads)
                 out[(uint64_t)(i >> 9) * frame_stride + (uint64_t)rank * 512u + (i & 511)] = 0.0f;
+            __syncthreads();   // the next rank is visible
+            rank = *s_next;
             continue;
         }
         if (tid == 0) {
@@ -307,6 +324,8 @@ __global__ void __launch_bounds__(kLeafThreads, 2) render_window_kernel(DeviceAs
                                       frame_stride, leaf);
         }
         if (!done) break;
+        __syncthreads();   // the next rank is visible
+        rank = *s_next;
     }
     win_tc_fence_before();
     __syncthreads();
@@ -451,7 +470,8 @@ __global__ void __launch_bounds__(256) render_window_oracle_kernel(DeviceAsset a
     }
 }
 
-void launch_render_window(const DeviceAsset& asset, int t0, int n, float* out, uint64_t frame_stride, cudaStream_t s)
+void launch_render_window(const DeviceAsset& asset, uint32_t seq, int t0, int n, float* out, uint64_t frame_stride,
+                          cudaStream_t s)
 {
     // Two CTAs per SM when the leaf stage allows; leaves whose window exceeds that stage are read
     // from global memory (the GLOBAL_FALLBACK instantiation).
@@ -472,7 +492,12 @@ void launch_render_window(const DeviceAsset& asset, int t0, int n, float* out, u
         cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
         const int fit = (int)((uint32_t)per_sm / (smem + (uint32_t)reserved));
         const int per = fit >= 2 ? 2 : 1;
-        kernel<<<sms * per, kLeafThreads, smem, s>>>(a, t0, n, out, frame_stride);
+        unsigned long long* slot = a.work + seq % kWorkSlots;
+        // inside a stream capture every replay starts from a cleared slot (see launch_leaf_variant)
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+            cudaMemsetAsync(slot, 0, sizeof(unsigned long long), s);
+        kernel<<<sms * per, kLeafThreads, smem, s>>>(a, t0, n, out, frame_stride, slot, seq + 1u);
     };
     if (a.g.max_window > a.g.stage_bytes) go(render_window_kernel<true>);
     else go(render_window_kernel<false>);
