@@ -326,6 +326,18 @@ def run_serving(args, local_rank):
     open_s_p = serve_once(vbt, assets, reqs, pinned, False, at_rate(lam_p))
     open_p_p = serve_once(vbt, assets, reqs, pinned, True, at_rate(lam_p))
     open_s_s = serve_once(vbt, assets, reqs, pinned, False, at_rate(lam_s))
+    # the same requests from a client that keeps its query batches and results on the GPU (a
+    # renderer): point inputs in device memory, every result device-resident
+    dev = {j: (torch.from_numpy(arg.view(np.int32)).to(f"cuda:{local_rank}"), None)
+           for j, (kind, i, arg) in enumerate(reqs) if kind == "points"}
+    serve_once(vbt, assets, reqs[:20], dev, False, None)   # warm-up
+    d_closed_s = serve_once(vbt, assets, reqs, dev, False, None)
+    d_closed_p = serve_once(vbt, assets, reqs, dev, True, None)
+    d_lam_p = 0.8 * d_closed_p["requests_per_s"]
+    d_lam_s = 0.8 * d_closed_s["requests_per_s"]
+    d_open_s_p = serve_once(vbt, assets, reqs, dev, False, at_rate(d_lam_p))
+    d_open_p_p = serve_once(vbt, assets, reqs, dev, True, at_rate(d_lam_p))
+    d_open_s_s = serve_once(vbt, assets, reqs, dev, False, at_rate(d_lam_s))
     for a in assets:
         a.close()
     return {"workload": "serving mix: 70% point batches of 1e3-1e6 uniform (x,y,z,t), 20% z-slices over 1-16 "
@@ -338,7 +350,14 @@ def run_serving(args, local_rank):
                        "poisson_at_0.8x_served_capacity": open_s_s},
             "plain": {"closed_loop": closed_p, "poisson_at_0.8x_plain_capacity": open_p_p},
             "throughput_ratio_closed_loop": closed_s["decoded_values_per_s"] / closed_p["decoded_values_per_s"],
-            "arrival_rates_req_per_s": {"0.8x_plain": lam_p, "0.8x_served": lam_s}}
+            "arrival_rates_req_per_s": {"0.8x_plain": lam_p, "0.8x_served": lam_s},
+            "device_resident": {
+                "workload": "the same requests with point inputs in device memory and every result device-resident",
+                "served": {"closed_loop": d_closed_s, "poisson_at_0.8x_plain_capacity": d_open_s_p,
+                           "poisson_at_0.8x_served_capacity": d_open_s_s},
+                "plain": {"closed_loop": d_closed_p, "poisson_at_0.8x_plain_capacity": d_open_p_p},
+                "throughput_ratio_closed_loop": d_closed_s["decoded_values_per_s"] / d_closed_p["decoded_values_per_s"],
+                "arrival_rates_req_per_s": {"0.8x_plain": d_lam_p, "0.8x_served": d_lam_s}}}
 
 
 # ------------------------------------------------------------------------------ full frames

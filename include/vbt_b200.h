@@ -241,14 +241,17 @@ typedef struct {
 typedef struct {
     uint32_t kind;               /* VBT_REQ_* */
     uint32_t asset;              /* id returned by vbt_server_add_asset */
-    const uint32_t* points;      /* POINTS: host array; must stay valid until the request is done */
+    const uint32_t* points;      /* POINTS: host array (pageable or pinned) or device memory (a
+                                  * client that keeps its query batches on the GPU); must stay valid
+                                  * until the request is done */
     uint64_t n_points;
     uint32_t z;                  /* SLICE */
     int32_t t0, t1;
     const int32_t* frames;       /* FRAMES: host array (copied at submit) */
     uint32_t n_frames;
-    float* host_out;             /* result destination on the host, or NULL to keep the result in
-                                  * device memory until vbt_serve_release */
+    float* host_out;             /* result destination (host memory, pinned or pageable, or device
+                                  * memory), or NULL to keep the result in the server's device
+                                  * memory until vbt_serve_release */
 } vbt_request;
 
 typedef struct {

@@ -257,3 +257,34 @@ def test_device_resident_results(vbt, cuda, assets):
     assert np.array_equal(got.view(np.uint32), d.cpu().numpy().view(np.uint32))
     srv.release(t)
     srv.close()
+
+
+def test_device_resident_requests(vbt, cuda, assets):
+    """A client that keeps its query batches and results on the GPU: point inputs in device memory,
+    results written to device buffers (and slices/frames into device buffers), merged with host
+    requests in one server; every result equals the host-buffer path bit for bit."""
+    reqs = make_requests(assets, seed=9, n=24)
+    ref = run_alone(vbt, cuda, assets, reqs)
+    srv = vbt.Server(hbm_budget_bytes=256 << 20, slots=4)
+    ids = [srv.add_asset(a) for a in assets]
+    keep, tickets = [], []
+    for j, r in enumerate(reqs):
+        kind, i, arg = r
+        out = cuda.empty(max(out_size(assets[i], r), 1), dtype=cuda.float32, device="cuda")
+        if kind == "points":
+            q = cuda.from_numpy(arg.view(np.int32)).to("cuda")   # the same bits, in device memory
+            tickets.append(srv.submit_points(ids[i], q, out))
+            keep.append((q, out))
+        elif kind == "slice":
+            tickets.append(srv.submit_slice(ids[i], arg[0], arg[1], arg[2], out))
+            keep.append((out,))
+        else:
+            tickets.append(srv.submit_frames(ids[i], arg, out))
+            keep.append((out,))
+    for j, t in enumerate(tickets):
+        res = srv.wait(t)
+        assert res.status == 0, (reqs[j][0], res.status)
+        srv.release(t)
+        got = keep[j][-1][:len(ref[j])].cpu().numpy()
+        assert np.array_equal(got.view(np.uint32), ref[j].view(np.uint32)), (j, reqs[j][0])
+    srv.close()

@@ -368,22 +368,29 @@ class Server:
         self._keep[t.value] = keep
         return t.value
 
+    @staticmethod
+    def _buf(x):
+        """Address of a numpy array (host) or a torch tensor (host or device memory), or None."""
+        if x is None:
+            return None
+        return x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data
+
     def submit_points(self, asset_id, xyzt, host_out=None):
-        """xyzt: contiguous uint32 numpy array [n, 4]; host_out: float32 numpy array [n], or None to
-        keep the result in device memory until release()."""
-        req = Request(kind=REQ_POINTS, asset=asset_id, points=xyzt.ctypes.data, n_points=xyzt.shape[0],
-                      host_out=None if host_out is None else host_out.ctypes.data)
+        """xyzt: contiguous uint32 [n, 4] in host memory (numpy, or a pinned torch tensor) or device
+        memory (a CUDA torch tensor); host_out: float32 [n] likewise, or None to keep the result in
+        device memory until release()."""
+        req = Request(kind=REQ_POINTS, asset=asset_id, points=self._buf(xyzt), n_points=xyzt.shape[0],
+                      host_out=self._buf(host_out))
         return self._submit(req, (xyzt, host_out))
 
     def submit_slice(self, asset_id, z, t0, t1, host_out=None):
-        req = Request(kind=REQ_SLICE, asset=asset_id, z=z, t0=t0, t1=t1,
-                      host_out=None if host_out is None else host_out.ctypes.data)
+        req = Request(kind=REQ_SLICE, asset=asset_id, z=z, t0=t0, t1=t1, host_out=self._buf(host_out))
         return self._submit(req, (host_out,))
 
     def submit_frames(self, asset_id, frames, host_out=None):
         fr = (C.c_int32 * len(frames))(*frames)
         req = Request(kind=REQ_FRAMES, asset=asset_id, frames=C.cast(fr, C.c_void_p), n_frames=len(frames),
-                      host_out=None if host_out is None else host_out.ctypes.data)
+                      host_out=self._buf(host_out))
         return self._submit(req, (fr, host_out))
 
     def poll(self, ticket):

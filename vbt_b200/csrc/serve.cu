@@ -128,6 +128,9 @@ struct Unit {
     uint64_t points = 0;
 };
 
+// Memory the copy engines reach directly: pinned host memory, or device (or managed) memory of
+// a GPU -- a client that keeps its query batches and results on the GPU.  Pageable host memory
+// goes through the server's pinned staging.
 bool is_pinned(const void* p)
 {
     if (!p) return false;
@@ -136,7 +139,7 @@ bool is_pinned(const void* p)
         cudaGetLastError();
         return false;
     }
-    return at.type == cudaMemoryTypeHost;
+    return at.type == cudaMemoryTypeHost || at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
 // Segment table of a k-request point unit: starts[k+1], asset[k], 8-byte aligned outs[k].
@@ -358,7 +361,7 @@ void vbt_server::launch(Unit* u, int slot)
             const uint64_t b = 16ull * r->r.n_points;
             if (b) {
                 if (r->pinned_in) {
-                    cudaMemcpyAsync(dq + 16ull * q, r->r.points, b, cudaMemcpyHostToDevice, st);
+                    cudaMemcpyAsync(dq + 16ull * q, r->r.points, b, cudaMemcpyDefault, st);
                 } else {
                     std::memcpy(hpage, r->r.points, b);
                     cudaMemcpyAsync(dq + 16ull * q, hpage, b, cudaMemcpyHostToDevice, st);
@@ -392,7 +395,7 @@ void vbt_server::launch(Unit* u, int slot)
         const uint64_t b = 4ull * r->result_floats;
         if (r->r.host_out && b) {
             void* dst = r->pinned_out ? static_cast<void*>(r->r.host_out) : static_cast<void*>(h_stage + r->stage_out.off);
-            cudaMemcpyAsync(dst, d_arena + r->dev_result.off, b, cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(dst, d_arena + r->dev_result.off, b, cudaMemcpyDefault, st);
         }
     }
     cudaMemcpyAsync(h_err + (size_t)slot * kMaxUnitRequests, d_err, 8ull * k, cudaMemcpyDeviceToHost, st);
