@@ -315,3 +315,36 @@ def test_unsorted_keys_and_descending_frames(vbt, cuda, oracle):
         for i, t in enumerate(ts):
             assert same_bits(got[i], f2.frame(t)), t
     a.close()
+
+
+@pytest.mark.parametrize("name", ["cfg2_plume", "mix_fire_flames"])
+def test_point_queries_sparse_volume(oracle, cuda, vbt, name):
+    """Volumes whose leaves are mostly EMPTY take the compacting point-query kernel (trivial
+    queries answered first, the rest decoded from a per-CTA list); values equal the oracle's, also
+    through the merged serving launch."""
+    p = os.path.join(ASSETS, name + ".vbtp")
+    if not os.path.exists(p):
+        pytest.skip(f"{name} not generated")
+    f = oracle.load(p)
+    a = vbt.Asset(p)
+    rng = np.random.default_rng(17)
+    X, Y, Z = a.dims
+    for nq in (1000, 300_000):
+        q = np.stack([rng.integers(0, X, nq), rng.integers(0, Y, nq), rng.integers(0, Z, nq),
+                      rng.integers(-2, a.frames + 2, nq)], 1).astype(np.int64).astype(np.uint32)
+        dq = cuda.from_numpy(q.view(np.int32)).cuda()
+        out = cuda.empty(nq, dtype=cuda.float32, device="cuda")
+        a.query_points(dq, out)
+        a.sync_status()
+        got = out.cpu().numpy()
+        want = f.query(q, threads=8)
+        assert same_bits(got, want), name
+        srv = vbt.Server(hbm_budget_bytes=256 << 20, slots=2)
+        sid = srv.add_asset(a)
+        ho = np.zeros(nq, np.float32)
+        t = srv.submit_points(sid, np.ascontiguousarray(q), ho)
+        assert srv.wait(t).status == 0
+        srv.release(t)
+        srv.close()
+        assert same_bits(ho, want), name
+    a.close()

@@ -20,6 +20,7 @@ struct vbt_asset {
     vbtb::DeviceAsset dev{};
     uint32_t epoch = 0;
     std::atomic<uint32_t> launch_seq{0};   // decode launches: selects and tags a work-counter slot
+    bool sparse = false;   // render-temporal image given at creation with most leaves EMPTY (point-query shape)
     uint64_t device_bytes = 0;
     std::vector<void*> allocations;
     // staging for the host-buffer calls (grow-only)

@@ -225,6 +225,15 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     const uint64_t scale_off = 52, off_off = scale_off + 4ull * h.coarse_ac_scale_count;
     const uint64_t pay_off = off_off + 4ull * ((uint64_t)h.leaf_count + 1u);
     const uint64_t words = (len - pay_off) / 4u;
+    if (h.profile_type != 2u) {   // route tags of the leaves (word 0 of each non-empty block): a shape hint only
+        uint64_t active = 0;
+        for (uint32_t i = 0; i < h.leaf_count; ++i) {
+            const uint32_t w0 = rd32(b + off_off + 4ull * i), w1 = rd32(b + off_off + 4ull * i + 4u);
+            if (w1 > w0 && w0 < words && (rd32(b + pay_off + 4ull * w0) & 3u) != 0u) ++active;
+        }
+        a->sparse = 2u * active < (uint64_t)h.leaf_count;
+        a->dev.g.sparse = a->sparse ? 1u : 0u;
+    }
     AssetGeom& g = a->dev.g;
     g.width = h.width;
     g.height = h.height;
@@ -480,7 +489,7 @@ int vbt_query_points(vbt_asset* a, const uint32_t* q, uint64_t n, float* out, vo
     if (!a || (n && (!q || !out))) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");
     if (((uintptr_t)q & 15u) != 0u) return fail(VBT_STATUS_INVALID_ARGUMENT, "query buffer must be 16-byte aligned");
     DeviceGuard guard(a->device);
-    launch_query_points(a->dev, q, n, out, static_cast<cudaStream_t>(stream));
+    launch_query_points(a->dev, q, n, out, a->sparse, static_cast<cudaStream_t>(stream));
     return check_launch("query_points_kernel");
 }
 
@@ -523,7 +532,8 @@ int vbt_query_points_host(vbt_asset* a, const uint32_t* q, uint64_t n, float* ou
         return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     CUDA_TRY(cudaMemcpyAsync(a->stage_in, q, 16ull * n, cudaMemcpyHostToDevice, s));
-    launch_query_points(a->dev, static_cast<const uint32_t*>(a->stage_in), n, static_cast<float*>(a->stage_out), s);
+    launch_query_points(a->dev, static_cast<const uint32_t*>(a->stage_in), n, static_cast<float*>(a->stage_out),
+                        a->sparse, s);
     if ((st = check_launch("query_points_kernel"))) return st;
     CUDA_TRY(cudaMemcpyAsync(out, a->stage_out, 4ull * n, cudaMemcpyDeviceToHost, s));
     return vbt_asset_sync_status(a, stream, nullptr);

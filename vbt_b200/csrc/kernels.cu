@@ -1191,6 +1191,99 @@ __device__ __forceinline__ float point_value(const DeviceAsset& a, uint4 qq, uns
     return rt_point(a, e, w, h, d, lx, ly, lz, clamp_frame((int)t, (int)a.g.frames));
 }
 
+// True when point_value returns 0 without decoding anything and without recording an error: a
+// render-temporal query in an EMPTY leaf or outside the volume.
+__device__ __forceinline__ bool point_trivial(const DeviceAsset& a, uint4 qq)
+{
+    if (a.g.profile == 2u) return false;
+    const uint32_t bx = min(a.g.lcx - 1u, qq.x >> 3), by = min(a.g.lcy - 1u, qq.y >> 3), bz = min(a.g.lcz - 1u, qq.z >> 3);
+    const uint32_t leaf = (bz * a.g.lcy + by) * a.g.lcx + bx;
+    const uint32_t info = __ldg(&a.entries[leaf].info), header = __ldg(&a.entries[leaf].header);
+    if (((info >> 16) & 0xFFu) != kOk) return false;   // point_value records the status
+    if ((header & 3u) == kModeEmpty) return true;
+    uint32_t gx, gy, gz;
+    int w, h, d;
+    leaf_extent(a.g, leaf, gx, gy, gz, w, h, d);
+    return (int)(qq.x - bx * 8u) >= w || (int)(qq.y - by * 8u) >= h || (int)(qq.z - bz * 8u) >= d;
+}
+
+// Point queries in chunks of `per` x 128 per CTA.  A first pass answers the trivial ones (EMPTY
+// leaf, outside the volume); a warp with at least half its lanes non-trivial decodes them in
+// place, a sparser warp passes them to a shared-memory list that the CTA's warps then decode with
+// every lane busy -- in a sparse volume most random queries are trivial, and a warp that decoded
+// its few non-trivial lanes in place would leave the rest idle.  Values are point_value's either
+// way.  `per` is chosen on the host so that the grid still fills the GPU.
+constexpr int kPqThreads = 128, kPqMaxPer = 8, kPqMaxChunk = kPqThreads * kPqMaxPer;
+
+template <class Resolve>
+__device__ __forceinline__ void query_chunk(uint64_t n, int per, const uint4* __restrict__ q, const Resolve& resolve)
+{
+    __shared__ uint32_t s_list[kPqMaxChunk];
+    __shared__ uint32_t s_count;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const uint64_t base = (uint64_t)blockIdx.x * (uint64_t)(per * kPqThreads);
+    if (!resolve.sparse(base)) {   // a chunk of a mostly active volume: each thread its own queries
+        for (int r = 0; r < per; ++r) {
+            const uint64_t i = base + (uint64_t)(r * kPqThreads + tid);
+            if (i < n) resolve.second(i, q[i]);
+        }
+        return;
+    }
+    if (tid == 0) s_count = 0u;
+    __syncthreads();
+    for (int r = 0; r < per; ++r) {
+        const uint32_t j = (uint32_t)(r * kPqThreads + tid);
+        const uint64_t i = base + j;
+        bool need = false;
+        uint4 qq = make_uint4(0u, 0u, 0u, 0u);
+        if (i < n) {
+            qq = q[i];
+            need = resolve.first(i, qq);
+        }
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, need);
+        if (__popc(m) >= 16) {
+            if (need) resolve.second(i, qq);
+            continue;
+        }
+        uint32_t wbase = 0u;
+        if (lane == 0 && m) wbase = atomicAdd(&s_count, (uint32_t)__popc(m));
+        wbase = __shfl_sync(0xFFFFFFFFu, wbase, 0);
+        if (need) s_list[wbase + (uint32_t)__popc(m & ((1u << lane) - 1u))] = j;
+    }
+    __syncthreads();
+    const uint32_t cnt = s_count;
+    for (uint32_t k = (uint32_t)tid; k < cnt; k += kPqThreads) {
+        const uint64_t i = base + s_list[k];
+        resolve.second(i, q[i]);
+    }
+}
+
+// Queries per thread: the largest of 8, 4, 2, 1 that still gives four CTAs per SM.
+static int query_per_thread(uint64_t n)
+{
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t want = 4ull * (uint64_t)(sms > 0 ? sms : 1);
+    int per = kPqMaxPer;
+    while (per > 1 && (n + (uint64_t)per * kPqThreads - 1) / ((uint64_t)per * kPqThreads) < want) per >>= 1;
+    return per;
+}
+
+struct OneAssetQueries {
+    const DeviceAsset& a;
+    float* __restrict__ out;
+    __device__ __forceinline__ bool sparse(uint64_t) const { return a.g.sparse != 0u; }
+    __device__ __forceinline__ bool first(uint64_t i, uint4 qq) const
+    {
+        if (!point_trivial(a, qq)) return true;
+        out[i] = 0.0f;
+        return false;
+    }
+    __device__ __forceinline__ void second(uint64_t i, uint4 qq) const { out[i] = point_value(a, qq, a.err); }
+};
+
+// One thread per query: the shape for volumes whose leaves are mostly active.
 __global__ void __launch_bounds__(128) query_points_kernel(DeviceAsset a, const uint32_t* __restrict__ q, uint64_t n,
                                                            float* __restrict__ out)
 {
@@ -1199,10 +1292,57 @@ __global__ void __launch_bounds__(128) query_points_kernel(DeviceAsset a, const 
     out[i] = point_value(a, reinterpret_cast<const uint4*>(q)[i], a.err);
 }
 
+// Compacted chunks: the shape for sparse volumes.
+__global__ void __launch_bounds__(kPqThreads) query_points_compact_kernel(DeviceAsset a,
+                                                                          const uint32_t* __restrict__ q, uint64_t n,
+                                                                          int per, float* __restrict__ out)
+{
+    query_chunk(n, per, reinterpret_cast<const uint4*>(q), OneAssetQueries{a, out});
+}
+
 // Point queries of several requests over several resident assets in one launch.  The segment
 // table holds starts[0..k] (each request's first query; starts[k] = n), asset[k] (request r reads
 // assets[asset[r]]) and, 8-byte aligned after them, outs[k] (request r's result array).  Request
 // r's decode errors go to errs[r].
+struct BatchQueries {
+    const DeviceAsset* __restrict__ assets;
+    const uint32_t* __restrict__ seg;
+    uint32_t k;
+    unsigned long long* errs;
+    __device__ __forceinline__ int request(uint64_t i) const
+    {
+        int lo = 0, hi = (int)k - 1;
+        while (lo < hi) {   // the last request whose first query is at or before i
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(seg + mid) <= (uint32_t)i) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    }
+    // the chunk starting at query i takes the compacting path when its first query's asset is sparse
+    __device__ __forceinline__ bool sparse(uint64_t i) const
+    {
+        return assets[__ldg(seg + k + 1 + request(i))].g.sparse != 0u;
+    }
+    __device__ __forceinline__ void put(int r, uint64_t i, float v) const
+    {
+        const unsigned long long* outs = reinterpret_cast<const unsigned long long*>(seg + ((2u * k + 2u) & ~1u));
+        reinterpret_cast<float*>(__ldg(outs + r))[i - __ldg(seg + r)] = v;
+    }
+    __device__ __forceinline__ bool first(uint64_t i, uint4 qq) const
+    {
+        const int r = request(i);
+        if (!point_trivial(assets[__ldg(seg + k + 1 + r)], qq)) return true;
+        put(r, i, 0.0f);
+        return false;
+    }
+    __device__ __forceinline__ void second(uint64_t i, uint4 qq) const
+    {
+        const int r = request(i);
+        put(r, i, point_value(assets[__ldg(seg + k + 1 + r)], qq, errs + r));
+    }
+};
+
 __global__ void __launch_bounds__(128) query_points_batch_kernel(const DeviceAsset* __restrict__ assets,
                                                                  const uint32_t* __restrict__ seg, uint32_t k,
                                                                  const uint4* __restrict__ q, uint64_t n,
@@ -1210,28 +1350,42 @@ __global__ void __launch_bounds__(128) query_points_batch_kernel(const DeviceAss
 {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int lo = 0, hi = (int)k - 1;
-    while (lo < hi) {   // the last request whose first query is at or before i
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(seg + mid) <= (uint32_t)i) lo = mid;
-        else hi = mid - 1;
-    }
-    const unsigned long long* outs = reinterpret_cast<const unsigned long long*>(seg + ((2u * k + 2u) & ~1u));
-    float* o = reinterpret_cast<float*>(__ldg(outs + lo));
-    o[i - __ldg(seg + lo)] = point_value(assets[__ldg(seg + k + 1 + lo)], q[i], errs + lo);
+    const BatchQueries b{assets, seg, k, errs};
+    b.second(i, q[i]);
+}
+
+__global__ void __launch_bounds__(kPqThreads) query_points_batch_compact_kernel(
+    const DeviceAsset* __restrict__ assets, const uint32_t* __restrict__ seg, uint32_t k, const uint4* __restrict__ q,
+    uint64_t n, int per, unsigned long long* errs)
+{
+    query_chunk(n, per, q, BatchQueries{assets, seg, k, errs});
 }
 
 void launch_query_points_batch(const DeviceAsset* assets, const uint32_t* seg, uint32_t k, const uint4* q, uint64_t n,
-                               unsigned long long* errs, cudaStream_t s)
+                               unsigned long long* errs, int sparse, cudaStream_t s)
 {
     if (n == 0 || k == 0) return;
-    query_points_batch_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(assets, seg, k, q, n, errs);
+    if (sparse == 0) {
+        query_points_batch_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(assets, seg, k, q, n, errs);
+        return;
+    }
+    // with requests on mostly active volumes in the launch, one query per thread for their chunks
+    const int per = sparse == 2 ? query_per_thread(n) : 1;
+    const uint64_t chunk = (uint64_t)per * kPqThreads;
+    query_points_batch_compact_kernel<<<(unsigned)((n + chunk - 1) / chunk), kPqThreads, 0, s>>>(assets, seg, k, q, n,
+                                                                                                   per, errs);
 }
 
-void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, cudaStream_t s)
+void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, bool sparse, cudaStream_t s)
 {
     if (n == 0) return;
-    query_points_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, q, n, out);
+    if (!sparse) {
+        query_points_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, q, n, out);
+        return;
+    }
+    const int per = query_per_thread(n);
+    const uint64_t chunk = (uint64_t)per * kPqThreads;
+    query_points_compact_kernel<<<(unsigned)((n + chunk - 1) / chunk), kPqThreads, 0, s>>>(a, q, n, per, out);
 }
 
 // Z-slice over [t0, t1): one warp per (leaf of the z layer, frame); lanes 0..7 produce rows.

@@ -15,6 +15,7 @@ struct AssetGeom {
     uint64_t payload_words;
     uint32_t stage_bytes;   // shared-memory leaf stage of the render decode kernel (0 = none)
     uint32_t max_window;    // largest 16-byte-aligned window of a non-EMPTY leaf
+    uint32_t sparse;        // 1: render-temporal with most leaves EMPTY (the point-query shape)
 };
 
 struct DeviceAsset {
@@ -83,12 +84,13 @@ void launch_sci_window_oracle(const DeviceAsset& a, int t0, int n, const float* 
 // Studio dispatch shape, VBTStudio/frontend/src/volume_renderer.cpp:704-735).
 void launch_decode_cache_plain(const DeviceAsset& a, int frame, float* out, cudaStream_t s);
 // Point queries: q[4*i..] = (x, y, z, t); out[i].
-void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, cudaStream_t s);
+// sparse: most leaves are EMPTY (the compacting kernel), else one thread per query
+void launch_query_points(const DeviceAsset& a, const uint32_t* q, uint64_t n, float* out, bool sparse, cudaStream_t s);
 // Point queries of k requests over several assets in one launch (a device array of DeviceAsset).
 // seg: starts[0..k] (first query of each request, starts[k] = n), asset[k], then 8-byte aligned
 // outs[k] (result arrays, as 64-bit addresses); decode errors of request r are recorded in errs[r].
 void launch_query_points_batch(const DeviceAsset* assets, const uint32_t* seg, uint32_t k, const uint4* q, uint64_t n,
-                               unsigned long long* errs, cudaStream_t s);
+                               unsigned long long* errs, int sparse, cudaStream_t s);   // sparse: 0 none, 1 some, 2 all
 // Z-slice over a frame range: out[(t - t0) * X*Y + y*X + x] for t in [t0, t1).
 void launch_query_slice(const DeviceAsset& a, uint32_t z, int t0, int t1, float* out, cudaStream_t s);
 

@@ -370,8 +370,13 @@ void vbt_server::launch(Unit* u, int slot)
             }
             q += r->r.n_points;
         }
+        uint64_t sparse_points = 0;
+        for (Req* r : u->reqs)
+            if (assets[r->r.asset]->sparse) sparse_points += r->r.n_points;
         launch_query_points_batch(d_assets, reinterpret_cast<const uint32_t*>(dseg), k,
-                                  reinterpret_cast<const uint4*>(dq), u->points, d_err, st);
+                                  reinterpret_cast<const uint4*>(dq), u->points, d_err,
+                                  sparse_points == 0u ? 0 : (sparse_points == u->points ? 2 : 1),
+                                  st);
         nl = 1;
     } else {
         vbt_asset* a = assets[r0->r.asset];
