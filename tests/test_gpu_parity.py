@@ -279,7 +279,7 @@ def test_corrupted_asset_reports_leaf_status(vbt, cuda, oracle):
     a.close()
 
 
-def test_unsorted_keys_and_descending_frames(vbt, cuda, oracle):
+def test_unsorted_keys_and_descending_frames(vbt, cuda, oracle, tmp_path):
     """Leaves whose key frames are not strictly increasing (here: one key frame byte rewritten)
     lose the sorted flag and take the reference-search path; descending frame lists take it too.
     Both must stay bit-exact with the oracle."""
@@ -296,8 +296,7 @@ def test_unsorted_keys_and_descending_frames(vbt, cuda, oracle):
     ks = int(desc[c] & 0xFFFF)
     kb = leaf0 + v.coarse.key_off
     raw[kb + 3 * (ks + 1)] = raw[kb + 3 * ks]          # duplicate the first key's frame
-    path2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "_work", "unsorted_tiny.vbtp")
-    os.makedirs(os.path.dirname(path2), exist_ok=True)
+    path2 = str(tmp_path / "unsorted_tiny.vbtp")
     open(path2, "wb").write(raw)
     a = vbt.Asset(data=bytes(raw))
     f2 = oracle.load(path2)
