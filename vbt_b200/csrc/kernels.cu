@@ -609,7 +609,7 @@ __device__ __forceinline__ float tri_small(const float* __restrict__ g, int r, c
 }
 
 // Sparse-event residual for local voxel li at frame t (render/src/scientific_decode.cpp:235-295).
-__device__ float sci_sparse(SciReader& rd, uint64_t base, uint32_t hdr, int keep, uint32_t li, uint32_t t)
+__device__ __forceinline__ float sci_sparse(SciReader& rd, uint64_t base, uint32_t hdr, int keep, uint32_t li, uint32_t t)
 {
     const uint32_t count = (hdr >> 16) & 0x0FFFu;
     if (count == 0u) return 0.0f;
@@ -1058,7 +1058,7 @@ void launch_decode_cache_plain(const DeviceAsset& a, int frame, float* out, cuda
 // ---------------------------------------------------------------------------------------------
 // (c) point queries: one thread per query, decoding only the corner controls it needs.
 
-__device__ float rt_point(const DeviceAsset& a, const LeafEntry& e, int w, int h, int d, int lx, int ly, int lz,
+__device__ __forceinline__ float rt_point(const DeviceAsset& a, const LeafEntry& e, int w, int h, int d, int lx, int ly, int lz,
                           int frame)
 {
     const uint32_t* __restrict__ pw = a.payload;
@@ -1104,7 +1104,7 @@ __device__ float rt_point(const DeviceAsset& a, const LeafEntry& e, int w, int h
     return v;
 }
 
-__device__ float sci_point(const DeviceAsset& a, const LeafEntry& e, uint32_t lx, uint32_t ly, uint32_t lz, uint32_t t,
+__device__ __forceinline__ float sci_point(const DeviceAsset& a, const LeafEntry& e, uint32_t lx, uint32_t ly, uint32_t lz, uint32_t t,
                            bool& oob)
 {
     SciReader rd{a.payload, a.g.payload_words, false};
@@ -1207,12 +1207,12 @@ __device__ __forceinline__ bool point_trivial(const DeviceAsset& a, uint4 qq)
     return (int)(qq.x - bx * 8u) >= w || (int)(qq.y - by * 8u) >= h || (int)(qq.z - bz * 8u) >= d;
 }
 
-// Point queries in chunks of `per` x 128 per CTA.  A first pass answers the trivial ones (EMPTY
-// leaf, outside the volume); a warp with at least half its lanes non-trivial decodes them in
-// place, a sparser warp passes them to a shared-memory list that the CTA's warps then decode with
-// every lane busy -- in a sparse volume most random queries are trivial, and a warp that decoded
-// its few non-trivial lanes in place would leave the rest idle.  Values are point_value's either
-// way.  `per` is chosen on the host so that the grid still fills the GPU.
+// Point queries in chunks of `per` x 128 per CTA.  In a chunk of a sparse volume a first pass
+// answers the trivial queries (EMPTY leaf, outside the volume) and passes the others to a
+// shared-memory list that the CTA's warps then decode with every lane busy -- most random queries
+// there are trivial, and a warp that decoded its few non-trivial lanes in place would leave the
+// rest idle.  Chunks of other volumes decode every query in place.  Values are point_value's
+// either way.  `per` is chosen on the host so that the grid still fills the GPU.
 constexpr int kPqThreads = 128, kPqMaxPer = 8, kPqMaxChunk = kPqThreads * kPqMaxPer;
 
 template <class Resolve>
@@ -1241,10 +1241,6 @@ __device__ __forceinline__ void query_chunk(uint64_t n, int per, const uint4* __
             need = resolve.first(i, qq);
         }
         const unsigned m = __ballot_sync(0xFFFFFFFFu, need);
-        if (__popc(m) >= 16) {
-            if (need) resolve.second(i, qq);
-            continue;
-        }
         uint32_t wbase = 0u;
         if (lane == 0 && m) wbase = atomicAdd(&s_count, (uint32_t)__popc(m));
         wbase = __shfl_sync(0xFFFFFFFFu, wbase, 0);
@@ -1293,7 +1289,7 @@ __global__ void __launch_bounds__(128) query_points_kernel(DeviceAsset a, const 
 }
 
 // Compacted chunks: the shape for sparse volumes.
-__global__ void __launch_bounds__(kPqThreads) query_points_compact_kernel(DeviceAsset a,
+__global__ void __launch_bounds__(kPqThreads) query_points_compact_kernel(const __grid_constant__ DeviceAsset a,
                                                                           const uint32_t* __restrict__ q, uint64_t n,
                                                                           int per, float* __restrict__ out)
 {
@@ -1350,8 +1346,15 @@ __global__ void __launch_bounds__(128) query_points_batch_kernel(const DeviceAss
 {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const BatchQueries b{assets, seg, k, errs};
-    b.second(i, q[i]);
+    int lo = 0, hi = (int)k - 1;
+    while (lo < hi) {   // the last request whose first query is at or before i
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(seg + mid) <= (uint32_t)i) lo = mid;
+        else hi = mid - 1;
+    }
+    const unsigned long long* outs = reinterpret_cast<const unsigned long long*>(seg + ((2u * k + 2u) & ~1u));
+    float* o = reinterpret_cast<float*>(__ldg(outs + lo));
+    o[i - __ldg(seg + lo)] = point_value(assets[__ldg(seg + k + 1 + lo)], q[i], errs + lo);
 }
 
 __global__ void __launch_bounds__(kPqThreads) query_points_batch_compact_kernel(
