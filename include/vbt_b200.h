@@ -103,6 +103,15 @@ int vbt_get_leaf_table(vbt_asset* asset, uint32_t* rows);
  * `grid` = CTAs of the persistent launch (0 = one wave of the device). */
 int vbt_decode_cache(vbt_asset* asset, const int* frames, int nframes, float* d_out, uint64_t frame_stride,
                      int grid, void* stream);
+/* The reference Studio's control cache (VBTStudio/frontend/shaders/vbt_cache.comp:168-236), for
+ * consumers written against it: d_out[f * frame_stride + rank * 576 + slot] over the active leaves
+ * of the current page table (vbt_build_page_table first) and frames[0..nframes) (clamped as the
+ * reference clamps, 1..64 frames).  Slot s < 64 holds coarse control s; from slot 64 on, the fine
+ * grid's controls (FINE6) or the Mode2 shell residual controls; other slots hold 0.  Values are
+ * the reference CPU decoder's (decodeRenderTemporalControlValue, src/render_temporal_decode.cpp:
+ * 304-356); render-temporal assets only. */
+int vbt_decode_control_cache(vbt_asset* asset, const int* frames, int nframes, float* d_out, uint64_t frame_stride,
+                             void* stream);
 /* Plain per-leaf launch (one CTA per leaf of the grid, one frame), for comparison. */
 int vbt_decode_cache_plain(vbt_asset* asset, int frame, float* d_out, void* stream);
 /* Dense frames d_out[f * X*Y*Z + (z*Y + y)*X + x] (decodeFrameToDense /

@@ -347,3 +347,47 @@ def test_point_queries_sparse_volume(oracle, cuda, vbt, name):
         srv.close()
         assert same_bits(ho, want), name
     a.close()
+
+
+@pytest.mark.parametrize("path", [p for p in asset_paths() if "sci" not in os.path.basename(p)],
+                         ids=os.path.basename)
+def test_control_cache(loaded, oracle, cuda, path):
+    """The Studio's 576-slot control cache: every slot of sampled active leaves equals the oracle's
+    control decode (coarse in slots 0..63, fine or Mode2 shell controls from 64, zeros elsewhere)."""
+    a, f = loaded(path)
+    a.build_page_table()
+    compact, n = a.page_table()
+    frames = [-1, 0, f.frames // 2, f.frames - 1, f.frames + 2]
+    out = cuda.full((len(frames), max(n, 1), 576), float("nan"), dtype=cuda.float32, device="cuda")
+    a.decode_control_cache(frames, out, frame_stride=max(n, 1) * 576)
+    a.sync_status()
+    got = out.cpu().numpy()
+    off, pay = f.offsets(), f.payload()
+    raw = pay.view(np.uint8)
+    leaves = np.flatnonzero(compact != 0xFFFFFFFF)
+    assert len(leaves) == n
+    for leaf in leaves[::max(1, len(leaves) // 16)]:
+        blk = raw[4 * int(off[leaf]):4 * int(off[leaf + 1])]
+        st, v = oracle.parse_leaf(blk)
+        assert st == 0
+        h = v.header
+
+        def ctrl(start, nbytes, codec, cc, bins, kf, ci, t):
+            s, val = oracle.decode_control(blk[start:start + nbytes], codec, cc, bins, kf, nbytes, f.frames, ci, t)
+            assert s == 0
+            return val
+
+        for j, t in enumerate(frames):
+            want = np.zeros(576, np.float32)
+            cc = h.coarse_res ** 3
+            for s in range(min(64, cc)):
+                want[s] = ctrl(v.coarse_off, v.coarse.total, h.coarse_codec, cc, 8, v.coarse_kf, s, t)
+            if h.mode == 3:
+                cf = h.fine_res ** 3
+                for ci in range(min(512, cf)):
+                    want[64 + ci] = ctrl(v.fine_off, v.fine.total, h.fine_codec, cf, 8, v.fine_kf, ci, t)
+            elif h.mode == 2:
+                for ci in range(min(512, v.shell_active)):
+                    want[64 + ci] = ctrl(v.shell_residual_off, v.shell_residual_bytes, h.fine_codec,
+                                         v.shell_active, 4, v.fine_kf, ci, t)
+            assert same_bits(got[j, compact[leaf]], want), (os.path.basename(path), int(leaf), t)

@@ -98,6 +98,7 @@ _sig = {
     "vbt_build_page_table_noalloc": ([_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp], C.c_int),
     "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_selftest_key_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
+    "vbt_decode_control_cache": ([_vp, C.POINTER(C.c_int), C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_window_error": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, C.POINTER(C.c_double), _vp], C.c_int),
     "vbt_autotune_cache": ([_vp, C.c_int, _vp, C.c_uint64, C.POINTER(Tuning), _vp], C.c_int),
     "vbt_set_tuning": ([_vp, C.POINTER(Tuning)], C.c_int),
@@ -249,6 +250,13 @@ class Asset:
         if frame_stride is None:
             frame_stride = self.active_count * 512
         _check(_lib.vbt_decode_cache(self._h, fr, len(frames), _addr(out), frame_stride, grid, _stream(stream)))
+
+    def decode_control_cache(self, frames, out, frame_stride=None, stream=None):
+        """The Studio's 576-slot control cache of `frames` over the current page table's active
+        leaves: out[f * frame_stride + rank * 576 + slot]."""
+        fr = (C.c_int * len(frames))(*frames)
+        stride = self.active_count * 576 if frame_stride is None else frame_stride
+        _check(_lib.vbt_decode_control_cache(self._h, fr, len(frames), _addr(out), stride, _stream(stream)))
 
     def decode_window(self, t0, n, out, frame_stride=None, stream=None):
         """(d) window decode on the tensor cores of frames [t0, t0 + n) into `out` in the cache

@@ -464,6 +464,18 @@ int vbt_decode_cache(vbt_asset* a, const int* frames, int nframes, float* out, u
     return check_launch("decode_kernel<cache>");
 }
 
+int vbt_decode_control_cache(vbt_asset* a, const int* frames, int nframes, float* out, uint64_t stride, void* stream)
+{
+    if (!a || !out) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    if (a->hdr.profile_type == 2u)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "the control cache covers render-temporal assets");
+    int st = check_frames(a, frames, nframes);
+    if (st) return st;
+    DeviceGuard guard(a->device);
+    launch_control_cache(a->dev, frames, nframes, out, stride, static_cast<cudaStream_t>(stream));
+    return check_launch("control_cache_kernel");
+}
+
 int vbt_decode_cache_plain(vbt_asset* a, int frame, float* out, void* stream)
 {
     if (!a || !out) return fail(VBT_STATUS_INVALID_ARGUMENT, "null argument");

@@ -985,6 +985,61 @@ void launch_decode_cache(const DeviceAsset& a, uint32_t seq, const int* frames, 
         launch_rt_leaf(a, seq, fl, out, stride, grid, false, s);
 }
 
+// The current-frame control cache of the reference Studio (VBTStudio/frontend/shaders/
+// vbt_cache.comp:168-236): 576 slots per active leaf and frame -- coarse control s in slot s < 64,
+// from slot 64 on the fine grid's controls (FINE6) or the Mode2 shell residual controls, 0 in every
+// slot past a leaf's controls.  Values are the reference CPU decoder's (decode_control; the shader
+// blends with mix(), which can differ in the last bit).  One CTA per active leaf at a time.
+constexpr uint32_t kControlCacheStride = 576u;
+
+__global__ void __launch_bounds__(256) control_cache_kernel(DeviceAsset a, FrameList fl, float* __restrict__ out,
+                                                            uint64_t frame_stride)
+{
+    const uint32_t n_leaves = *(volatile const uint32_t*)a.counters;
+    const int total = (int)a.g.frames;
+    const uint32_t* __restrict__ pw = a.payload;
+    for (uint32_t rank = blockIdx.x; rank < n_leaves; rank += gridDim.x) {
+        const uint32_t leaf = __ldg(a.active_list + rank);
+        const LeafEntry e = a.entries[leaf];
+        const uint32_t st = entry_status(e);
+        const bool ok = st == kOk && (e.header & 3u) != kModeEmpty;
+        if (st != kOk && threadIdx.x == 0) record_error(a.err, leaf, st);
+        const uint64_t base = 4ull * e.word_off;
+        const uint32_t cres = (e.header >> 6) & 7u, fres = (e.header >> 9) & 7u;
+        const bool fine = (e.info & kFlagFine) != 0u, shell = (e.info & kFlagShell) != 0u;
+        const StreamRef cs{base + 8u, cres * cres * cres, 8u, e.kf & 0xFFFFu, (e.header >> 2) & 3u};
+        const StreamRef fs{base + 8u + e.coarse_bytes, fres * fres * fres, 8u, e.kf >> 16, (e.header >> 4) & 3u};
+        const StreamRef ss{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
+        for (int j = 0; j < fl.n; ++j) {
+            const int t = clamp_frame(fl.f[j], total);
+            const uint32_t b8 = time_bin(t, 8u, total), b4 = time_bin(t, 4u, total);
+            float* o = out + (uint64_t)j * frame_stride + (uint64_t)rank * kControlCacheStride;
+            for (uint32_t slot = threadIdx.x; slot < kControlCacheStride; slot += blockDim.x) {
+                float v = 0.0f;
+                if (ok) {
+                    if (slot < 64u) {
+                        if (slot < cs.controls) v = decode_control(pw, cs, slot, t, b8);
+                    } else {
+                        const uint32_t ci = slot - 64u;
+                        if (fine && ci < fs.controls) v = decode_control(pw, fs, ci, t, b8);
+                        else if (shell && ci < ss.controls) v = decode_control(pw, ss, ci, t, b4);
+                    }
+                }
+                o[slot] = v;
+            }
+        }
+    }
+}
+
+void launch_control_cache(const DeviceAsset& a, const int* frames, int nframes, float* out, uint64_t stride,
+                          cudaStream_t s)
+{
+    FrameList fl{};
+    fl.n = nframes;
+    for (int i = 0; i < nframes; ++i) fl.f[i] = frames[i];
+    control_cache_kernel<<<default_grid(), 256, 0, s>>>(a, fl, out, stride);
+}
+
 void launch_decode_dense(const DeviceAsset& a, uint32_t seq, const int* frames, int nframes, float* out, int grid,
                          cudaStream_t s)
 {

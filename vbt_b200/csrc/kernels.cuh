@@ -73,6 +73,8 @@ int decode_warp_grid();
 void launch_sci_window(const DeviceAsset& a, int t0, int n, float* out, uint64_t frame_stride, cudaStream_t s);
 // FP64 oracle of a scientific window: stats[0] max |err| (double bits), stats[1] sum err^2
 // (double), stats[2] / stats[3] oracle min / max (order-preserving bits).
+void launch_control_cache(const DeviceAsset& a, const int* frames, int nframes, float* out, uint64_t stride,
+                          cudaStream_t s);
 void launch_render_window(const DeviceAsset& a, uint32_t seq, int t0, int n, float* out, uint64_t frame_stride,
                           cudaStream_t s);
 void launch_render_window_oracle(const DeviceAsset& a, int t0, int n, const float* vals, uint64_t frame_stride,
