@@ -112,6 +112,38 @@ int vbt_decode_cache(vbt_asset* asset, const int* frames, int nframes, float* d_
  * 304-356); render-temporal assets only. */
 int vbt_decode_control_cache(vbt_asset* asset, const int* frames, int nframes, float* d_out, uint64_t frame_stride,
                              void* stream);
+/* ---- Ray sampling from the control cache ------------------------------------------------------
+ * The Studio's sampler (VBTStudio/frontend/shaders/vbt_sample.comp:322-622) as plain CUDA, one
+ * thread per ray, results in a device buffer.  Rays and results are the shader's SmokeRayPacked
+ * and VbtSampleResult.  d_controls is the control cache of frame params->frame_index
+ * (vbt_decode_control_cache) over the current page table.  render_mode 0 accumulates the field
+ * along each ray over step_count steps (surface_model != 0: into 8 depth bins, primary then
+ * auxiliary); render_mode 1 traces the surface phi = surface_iso (primary = normal, hit t or -1;
+ * auxiliary = thickness, floor flag, floor shadow, |n . -dir|).  Single precision, each operation
+ * rounded, GLSL mix / min / max / clamp; round() rounds halves away from zero; a coarse grid over
+ * 64 controls is decoded from the payload.  Render-temporal assets; both buffers 16-byte aligned. */
+typedef struct {
+    float origin_tmin[4]; /* origin x, y, z and t_min */
+    float dir_tmax[4];    /* direction x, y, z and t_max */
+} vbt_ray;
+typedef struct {
+    float primary[4];
+    float auxiliary[4];
+} vbt_sample_result;
+typedef struct {
+    uint32_t step_count;
+    int32_t frame_index;
+    float bbox_min[3];         /* world position of voxel (0, 0, 0) */
+    uint32_t render_mode;      /* 0 density accumulation, 1 level-set surface */
+    float voxel_size, background_value, surface_iso, surface_epsilon_voxels, surface_normal_step, max_step_voxels;
+    uint32_t surface_model;
+    float floor_height;
+    uint32_t shadow_steps;
+    uint32_t up_axis;          /* the shader's `padding`: 2 = z up for the floor plane and key light */
+} vbt_sample_params;
+int vbt_sample_rays(vbt_asset* asset, const float* d_controls, const vbt_sample_params* params, const vbt_ray* d_rays,
+                    uint32_t n, vbt_sample_result* d_out, void* stream);
+
 /* Plain per-leaf launch (one CTA per leaf of the grid, one frame), for comparison. */
 int vbt_decode_cache_plain(vbt_asset* asset, int frame, float* d_out, void* stream);
 /* Dense frames d_out[f * X*Y*Z + (z*Y + y)*X + x] (decodeFrameToDense /

@@ -40,6 +40,15 @@ class VoHeader(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("mode", "coarse_codec", "fine_codec", "coarse_res", "fine_res")]
 
 
+class VoSampleParams(C.Structure):
+    """vo_sample_params (vbt_oracle.h); the same layout as vbt_sample_params (include/vbt_b200.h)."""
+    _fields_ = [("step_count", C.c_uint32), ("frame_index", C.c_int32), ("bbox_min", C.c_float * 3),
+                ("render_mode", C.c_uint32), ("voxel_size", C.c_float), ("background_value", C.c_float),
+                ("surface_iso", C.c_float), ("surface_epsilon_voxels", C.c_float), ("surface_normal_step", C.c_float),
+                ("max_step_voxels", C.c_float), ("surface_model", C.c_uint32), ("floor_height", C.c_float),
+                ("shadow_steps", C.c_uint32), ("up_axis", C.c_uint32)]
+
+
 class VoLeafView(C.Structure):
     _fields_ = [("header", VoHeader), ("coarse_kf", C.c_uint32), ("fine_kf", C.c_uint32),
                 ("coarse_off", C.c_uint32), ("fine_off", C.c_uint32), ("total", C.c_uint32),
@@ -67,6 +76,8 @@ class Oracle:
         L.vo_query_points.argtypes = [C.POINTER(VoFile), u32p, C.c_uint64, f32p, C.c_int]
         L.vo_sci_frame.argtypes = [C.POINTER(VoFile), C.c_uint32, f32p, C.c_int]
         L.vo_sci_query_points.argtypes = [C.POINTER(VoFile), u32p, C.c_uint64, f32p, C.c_int]
+        L.vo_control_cache.argtypes = [C.POINTER(VoFile), C.c_int, u32p, f32p]
+        L.vo_sample_rays.argtypes = [C.POINTER(VoFile), f32p, u32p, C.POINTER(VoSampleParams), f32p, C.c_uint32, f32p]
         L.vo_decode_control.argtypes = [u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
                                         C.c_int, C.c_uint32, C.c_int, f32p]
         L.vo_decode_shell_voxel.argtypes = [u8p, C.POINTER(VoLeafView), C.c_int, C.c_uint32, C.c_int, f32p]
@@ -159,6 +170,24 @@ class OracleFile:
         if st:
             raise RuntimeError(f"oracle status {st}")
         return out[: n * 512].reshape(n, 512)
+
+    def control_cache(self, t, compact):
+        """The Studio's 576-slot control cache of frame t (vbt_cache.comp), [active, 576]."""
+        n = int(np.count_nonzero(compact != 0xFFFFFFFF))
+        out = np.zeros(max(n, 1) * 576, np.float32)
+        c = np.ascontiguousarray(compact, np.uint32)
+        self.o.lib.vo_control_cache(C.byref(self.f), t, _ptr(c, u32p), _ptr(out, f32p))
+        return out[: n * 576].reshape(n, 576)
+
+    def sample_rays(self, cache, compact, params, rays):
+        """The Studio's ray sampler (vbt_sample.comp): rays [n, 8] -> results [n, 8]."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.zeros_like(r)
+        cc = np.ascontiguousarray(cache, np.float32).reshape(-1)
+        c = np.ascontiguousarray(compact, np.uint32)
+        self.o.lib.vo_sample_rays(C.byref(self.f), _ptr(cc, f32p), _ptr(c, u32p), C.byref(params), _ptr(r, f32p),
+                                  r.shape[0], _ptr(out, f32p))
+        return out
 
     def query(self, xyzt, threads=0):
         q = np.ascontiguousarray(xyzt, np.uint32)

@@ -98,6 +98,24 @@ void vo_sci_query_points(const vo_file* f, const uint32_t* xyzt, uint64_t n, flo
 double vo_dct_basis_f64(int total, int index, int k);
 float vo_dct_basis(int total, int index, int k);
 
+/* The Studio's control cache and ray sampler (vbt_sample_oracle.c): the push constants of
+ * VBTStudio/frontend/shaders/vbt_sample.comp:38-66 that are not the asset's own geometry.
+ * up_axis is the shader's `padding` field (2: z up for the floor plane and key light). */
+typedef struct {
+    uint32_t step_count;
+    int32_t frame_index;
+    float bbox_min[3];
+    uint32_t render_mode;      /* 0 density accumulation, 1 level-set surface */
+    float voxel_size, background_value, surface_iso, surface_epsilon_voxels, surface_normal_step, max_step_voxels;
+    uint32_t surface_model;
+    float floor_height;
+    uint32_t shadow_steps;
+    uint32_t up_axis;
+} vo_sample_params;
+int vo_control_cache(const vo_file* f, int frame, const uint32_t* compact, float* cache576);
+void vo_sample_rays(const vo_file* f, const float* cache576, const uint32_t* compact, const vo_sample_params* p,
+                    const float* rays, uint32_t n, float* results);
+
 #ifdef __cplusplus
 }
 #endif

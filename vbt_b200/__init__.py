@@ -50,6 +50,15 @@ class Request(C.Structure):
                 ("n_frames", C.c_uint32), ("host_out", C.c_void_p)]
 
 
+class SampleParams(C.Structure):
+    """vbt_sample_params: the sampler's settings besides the asset's geometry."""
+    _fields_ = [("step_count", C.c_uint32), ("frame_index", C.c_int32), ("bbox_min", C.c_float * 3),
+                ("render_mode", C.c_uint32), ("voxel_size", C.c_float), ("background_value", C.c_float),
+                ("surface_iso", C.c_float), ("surface_epsilon_voxels", C.c_float), ("surface_normal_step", C.c_float),
+                ("max_step_voxels", C.c_float), ("surface_model", C.c_uint32), ("floor_height", C.c_float),
+                ("shadow_steps", C.c_uint32), ("up_axis", C.c_uint32)]
+
+
 class RequestResult(C.Structure):
     _fields_ = [("status", C.c_int), ("bad_leaf", C.c_uint32), ("result_floats", C.c_uint64),
                 ("device_result", C.c_void_p), ("submit_ms", C.c_double), ("start_ms", C.c_double),
@@ -98,6 +107,7 @@ _sig = {
     "vbt_build_page_table_noalloc": ([_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp], C.c_int),
     "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_selftest_key_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
+    "vbt_sample_rays": ([_vp, _vp, C.POINTER(SampleParams), _vp, C.c_uint32, _vp, _vp], C.c_int),
     "vbt_decode_control_cache": ([_vp, C.POINTER(C.c_int), C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_window_error": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, C.POINTER(C.c_double), _vp], C.c_int),
     "vbt_autotune_cache": ([_vp, C.c_int, _vp, C.c_uint64, C.POINTER(Tuning), _vp], C.c_int),
@@ -257,6 +267,13 @@ class Asset:
         fr = (C.c_int * len(frames))(*frames)
         stride = self.active_count * 576 if frame_stride is None else frame_stride
         _check(_lib.vbt_decode_control_cache(self._h, fr, len(frames), _addr(out), stride, _stream(stream)))
+
+    def sample_rays(self, controls, params, rays, out, stream=None):
+        """Ray sampling from the control cache `controls` of frame params.frame_index: rays [n, 8]
+        (origin, t_min, direction, t_max) and out [n, 8] float32 device tensors."""
+        n = rays.shape[0]
+        _check(_lib.vbt_sample_rays(self._h, _addr(controls), C.byref(params), _addr(rays), n, _addr(out),
+                                    _stream(stream)))
 
     def decode_window(self, t0, n, out, frame_stride=None, stream=None):
         """(d) window decode on the tensor cores of frames [t0, t0 + n) into `out` in the cache
