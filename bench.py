@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-window", action="store_true")
     p.add_argument("--no-full-frame", action="store_true")
+    p.add_argument("--no-sampler", action="store_true")
     p.add_argument("--serve-requests", type=int, default=300)
     return p.parse_args()
 
@@ -506,6 +507,115 @@ def run_window_render(args, local_rank, reps=5):
     return out
 
 
+# ------------------------------------------------------------------------------ ray sampler
+def camera_rays(dims, width, height, fov_deg=40.0):
+    """A pinhole camera outside the volume looking at its centre: rays [width * height, 8] float32
+    (origin, t_min = 0, direction, t_max), each starting where it enters the volume's box and
+    ending where it leaves it (t_max = 0 for rays that miss), as a ray generator hands them over."""
+    X, Y, Z = dims
+    centre = np.array([X / 2.0, Y / 2.0, Z / 2.0])
+    eye = centre + np.array([0.35 * X, -1.6 * Y, 0.45 * Z])
+    fwd = centre - eye
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, [0.0, 0.0, 1.0])
+    right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    h = np.tan(np.radians(fov_deg) / 2.0)
+    u = (np.arange(width) + 0.5) / width * 2.0 - 1.0
+    v = (np.arange(height) + 0.5) / height * 2.0 - 1.0
+    uu, vv = np.meshgrid(u * h * width / height, v * h)
+    d = fwd[None, None, :] + uu[..., None] * right + vv[..., None] * up
+    d /= np.linalg.norm(d, axis=2, keepdims=True)
+    d = d.reshape(-1, 3)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = 1.0 / d
+        t0 = (np.zeros(3) - eye) * inv
+        t1 = (np.array([X - 1.0, Y - 1.0, Z - 1.0]) - eye) * inv
+    near = np.maximum(np.minimum(t0, t1).max(axis=1), 0.0)
+    far = np.maximum(t0, t1).min(axis=1)
+    hit = far > near
+    rays = np.zeros((height * width, 8), np.float32)
+    rays[:, 0:3] = eye + d * np.where(hit, near, 0.0)[:, None]
+    rays[:, 4:7] = d
+    rays[:, 7] = np.where(hit, far - near, 0.0)
+    return rays
+
+
+def run_sampler(args, local_rank, reps=5):
+    """Ray sampling from the control cache (vbt_sample_rays; the Studio's vbt_sample.comp) on one
+    B200: a 1920 x 1080 pinhole view of the plume (density accumulation, 256 steps per ray) and of
+    the level set (surface tracing with thickness and floor shadow, up to 160 steps), one frame's
+    control cache built first.  Rays/s and samples/s of device time, beside the C restatement of
+    the shader (the oracle) on the host threads for a bounded sample of the same rays."""
+    import torch
+    import vbt_b200 as vbt
+    from oracle.oracle import Oracle, VoSampleParams
+    scenes = [("cfg2_plume", 0, 256, 0), ("mix_sdf", 1, 160, 1)]
+    out = {}
+    orc = None
+    for name, mode, steps, model in scenes:
+        path = os.path.join(ROOT, "assets", name + ".vbtp")
+        if not os.path.exists(path):
+            continue
+        a = vbt.Asset(path, device=local_rank)
+        a.build_page_table()
+        frame = a.frames // 2
+        n_act = a.active_count
+        dev = f"cuda:{local_rank}"
+        ctrl = torch.empty((1, max(n_act, 1), 576), dtype=torch.float32, device=dev)
+        rays = camera_rays(a.dims, 1920, 1080)
+        d_rays = torch.from_numpy(rays).to(dev)
+        res = torch.empty_like(d_rays)
+        p = vbt.SampleParams()
+        p.step_count, p.frame_index, p.render_mode, p.voxel_size = steps, frame, mode, 1.0
+        p.background_value = 1.0 if mode == 1 else 0.0
+        p.surface_iso, p.surface_epsilon_voxels, p.surface_normal_step, p.max_step_voxels = 0.0, 0.5, 1.0, 4.0
+        p.surface_model, p.floor_height, p.shadow_steps, p.up_axis = model, 1.0, 48, 2
+        s = torch.cuda.Stream(device=dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+               torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        with torch.cuda.stream(s):
+            a.decode_control_cache([frame], ctrl, frame_stride=max(n_act, 1) * 576, stream=s)
+            a.sample_rays(ctrl, p, d_rays, res, stream=s)
+            for e0, e1, e2 in ev:
+                e0.record(s)
+                a.decode_control_cache([frame], ctrl, frame_stride=max(n_act, 1) * 576, stream=s)
+                e1.record(s)
+                a.sample_rays(ctrl, p, d_rays, res, stream=s)
+                e2.record(s)
+        s.synchronize()
+        a.sync_status(s)
+        cache_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1, _ in ev)
+        ray_ms = statistics.mean(e1.elapsed_time(e2) for _, e1, e2 in ev)
+        n = rays.shape[0]
+        entry = {"rays": n, "render_mode": mode, "step_count": steps, "frame": frame,
+                 "control_cache_ms": cache_ms, "sample_ms": ray_ms, "rays_per_s": n / (ray_ms * 1e-3)}
+        if mode == 0:
+            entry["samples_per_s"] = n * steps / (ray_ms * 1e-3)
+        else:
+            entry["rays_hit"] = int((res[:, 3] >= 0).sum().item())
+        # the C restatement on the host threads, on a bounded sample of the rays
+        if not args.no_cpu:
+            orc = orc or Oracle()
+            f = orc.load(path)
+            compact, _ = f.page_table()
+            cache = f.control_cache(frame, compact)
+            q = VoSampleParams()
+            for fld, _ in VoSampleParams._fields_:
+                if fld != "bbox_min":
+                    setattr(q, fld, getattr(p, fld))
+            m = 20000 if mode == 0 else 50000
+            sample = rays[:: max(1, n // m)][:m]
+            t0 = time.perf_counter()
+            f.sample_rays(cache, compact, q, sample)
+            el = time.perf_counter() - t0
+            entry["cpu_restatement"] = {"rays_per_s": sample.shape[0] / el, "cores": os.cpu_count(),
+                                        "sample": f"{sample.shape[0]} of the {n} rays"}
+        out[name] = entry
+        a.close()
+    return out or {"skipped": "assets not generated"}
+
+
 # ------------------------------------------------------------------------------ arms
 def run_reference(args, rank, world):
     """The reference's own CPU decoder on the host cores, same metric and workload; each step is
@@ -677,6 +787,10 @@ def run_ours(args, rank, local_rank, world):
     if rank == 0 and world == 1 and not args.no_full_frame:
         full_frame = run_full_frame(args, local_rank, a, rows)
 
+    sampler = None
+    if rank == 0 and world == 1 and not args.no_sampler:
+        sampler = run_sampler(args, local_rank)
+
     window = window_render = None
     if rank == 0 and world == 1 and not args.no_window:
         window = run_window(args, local_rank)
@@ -713,7 +827,7 @@ def run_ours(args, rank, local_rank, world):
                 "plain": {"value": plain_value, "unit": "voxels/s", "ms_per_step": plain_ms,
                           "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
                 "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "precision_window": window,
-                "precision_window_render": window_render, "full_frame": full_frame,
+                "precision_window_render": window_render, "full_frame": full_frame, "ray_sampler": sampler,
                 "gpu_launches": args.steps * (1 + len(chunks)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
