@@ -144,6 +144,17 @@ typedef struct {
 int vbt_sample_rays(vbt_asset* asset, const float* d_controls, const vbt_sample_params* params, const vbt_ray* d_rays,
                     uint32_t n, vbt_sample_result* d_out, void* stream);
 
+/* ---- VBTPACK4 writer, payload half ------------------------------------------------------------
+ * What writeRenderTemporalProbeFile (src/render_temporal_kf_probe_main.cpp:2561-2585) builds on
+ * the host, on the GPU: leaf_count packed leaf blocks (any byte lengths, 0 included) concatenated
+ * in d_blocks, block i at bytes [d_block_offsets[i], d_block_offsets[i + 1]) -> d_offsets
+ * (leaf_count + 1 word offsets) and d_payload (each block padded with zero bytes to whole words, in
+ * leaf order).  *total_words = d_offsets[leaf_count]; VBT_STATUS_LIMIT when it exceeds
+ * payload_capacity_words or 2^32 words (d_payload is then not written).  The file is the 52-byte
+ * header, d_offsets and d_payload.  Synchronises `stream` once (to read the payload size). */
+int vbt_pack_payload(const uint8_t* d_blocks, const uint64_t* d_block_offsets, uint32_t leaf_count, uint32_t* d_offsets,
+                     uint32_t* d_payload, uint64_t payload_capacity_words, uint64_t* total_words, void* stream);
+
 /* Plain per-leaf launch (one CTA per leaf of the grid, one frame), for comparison. */
 int vbt_decode_cache_plain(vbt_asset* asset, int frame, float* d_out, void* stream);
 /* Dense frames d_out[f * X*Y*Z + (z*Y + y)*X + x] (decodeFrameToDense /

@@ -62,6 +62,19 @@ def build(ref=False):
     subprocess.check_call(["make", "-s", "-C", HERE, "-j8"] + targets)
 
 
+def pack_payload(blocks):
+    """The payload half of writeRenderTemporalProbeFile (src/render_temporal_kf_probe_main.cpp:
+    2561-2585): offsetsWords[i] = payload bytes so far / 4, each leaf block padded with zero bytes
+    to a multiple of 4, offsetsWords[n] = payload words.  blocks: list of bytes."""
+    offsets = np.zeros(len(blocks) + 1, np.uint32)
+    pool = bytearray()
+    for i, b in enumerate(blocks):
+        offsets[i] = len(pool) // 4
+        pool += bytes(b) + b"\0" * ((4 - len(b) % 4) % 4)
+    offsets[-1] = len(pool) // 4
+    return offsets, np.frombuffer(bytes(pool), np.uint32).copy()
+
+
 class Oracle:
     def __init__(self):
         if not os.path.exists(ORACLE_SO):

@@ -167,3 +167,19 @@ def test_corrupted_leaves_statuses(oracle, reference):
                         assert st == ERR[err]
                 checked += 1
     assert checked > 100
+
+
+def test_pack_payload_restatement_rebuilds_reference_files():
+    """oracle.pack_payload (writeRenderTemporalProbeFile's payload loop) reproduces the payload and
+    offsets of files the reference encoder wrote."""
+    from oracle.oracle import pack_payload
+    for name in ("tiny_density", "tiny_levelset"):
+        raw = open(os.path.join(GOLDEN, "assets", name + ".vbtp"), "rb").read()
+        h = np.frombuffer(raw[8:52], np.uint32)
+        leaf_count, scale_count = int(h[8]), int(h[10])
+        off_at = 52 + 4 * scale_count
+        offsets = np.frombuffer(raw[off_at:off_at + 4 * (leaf_count + 1)], np.uint32)
+        pay_at = off_at + 4 * (leaf_count + 1)
+        blocks = [raw[pay_at + 4 * int(offsets[i]):pay_at + 4 * int(offsets[i + 1])] for i in range(leaf_count)]
+        off, pay = pack_payload(blocks)
+        assert raw[:off_at] + off.tobytes() + pay.tobytes() == raw

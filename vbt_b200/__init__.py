@@ -107,6 +107,7 @@ _sig = {
     "vbt_build_page_table_noalloc": ([_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp], C.c_int),
     "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_selftest_key_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
+    "vbt_pack_payload": ([_vp, _vp, C.c_uint32, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64), _vp], C.c_int),
     "vbt_sample_rays": ([_vp, _vp, C.POINTER(SampleParams), _vp, C.c_uint32, _vp, _vp], C.c_int),
     "vbt_decode_control_cache": ([_vp, C.POINTER(C.c_int), C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_window_error": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, C.POINTER(C.c_double), _vp], C.c_int),
@@ -342,6 +343,17 @@ class Asset:
     def decode_frames_host(self, frames, out, stream=None):
         fr = (C.c_int32 * len(frames))(*frames)
         _check(_lib.vbt_decode_frames_host(self._h, fr, len(frames), out.ctypes.data, _stream(stream)))
+
+
+def pack_payload(blocks, block_offsets, offsets, payload, stream=None):
+    """VBTPACK4 payload assembly on the GPU: blocks (uint8 device tensor), block_offsets (int64
+    device tensor, n + 1 byte offsets) -> offsets (int32 device tensor, n + 1 word offsets) and
+    payload (int32 device tensor); returns the payload size in words."""
+    total = C.c_uint64()
+    n = block_offsets.shape[0] - 1
+    _check(_lib.vbt_pack_payload(_addr(blocks), _addr(block_offsets), n, _addr(offsets), _addr(payload),
+                                 payload.numel() if payload is not None else 0, C.byref(total), _stream(stream)))
+    return total.value
 
 
 def selftest_key_division(b_max=65535, device=0):
