@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvbtref.so")
+KFREF_SO = os.path.join(HERE, "_ref", "libkfref.so")
 
 u8p = C.POINTER(C.c_uint8)
 u32p = C.POINTER(C.c_uint32)
@@ -47,6 +48,24 @@ class VoSampleParams(C.Structure):
                 ("surface_iso", C.c_float), ("surface_epsilon_voxels", C.c_float), ("surface_normal_step", C.c_float),
                 ("max_step_voxels", C.c_float), ("surface_model", C.c_uint32), ("floor_height", C.c_float),
                 ("shadow_steps", C.c_uint32), ("up_axis", C.c_uint32)]
+
+
+class VoKeyframeProfile(C.Structure):
+    """vo_keyframe_profile (vbt_oracle.h); the same layout as vbt_keyframe_profile (include/vbt_b200.h).
+    Defaults are the reference encoder's (src/render_temporal_kf_probe_main.cpp:51-58, :477)."""
+    _fields_ = [("eps_abs", C.c_float), ("eps_rel", C.c_float), ("gamma_delta", C.c_float),
+                ("render_cutoff", C.c_float), ("cutoff_band", C.c_float), ("cutoff_temporal_protect", C.c_uint32),
+                ("iso_surface_protect", C.c_uint32), ("iso_value", C.c_float), ("iso_band", C.c_float),
+                ("bg_threshold", C.c_double)]
+
+    def __init__(self, **kw):
+        d = dict(eps_abs=1e-5, eps_rel=0.02, gamma_delta=0.2, render_cutoff=0.0003, cutoff_band=0.0001,
+                 cutoff_temporal_protect=1, iso_surface_protect=0, iso_value=0.0, iso_band=0.0)
+        d.update(kw)
+        if "bg_threshold" not in kw:   # bgZeroRatio * cutoff in float, as the encoder forms it
+            c = np.float32(d["render_cutoff"])
+            d["bg_threshold"] = float(np.float32(0.3) * c) if c > 0 else -1.0
+        super().__init__(**d)
 
 
 class VoLeafView(C.Structure):
@@ -102,6 +121,40 @@ class Oracle:
         L.vo_float_to_half.restype = C.c_uint16
         L.vo_dct_basis.restype = C.c_float
         L.vo_dct_basis_f64.restype = C.c_double
+        i32p = C.POINTER(C.c_int)
+        L.vo_detect_keyframes.argtypes = [f32p, C.c_int, C.POINTER(VoKeyframeProfile), i32p, i32p]
+        L.vo_reconstruct.argtypes = [f32p, C.c_int, i32p, C.c_int, f32p]
+        L.vo_keyframe_pass.argtypes = [f32p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(VoKeyframeProfile), u32p,
+                                       u32p, u8p, f32p, C.POINTER(C.c_double), C.c_int]
+
+    def detect_keyframes(self, series, profile):
+        """(keys, used_protect) of detectDensityKeyFrames on one series."""
+        v = np.ascontiguousarray(series, np.float32)
+        keys = np.zeros(max(1, v.size), np.int32)
+        used = C.c_int()
+        k = self.lib.vo_detect_keyframes(_ptr(v, f32p), v.size, C.byref(profile), _ptr(keys, C.POINTER(C.c_int)),
+                                         C.byref(used))
+        return keys[:k].copy(), bool(used.value)
+
+    def reconstruct(self, series, keys):
+        v = np.ascontiguousarray(series, np.float32)
+        k = np.ascontiguousarray(keys, np.int32)
+        out = np.zeros(v.size, np.float32)
+        self.lib.vo_reconstruct(_ptr(v, f32p), v.size, _ptr(k, C.POINTER(C.c_int)), k.size, _ptr(out, f32p))
+        return out
+
+    def keyframe_pass(self, frames, profile, threads=0):
+        """The encoder's per-voxel pass over frames[T, S] (frame-major): dict of key_mask [W, S] u32,
+        key_count [S] u32, flags [S] u8, recon [T, S] f32 and err2 [S] f64."""
+        v = np.ascontiguousarray(frames, np.float32)
+        T, S = v.shape
+        W = (T + 31) // 32
+        out = dict(key_mask=np.zeros((W, S), np.uint32), key_count=np.zeros(S, np.uint32),
+                   flags=np.zeros(S, np.uint8), recon=np.zeros((T, S), np.float32), err2=np.zeros(S, np.float64))
+        self.lib.vo_keyframe_pass(_ptr(v, f32p), S, T, S, C.byref(profile), _ptr(out["key_mask"], u32p),
+                                  _ptr(out["key_count"], u32p), _ptr(out["flags"], u8p), _ptr(out["recon"], f32p),
+                                  _ptr(out["err2"], C.POINTER(C.c_double)), threads if threads else os.cpu_count())
+        return out
 
     def load(self, path):
         return OracleFile(self, path)
@@ -344,3 +397,45 @@ class Reference:
         if n < 0:
             raise RuntimeError(self.error())
         return out[:n].copy()
+
+
+class KeyframeReference:
+    """The reference encoder's detectDensityKeyFrames / reconstructFromKeys, compiled from its source
+    (oracle/_ref/libkfref.so, see kf_ref_shim.cpp)."""
+
+    def __init__(self):
+        if not os.path.exists(KFREF_SO):
+            raise FileNotFoundError(KFREF_SO)
+        L = self.lib = C.CDLL(KFREF_SO)
+        i32p = C.POINTER(C.c_int)
+        L.vbtref_detect_keyframes.argtypes = [f32p, C.c_int, C.POINTER(VoKeyframeProfile), i32p, i32p]
+        L.vbtref_reconstruct.argtypes = [f32p, C.c_int, i32p, C.c_int, f32p]
+        L.vbtref_temporal_pass.argtypes = [f32p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(VoKeyframeProfile),
+                                           u32p, C.POINTER(C.c_double), C.c_int]
+
+    def detect_keyframes(self, series, profile):
+        v = np.ascontiguousarray(series, np.float32)
+        keys = np.zeros(max(1, 4 * v.size + 4), np.int32)
+        used = C.c_int()
+        k = self.lib.vbtref_detect_keyframes(_ptr(v, f32p), v.size, C.byref(profile),
+                                             _ptr(keys, C.POINTER(C.c_int)), C.byref(used))
+        return keys[:k].copy(), bool(used.value)
+
+    def reconstruct(self, series, keys):
+        v = np.ascontiguousarray(series, np.float32)
+        k = np.ascontiguousarray(keys, np.int32)
+        out = np.zeros(v.size, np.float32)
+        self.lib.vbtref_reconstruct(_ptr(v, f32p), v.size, _ptr(k, C.POINTER(C.c_int)), k.size, _ptr(out, f32p))
+        return out
+
+    def temporal_pass(self, frames, profile, threads=0, series=None):
+        """(key_count [S], err2 [S]) of the encoder's per-voxel loop over frames[T, S] (frame-major);
+        `series` limits the pass to the first columns."""
+        v = np.ascontiguousarray(frames, np.float32)
+        T, S = v.shape
+        n = S if series is None else int(series)
+        kc = np.zeros(n, np.uint32)
+        e2 = np.zeros(n, np.float64)
+        self.lib.vbtref_temporal_pass(_ptr(v, f32p), n, T, S, C.byref(profile), _ptr(kc, u32p),
+                                      _ptr(e2, C.POINTER(C.c_double)), threads)
+        return kc, e2

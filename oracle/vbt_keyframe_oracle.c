@@ -1,0 +1,281 @@
+/*
+ * vbt_keyframe_oracle.c -- CPU restatement of the encoder's per-voxel keyframe pass.
+ *
+ * TEST INFRASTRUCTURE ONLY: the parity checker for vbt_detect_keyframes (vbt_b200/csrc/
+ * keyframes.cu).  Pinned against the reference itself: oracle/_ref/libkfref.so runs the
+ * reference's own detectDensityKeyFrames and reconstructFromKeys, and tests/golden/keyframes.npz
+ * holds their outputs on seeded series (tests/golden/make_keyframes.py).
+ *
+ * Follows src/render_temporal_kf_probe_main.cpp:
+ *   computeStats             :200-225   mean, stddev, 90th-percentile |delta|
+ *   cutoffState              :227-233
+ *   epsilonAt                :235-247
+ *   dpRecurse                :249-276   split at the largest normalised error, recurse
+ *   addIsoSurfaceKeyFrames   :2051-2078
+ *   detectDensityKeyFrames   :2080-2167
+ *   reconstructFromKeys      :2169-2201
+ *   per-voxel leaf loop      :619-659   background test, keys, reconstruction, squared error
+ * Floating point is kept in the reference's types (float where it computes in float, double
+ * where it promotes), with no contraction (built with -ffp-contract=off).  Values are finite.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "vbt_oracle.h"
+
+/* std::max / std::min: the first argument unless the comparison says otherwise. */
+static float fmax_r(float a, float b) { return a < b ? b : a; }
+static double dmax_r(double a, double b) { return a < b ? b : a; }
+
+typedef struct {
+    float mean, stddev, delta_scale;
+} kf_stats;
+
+static int cmp_f32(const void* a, const void* b)
+{
+    const float x = *(const float*)a, y = *(const float*)b;
+    return (x > y) - (x < y);
+}
+
+/* computeStats (:200-225). */
+static kf_stats kf_compute_stats(const float* v, int n, float* scratch)
+{
+    kf_stats s = {0.0f, 0.0f, 1.0f};
+    if (n == 0) return s;
+    double sum = 0.0, sum2 = 0.0;
+    for (int i = 0; i < n; ++i) {
+        sum += v[i];
+        sum2 += (double)v[i] * v[i];
+    }
+    s.mean = (float)(sum / (double)n);
+    const double var = dmax_r(0.0, sum2 / (double)n - (double)s.mean * s.mean);
+    s.stddev = (float)sqrt(var);
+    if (n >= 2) {
+        const int m = n - 1;
+        for (int i = 1; i < n; ++i) scratch[i - 1] = fabsf(v[i] - v[i - 1]);
+        qsort(scratch, (size_t)m, sizeof(float), cmp_f32);
+        const int idx = (m - 1) < (m * 9) / 10 ? (m - 1) : (m * 9) / 10;
+        s.delta_scale = fmax_r(1e-6f, scratch[idx]);
+    }
+    return s;
+}
+
+/* cutoffState (:227-233). */
+static int kf_cutoff_state(float v, float cutoff, float band)
+{
+    if (cutoff <= 0.0f) return 1;
+    if (v < cutoff - band) return 0;
+    if (v > cutoff + band) return 2;
+    return 1;
+}
+
+/* epsilonAt (:235-247). */
+static float kf_epsilon_at(const float* v, int t, const vo_keyframe_profile* p, const kf_stats* st)
+{
+    float eps = p->eps_abs + p->eps_rel * fmax_r(fabsf(v[t]), st->stddev);
+    if (p->gamma_delta > 0.0f && t > 0) {
+        const float delta = fabsf(v[t] - v[t - 1]) / fmax_r(1e-6f, st->delta_scale);
+        eps /= (1.0f + p->gamma_delta * delta);
+    }
+    return fmax_r(eps, fmax_r(1e-6f, p->eps_abs * 0.1f));
+}
+
+/* dpRecurse (:249-276): marks the split frames in `key`, counts them in *splits. */
+static void kf_split(const float* v, int a, int b, const vo_keyframe_profile* p, const kf_stats* st,
+                     uint8_t* key, int* splits)
+{
+    if (b - a <= 1) return;
+    const double v0 = v[a], v1 = v[b];
+    double best = 0.0;
+    int split = -1;
+    for (int t = a + 1; t < b; ++t) {
+        const double alpha = (double)(t - a) / (double)(b - a);
+        const double pred = v0 + alpha * (v1 - v0);
+        const double eps = kf_epsilon_at(v, t, p, st);
+        const double e = fabs((double)v[t] - pred) / eps;
+        if (e > best) {
+            best = e;
+            split = t;
+        }
+    }
+    if (best > 1.0 && split != -1) {
+        key[split] = 1;
+        ++*splits;
+        kf_split(v, a, split, p, st, key, splits);
+        kf_split(v, split, b, p, st, key, splits);
+    }
+}
+
+static void kf_push(uint8_t* key, int t, long* pushes)
+{
+    key[t] = 1;
+    ++*pushes;
+}
+
+/* detectDensityKeyFrames (:2080-2167) without the validation-experiment switches (they are
+ * compiled out of the reference unless VBT_VALIDATION_EXPERIMENTS is defined). */
+int vo_detect_keyframes(const float* values, int n, const vo_keyframe_profile* p, int* keys, int* used_protect)
+{
+    if (used_protect) *used_protect = 0;
+    if (n <= 0) return 0;
+    if (n == 1) {
+        keys[0] = 0;
+        return 1;
+    }
+    float* scratch = (float*)malloc((size_t)n * sizeof(float));
+    uint8_t* key = (uint8_t*)calloc((size_t)n, 1);
+    const kf_stats st = kf_compute_stats(values, n, scratch);
+    const float eps_floor = fmax_r(1e-6f, p->eps_abs * 0.1f);
+    double sum = 0.0, sum2 = 0.0;
+    for (int i = 0; i < n; ++i) {
+        sum += values[i];
+        sum2 += (double)values[i] * values[i];
+    }
+    const double mean = sum / (double)n;
+    const double var = dmax_r(0.0, sum2 / (double)n - mean * mean);
+    if (var < (double)eps_floor * eps_floor) {
+        free(scratch);
+        free(key);
+        keys[0] = 0;
+        return 1;
+    }
+    long pushes = 2;
+    int splits = 0;
+    key[0] = key[n - 1] = 1;
+    kf_split(values, 0, n - 1, p, &st, key, &splits);
+    pushes += splits;
+    int used = 0;
+    if (p->cutoff_temporal_protect && p->render_cutoff > 0.0f && p->cutoff_band >= 0.0f) {
+        const float cutoff = p->render_cutoff, band = p->cutoff_band;
+        for (int t = 0; t < n; ++t) {
+            const int s = kf_cutoff_state(values[t], cutoff, band);
+            if (s == 1) {
+                kf_push(key, t, &pushes);
+                if (t > 0) kf_push(key, t - 1, &pushes);
+                if (t + 1 < n) kf_push(key, t + 1, &pushes);
+                used = 1;
+            }
+            if (t > 0 && kf_cutoff_state(values[t - 1], cutoff, band) != s) {
+                kf_push(key, t - 1, &pushes);
+                kf_push(key, t, &pushes);
+                if (t + 1 < n) kf_push(key, t + 1, &pushes);
+                used = 1;
+            }
+        }
+    }
+    if (p->iso_surface_protect) {
+        /* addIsoSurfaceKeyFrames (:2051-2078); it sorts and de-duplicates the whole key list, so
+         * "keys were added" compares the distinct count after it with the pushes before it. */
+        const long before = pushes;
+        const float band = fmax_r(0.0f, p->iso_band);
+        for (int t = 0; t < n; ++t) {
+            const float cur = values[t] - p->iso_value;
+            if (fabsf(cur) <= band) {
+                if (t > 0) key[t - 1] = 1;
+                key[t] = 1;
+                if (t + 1 < n) key[t + 1] = 1;
+            }
+            if (t > 0) {
+                const float prev = values[t - 1] - p->iso_value;
+                if ((prev >= 0.0f) != (cur >= 0.0f)) {
+                    for (int u = t - 2; u <= t + 1; ++u)
+                        if (u >= 0 && u < n) key[u] = 1;
+                }
+            }
+        }
+        long distinct = 0;
+        for (int t = 0; t < n; ++t) distinct += key[t];
+        used = used || distinct > before;
+    }
+    int k = 0;
+    for (int t = 0; t < n; ++t)
+        if (key[t]) keys[k++] = t;
+    free(scratch);
+    free(key);
+    if (used_protect) *used_protect = used;
+    return k;
+}
+
+/* reconstructFromKeys (:2169-2201). */
+void vo_reconstruct(const float* values, int n, const int* keys, int key_count, float* out)
+{
+    if (n <= 0) return;
+    if (key_count == 0) {
+        memcpy(out, values, (size_t)n * sizeof(float));
+        return;
+    }
+    if (key_count == 1) {
+        for (int t = 0; t < n; ++t) out[t] = values[keys[0]];
+        return;
+    }
+    int seg = 0;
+    for (int t = 0; t < n; ++t) {
+        while (seg + 1 < key_count && t > keys[seg + 1]) ++seg;
+        if (seg + 1 >= key_count) {
+            out[t] = values[keys[key_count - 1]];
+            continue;
+        }
+        const int a = keys[seg], b = keys[seg + 1];
+        if (t <= a) {
+            out[t] = values[a];
+            continue;
+        }
+        const double alpha = (double)(t - a) / (double)(b - a);
+        out[t] = (float)((double)values[a] + alpha * (double)(values[b] - values[a]));
+    }
+}
+
+/* The per-voxel body of the encoder's leaf loop (:619-659) over independent series; series s at
+ * values[t * frame_stride + s].  key_mask is word-major: bit t%32 of key_mask[(t/32) * series + s].
+ * flags: bit 0 background-zeroed (no keys, counted as 1, reconstruction 0), bit 1 protected keys
+ * added.  recon (optional) uses the input's layout; err2 (optional) is the series' squared error. */
+void vo_keyframe_pass(const float* values, uint64_t series, int frames, uint64_t frame_stride,
+                      const vo_keyframe_profile* p, uint32_t* key_mask, uint32_t* key_count, uint8_t* flags,
+                      float* recon, double* err2, int threads)
+{
+    const int words = (frames + 31) / 32;
+#pragma omp parallel num_threads(threads > 0 ? threads : 1) if (threads != 1)
+    {
+        float* v = (float*)malloc((size_t)frames * sizeof(float));
+        float* r = (float*)malloc((size_t)frames * sizeof(float));
+        int* keys = (int*)malloc((size_t)frames * sizeof(int));
+#pragma omp for schedule(dynamic, 256)
+        for (long long s = 0; s < (long long)series; ++s) {
+            float vmax = 0.0f;
+            for (int t = 0; t < frames; ++t) {
+                v[t] = values[(uint64_t)t * frame_stride + (uint64_t)s];
+                vmax = fmax_r(vmax, v[t]);
+            }
+            for (int w = 0; w < words; ++w) key_mask[(uint64_t)w * series + (uint64_t)s] = 0u;
+            double e2 = 0.0;
+            if (p->bg_threshold >= 0.0 && (double)vmax < p->bg_threshold) {
+                for (int t = 0; t < frames; ++t) {
+                    const double d = (double)v[t];
+                    e2 += d * d;
+                    r[t] = 0.0f;
+                }
+                key_count[s] = 1;
+                flags[s] = 1;
+            } else {
+                int used = 0;
+                const int k = vo_detect_keyframes(v, frames, p, keys, &used);
+                vo_reconstruct(v, frames, keys, k, r);
+                for (int t = 0; t < frames; ++t) {
+                    const double d = (double)v[t] - (double)r[t];
+                    e2 += d * d;
+                }
+                for (int i = 0; i < k; ++i)
+                    key_mask[(uint64_t)(keys[i] / 32) * series + (uint64_t)s] |= 1u << (keys[i] % 32);
+                key_count[s] = (uint32_t)k;
+                flags[s] = used ? 2 : 0;
+            }
+            if (recon)
+                for (int t = 0; t < frames; ++t) recon[(uint64_t)t * frame_stride + (uint64_t)s] = r[t];
+            if (err2) err2[s] = e2;
+        }
+        free(v);
+        free(r);
+        free(keys);
+    }
+}

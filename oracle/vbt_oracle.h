@@ -116,6 +116,20 @@ int vo_control_cache(const vo_file* f, int frame, const uint32_t* compact, float
 void vo_sample_rays(const vo_file* f, const float* cache576, const uint32_t* compact, const vo_sample_params* p,
                     const float* rays, uint32_t n, float* results);
 
+/* The encoder's per-voxel keyframe pass (vbt_keyframe_oracle.c): DensityTemporalProfile of
+ * src/render_temporal_kf_probe_main.cpp:81-95 plus the background threshold of :477 (< 0: off). */
+typedef struct {
+    float eps_abs, eps_rel, gamma_delta, render_cutoff, cutoff_band;
+    uint32_t cutoff_temporal_protect, iso_surface_protect;
+    float iso_value, iso_band;
+    double bg_threshold;
+} vo_keyframe_profile;
+int vo_detect_keyframes(const float* values, int n, const vo_keyframe_profile* p, int* keys, int* used_protect);
+void vo_reconstruct(const float* values, int n, const int* keys, int key_count, float* out);
+void vo_keyframe_pass(const float* values, uint64_t series, int frames, uint64_t frame_stride,
+                      const vo_keyframe_profile* p, uint32_t* key_mask, uint32_t* key_count, uint8_t* flags,
+                      float* recon, double* err2, int threads);
+
 #ifdef __cplusplus
 }
 #endif
