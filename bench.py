@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-window", action="store_true")
     p.add_argument("--no-full-frame", action="store_true")
     p.add_argument("--no-sampler", action="store_true")
+    p.add_argument("--no-keyframes", action="store_true")
     p.add_argument("--serve-requests", type=int, default=300)
     return p.parse_args()
 
@@ -572,6 +573,7 @@ def run_sampler(args, local_rank, reps=5):
         p.surface_iso, p.surface_epsilon_voxels, p.surface_normal_step, p.max_step_voxels = 0.0, 0.5, 1.0, 4.0
         p.surface_model, p.floor_height, p.shadow_steps, p.up_axis = model, 1.0, 48, 2
         s = torch.cuda.Stream(device=dev)
+        s.wait_stream(torch.cuda.current_stream(dev))      # the rays were copied on the current stream
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
                torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
         with torch.cuda.stream(s):
@@ -614,6 +616,106 @@ def run_sampler(args, local_rank, reps=5):
         out[name] = entry
         a.close()
     return out or {"skipped": "assets not generated"}
+
+
+# ------------------------------------------------------------------------------ keyframe pass
+def gpu_blobs(shape_xyz, frames, n_blobs, seed, dev, noise=0.01):
+    """The config-1 blob recipe (tests/golden/make_assets.py: blobs) evaluated on the GPU: frames
+    [T, Z*Y*X] float32, blob parameters from the same seeded draws, the noise from a seeded torch
+    generator."""
+    import torch
+    rng = np.random.default_rng(seed)
+    X, Y, Z = shape_xyz
+    sig = rng.uniform(4.0, 10.0, n_blobs)
+    amp = rng.uniform(0.2, 1.0, n_blobs)
+    c0 = rng.uniform(0.2, 0.8, (n_blobs, 3)) * np.array([X, Y, Z])
+    d = rng.normal(size=(n_blobs, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    vel = d * rng.uniform(0.0, 1.0, (n_blobs, 1))
+    zz, yy, xx = torch.meshgrid(torch.arange(Z, device=dev, dtype=torch.float32),
+                                torch.arange(Y, device=dev, dtype=torch.float32),
+                                torch.arange(X, device=dev, dtype=torch.float32), indexing="ij")
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    out = torch.empty((frames, Z * Y * X), dtype=torch.float32, device=dev)
+    for t in range(frames):
+        f = torch.randn((Z, Y, X), generator=gen, device=dev, dtype=torch.float32) * noise
+        for b in range(n_blobs):
+            c = c0[b] + vel[b] * t
+            r2 = (xx - float(c[0])) ** 2 + (yy - float(c[1])) ** 2 + (zz - float(c[2])) ** 2
+            f += float(amp[b]) * torch.exp(-r2 / float(2.0 * sig[b] ** 2))
+        out[t] = f.reshape(-1)
+    return out
+
+
+def run_keyframes(args, local_rank, reps=3, work=None):
+    """The encoder's per-voxel keyframe pass (vbt_detect_keyframes: background test,
+    detectDensityKeyFrames, reconstructFromKeys, squared error) on one B200, with the encoder's
+    default profile, over (1) the config-1 field itself (64^3 x 24 blobs, tests/golden/
+    make_assets.py) and (2) the same recipe at the plume's size, 256^3 x 96, generated on the GPU.
+    Device time of the whole pass (inputs resident, outputs: key masks, counts, flags,
+    reconstruction, errors, totals); beside it the reference's own detector (oracle/_ref/libkfref.so)
+    on all host threads for a bounded sample of the same series, whose key counts are checked
+    against the GPU's."""
+    import torch
+    import vbt_b200 as vbt
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_assets import blobs
+    dev = f"cuda:{local_rank}"
+    out = {}
+    ref = None
+    try:
+        from oracle.oracle import KeyframeReference, VoKeyframeProfile
+        ref = KeyframeReference()
+    except (OSError, ImportError):
+        pass
+    work = work or [("config1_blobs_64^3x24",
+                     lambda: torch.from_numpy(blobs((64, 64, 64), 24, 6, 1).reshape(24, -1)).to(dev)),
+                    ("blobs_256^3x96", lambda: gpu_blobs((256, 256, 256), 96, 6, 2, dev))]
+    prof = vbt.KeyframeProfile()
+    for name, make in work:
+        frames = make()
+        T, S = frames.shape
+        W = (T + 31) // 32
+        mask = torch.empty((W, S), dtype=torch.int32, device=dev)
+        cnt = torch.empty(S, dtype=torch.int32, device=dev)
+        flags = torch.empty(S, dtype=torch.uint8, device=dev)
+        recon = torch.empty_like(frames)
+        err2 = torch.empty(S, dtype=torch.float64, device=dev)
+        tot = torch.empty(40, dtype=torch.uint8, device=dev)
+        s = torch.cuda.Stream(device=dev)
+        s.wait_stream(torch.cuda.current_stream(dev))      # the frames were made on the current stream
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        with torch.cuda.stream(s):
+            vbt.detect_keyframes(frames, prof, mask, cnt, flags, recon, err2, tot, stream=s)
+            for e0, e1 in ev:
+                e0.record(s)
+                vbt.detect_keyframes(frames, prof, mask, cnt, flags, recon, err2, tot, stream=s)
+                e1.record(s)
+        s.synchronize()
+        ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+        t = vbt.keyframe_totals(tot)
+        moved = S * T * 4 * 2 + S * (W * 4 + 4 + 1 + 8)
+        entry = {"series": S, "frames": T, "pass_ms": ms, "series_per_s": S / (ms * 1e-3),
+                 "values_per_s": S * T / (ms * 1e-3), "bytes_moved": moved, "gb_per_s": moved / (ms * 1e-3) / 1e9,
+                 "keys_per_series": t.total_keys / S, "max_keys": t.max_keys,
+                 "background_series": t.background_series, "protected_series": t.protected_series,
+                 "bound": "fp64/integer issue (the pass reads and writes each value once)"}
+        if ref is not None and not args.no_cpu:
+            n = min(S, 65536 if T > 32 else S)
+            sample = frames[:, :n].cpu().numpy()
+            threads = os.cpu_count()
+            t0 = time.perf_counter()
+            kc, _ = ref.temporal_pass(sample, VoKeyframeProfile(), threads=threads)
+            el = time.perf_counter() - t0
+            entry["cpu_reference"] = {"series_per_s": n / el, "cores": threads, "kind": "reference",
+                                      "sample": f"the first {n} of {S} series"}
+            entry["sample_key_counts_equal"] = bool(np.array_equal(kc, cnt[:n].cpu().numpy().view(np.uint32)))
+            entry["speedup_vs_cpu_reference"] = entry["series_per_s"] / entry["cpu_reference"]["series_per_s"]
+        out[name] = entry
+        del frames, recon, mask
+        torch.cuda.empty_cache()
+    return out
 
 
 # ------------------------------------------------------------------------------ arms
@@ -791,6 +893,10 @@ def run_ours(args, rank, local_rank, world):
     if rank == 0 and world == 1 and not args.no_sampler:
         sampler = run_sampler(args, local_rank)
 
+    keyframes = None
+    if rank == 0 and world == 1 and not args.no_keyframes:
+        keyframes = run_keyframes(args, local_rank)
+
     window = window_render = None
     if rank == 0 and world == 1 and not args.no_window:
         window = run_window(args, local_rank)
@@ -828,6 +934,7 @@ def run_ours(args, rank, local_rank, world):
                           "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
                 "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "precision_window": window,
                 "precision_window_render": window_render, "full_frame": full_frame, "ray_sampler": sampler,
+                "keyframe_pass": keyframes,
                 "gpu_launches": args.steps * (1 + len(chunks)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)

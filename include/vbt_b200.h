@@ -155,6 +155,41 @@ int vbt_sample_rays(vbt_asset* asset, const float* d_controls, const vbt_sample_
 int vbt_pack_payload(const uint8_t* d_blocks, const uint64_t* d_block_offsets, uint32_t leaf_count, uint32_t* d_offsets,
                      uint32_t* d_payload, uint64_t payload_capacity_words, uint64_t* total_words, void* stream);
 
+/* ---- Encoder keyframe pass ---------------------------------------------------------------------
+ * The per-voxel body of the reference encoder's leaf loop (src/render_temporal_kf_probe_main.cpp:
+ * 619-659) over `series` independent series of `frames` finite values, series s at
+ * d_values[t * frame_stride + s] (a raw frame-major volume: s = (z*Y + y)*X + x, frame_stride =
+ * X*Y*Z): the background test (max(0, values) < bg_threshold, when bg_threshold >= 0),
+ * detectDensityKeyFrames (:2080-2167) and reconstructFromKeys (:2169-2201).
+ *   d_key_mask   word-major key sets: bit t % 32 of d_key_mask[(t / 32) * series + s]
+ *   d_key_count  the count the encoder adds up: the keys, or 1 for a background-zeroed series
+ *   d_flags      bit 0 background-zeroed (no keys, reconstruction 0); bit 1 usedCutoffProtect
+ *   d_recon      optional, the reconstruction in the input's layout
+ *   d_err2       optional, the series' squared error summed over frames in frame order
+ *   d_totals     optional, overwritten: the leaf loop's totals (totalKeyframes, maxKeyframes,
+ *                temporalProtectedSeries, backgroundZeroedVoxels, and the squared error, whose
+ *                summation order differs from the reference's running sum)
+ * Everything but d_totals->err2 equals the reference bit for bit.  frames <= 1024. */
+typedef struct {
+    float eps_abs, eps_rel, gamma_delta, render_cutoff, cutoff_band;   /* DensityTemporalProfile, :81-95 */
+    uint32_t cutoff_temporal_protect, iso_surface_protect;
+    float iso_value, iso_band;
+    double bg_threshold;   /* :477, bgZeroRatio * cutoff (formed in float); < 0 disables the test */
+} vbt_keyframe_profile;
+typedef struct {
+    uint64_t total_keys, protected_series, background_series;
+    uint32_t max_keys, pad;
+    double err2;
+} vbt_keyframe_totals;
+int vbt_detect_keyframes(const float* d_values, uint64_t series, uint32_t frames, uint64_t frame_stride,
+                         const vbt_keyframe_profile* profile, uint32_t* d_key_mask, uint32_t* d_key_count,
+                         uint8_t* d_flags, float* d_recon, double* d_err2, vbt_keyframe_totals* d_totals,
+                         void* stream);
+/* Self-check of the division the keyframe pass uses for alpha = a / b (no reference counterpart):
+ * every 1 <= b <= b_max, 0 <= a <= b against the IEEE quotient on `device`; result[0] = mismatches,
+ * result[1] = (b << 16 | a) of the first, or all ones. */
+int vbt_selftest_keyframe_division(uint32_t b_max, uint64_t* result, int device);
+
 /* Plain per-leaf launch (one CTA per leaf of the grid, one frame), for comparison. */
 int vbt_decode_cache_plain(vbt_asset* asset, int frame, float* d_out, void* stream);
 /* Dense frames d_out[f * X*Y*Z + (z*Y + y)*X + x] (decodeFrameToDense /

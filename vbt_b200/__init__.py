@@ -59,6 +59,29 @@ class SampleParams(C.Structure):
                 ("shadow_steps", C.c_uint32), ("up_axis", C.c_uint32)]
 
 
+class KeyframeProfile(C.Structure):
+    """vbt_keyframe_profile: the encoder's DensityTemporalProfile and background threshold.  The
+    defaults are the reference encoder's (src/render_temporal_kf_probe_main.cpp:51-58, :477)."""
+    _fields_ = [("eps_abs", C.c_float), ("eps_rel", C.c_float), ("gamma_delta", C.c_float),
+                ("render_cutoff", C.c_float), ("cutoff_band", C.c_float), ("cutoff_temporal_protect", C.c_uint32),
+                ("iso_surface_protect", C.c_uint32), ("iso_value", C.c_float), ("iso_band", C.c_float),
+                ("bg_threshold", C.c_double)]
+
+    def __init__(self, **kw):
+        d = dict(eps_abs=1e-5, eps_rel=0.02, gamma_delta=0.2, render_cutoff=0.0003, cutoff_band=0.0001,
+                 cutoff_temporal_protect=1, iso_surface_protect=0, iso_value=0.0, iso_band=0.0)
+        d.update(kw)
+        if "bg_threshold" not in kw:   # bgZeroRatio (0.3) * cutoff, formed in float as the encoder does
+            c = C.c_float(d["render_cutoff"]).value
+            d["bg_threshold"] = float(C.c_float(C.c_float(0.3).value * c).value) if c > 0 else -1.0
+        super().__init__(**d)
+
+
+class KeyframeTotals(C.Structure):
+    _fields_ = [("total_keys", C.c_uint64), ("protected_series", C.c_uint64), ("background_series", C.c_uint64),
+                ("max_keys", C.c_uint32), ("pad", C.c_uint32), ("err2", C.c_double)]
+
+
 class RequestResult(C.Structure):
     _fields_ = [("status", C.c_int), ("bad_leaf", C.c_uint32), ("result_floats", C.c_uint64),
                 ("device_result", C.c_void_p), ("submit_ms", C.c_double), ("start_ms", C.c_double),
@@ -108,6 +131,9 @@ _sig = {
     "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_selftest_key_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_pack_payload": ([_vp, _vp, C.c_uint32, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64), _vp], C.c_int),
+    "vbt_detect_keyframes": ([_vp, C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(KeyframeProfile), _vp, _vp, _vp,
+                              _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_selftest_keyframe_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_sample_rays": ([_vp, _vp, C.POINTER(SampleParams), _vp, C.c_uint32, _vp, _vp], C.c_int),
     "vbt_decode_control_cache": ([_vp, C.POINTER(C.c_int), C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_window_error": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, C.POINTER(C.c_double), _vp], C.c_int),
@@ -354,6 +380,34 @@ def pack_payload(blocks, block_offsets, offsets, payload, stream=None):
     _check(_lib.vbt_pack_payload(_addr(blocks), _addr(block_offsets), n, _addr(offsets), _addr(payload),
                                  payload.numel() if payload is not None else 0, C.byref(total), _stream(stream)))
     return total.value
+
+
+def detect_keyframes(values, profile, key_mask, key_count, flags, recon=None, err2=None, totals=None,
+                     series=None, stream=None):
+    """The encoder's per-voxel keyframe pass on the GPU over values [frames, stride] (float32 device
+    tensor, frame-major; the first `series` columns, default all): key_mask [ceil(frames / 32),
+    series] int32, key_count [series] int32, flags [series] uint8, and optionally recon (the
+    reconstruction, shaped like values), err2 [series] float64 and totals (a 40-byte device buffer
+    read back by keyframe_totals)."""
+    frames, stride = values.shape
+    n = stride if series is None else int(series)
+    _check(_lib.vbt_detect_keyframes(_addr(values), n, frames, stride, C.byref(profile), _addr(key_mask),
+                                     _addr(key_count), _addr(flags), _addr(recon), _addr(err2), _addr(totals),
+                                     _stream(stream)))
+
+
+def keyframe_totals(buf):
+    """KeyframeTotals from the device buffer `detect_keyframes` filled (a uint8 tensor of 40 bytes)."""
+    raw = bytes(buf.cpu().numpy().tobytes())
+    return KeyframeTotals.from_buffer_copy(raw[:C.sizeof(KeyframeTotals)])
+
+
+def selftest_keyframe_division(b_max=1024, device=0):
+    """(mismatches, smallest failing b << 16 | a) of the keyframe pass's integer quotient
+    a / b against IEEE division, over every 0 <= a <= b <= b_max."""
+    r = (C.c_uint64 * 2)()
+    _check(_lib.vbt_selftest_keyframe_division(b_max, r, device))
+    return int(r[0]), int(r[1])
 
 
 def selftest_key_division(b_max=65535, device=0):

@@ -24,7 +24,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true"
               "--expt-relaxed-constexpr", "-ccbin", "/usr/bin/g++"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
              "-I", "/usr/local/cuda/include"]
-CU_SOURCES = ["kernels.cu", "scalar.cu", "capi.cu", "noalloc.cu", "serve.cu", "tune.cu", "sample.cu", "writer.cu"]
+CU_SOURCES = ["kernels.cu", "scalar.cu", "capi.cu", "noalloc.cu", "serve.cu", "tune.cu", "sample.cu", "writer.cu", "keyframes.cu"]
 CXX_SOURCES = ["facade.cpp"]
 
 

@@ -1,0 +1,520 @@
+// keyframes.cu -- the encoder's per-voxel keyframe pass on the GPU (vbt_detect_keyframes).
+//
+// For every voxel series of a raw frame-major volume, what the reference encoder's leaf loop does
+// per voxel (src/render_temporal_kf_probe_main.cpp:619-659): the background test on the running
+// max, detectDensityKeyFrames (:2080-2167: statistics, the constant test, dpRecurse's recursive
+// split at the largest normalised error, cutoff and iso-surface protection), reconstructFromKeys
+// (:2169-2201) and the squared error.  Keys, flags, reconstruction and error equal the reference's
+// bit for bit.
+//
+// One thread owns one series.  A CTA stages its NV series (all frames) in shared memory as
+// [frame][series], so lanes reading different frames of their own series never share a bank, and
+// keeps the key set as a bitmask column beside it.  The recursion becomes a cursor walk over the
+// key set (split the interval at the cursor until it holds, then step to the next key), flattened
+// so that one loop iteration evaluates one frame of whatever interval each lane is in: lanes of a
+// warp stay busy however different their splits are.
+//
+// Per evaluated frame the reference divides twice in double.  Here alpha = (t-a)/(b-a) comes from
+// the correctly rounded reciprocal of b-a and one Markstein correction (exact for every integer
+// pair this kernel meets; vbt_selftest_keyframe_division checks them all), and the normalised error
+// is first bracketed by an approximation good to 2^-20 relative: only when it lies within 2^-15 of
+// the running maximum (or of 1.0 for the split decision) is the exact double quotient formed.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/vbt_b200.h"
+
+namespace vbtb {
+int set_last_error(int status, const std::string& msg);
+}
+
+namespace {
+
+constexpr uint32_t kKfMaxFrames = 1024;
+constexpr double kHi = 1.0 + 1.0 / 32768.0;   // approximation margins (the approximation is good to 2^-20)
+constexpr double kLo = 1.0 - 1.0 / 32768.0;
+
+// std::max(a, b): a unless a < b.
+__device__ __forceinline__ float fmax_r(float a, float b) { return a < b ? b : a; }
+__device__ __forceinline__ double dmax_r(double a, double b) { return a < b ? b : a; }
+
+// a / b for integers 0 <= a <= b <= 1024 held in doubles, given y = RN(1 / b): Markstein's
+// correction step q = q0 + (a - q0 b) y, with the residual exact in an fma.
+__device__ __forceinline__ double div_int_rn(double a, double b, double y)
+{
+    const double q0 = __dmul_rn(a, y);
+    const double r = __fma_rn(-q0, b, a);
+    return __fma_rn(r, y, q0);
+}
+
+// RN(1 / k) for k = 1 .. kKfMaxFrames (entry 0 unused), written by kf_rcp_init_kernel ahead of every
+// pass on the pass's stream: one cached load where an interval or a key segment starts.
+__device__ double g_kf_rcp[kKfMaxFrames + 1];
+
+__global__ void kf_rcp_init_kernel()
+{
+    for (uint32_t k = 1u + threadIdx.x; k <= kKfMaxFrames; k += blockDim.x) g_kf_rcp[k] = __drcp_rn((double)k);
+}
+
+struct KfTotals {
+    unsigned long long total_keys, protected_series, background_series;
+    unsigned int max_keys, pad;
+    double err2;
+};
+
+// cutoffState (:227-233).
+__device__ __forceinline__ int cutoff_state(float v, float cutoff, float band)
+{
+    if (cutoff <= 0.0f) return 1;
+    if (v < __fsub_rn(cutoff, band)) return 0;
+    if (v > __fadd_rn(cutoff, band)) return 2;
+    return 1;
+}
+
+template <int NV>
+struct Column {
+    const float* v;   // v[t * NV]
+    uint32_t* m;      // m[w * NV]
+    __device__ __forceinline__ float at(int t) const { return v[t * NV]; }
+    __device__ __forceinline__ void set(int t) const { m[(t >> 5) * NV] |= 1u << (t & 31); }
+    // The first key after frame a (the last frame is always a key, and a lies before it).
+    __device__ __forceinline__ int next_key(int a, int words) const
+    {
+        int w = (a + 1) >> 5;
+        uint32_t bits = m[w * NV] & (0xFFFFFFFFu << ((a + 1) & 31));
+        while (bits == 0u && w + 1 < words) bits = m[++w * NV];
+        return bits ? (w << 5) + __ffs(bits) - 1 : -1;
+    }
+};
+
+struct SeriesStats {
+    float stddev, ds;   // computeStats' stddev and max(1e-6, deltaScale)
+};
+
+// epsilonAt (:235-247), exactly.
+__device__ __forceinline__ float eps_exact(float x, float prev, bool has_prev, const vbt_keyframe_profile& p,
+                                           const SeriesStats& st, float floor_)
+{
+    float eps = __fadd_rn(p.eps_abs, __fmul_rn(p.eps_rel, fmax_r(fabsf(x), st.stddev)));
+    if (p.gamma_delta > 0.0f && has_prev) {
+        const float delta = __fdiv_rn(fabsf(__fsub_rn(x, prev)), st.ds);
+        eps = __fdiv_rn(eps, __fadd_rn(1.0f, __fmul_rn(p.gamma_delta, delta)));
+    }
+    return fmax_r(eps, floor_);
+}
+
+struct SeriesOut {
+    uint32_t count;
+    uint8_t flag;
+    double e2;
+};
+
+// The leaf loop's body for one series: key bits into col.m, the reconstruction into recon[t * fstride]
+// (when not null); returns the key count, the flags and the squared error.
+template <int NV>
+__device__ __forceinline__ SeriesOut keyframe_series(const Column<NV>& col, float* top, int n, int words,
+                                                  const vbt_keyframe_profile& p, float* recon,
+                                                  unsigned long long fstride)
+{
+    for (int w = 0; w < words; ++w) col.m[w * NV] = 0u;
+
+    // One pass: the running max of the leaf loop, and the sums of computeStats and of the constant test.
+    float vmax = 0.0f;
+    double sum = 0.0, sum2 = 0.0;
+    for (int t = 0; t < n; ++t) {
+        const float x = col.at(t);
+        vmax = fmax_r(vmax, x);
+        const double xd = (double)x;
+        sum = __dadd_rn(sum, xd);
+        sum2 = __dadd_rn(sum2, __dmul_rn(xd, xd));
+    }
+
+    uint32_t count;
+    uint8_t flag = 0;
+    double e2 = 0.0;
+    const float floor_ = fmax_r(1e-6f, __fmul_rn(p.eps_abs, 0.1f));
+    const double nd = (double)n;
+    const double mean = __ddiv_rn(sum, nd);
+    const double var_c = dmax_r(0.0, __dsub_rn(__ddiv_rn(sum2, nd), __dmul_rn(mean, mean)));
+    const bool background = p.bg_threshold >= 0.0 && (double)vmax < p.bg_threshold;
+    if (background || n == 1 || var_c < __dmul_rn((double)floor_, (double)floor_)) {
+        // Background-zeroed (reconstruction 0, counted as one key), or a single key at frame 0
+        // (one frame, or variance under the epsilon floor): the reconstruction is the first value.
+        const float fill = background ? 0.0f : col.at(0);
+        if (background) {
+            e2 = sum2;      // the same sequence of squares the leaf loop sums
+            flag = 1;
+        } else {
+            col.set(0);
+            for (int t = 0; t < n; ++t) {
+                const double d = __dsub_rn((double)col.at(t), (double)fill);
+                e2 = __dadd_rn(e2, __dmul_rn(d, d));
+            }
+        }
+        count = 1;
+        if (recon)
+            for (int t = 0; t < n; ++t) recon[(unsigned long long)t * fstride] = fill;
+    } else {
+        // computeStats (:200-225).
+        SeriesStats st;
+        {
+            const float mean_f = __double2float_rn(mean);
+            const double var_s =
+                dmax_r(0.0, __dsub_rn(__ddiv_rn(sum2, nd), __dmul_rn((double)mean_f, (double)mean_f)));
+            st.stddev = __double2float_rn(__dsqrt_rn(var_s));
+            // deltas[min(m - 1, 9m / 10)] of the sorted |delta|s = the r-th largest, r = m - that index:
+            // kept as an ascending list of the r largest seen.
+            const int m = n - 1;
+            const int r = m - min(m - 1, (m * 9) / 10);
+            int cnt = 0;
+            float prev = col.at(0);
+            for (int t = 1; t < n; ++t) {
+                const float x = col.at(t);
+                const float d = fabsf(__fsub_rn(x, prev));
+                prev = x;
+                if (cnt < r) {
+                    int k = cnt++;
+                    while (k > 0 && top[(k - 1) * NV] > d) {
+                        top[k * NV] = top[(k - 1) * NV];
+                        --k;
+                    }
+                    top[k * NV] = d;
+                } else if (d > top[0]) {
+                    int k = 0;
+                    while (k + 1 < r && top[(k + 1) * NV] < d) {
+                        top[k * NV] = top[(k + 1) * NV];
+                        ++k;
+                    }
+                    top[k * NV] = d;
+                }
+            }
+            st.ds = fmax_r(1e-6f, fmax_r(1e-6f, top[0]));
+        }
+        const bool gamma_on = p.gamma_delta > 0.0f;
+        const float inv_ds = __frcp_rn(st.ds), inv_floor = __frcp_rn(floor_);
+        auto exact_err = [&](int t, double num) {
+            const float e = eps_exact(col.at(t), t > 0 ? col.at(t - 1) : 0.0f, t > 0, p, st, floor_);
+            return __ddiv_rn(num, (double)e);
+        };
+
+        // dpRecurse (:249-276) as a cursor walk over the key set.
+        col.set(0);
+        col.set(n - 1);
+        uint32_t pushes = 2;
+        int a = 0, b = n - 1;
+        double v0 = (double)col.at(a), dv = __dsub_rn((double)col.at(b), v0);
+        double den = (double)(b - a), y = __ldg(g_kf_rcp + (b - a));
+        float xp = col.at(a);      // frame t - 1
+        int t = a + 1, lead = -1;
+        double lead_a = 0.0, lead_num = 0.0, lead_e = 0.0;
+        bool lead_exact = true;    // lead_e holds the leader's exact error (0 for no leader)
+        for (;;) {
+            if (t < b) {
+                const float x = col.at(t);
+                const double alpha = div_int_rn((double)(t - a), den, y);
+                const double pred = __dadd_rn(v0, __dmul_rn(alpha, dv));
+                const double num = fabs(__dsub_rn((double)x, pred));
+                if (num != 0.0) {
+                    // 1 / epsilonAt = min((1 + gamma delta) / e0, 1 / floor), to 2^-21 relative
+                    const float e0 = __fadd_rn(p.eps_abs, __fmul_rn(p.eps_rel, fmax_r(fabsf(x), st.stddev)));
+                    float r = __frcp_rn(e0);
+                    if (gamma_on) r *= fmaf(p.gamma_delta, fabsf(x - xp) * inv_ds, 1.0f);
+                    const double e_a = num * (double)fminf(r, inv_floor);
+                    if (e_a > lead_a * kHi) {
+                        lead = t;
+                        lead_a = e_a;
+                        lead_num = num;
+                        lead_exact = false;
+                    } else if (!(e_a < lead_a * kLo)) {
+                        if (!lead_exact) {
+                            lead_e = exact_err(lead, lead_num);
+                            lead_exact = true;
+                        }
+                        const double e = exact_err(t, num);
+                        if (e > lead_e) {
+                            lead = t;
+                            lead_a = e_a;
+                            lead_num = num;
+                            lead_e = e;
+                        }
+                    }
+                }
+                xp = x;
+                ++t;
+                continue;
+            }
+            bool split = false;
+            if (lead >= 0) {
+                if (lead_a > kHi) split = true;
+                else if (!(lead_a < kLo)) split = (lead_exact ? lead_e : exact_err(lead, lead_num)) > 1.0;
+            }
+            if (split) {
+                col.set(lead);
+                ++pushes;
+                b = lead;
+            } else {
+                a = b;
+                if (a >= n - 1) break;
+                b = col.next_key(a, words);
+                if (b < 0) break;   // unreachable: frame n - 1 is a key
+            }
+            xp = col.at(a);
+            v0 = (double)xp;
+            dv = __dsub_rn((double)col.at(b), v0);
+            den = (double)(b - a);
+            y = __ldg(g_kf_rcp + (b - a));
+            t = a + 1;
+            lead = -1;
+            lead_a = 0.0;
+            lead_e = 0.0;
+            lead_exact = true;
+        }
+
+        // Cutoff protection (:2125-2146).
+        bool used = false;
+        if (p.cutoff_temporal_protect && p.render_cutoff > 0.0f && p.cutoff_band >= 0.0f) {
+            int prev_state = 0;
+            for (int u = 0; u < n; ++u) {
+                const int cs = cutoff_state(col.at(u), p.render_cutoff, p.cutoff_band);
+                if (cs == 1) {
+                    if (u > 0) col.set(u - 1);
+                    col.set(u);
+                    if (u + 1 < n) col.set(u + 1);
+                    pushes += 1u + (u > 0) + (u + 1 < n);
+                    used = true;
+                }
+                if (u > 0 && prev_state != cs) {
+                    col.set(u - 1);
+                    col.set(u);
+                    if (u + 1 < n) col.set(u + 1);
+                    pushes += 2u + (u + 1 < n);
+                    used = true;
+                }
+                prev_state = cs;
+            }
+        }
+        count = 0;
+        if (p.iso_surface_protect) {
+            // addIsoSurfaceKeyFrames (:2051-2078); "added" compares the distinct keys after it with
+            // the list length before it, duplicates included.
+            const float band = fmax_r(0.0f, p.iso_band);
+            float prev = 0.0f;
+            for (int u = 0; u < n; ++u) {
+                const float cur = __fsub_rn(col.at(u), p.iso_value);
+                if (fabsf(cur) <= band) {
+                    if (u > 0) col.set(u - 1);
+                    col.set(u);
+                    if (u + 1 < n) col.set(u + 1);
+                }
+                if (u > 0 && (prev >= 0.0f) != (cur >= 0.0f)) {
+                    if (u > 1) col.set(u - 2);
+                    col.set(u - 1);
+                    col.set(u);
+                    if (u + 1 < n) col.set(u + 1);
+                }
+                prev = cur;
+            }
+            for (int w = 0; w < words; ++w) count += __popc(col.m[w * NV]);
+            used = used || count > pushes;
+        } else {
+            for (int w = 0; w < words; ++w) count += __popc(col.m[w * NV]);
+        }
+        flag = used ? 2 : 0;
+
+        // reconstructFromKeys (:2169-2201): frame 0 is the first key and frame n - 1 the last, so
+        // every later frame lies in (a, b] of two consecutive keys.
+        int ka = 0, kb = col.next_key(0, words);
+        float va = col.at(0), vb = col.at(kb);
+        double kden = (double)kb, ky = __ldg(g_kf_rcp + kb);
+        for (int u = 0; u < n; ++u) {
+            const float x = col.at(u);
+            float out;
+            if (u == 0) {
+                out = va;
+            } else {
+                if (u > kb) {
+                    ka = kb;
+                    kb = col.next_key(ka, words);
+                    va = vb;
+                    vb = col.at(kb);
+                    kden = (double)(kb - ka);
+                    ky = __ldg(g_kf_rcp + (kb - ka));
+                }
+                const double alpha = div_int_rn((double)(u - ka), kden, ky);
+                out = __double2float_rn(__dadd_rn((double)va, __dmul_rn(alpha, (double)__fsub_rn(vb, va))));
+            }
+            const double d = __dsub_rn((double)x, (double)out);
+            e2 = __dadd_rn(e2, __dmul_rn(d, d));
+            if (recon) recon[(unsigned long long)u * fstride] = out;
+        }
+    }
+
+    return SeriesOut{count, flag, e2};
+}
+
+template <int NV>
+__global__ void __launch_bounds__(NV) keyframe_pass_kernel(const float* __restrict__ values, unsigned long long series,
+                                                           int n, unsigned long long fstride, vbt_keyframe_profile p,
+                                                           int rmax, uint32_t* __restrict__ key_mask,
+                                                           uint32_t* __restrict__ key_count, uint8_t* __restrict__ flags,
+                                                           float* __restrict__ recon, double* __restrict__ err2_out,
+                                                           KfTotals* __restrict__ totals)
+{
+    extern __shared__ __align__(16) float kf_smem[];
+    const int words = (n + 31) >> 5;
+    float* sv = kf_smem;                                               // [n][NV]
+    uint32_t* sm = reinterpret_cast<uint32_t*>(sv + n * NV);           // [words][NV]
+    float* stop = reinterpret_cast<float*>(sm + words * NV);           // [rmax][NV]
+    const int j = threadIdx.x;
+    const unsigned long long base = (unsigned long long)blockIdx.x * NV;
+
+    for (int idx = j; idx < n * NV; idx += NV) {
+        const int t = idx / NV, c = idx - t * NV;
+        const unsigned long long s = base + (unsigned long long)c;
+        sv[idx] = s < series ? __ldcs(values + (unsigned long long)t * fstride + s) : 0.0f;
+    }
+    __syncthreads();
+
+    const unsigned long long s = base + (unsigned long long)j;
+    const bool valid = s < series;
+    SeriesOut r{0u, 0, 0.0};
+    if (valid) {
+        const Column<NV> col{sv + j, sm + j};
+        r = keyframe_series<NV>(col, stop + j, n, words, p, recon ? recon + s : nullptr, fstride);
+        for (int w = 0; w < words; ++w) key_mask[(unsigned long long)w * series + s] = col.m[w * NV];
+        key_count[s] = r.count;
+        flags[s] = r.flag;
+        if (err2_out) err2_out[s] = r.e2;
+    }
+
+    if (totals) {   // every lane of the warp is here (none returned early); idle lanes add zeros
+        unsigned long long keys = r.count, prot = (r.flag >> 1) & 1u, bg = r.flag & 1u;
+        unsigned int kmax = r.count;
+        double e = r.e2;
+        for (int o = 16; o > 0; o >>= 1) {
+            keys += __shfl_xor_sync(0xFFFFFFFFu, keys, o);
+            prot += __shfl_xor_sync(0xFFFFFFFFu, prot, o);
+            bg += __shfl_xor_sync(0xFFFFFFFFu, bg, o);
+            kmax = max(kmax, __shfl_xor_sync(0xFFFFFFFFu, kmax, o));
+            e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&totals->total_keys, keys);
+            atomicAdd(&totals->protected_series, prot);
+            atomicAdd(&totals->background_series, bg);
+            atomicMax(&totals->max_keys, kmax);
+            atomicAdd(&totals->err2, e);
+        }
+    }
+}
+
+// Every a / b with 1 <= b <= b_max and 0 <= a <= b through div_int_rn against the IEEE quotient.
+__global__ void keyframe_division_check_kernel(uint32_t b_max, unsigned long long* bad, unsigned long long* first)
+{
+    unsigned long long local = 0;
+    for (uint32_t b = 1u + blockIdx.x; b <= b_max; b += gridDim.x) {
+        const double bd = (double)b, y = __drcp_rn(bd);
+        for (uint32_t a = threadIdx.x; a <= b; a += blockDim.x) {
+            const double q = div_int_rn((double)a, bd, y);
+            if (__double_as_longlong(q) != __double_as_longlong(__ddiv_rn((double)a, bd))) {
+                ++local;
+                atomicMin(first, ((unsigned long long)b << 16) | a);
+            }
+        }
+    }
+    if (local) atomicAdd(bad, local);
+}
+
+template <int NV>
+size_t kf_smem_bytes(int n, int rmax)
+{
+    return (size_t)NV * 4u * ((size_t)n + (size_t)((n + 31) / 32) + (size_t)rmax);
+}
+
+}  // namespace
+
+static_assert(sizeof(KfTotals) == sizeof(vbt_keyframe_totals), "vbt_keyframe_totals layout");
+
+extern "C" int vbt_detect_keyframes(const float* d_values, uint64_t series, uint32_t frames, uint64_t frame_stride,
+                                    const vbt_keyframe_profile* profile, uint32_t* d_key_mask, uint32_t* d_key_count,
+                                    uint8_t* d_flags, float* d_recon, double* d_err2, vbt_keyframe_totals* d_totals,
+                                    void* stream)
+{
+    using vbtb::set_last_error;
+    if (!profile) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null profile");
+    if (frames == 0) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "frames must be at least 1");
+    if (frames > kKfMaxFrames) return set_last_error(VBT_STATUS_LIMIT, "frames above 1024");
+    if (frame_stride < series) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "frame_stride smaller than series");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (d_totals) {
+        const cudaError_t e = cudaMemsetAsync(d_totals, 0, sizeof(vbt_keyframe_totals), s);
+        if (e != cudaSuccess) return set_last_error(VBT_STATUS_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    }
+    if (series == 0) return VBT_STATUS_OK;
+    if (!d_values || !d_key_mask || !d_key_count || !d_flags)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    const int n = (int)frames;
+    const int m = n - 1;
+    const int rmax = n >= 2 ? m - (m - 1 < (m * 9) / 10 ? m - 1 : (m * 9) / 10) : 1;
+    int dev = 0, smem_max = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    KfTotals* totals = reinterpret_cast<KfTotals*>(d_totals);
+    const unsigned long long fs = frame_stride;
+    kf_rcp_init_kernel<<<1, 1024, 0, s>>>();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_last_error(VBT_STATUS_CUDA, std::string("kf_rcp_init_kernel: ") + cudaGetErrorString(e));
+    if (kf_smem_bytes<64>(n, rmax) <= (size_t)smem_max) {
+        const size_t smem = kf_smem_bytes<64>(n, rmax);
+        e = cudaFuncSetAttribute(keyframe_pass_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) {
+            const unsigned long long grid = (series + 63) / 64;
+            keyframe_pass_kernel<64><<<(unsigned)grid, 64, smem, s>>>(d_values, series, n, fs, *profile, rmax, d_key_mask,
+                                                                      d_key_count, d_flags, d_recon, d_err2, totals);
+            e = cudaGetLastError();
+        }
+    } else {
+        const size_t smem = kf_smem_bytes<32>(n, rmax);
+        e = cudaFuncSetAttribute(keyframe_pass_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) {
+            const unsigned long long grid = (series + 31) / 32;
+            keyframe_pass_kernel<32><<<(unsigned)grid, 32, smem, s>>>(d_values, series, n, fs, *profile, rmax, d_key_mask,
+                                                                      d_key_count, d_flags, d_recon, d_err2, totals);
+            e = cudaGetLastError();
+        }
+    }
+    return e == cudaSuccess ? VBT_STATUS_OK
+                            : set_last_error(VBT_STATUS_CUDA, std::string("keyframe_pass_kernel: ") + cudaGetErrorString(e));
+}
+
+extern "C" int vbt_selftest_keyframe_division(uint32_t b_max, uint64_t* result, int device)
+{
+    using vbtb::set_last_error;
+    if (!result) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    if (b_max < 1u || b_max > 65535u) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "b_max must lie in [1, 65535]");
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        return set_last_error(VBT_STATUS_CUDA, "no CUDA device");
+    if (device < 0 || device >= dev_count) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "device out of range");
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    unsigned long long* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, 2 * sizeof(unsigned long long));
+    unsigned long long h[2] = {0ull, ~0ull};
+    if (e == cudaSuccess) e = cudaMemcpy(d, h, sizeof(h), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        keyframe_division_check_kernel<<<8 * (sms > 0 ? sms : 1), 256>>>(b_max, d, d + 1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return set_last_error(VBT_STATUS_CUDA, std::string("keyframe division check: ") + cudaGetErrorString(e));
+    result[0] = h[0];
+    result[1] = h[1];
+    return VBT_STATUS_OK;
+}
