@@ -696,11 +696,35 @@ def run_keyframes(args, local_rank, reps=3, work=None):
         ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
         t = vbt.keyframe_totals(tot)
         moved = S * T * 4 * 2 + S * (W * 4 + 4 + 1 + 8)
+        e2e = None
+        if S * T * 4 <= (1 << 30):
+            # end to end from pinned host memory: frames in; reconstruction, key masks, counts and
+            # flags out, every step
+            h_in = frames.cpu().pin_memory()
+            h_recon = torch.empty(recon.shape, dtype=recon.dtype).pin_memory()
+            h_mask = torch.empty(mask.shape, dtype=mask.dtype).pin_memory()
+            h_cnt = torch.empty(cnt.shape, dtype=cnt.dtype).pin_memory()
+            h_flags = torch.empty(flags.shape, dtype=flags.dtype).pin_memory()
+            ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+            with torch.cuda.stream(s):
+                for e0, e1 in ev2:
+                    e0.record(s)
+                    frames.copy_(h_in, non_blocking=True)
+                    vbt.detect_keyframes(frames, prof, mask, cnt, flags, recon, None, None, stream=s)
+                    h_recon.copy_(recon, non_blocking=True)
+                    h_mask.copy_(mask, non_blocking=True)
+                    h_cnt.copy_(cnt, non_blocking=True)
+                    h_flags.copy_(flags, non_blocking=True)
+                    e1.record(s)
+            s.synchronize()
+            e2e_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev2)
+            e2e = {"series_per_s": S / (e2e_ms * 1e-3), "ms": e2e_ms, "h2d_bytes": S * T * 4,
+                   "d2h_bytes": S * T * 4 + S * (W * 4 + 4 + 1)}
         entry = {"series": S, "frames": T, "pass_ms": ms, "series_per_s": S / (ms * 1e-3),
                  "values_per_s": S * T / (ms * 1e-3), "bytes_moved": moved, "gb_per_s": moved / (ms * 1e-3) / 1e9,
                  "keys_per_series": t.total_keys / S, "max_keys": t.max_keys,
                  "background_series": t.background_series, "protected_series": t.protected_series,
-                 "bound": "fp64/integer issue (the pass reads and writes each value once)"}
+                 "bound": "fp64/integer issue (the pass reads and writes each value once)", "e2e": e2e}
         if ref is not None and not args.no_cpu:
             n = min(S, 65536 if T > 32 else S)
             sample = frames[:, :n].cpu().numpy()

@@ -157,9 +157,12 @@ int vbt_pack_payload(const uint8_t* d_blocks, const uint64_t* d_block_offsets, u
 
 /* ---- Encoder keyframe pass ---------------------------------------------------------------------
  * The per-voxel body of the reference encoder's leaf loop (src/render_temporal_kf_probe_main.cpp:
- * 619-659) over `series` independent series of `frames` finite values, series s at
- * d_values[t * frame_stride + s] (a raw frame-major volume: s = (z*Y + y)*X + x, frame_stride =
- * X*Y*Z): the background test (max(0, values) < bg_threshold, when bg_threshold >= 0),
+ * 619-659) over `series` independent series of `frames` finite values, value t of series s at
+ * d_values[t * frame_stride + s * series_stride] in either of RawVolume4D's orders
+ * (src/raw_volume.cpp:58-75): frame-major, series_stride = 1 and frame_stride >= series (s =
+ * (z*Y + y)*X + x, frame_stride = X*Y*Z), or time-fastest, frame_stride = 1 and series_stride >=
+ * frames; other layouts are VBT_STATUS_INVALID_ARGUMENT.  The background test (max(0, values) <
+ * bg_threshold, when bg_threshold >= 0),
  * detectDensityKeyFrames (:2080-2167) and reconstructFromKeys (:2169-2201).
  *   d_key_mask   word-major key sets: bit t % 32 of d_key_mask[(t / 32) * series + s]
  *   d_key_count  the count the encoder adds up: the keys, or 1 for a background-zeroed series
@@ -182,7 +185,7 @@ typedef struct {
     double err2;
 } vbt_keyframe_totals;
 int vbt_detect_keyframes(const float* d_values, uint64_t series, uint32_t frames, uint64_t frame_stride,
-                         const vbt_keyframe_profile* profile, uint32_t* d_key_mask, uint32_t* d_key_count,
+                         uint64_t series_stride, const vbt_keyframe_profile* profile, uint32_t* d_key_mask, uint32_t* d_key_count,
                          uint8_t* d_flags, float* d_recon, double* d_err2, vbt_keyframe_totals* d_totals,
                          void* stream);
 /* Self-check of the division the keyframe pass uses for alpha = a / b (no reference counterpart):

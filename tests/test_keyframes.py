@@ -122,6 +122,58 @@ def test_frame_counts_and_padding(vbt, cuda, oracle, T):
     assert np.isnan(got["recon"][:, S:]).all()            # padding columns untouched
 
 
+EDGE_PROFILES = [dict(eps_abs=0.0), dict(gamma_delta=0.0, eps_rel=0.001), dict(gamma_delta=5.0),
+                 dict(render_cutoff=-1.0, iso_surface_protect=1, iso_value=0.5, iso_band=0.0),
+                 dict(render_cutoff=-1.0, iso_surface_protect=1, iso_value=-2.0, iso_band=0.3, eps_rel=0.1),
+                 dict(cutoff_band=0.0, render_cutoff=0.5), dict(eps_abs=1e-2, eps_rel=0.0)]
+
+
+@pytest.mark.parametrize("pi", range(len(EDGE_PROFILES)))
+def test_edge_profiles(vbt, cuda, oracle, pi):
+    """Profiles away from the encoder's defaults over signed, piecewise-constant, oscillating and
+    random-walk series at magnitudes from 1e-30 to 1e30."""
+    rng = np.random.default_rng(100 + pi)
+    T, S = 96, 4000
+    t = np.arange(T)[:, None]
+    kind = rng.integers(0, 4, S)
+    walk = np.cumsum(rng.normal(0, 1, (T, S)), axis=0)
+    osc = np.sin(t * rng.uniform(0.05, 0.6, S)) * 3.0 - 1.0
+    steps = np.repeat(rng.normal(0, 1, (T // 3 + 1, S)), 3, axis=0)[:T]
+    noise = rng.normal(0, 1, (T, S))
+    f = np.choose(kind, [noise, osc, steps, walk])
+    f = f * np.array([1e-30, 1e-6, 1.0, 1e3, 1e30])[rng.integers(0, 5, S)]
+    frames = f.astype(np.float32)
+    prof = vbt.KeyframeProfile(**EDGE_PROFILES[pi])
+    got = run_gpu(vbt, cuda, frames, prof)
+    want = oracle.keyframe_pass(frames, oracle_prof(prof))
+    compare(got, want, S, EDGE_PROFILES[pi])
+
+
+def test_time_fastest_layout(vbt, cuda, oracle):
+    """RawVolume4D's time-fastest order: each series contiguous (rows padded past the frame count);
+    the reconstruction comes back in the same layout."""
+    T, S = 96, 5000
+    frames = blob_frames(T, S, seed=21)
+    rows = np.zeros((S, T + 5), np.float32)
+    rows[:, :T] = frames.T
+    d_v = cuda.from_numpy(rows).cuda()[:, :T]
+    W = (T + 31) // 32
+    mask = cuda.zeros((W, S), dtype=cuda.int32, device="cuda")
+    cnt = cuda.zeros(S, dtype=cuda.int32, device="cuda")
+    fl = cuda.zeros(S, dtype=cuda.uint8, device="cuda")
+    recon_full = cuda.full((S, T + 5), float("nan"), dtype=cuda.float32, device="cuda")
+    recon = recon_full[:, :T]
+    err2 = cuda.zeros(S, dtype=cuda.float64, device="cuda")
+    prof = vbt.KeyframeProfile()
+    vbt.detect_keyframes(d_v, prof, mask, cnt, fl, recon, err2, time_fastest=True)
+    cuda.cuda.synchronize()
+    want = oracle.keyframe_pass(frames, oracle_prof(prof))
+    got = dict(key_mask=mask.cpu().numpy().view(np.uint32), key_count=cnt.cpu().numpy().view(np.uint32),
+               flags=fl.cpu().numpy(), recon=np.ascontiguousarray(recon.cpu().numpy().T), err2=err2.cpu().numpy())
+    compare(got, want, S, "time fastest")
+    assert np.isnan(recon_full.cpu().numpy()[:, T:]).all()
+
+
 def test_rejects_bad_arguments(vbt, cuda):
     prof = vbt.KeyframeProfile()
     v = cuda.zeros((1025, 64), dtype=cuda.float32, device="cuda")

@@ -103,3 +103,38 @@ def test_pass_against_reference(oracle, kfref):
     assert (out["flags"] & 1).sum() > 100
     assert np.array_equal(out["key_count"], kc)
     assert np.array_equal(out["err2"].view(np.uint64), e2.view(np.uint64))
+
+
+def test_edge_profiles_against_reference(oracle, kfref):
+    """Profiles and values away from the encoder's defaults: no absolute epsilon (the floor alone
+    bounds it), no gamma, a large gamma, signed level-set values around a nonzero iso value with
+    and without a band, huge and tiny magnitudes, and a cutoff band of zero."""
+    rng = np.random.default_rng(91)
+    profiles = [dict(eps_abs=0.0), dict(gamma_delta=0.0, eps_rel=0.001), dict(gamma_delta=5.0),
+                dict(render_cutoff=-1.0, iso_surface_protect=1, iso_value=0.5, iso_band=0.0),
+                dict(render_cutoff=-1.0, iso_surface_protect=1, iso_value=-2.0, iso_band=0.3, eps_rel=0.1),
+                dict(cutoff_band=0.0, render_cutoff=0.5), dict(eps_abs=1e-2, eps_rel=0.0)]
+    scales = [1e-30, 1e-6, 1.0, 1e3, 1e30]
+    n = 0
+    for it in range(2400):
+        T = int(rng.choice([2, 3, 9, 40, 96, 200]))
+        kind = it % 4
+        t = np.arange(T)
+        if kind == 0:
+            v = rng.normal(0, 1, T)
+        elif kind == 1:
+            v = np.sin(t * rng.uniform(0.05, 0.6)) * 3.0 - 1.0
+        elif kind == 2:
+            v = np.repeat(rng.normal(0, 1, T // 3 + 1), 3)[:T]         # piecewise constant
+        else:
+            v = np.cumsum(rng.normal(0, 1, T))
+        v = (v * scales[it % len(scales)]).astype(np.float32)
+        p = profile(profiles[it % len(profiles)])
+        k, u = oracle.detect_keyframes(v, p)
+        k2, u2 = kfref.detect_keyframes(v, p)
+        assert np.array_equal(k, k2) and u == u2, (it, T, profiles[it % len(profiles)])
+        r = oracle.reconstruct(v, k)
+        r2 = kfref.reconstruct(v, k2)
+        assert np.array_equal(r.view(np.uint32), r2.view(np.uint32)), it
+        n += 1
+    assert n == 2400

@@ -131,8 +131,8 @@ _sig = {
     "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_selftest_key_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_pack_payload": ([_vp, _vp, C.c_uint32, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64), _vp], C.c_int),
-    "vbt_detect_keyframes": ([_vp, C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(KeyframeProfile), _vp, _vp, _vp,
-                              _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_detect_keyframes": ([_vp, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, C.POINTER(KeyframeProfile), _vp,
+                              _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "vbt_selftest_keyframe_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_sample_rays": ([_vp, _vp, C.POINTER(SampleParams), _vp, C.c_uint32, _vp, _vp], C.c_int),
     "vbt_decode_control_cache": ([_vp, C.POINTER(C.c_int), C.c_int, _vp, C.c_uint64, _vp], C.c_int),
@@ -383,15 +383,24 @@ def pack_payload(blocks, block_offsets, offsets, payload, stream=None):
 
 
 def detect_keyframes(values, profile, key_mask, key_count, flags, recon=None, err2=None, totals=None,
-                     series=None, stream=None):
-    """The encoder's per-voxel keyframe pass on the GPU over values [frames, stride] (float32 device
-    tensor, frame-major; the first `series` columns, default all): key_mask [ceil(frames / 32),
-    series] int32, key_count [series] int32, flags [series] uint8, and optionally recon (the
-    reconstruction, shaped like values), err2 [series] float64 and totals (a 40-byte device buffer
-    read back by keyframe_totals)."""
-    frames, stride = values.shape
-    n = stride if series is None else int(series)
-    _check(_lib.vbt_detect_keyframes(_addr(values), n, frames, stride, C.byref(profile), _addr(key_mask),
+                     series=None, time_fastest=False, stream=None):
+    """The encoder's per-voxel keyframe pass on the GPU.  values: a float32 device tensor, frame-major
+    [frames, >= series] or, with time_fastest, [series, >= frames] (rows may be padded); `series`
+    defaults to all of them.  Outputs: key_mask [ceil(frames / 32), series] int32, key_count
+    [series] int32, flags [series] uint8, and optionally recon (the reconstruction, in values'
+    layout), err2 [series] float64 and totals (a 40-byte device buffer read back by
+    keyframe_totals)."""
+    if time_fastest:
+        rows, frames = values.shape
+        ss, fs = values.stride()
+        n = rows if series is None else int(series)
+    else:
+        frames, cols = values.shape
+        fs, ss = values.stride()
+        n = cols if series is None else int(series)
+    if recon is not None and tuple(recon.stride()) != tuple(values.stride()):
+        raise ValueError("recon must have the layout of values")
+    _check(_lib.vbt_detect_keyframes(_addr(values), n, frames, fs, ss, C.byref(profile), _addr(key_mask),
                                      _addr(key_count), _addr(flags), _addr(recon), _addr(err2), _addr(totals),
                                      _stream(stream)))
 

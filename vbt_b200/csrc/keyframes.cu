@@ -355,7 +355,8 @@ __device__ __forceinline__ SeriesOut keyframe_series(const Column<NV>& col, floa
 
 template <int NV>
 __global__ void __launch_bounds__(NV) keyframe_pass_kernel(const float* __restrict__ values, unsigned long long series,
-                                                           int n, unsigned long long fstride, vbt_keyframe_profile p,
+                                                           int n, unsigned long long fstride,
+                                                           unsigned long long sstride, vbt_keyframe_profile p,
                                                            int rmax, uint32_t* __restrict__ key_mask,
                                                            uint32_t* __restrict__ key_count, uint8_t* __restrict__ flags,
                                                            float* __restrict__ recon, double* __restrict__ err2_out,
@@ -369,10 +370,18 @@ __global__ void __launch_bounds__(NV) keyframe_pass_kernel(const float* __restri
     const int j = threadIdx.x;
     const unsigned long long base = (unsigned long long)blockIdx.x * NV;
 
-    for (int idx = j; idx < n * NV; idx += NV) {
-        const int t = idx / NV, c = idx - t * NV;
-        const unsigned long long s = base + (unsigned long long)c;
-        sv[idx] = s < series ? __ldcs(values + (unsigned long long)t * fstride + s) : 0.0f;
+    if (sstride == 1ull) {              // frame-major: a warp reads 32 neighbouring series of one frame
+        for (int idx = j; idx < n * NV; idx += NV) {
+            const int t = idx / NV, c = idx - t * NV;
+            const unsigned long long s = base + (unsigned long long)c;
+            sv[idx] = s < series ? __ldcs(values + (unsigned long long)t * fstride + s) : 0.0f;
+        }
+    } else {                            // time fastest: a warp reads 32 neighbouring frames of one series
+        for (int idx = j; idx < n * NV; idx += NV) {
+            const int c = idx / n, t = idx - c * n;
+            const unsigned long long s = base + (unsigned long long)c;
+            sv[t * NV + c] = s < series ? __ldcs(values + (unsigned long long)t * fstride + s * sstride) : 0.0f;
+        }
     }
     __syncthreads();
 
@@ -381,7 +390,7 @@ __global__ void __launch_bounds__(NV) keyframe_pass_kernel(const float* __restri
     SeriesOut r{0u, 0, 0.0};
     if (valid) {
         const Column<NV> col{sv + j, sm + j};
-        r = keyframe_series<NV>(col, stop + j, n, words, p, recon ? recon + s : nullptr, fstride);
+        r = keyframe_series<NV>(col, stop + j, n, words, p, recon ? recon + s * sstride : nullptr, fstride);
         for (int w = 0; w < words; ++w) key_mask[(unsigned long long)w * series + s] = col.m[w * NV];
         key_count[s] = r.count;
         flags[s] = r.flag;
@@ -437,6 +446,7 @@ size_t kf_smem_bytes(int n, int rmax)
 static_assert(sizeof(KfTotals) == sizeof(vbt_keyframe_totals), "vbt_keyframe_totals layout");
 
 extern "C" int vbt_detect_keyframes(const float* d_values, uint64_t series, uint32_t frames, uint64_t frame_stride,
+                                    uint64_t series_stride,
                                     const vbt_keyframe_profile* profile, uint32_t* d_key_mask, uint32_t* d_key_count,
                                     uint8_t* d_flags, float* d_recon, double* d_err2, vbt_keyframe_totals* d_totals,
                                     void* stream)
@@ -445,7 +455,12 @@ extern "C" int vbt_detect_keyframes(const float* d_values, uint64_t series, uint
     if (!profile) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null profile");
     if (frames == 0) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "frames must be at least 1");
     if (frames > kKfMaxFrames) return set_last_error(VBT_STATUS_LIMIT, "frames above 1024");
-    if (frame_stride < series) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "frame_stride smaller than series");
+    const bool frame_major = series_stride == 1u && frame_stride >= series;
+    const bool time_fastest = frame_stride == 1u && series_stride >= frames;
+    if (!frame_major && !time_fastest)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT,
+                              "layout must be frame-major (series_stride 1, frame_stride >= series) or time-fastest "
+                              "(frame_stride 1, series_stride >= frames)");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (d_totals) {
         const cudaError_t e = cudaMemsetAsync(d_totals, 0, sizeof(vbt_keyframe_totals), s);
@@ -461,7 +476,7 @@ extern "C" int vbt_detect_keyframes(const float* d_values, uint64_t series, uint
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     KfTotals* totals = reinterpret_cast<KfTotals*>(d_totals);
-    const unsigned long long fs = frame_stride;
+    const unsigned long long fs = frame_stride, ss = frame_major ? 1ull : series_stride;
     kf_rcp_init_kernel<<<1, 1024, 0, s>>>();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_last_error(VBT_STATUS_CUDA, std::string("kf_rcp_init_kernel: ") + cudaGetErrorString(e));
@@ -470,7 +485,7 @@ extern "C" int vbt_detect_keyframes(const float* d_values, uint64_t series, uint
         e = cudaFuncSetAttribute(keyframe_pass_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess) {
             const unsigned long long grid = (series + 63) / 64;
-            keyframe_pass_kernel<64><<<(unsigned)grid, 64, smem, s>>>(d_values, series, n, fs, *profile, rmax, d_key_mask,
+            keyframe_pass_kernel<64><<<(unsigned)grid, 64, smem, s>>>(d_values, series, n, fs, ss, *profile, rmax, d_key_mask,
                                                                       d_key_count, d_flags, d_recon, d_err2, totals);
             e = cudaGetLastError();
         }
@@ -479,7 +494,7 @@ extern "C" int vbt_detect_keyframes(const float* d_values, uint64_t series, uint
         e = cudaFuncSetAttribute(keyframe_pass_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess) {
             const unsigned long long grid = (series + 31) / 32;
-            keyframe_pass_kernel<32><<<(unsigned)grid, 32, smem, s>>>(d_values, series, n, fs, *profile, rmax, d_key_mask,
+            keyframe_pass_kernel<32><<<(unsigned)grid, 32, smem, s>>>(d_values, series, n, fs, ss, *profile, rmax, d_key_mask,
                                                                       d_key_count, d_flags, d_recon, d_err2, totals);
             e = cudaGetLastError();
         }
