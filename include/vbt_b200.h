@@ -172,7 +172,8 @@ int vbt_pack_payload(const uint8_t* d_blocks, const uint64_t* d_block_offsets, u
  *   d_totals     optional, overwritten: the leaf loop's totals (totalKeyframes, maxKeyframes,
  *                temporalProtectedSeries, backgroundZeroedVoxels, and the squared error, whose
  *                summation order differs from the reference's running sum)
- * Everything but d_totals->err2 equals the reference bit for bit.  frames <= 1024. */
+ * Everything but d_totals->err2 equals the reference bit for bit.  frames <= 1024 and series < 2^36
+ * (VBT_STATUS_LIMIT beyond). */
 typedef struct {
     float eps_abs, eps_rel, gamma_delta, render_cutoff, cutoff_band;   /* DensityTemporalProfile, :81-95 */
     uint32_t cutoff_temporal_protect, iso_surface_protect;

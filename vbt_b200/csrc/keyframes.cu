@@ -467,6 +467,7 @@ extern "C" int vbt_detect_keyframes(const float* d_values, uint64_t series, uint
         if (e != cudaSuccess) return set_last_error(VBT_STATUS_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
     }
     if (series == 0) return VBT_STATUS_OK;
+    if ((series + 63u) / 32u > 0x7FFFFFFFull) return set_last_error(VBT_STATUS_LIMIT, "series above 2^36");
     if (!d_values || !d_key_mask || !d_key_count || !d_flags)
         return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
     const int n = (int)frames;
