@@ -155,6 +155,42 @@ int vbt_sample_rays(vbt_asset* asset, const float* d_controls, const vbt_sample_
 int vbt_pack_payload(const uint8_t* d_blocks, const uint64_t* d_block_offsets, uint32_t leaf_count, uint32_t* d_offsets,
                      uint32_t* d_payload, uint64_t payload_capacity_words, uint64_t* total_words, void* stream);
 
+/* ---- VBTPACK4 writer, leaves from control streams -----------------------------------------------
+ * packRenderTemporalControlStream (src/render_temporal_decode.cpp:201-264) for every stream and
+ * buildRenderTemporalPackedLeafBytes (src/render_temporal_payload.cpp:199-232; the Mode2 shell
+ * overload :348-386), 4-byte aligned as the encoder writes them, for leaf_count leaves at once,
+ * straight into the payload: d_offsets (leaf_count + 1 word offsets) and d_payload, as
+ * vbt_pack_payload lays them out.  Per leaf, a vbt_leaf_streams names its packed header word
+ * (packRenderTemporalHeader: mode, codecs, resolutions), its prefix, and where its streams' rows
+ * start in the shared arrays:
+ *   d_descriptors  one RenderTemporalControlDescriptor per control row (keyStart | keyCount << 16 |
+ *                  reserved << 24), control_rows rows
+ *   d_bins         8 bytes per control row, the stream's time-bin index (4-bin Mode2 residual
+ *                  streams use the first 4)
+ *   d_key_frames / d_key_values  key_rows keyframes (frame, value); FP16 streams store the value
+ *                  as renderTemporalFloatToHalfBits(value)
+ *   d_occupancy    occupancy_rows 80-byte Mode2 shell occupancy sections (4-byte aligned)
+ * A stream has resolution^3 controls (the Mode2 residual stream: the occupancy's active voxels),
+ * 8 time bins (Mode2 residual: 4) and the prefix's keyframe count.  Invalid streams
+ * (validateRenderTemporalControlStreamData, with the leaf's max_local as maxBinLocalKeys), FP16
+ * frames above 255 and rows outside the arrays give VBT_STATUS_INVALID_ARGUMENT with the
+ * reference's message and the lowest failing leaf; nothing is written then.  Synchronises
+ * `stream` once (to read the payload size). */
+typedef struct {
+    uint32_t header;                               /* packRenderTemporalHeader word */
+    uint16_t coarse_keyframes, fine_keyframes;     /* RenderTemporalPackedLeafPrefix */
+    uint32_t coarse_control, coarse_key;           /* first control row / keyframe of the coarse stream */
+    uint32_t fine_control, fine_key;               /* FINE6 stream, or the Mode2 shell residual stream */
+    uint32_t occupancy;                            /* Mode2: row of the leaf's occupancy section */
+    uint8_t coarse_max_local, fine_max_local;      /* the streams' maxBinLocalKeys */
+    uint8_t pad[2];
+} vbt_leaf_streams;
+int vbt_pack_leaves(const vbt_leaf_streams* d_leaves, uint32_t leaf_count, const uint32_t* d_descriptors,
+                    const uint8_t* d_bins, uint64_t control_rows, const uint16_t* d_key_frames,
+                    const float* d_key_values, uint64_t key_rows, const uint8_t* d_occupancy, uint64_t occupancy_rows,
+                    uint32_t* d_offsets, uint32_t* d_payload, uint64_t payload_capacity_words, uint64_t* total_words,
+                    void* stream);
+
 /* ---- Encoder keyframe pass ---------------------------------------------------------------------
  * The per-voxel body of the reference encoder's leaf loop (src/render_temporal_kf_probe_main.cpp:
  * 619-659) over `series` independent series of `frames` finite values, value t of series s at

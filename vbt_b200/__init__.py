@@ -131,6 +131,8 @@ _sig = {
     "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_selftest_key_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_pack_payload": ([_vp, _vp, C.c_uint32, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64), _vp], C.c_int),
+    "vbt_pack_leaves": ([_vp, C.c_uint32, _vp, _vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp, C.c_uint64, _vp, _vp,
+                         C.c_uint64, C.POINTER(C.c_uint64), _vp], C.c_int),
     "vbt_detect_keyframes": ([_vp, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, C.POINTER(KeyframeProfile), _vp,
                               _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "vbt_selftest_keyframe_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
@@ -379,6 +381,23 @@ def pack_payload(blocks, block_offsets, offsets, payload, stream=None):
     n = block_offsets.shape[0] - 1
     _check(_lib.vbt_pack_payload(_addr(blocks), _addr(block_offsets), n, _addr(offsets), _addr(payload),
                                  payload.numel() if payload is not None else 0, C.byref(total), _stream(stream)))
+    return total.value
+
+
+def pack_leaves(leaves, descriptors, bins, key_frames, key_values, occupancy, offsets, payload, stream=None):
+    """VBTPACK4 leaves from their control streams on the GPU, straight into the payload.  leaves: a
+    uint8 device tensor of 32-byte vbt_leaf_streams records; descriptors (int32, one per control
+    row), bins (uint8, 8 per control row), key_frames (int16/uint16), key_values (float32),
+    occupancy (uint8, 80 per Mode2 section, may be None); offsets (int32, n + 1) and payload
+    (int32) receive the result.  Returns the payload size in words."""
+    total = C.c_uint64()
+    n = leaves.numel() // 32
+    rows = lambda t, per=1: 0 if t is None else t.numel() // per  # noqa: E731
+    _check(_lib.vbt_pack_leaves(_addr(leaves), n, _addr(descriptors), _addr(bins),
+                                min(rows(descriptors), rows(bins, 8)), _addr(key_frames), _addr(key_values),
+                                min(rows(key_frames), rows(key_values)), _addr(occupancy),
+                                rows(occupancy, 80), _addr(offsets), _addr(payload),
+                                payload.numel() if payload is not None else 0, C.byref(total), _stream(stream)))
     return total.value
 
 
