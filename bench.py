@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-full-frame", action="store_true")
     p.add_argument("--no-sampler", action="store_true")
     p.add_argument("--no-keyframes", action="store_true")
+    p.add_argument("--no-writer", action="store_true")
     p.add_argument("--serve-requests", type=int, default=300)
     return p.parse_args()
 
@@ -742,6 +743,71 @@ def run_keyframes(args, local_rank, reps=3, work=None):
     return out
 
 
+# ------------------------------------------------------------------------------ writer
+def run_writer(args, local_rank, reps=5):
+    """The VBTPACK4 writer on one B200 (vbt_pack_leaves: every leaf's control streams packed and the
+    leaves assembled into the payload, one call) for the plume (32,768 leaves) and the config-4
+    style level set (Mode2 shell leaves), stream arrays resident; device time of the call, its
+    one host round trip for the payload size included.  Beside it the reference's own packer
+    (packRenderTemporalControlStream + buildRenderTemporalPackedLeafBytes + the payload
+    concatenation, oracle/_ref) on all host threads over the same arrays; both outputs are
+    checked against the file."""
+    import torch
+    import vbt_b200 as vbt
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from leafstreams import streams_from_file
+    dev = f"cuda:{local_rank}"
+    out = {}
+    for name in ("cfg2_plume", "mix_sdf"):
+        path = os.path.join(ROOT, "assets", name + ".vbtp")
+        if not os.path.exists(path):
+            continue
+        leaves, arr, _ = streams_from_file(path)
+        raw = open(path, "rb").read()
+        h = np.frombuffer(raw[8:52], np.uint32)
+        off_at = 52 + 4 * int(h[10])
+        want = np.frombuffer(raw[off_at + 4 * (int(h[8]) + 1):], np.uint32)
+        t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a).view(dt)).to(dev) if a.size else None  # noqa: E731
+        d_leaves = torch.from_numpy(leaves.view(np.uint8).copy()).to(dev)
+        d = [t(arr["descriptors"], np.int32), t(arr["bins"], np.uint8), t(arr["key_frames"], np.int16),
+             t(arr["key_values"], np.float32), t(arr["occupancy"], np.uint8)]
+        n = leaves.shape[0]
+        d_off = torch.empty(n + 1, dtype=torch.int32, device=dev)
+        d_pay = torch.empty(want.size + 64, dtype=torch.int32, device=dev)
+        s = torch.cuda.Stream(device=dev)
+        s.wait_stream(torch.cuda.current_stream(dev))
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        with torch.cuda.stream(s):
+            vbt.pack_leaves(d_leaves, *d, d_off, d_pay, stream=s)
+            for e0, e1 in ev:
+                e0.record(s)
+                total = vbt.pack_leaves(d_leaves, *d, d_off, d_pay, stream=s)
+                e1.record(s)
+        s.synchronize()
+        ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+        ok = total == want.size and np.array_equal(d_pay[:total].cpu().numpy().view(np.uint32), want)
+        entry = {"leaves": n, "active_leaves": int(((leaves["header"] & 3) != 0).sum()),
+                 "mode2_leaves": int(((leaves["header"] & 3) == 2).sum()), "payload_bytes": int(total) * 4,
+                 "call_ms": ms, "leaves_per_s": n / (ms * 1e-3), "payload_gb_per_s": total * 4 / (ms * 1e-3) / 1e9,
+                 "equals_file": bool(ok), "gpu_launches_per_call": 3}
+        if not args.no_cpu:
+            try:
+                from oracle.oracle import Reference
+                ref = Reference()
+                ref.pack_leaves(leaves, arr)
+                t0 = time.perf_counter()
+                for _ in range(3):
+                    r_off, r_pay = ref.pack_leaves(leaves, arr, threads=os.cpu_count())
+                el = (time.perf_counter() - t0) / 3
+                entry["cpu_reference"] = {"ms": el * 1e3, "leaves_per_s": n / el, "cores": os.cpu_count(),
+                                          "kind": "reference", "equals_file": bool(np.array_equal(r_pay, want))}
+                entry["speedup_vs_cpu_reference"] = el * 1e3 / ms
+            except (OSError, FileNotFoundError):
+                pass
+        out[name] = entry
+    return out or {"skipped": "assets not generated"}
+
+
 # ------------------------------------------------------------------------------ arms
 def run_reference(args, rank, world):
     """The reference's own CPU decoder on the host cores, same metric and workload; each step is
@@ -921,6 +987,10 @@ def run_ours(args, rank, local_rank, world):
     if rank == 0 and world == 1 and not args.no_keyframes:
         keyframes = run_keyframes(args, local_rank)
 
+    writer = None
+    if rank == 0 and world == 1 and not args.no_writer:
+        writer = run_writer(args, local_rank)
+
     window = window_render = None
     if rank == 0 and world == 1 and not args.no_window:
         window = run_window(args, local_rank)
@@ -958,7 +1028,7 @@ def run_ours(args, rank, local_rank, world):
                           "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
                 "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "precision_window": window,
                 "precision_window_render": window_render, "full_frame": full_frame, "ray_sampler": sampler,
-                "keyframe_pass": keyframes,
+                "keyframe_pass": keyframes, "writer": writer,
                 "gpu_launches": args.steps * (1 + len(chunks)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)

@@ -296,6 +296,9 @@ class Reference:
         L.vr_build_leaf.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u8p, C.c_size_t, u8p, C.c_size_t, u8p,
                                     C.c_size_t, C.c_int, u8p, C.c_size_t]
         L.vr_build_leaf.restype = C.c_long
+        L.vr_pack_leaves.argtypes = [u8p, C.c_uint32, u32p, u8p, C.POINTER(C.c_uint16), f32p, u8p, u32p, u32p,
+                                     C.c_size_t, C.c_int]
+        L.vr_pack_leaves.restype = C.c_long
         L.vr_generate_queries.argtypes = [C.c_uint32] * 4 + [C.c_int, C.c_uint32, C.c_uint32, u32p, u32p]
         L.vr_dct.argtypes = [f32p, f32p, C.c_int, C.c_int, f32p, f32p]
 
@@ -384,6 +387,26 @@ class Reference:
         if n < 0:
             raise RuntimeError(self.error())
         return out[:n].copy()
+
+    def pack_leaves(self, leaves, arr, threads=0):
+        """(offsets, payload) of the reference's packer over the stream arrays of vbt_pack_leaves
+        (leaves: 32-byte records as tests/leafstreams.py builds them)."""
+        rec = np.ascontiguousarray(leaves).view(np.uint8)
+        n = rec.size // 32
+        desc = np.ascontiguousarray(arr["descriptors"], np.uint32)
+        bins = np.ascontiguousarray(arr["bins"], np.uint8)
+        kf = np.ascontiguousarray(arr["key_frames"], np.uint16)
+        kv = np.ascontiguousarray(arr["key_values"], np.float32)
+        occ = np.ascontiguousarray(arr["occupancy"], np.uint8)
+        cap = 16 + 28 * n + desc.size + bins.size // 4 + 2 * kf.size
+        off = np.zeros(n + 1, np.uint32)
+        pay = np.zeros(cap, np.uint32)
+        w = self.lib.vr_pack_leaves(_ptr(rec, u8p), n, _ptr(desc, u32p), _ptr(bins, u8p),
+                                    _ptr(kf, C.POINTER(C.c_uint16)), _ptr(kv, f32p), _ptr(occ, u8p), _ptr(off, u32p),
+                                    _ptr(pay, u32p), cap, threads)
+        if w < 0:
+            raise RuntimeError(self.error())
+        return off, pay[:w]
 
     def build_leaf(self, packed_header, coarse_kf, fine_kf, coarse, fine, occ=None, align=True):
         c = np.ascontiguousarray(coarse, np.uint8)

@@ -383,6 +383,96 @@ long vr_build_leaf(uint32_t packedHeader, uint32_t coarseKf, uint32_t fineKf, co
     }
 }
 
+// The encoder's leaf packing and payload assembly over many leaves, from the stream arrays that
+// vbt_pack_leaves reads (32-byte records: header word, prefix counts, first control row / keyframe
+// of the coarse and fine streams, occupancy row, maxBinLocalKeys of both streams): per leaf the
+// reference's packRenderTemporalControlStream and buildRenderTemporalPackedLeafBytes on OpenMP
+// threads, then the offsets and padded payload as writeRenderTemporalProbeFile concatenates them
+// (src/render_temporal_kf_probe_main.cpp:2561-2585).  Returns the payload words, or -1.
+long vr_pack_leaves(const uint8_t* records, uint32_t n, const uint32_t* desc, const uint8_t* bins,
+                    const uint16_t* keyFrames, const float* keyValues, const uint8_t* occupancy, uint32_t* offsets,
+                    uint32_t* payload, size_t capWords, int threads)
+{
+    struct Rec {
+        uint32_t header;
+        uint16_t ckf, fkf;
+        uint32_t cc, ck, fc, fk, occ;
+        uint8_t cml, fml, pad[2];
+    };
+    static_assert(sizeof(Rec) == 32, "record layout");
+    std::vector<std::vector<uint8_t>> leaves(n);
+    bool failed = false;
+    auto stream = [&](uint32_t codec, uint32_t controls, uint32_t nb, uint32_t maxLocal, uint32_t firstControl,
+                      uint32_t firstKey, uint32_t keys) {
+        RenderTemporalControlStreamData s;
+        s.codec = RenderTemporalSequenceCodec(codec);
+        s.controlCount = uint16_t(controls);
+        s.timeBinCount = uint8_t(nb);
+        s.maxBinLocalKeys = uint8_t(maxLocal);
+        for (uint32_t c = 0; c < controls; ++c) {
+            const uint32_t d = desc[firstControl + c];
+            s.descriptors.push_back({uint16_t(d & 0xFFFFu), uint8_t((d >> 16) & 0xFFu), uint8_t(d >> 24)});
+            for (uint32_t b = 0; b < nb; ++b) s.binIndex.push_back(bins[size_t(firstControl + c) * 8u + b]);
+        }
+        for (uint32_t k = 0; k < keys; ++k) s.keyframes.push_back({keyFrames[firstKey + k], keyValues[firstKey + k]});
+        return packRenderTemporalControlStream(s, true);
+    };
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (long long i = 0; i < (long long)n; ++i) {
+        try {
+            Rec r;
+            std::memcpy(&r, records + size_t(i) * 32u, 32);
+            const auto header = unpackRenderTemporalHeader(r.header);
+            if (header.mode == TemporalFirstPackedMode::EMPTY) {
+                leaves[i] = buildRenderTemporalPackedLeafBytes(header, {}, {}, {}, true);
+                continue;
+            }
+            const auto prefix = makeRenderTemporalLeafPrefix(header.mode, r.ckf, r.fkf);
+            const uint32_t cres = header.coarseResolution, fres = header.fineResolution;
+            const auto coarse = stream(uint32_t(header.coarseCodec), cres * cres * cres, 8, r.cml, r.cc, r.ck, r.ckf);
+            if (header.mode == TemporalFirstPackedMode::TEMPORAL_FINE6) {
+                const auto fine = stream(uint32_t(header.fineCodec), fres * fres * fres, 8, r.fml, r.fc, r.fk, r.fkf);
+                leaves[i] = buildRenderTemporalPackedLeafBytes(header, prefix, coarse, fine, true);
+            } else if (header.mode == TemporalFirstPackedMode::TEMPORAL_FINE_COMPACT) {
+                const std::vector<uint8_t> occ(occupancy + size_t(r.occ) * 80u, occupancy + size_t(r.occ) * 80u + 80u);
+                const auto section = unpackRenderTemporalShellOccupancySection(occ.data(), occ.size());
+                const uint32_t active = renderTemporalShellActiveVoxelCount(section);
+                const auto residual = stream(uint32_t(header.fineCodec), active, kRenderTemporalShellPackedTimeBinCount,
+                                             r.fml, r.fc, r.fk, r.fkf);
+                leaves[i] = buildRenderTemporalPackedLeafBytes(header, prefix, coarse, occ, residual, true);
+            } else {
+                leaves[i] = buildRenderTemporalPackedLeafBytes(header, prefix, coarse, {}, true);
+            }
+        } catch (const std::exception& e) {
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+            {
+                failed = true;
+                g_err = e.what();
+            }
+        }
+    }
+    if (failed) return -1;
+    size_t words = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        offsets[i] = uint32_t(words);
+        const size_t w = (leaves[i].size() + 3u) / 4u;
+        if (words + w > capWords) {
+            g_err = "payload buffer too small";
+            return -1;
+        }
+        payload[words + w - 1] = 0u;
+        std::memcpy(payload + words, leaves[i].data(), leaves[i].size());
+        words += w;
+    }
+    offsets[n] = uint32_t(words);
+    return long(words);
+}
+
 // generateQueries + fillLeafIndices (render/src/query_patterns.cpp:29-90) into out[count][5]
 // (x, y, z, t, leafIndex); sorted[count][5] receives the same queries after sortQueriesByLeaf.
 int vr_generate_queries(uint32_t w, uint32_t h, uint32_t d, uint32_t frames, int pattern, uint32_t count,

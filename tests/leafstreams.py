@@ -1,7 +1,8 @@
 """Control streams of a VBTPACK4 file's leaves, unpacked into the arrays vbt_pack_leaves reads
 (test helper).
 
-The leaves are parsed with the oracle (parseRenderTemporalPackedLeaf's layout); each stream's
+The leaves are parsed with computeRenderTemporalLeafLayout's arithmetic (restated below; the oracle's
+parser checks it when given); each stream's
 descriptors, bin index and keyframes are copied out as the encoder held them before
 packRenderTemporalControlStream: descriptor words, 8 bin bytes per control (the first 4 for the
 Mode2 residual stream's 4 bins), keyframe frames and values (FP16 values widened to float32).  A
@@ -59,8 +60,30 @@ class _Builder:
                     occupancy=np.concatenate(self.occ) if self.occ else np.zeros(0, np.uint8))
 
 
-def streams_from_file(path, oracle):
-    """(leaves [L] LEAF_DTYPE, arrays dict, leaf byte blocks) of every leaf of the file."""
+def _layout(leaf, word):
+    """Offsets of a non-EMPTY leaf's sections (render_temporal_payload.cpp:143-197, and the Mode2
+    residual stream after the occupancy, :348-386): (coarse_kf, fine_kf, coarse key offset,
+    fine descriptor offset, fine key offset, active shell voxels)."""
+    ckf, fkf = (int(x) for x in np.frombuffer(leaf[4:8].tobytes(), "<u2"))
+    cres, fres = (word >> 6) & 7, (word >> 9) & 7
+    stride = lambda codec: 8 if codec == 1 else 3  # noqa: E731
+    cc = cres ** 3
+    ckey = 8 + 4 * cc + _align4(8 * cc)
+    fine = ckey + _align4(ckf * stride((word >> 2) & 3))
+    mode = word & 3
+    if mode == 3:
+        fc = fres ** 3
+        return ckf, fkf, ckey, fine, fine + 4 * fc + _align4(8 * fc), 0
+    if mode == 2:
+        act = int(np.unpackbits(np.asarray(leaf[fine:fine + 64], np.uint8)).sum())
+        r0 = fine + 80
+        return ckf, fkf, ckey, r0, r0 + 4 * act + _align4(4 * act), act
+    return ckf, fkf, ckey, 0, 0, 0
+
+
+def streams_from_file(path, oracle=None):
+    """(leaves [L] LEAF_DTYPE, arrays dict, leaf byte blocks) of every leaf of the file.  With an
+    oracle, every leaf's layout is checked against its parser."""
     raw = open(path, "rb").read()
     h = np.frombuffer(raw[8:52], np.uint32)
     leaf_count, scale_count = int(h[8]), int(h[10])
@@ -76,24 +99,28 @@ def streams_from_file(path, oracle):
         blocks.append(leaf.tobytes())
         word = int(np.frombuffer(leaf[:4].tobytes(), "<u4")[0])
         leaves[i]["header"] = word
-        st, v = oracle.parse_leaf(leaf)
-        assert st == 0, (path, i, st)
         mode = word & 3
         if mode == 0:
             continue
+        ckf, fkf, ckey, fdesc, fkey, act = _layout(leaf, word)
+        if oracle is not None:
+            st, v = oracle.parse_leaf(leaf)
+            assert st == 0 and (v.coarse_kf, v.fine_kf, v.coarse.key_off) == (ckf, fkf, ckey), (path, i)
+            if mode == 3:
+                assert (v.fine.desc_off, v.fine.key_off) == (fdesc, fkey), (path, i)
+            if mode == 2:
+                assert (v.shell_residual_off, v.shell_active) == (fdesc, act), (path, i)
         cres, fres = (word >> 6) & 7, (word >> 9) & 7
         ccodec, fcodec = (word >> 2) & 3, (word >> 4) & 3
-        leaves[i]["coarse_kf"], leaves[i]["fine_kf"] = v.coarse_kf, v.fine_kf
-        c = b.stream(leaf, v.coarse.desc_off, cres ** 3, 8, v.coarse.key_off, v.coarse_kf, ccodec)
+        leaves[i]["coarse_kf"], leaves[i]["fine_kf"] = ckf, fkf
+        c = b.stream(leaf, 8, cres ** 3, 8, ckey, ckf, ccodec)
         leaves[i]["coarse_control"], leaves[i]["coarse_key"], leaves[i]["coarse_max_local"] = c
         if mode == 3:
-            f = b.stream(leaf, v.fine.desc_off, fres ** 3, 8, v.fine.key_off, v.fine_kf, fcodec)
+            f = b.stream(leaf, fdesc, fres ** 3, 8, fkey, fkf, fcodec)
             leaves[i]["fine_control"], leaves[i]["fine_key"], leaves[i]["fine_max_local"] = f
         elif mode == 2:
             leaves[i]["occupancy"] = len(b.occ)
-            b.occ.append(np.asarray(leaf[v.fine.desc_off:v.fine.desc_off + 80], np.uint8).copy())
-            act = int(v.shell_active)
-            r0 = int(v.shell_residual_off)
-            f = b.stream(leaf, r0, act, 4, r0 + 4 * act + _align4(4 * act), v.fine_kf, fcodec)
+            b.occ.append(np.asarray(leaf[fdesc - 80:fdesc], np.uint8).copy())
+            f = b.stream(leaf, fdesc, act, 4, fkey, fkf, fcodec)
             leaves[i]["fine_control"], leaves[i]["fine_key"], leaves[i]["fine_max_local"] = f
     return leaves, b.arrays(), blocks
