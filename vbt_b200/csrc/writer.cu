@@ -199,40 +199,43 @@ __device__ __forceinline__ uint32_t float_to_half_bits(float value)
     return sign | ((uint32_t)exponent << 10) | (rounded & 0x3FFu);
 }
 
-// Byte k of a stream's keyframe section (zero past the last key).
-__device__ __forceinline__ uint32_t key_byte(const PackInputs& in, const StreamPlan& st, uint32_t k)
-{
-    const uint32_t key = k / st.key_stride(), part = k - key * st.key_stride();
-    if (key >= st.keys) return 0u;
-    const uint32_t frame = in.key_frame[st.first_key + key];
-    if (st.codec == 1u) {        // RenderTemporalPackedKeyframeFp32: u16 frame, u16 0, f32 value
-        if (part < 2u) return (frame >> (8u * part)) & 0xFFu;
-        if (part < 4u) return 0u;
-        return (__float_as_uint(in.key_value[st.first_key + key]) >> (8u * (part - 4u))) & 0xFFu;
-    }
-    if (part == 0u) return frame & 0xFFu;
-    return (float_to_half_bits(in.key_value[st.first_key + key]) >> (8u * (part - 1u))) & 0xFFu;
-}
-
 // Writes a stream at out[0 ..): descriptors, bin index and keyframes, each section padded to words.
+// Bin rows are 8 bytes apart and 4-byte aligned: an 8-bin section is a straight copy of its rows, a
+// 4-bin section the first word of each.  FP32 keys are two words each (frame and zero half, value);
+// FP16 keys go four at a time into three words (3 bytes each: frame, half low, half high).
 __device__ void write_stream(const PackInputs& in, const StreamPlan& st, uint32_t* out, uint32_t lane)
 {
     for (uint32_t c = lane; c < st.controls; c += 32u) out[c] = in.desc[st.first_control + c];
     out += st.controls;
-    const uint32_t nb = st.controls * st.bins;
-    for (uint32_t w = lane; w < st.bin_bytes() / 4u; w += 32u) {
-        uint32_t v = 0;
-        for (uint32_t b = 0; b < 4u; ++b) {
-            const uint32_t k = 4u * w + b;
-            if (k < nb) v |= (uint32_t)in.bins[(size_t)(st.first_control + k / st.bins) * 8u + k % st.bins] << (8u * b);
-        }
-        out[w] = v;
+    const uint32_t* rows = reinterpret_cast<const uint32_t*>(in.bins + (size_t)st.first_control * 8u);
+    if (st.bins == 8u) {
+        for (uint32_t w = lane; w < 2u * st.controls; w += 32u) out[w] = rows[w];
+    } else {                     // 4 bins
+        for (uint32_t c = lane; c < st.controls; c += 32u) out[c] = rows[2u * c];
     }
     out += st.bin_bytes() / 4u;
-    for (uint32_t w = lane; w < st.key_bytes() / 4u; w += 32u) {
-        uint32_t v = 0;
-        for (uint32_t b = 0; b < 4u; ++b) v |= key_byte(in, st, 4u * w + b) << (8u * b);
-        out[w] = v;
+    const uint16_t* fr = in.key_frame + st.first_key;
+    const float* val = in.key_value + st.first_key;
+    if (st.codec == 1u) {        // RenderTemporalPackedKeyframeFp32: u16 frame, u16 0, f32 value
+        for (uint32_t k = lane; k < st.keys; k += 32u) {
+            out[2u * k] = fr[k];
+            out[2u * k + 1u] = __float_as_uint(val[k]);
+        }
+        return;
+    }
+    const uint32_t words = st.key_bytes() / 4u;
+    for (uint32_t g = lane; 3u * g < words; g += 32u) {
+        uint32_t b[12];
+        for (uint32_t j = 0; j < 4u; ++j) {
+            const uint32_t k = 4u * g + j;
+            const bool on = k < st.keys;
+            const uint32_t h = on ? float_to_half_bits(val[k]) : 0u;
+            b[3u * j] = on ? (fr[k] & 0xFFu) : 0u;
+            b[3u * j + 1u] = h & 0xFFu;
+            b[3u * j + 2u] = h >> 8;
+        }
+        for (uint32_t q = 0; q < 3u && 3u * g + q < words; ++q)
+            out[3u * g + q] = b[4u * q] | (b[4u * q + 1u] << 8) | (b[4u * q + 2u] << 16) | (b[4u * q + 3u] << 24);
     }
 }
 
@@ -363,8 +366,8 @@ extern "C" int vbt_pack_leaves(const vbt_leaf_streams* d_leaves, uint32_t leaf_c
         return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
     if ((control_rows && (!d_descriptors || !d_bins)) || (key_rows && (!d_key_frames || !d_key_values)))
         return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null stream array");
-    if ((reinterpret_cast<uintptr_t>(d_occupancy) & 3u) != 0u)
-        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "occupancy sections must be 4-byte aligned");
+    if (((reinterpret_cast<uintptr_t>(d_occupancy) | reinterpret_cast<uintptr_t>(d_bins)) & 3u) != 0u)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "bin rows and occupancy sections must be 4-byte aligned");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned long long* d_tmp = nullptr;   // [0] total words, [1] lowest failing leaf << 2 | reason
     cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&d_tmp), 2 * sizeof(unsigned long long), s);
