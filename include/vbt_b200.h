@@ -143,6 +143,14 @@ typedef struct {
 } vbt_sample_params;
 int vbt_sample_rays(vbt_asset* asset, const float* d_controls, const vbt_sample_params* params, const vbt_ray* d_rays,
                     uint32_t n, vbt_sample_result* d_out, void* stream);
+/* The render tree's smoke sampler (render/shaders/vbt_smoke_sample.comp:124-336) as plain CUDA, one
+ * thread per ray: d_out[i] = the sum of params->step_count density samples along ray i at
+ * params->frame_index, each decoded straight from the payload (coarse stream, plus the FINE6 stream;
+ * Mode2 leaves contribute their coarse stream, as in the shader) with the shader's own control
+ * decode, whose lerp is mix(previous, next, w).  Uses step_count, frame_index and bbox_min only;
+ * no control cache.  Render-temporal assets; rays 16-byte aligned. */
+int vbt_smoke_sample_rays(vbt_asset* asset, const vbt_sample_params* params, const vbt_ray* d_rays, uint32_t n,
+                          float* d_out, void* stream);
 
 /* ---- VBTPACK4 writer, payload half ------------------------------------------------------------
  * What writeRenderTemporalProbeFile (src/render_temporal_kf_probe_main.cpp:2561-2585) builds on

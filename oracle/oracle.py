@@ -110,6 +110,7 @@ class Oracle:
         L.vo_sci_query_points.argtypes = [C.POINTER(VoFile), u32p, C.c_uint64, f32p, C.c_int]
         L.vo_control_cache.argtypes = [C.POINTER(VoFile), C.c_int, u32p, f32p]
         L.vo_sample_rays.argtypes = [C.POINTER(VoFile), f32p, u32p, C.POINTER(VoSampleParams), f32p, C.c_uint32, f32p]
+        L.vo_smoke_sample_rays.argtypes = [C.POINTER(VoFile), C.POINTER(VoSampleParams), f32p, C.c_uint32, f32p]
         L.vo_decode_control.argtypes = [u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
                                         C.c_int, C.c_uint32, C.c_int, f32p]
         L.vo_decode_shell_voxel.argtypes = [u8p, C.POINTER(VoLeafView), C.c_int, C.c_uint32, C.c_int, f32p]
@@ -253,6 +254,13 @@ class OracleFile:
         c = np.ascontiguousarray(compact, np.uint32)
         self.o.lib.vo_sample_rays(C.byref(self.f), _ptr(cc, f32p), _ptr(c, u32p), C.byref(params), _ptr(r, f32p),
                                   r.shape[0], _ptr(out, f32p))
+        return out
+
+    def smoke_sample_rays(self, params, rays):
+        """render/shaders/vbt_smoke_sample.comp over the payload: rays [n, 8] -> sums [n]."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.zeros(r.shape[0], np.float32)
+        self.o.lib.vo_smoke_sample_rays(C.byref(self.f), C.byref(params), _ptr(r, f32p), r.shape[0], _ptr(out, f32p))
         return out
 
     def query(self, xyzt, threads=0):

@@ -115,6 +115,8 @@ typedef struct {
 int vo_control_cache(const vo_file* f, int frame, const uint32_t* compact, float* cache576);
 void vo_sample_rays(const vo_file* f, const float* cache576, const uint32_t* compact, const vo_sample_params* p,
                     const float* rays, uint32_t n, float* results);
+/* render/shaders/vbt_smoke_sample.comp over the payload (step_count, frame_index, bbox_min of p). */
+void vo_smoke_sample_rays(const vo_file* f, const vo_sample_params* p, const float* rays, uint32_t n, float* out);
 
 /* The encoder's per-voxel keyframe pass (vbt_keyframe_oracle.c): DensityTemporalProfile of
  * src/render_temporal_kf_probe_main.cpp:81-95 plus the background threshold of :477 (< 0: off). */

@@ -121,6 +121,7 @@ static float sample_stream(const sampler* S, uint32_t compact_leaf, uint32_t slo
                            uint32_t stream_base, uint32_t codec, uint32_t res, uint32_t kf, uint32_t stream_bytes,
                            uint32_t w, uint32_t h, uint32_t d, float lx, float ly, float lz)
 {
+    if (res == 0u) return 0.0f;   /* no controls (locateCoord would count to 2^32) */
     uint32_t x0, x1, y0, y1, z0, z1;
     float tx, ty, tz;
     locate_coord(lx, w, res, &x0, &x1, &tx);
@@ -426,5 +427,161 @@ void vo_sample_rays(const vo_file* f, const float* cache, const uint32_t* compac
 #pragma omp parallel for schedule(dynamic, 64)
 #endif
     for (int64_t i = 0; i < (int64_t)n; ++i) sample_ray(&S, rays + 8 * i, results + 8 * i);
+    free(bad);
+}
+
+/* ---- render/shaders/vbt_smoke_sample.comp: density accumulated straight from the payload ------
+ * Each sample decodes the eight corner controls of the coarse stream (and of the FINE6 stream) with
+ * the shader's own decodeTemporalControlValue, whose lerp is mix(previous, next, w) with
+ * w = float(frame - f0) / float(f1 - f0) (divided with IEEE rounding); Mode2 leaves contribute
+ * their coarse stream only, as in the shader.  A leaf whose walker status is bad, and a stream of
+ * resolution 0 (where the shader's locateCoord would count to 2^32), contribute 0. */
+
+/* vbt_smoke_sample.comp:118-122 readPackedKeyframeFrame, :94-116 readPackedKeyframeValue */
+static uint32_t smoke_key_frame(const vo_file* f, uint32_t bw, uint32_t key_base, uint32_t codec, uint32_t i)
+{
+    return codec == 1u ? rd_u16(f, bw, key_base + i * 8u) : rd_byte(f, bw, key_base + i * 3u);
+}
+static float smoke_key_value(const vo_file* f, uint32_t bw, uint32_t key_base, uint32_t codec, uint32_t i)
+{
+    if (codec == 1u) {
+        const uint32_t bits = rd_u32(f, bw, key_base + i * 8u + 4u);
+        float v;
+        memcpy(&v, &bits, 4);
+        return v;
+    }
+    return vo_half_to_float((uint16_t)rd_u16(f, bw, key_base + i * 3u + 1u));
+}
+
+/* vbt_smoke_sample.comp:124-171 decodeTemporalControlValue */
+static float smoke_control(const vo_file* f, uint32_t bw, uint32_t stream_base, uint32_t codec, uint32_t cc,
+                           uint32_t kf, uint32_t ci, int total, int frame_index)
+{
+    const uint32_t bins_n = 8u;
+    if (ci >= cc) return 0.0f;
+    const uint32_t desc_bytes = cc * 4u;
+    const uint32_t key_base = stream_base + desc_bytes + align4u(cc * bins_n);
+    const uint32_t desc = stream_base + ci * 4u;
+    const uint32_t start = rd_u16(f, bw, desc), count = rd_byte(f, bw, desc + 2u);
+    if (count == 0u || start + count > kf) return 0.0f;
+    const int hi_frame = total - 1 > 0 ? total - 1 : 0;
+    const uint32_t frame = (uint32_t)(frame_index < 0 ? 0 : (frame_index > hi_frame ? hi_frame : frame_index));
+    const uint32_t tb = frame * bins_n / (uint32_t)(total > 1 ? total : 1);
+    const uint32_t bin = tb < bins_n - 1u ? tb : bins_n - 1u;
+    const uint32_t bins = stream_base + desc_bytes + ci * bins_n;
+    uint32_t lo = rd_byte(f, bw, bins + bin);
+    if (lo > count - 1u) lo = count - 1u;
+    uint32_t f0 = smoke_key_frame(f, bw, key_base, codec, start + lo);
+    if (f0 > frame) {
+        lo = 0u;
+        f0 = smoke_key_frame(f, bw, key_base, codec, start);
+    }
+    if (f0 >= frame || lo + 1u >= count) return smoke_key_value(f, bw, key_base, codec, start + lo);
+    uint32_t hi = count - 1u;
+    if (bin + 1u < bins_n) {
+        const uint32_t nb = rd_byte(f, bw, bins + bin + 1u) + 1u;
+        hi = nb < count - 1u ? nb : count - 1u;
+    }
+    if (hi < lo + 1u) hi = lo + 1u;
+    uint32_t f1 = smoke_key_frame(f, bw, key_base, codec, start + hi);
+    if (f1 < frame) {
+        hi = count - 1u;
+        f1 = smoke_key_frame(f, bw, key_base, codec, start + hi);
+    }
+    if (f1 <= frame) return smoke_key_value(f, bw, key_base, codec, start + hi);
+    while (hi > lo + 1u) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        const uint32_t fm = smoke_key_frame(f, bw, key_base, codec, start + mid);
+        if (fm < frame) {
+            lo = mid;
+            f0 = fm;
+        } else {
+            hi = mid;
+            f1 = fm;
+        }
+    }
+    const float next = smoke_key_value(f, bw, key_base, codec, start + hi);
+    if (f1 == frame) return next;
+    const float prev = smoke_key_value(f, bw, key_base, codec, start + lo);
+    return mixf(prev, next, (float)(frame - f0) / (float)(f1 - f0));
+}
+
+/* vbt_smoke_sample.comp:195-232 sampleControlStream */
+static float smoke_stream(const vo_file* f, const vo_sample_params* p, uint32_t bw, uint32_t stream_base,
+                          uint32_t codec, uint32_t res, uint32_t kf, uint32_t w, uint32_t h, uint32_t d, float lx,
+                          float ly, float lz)
+{
+    if (res == 0u) return 0.0f;
+    uint32_t x0, x1, y0, y1, z0, z1;
+    float tx, ty, tz;
+    locate_coord(lx, w, res, &x0, &x1, &tx);
+    locate_coord(ly, h, res, &y0, &y1, &ty);
+    locate_coord(lz, d, res, &z0, &z1, &tz);
+    const uint32_t cc = res * res * res;
+    const int T = (int)f->frames;
+#define SCTRL(x, y, z) smoke_control(f, bw, stream_base, codec, cc, kf, ((z) * res + (y)) * res + (x), T, p->frame_index)
+    const float v000 = SCTRL(x0, y0, z0), v100 = SCTRL(x1, y0, z0), v010 = SCTRL(x0, y1, z0), v110 = SCTRL(x1, y1, z0);
+    const float v001 = SCTRL(x0, y0, z1), v101 = SCTRL(x1, y0, z1), v011 = SCTRL(x0, y1, z1), v111 = SCTRL(x1, y1, z1);
+#undef SCTRL
+    const float c00 = mixf(v000, v100, tx), c10 = mixf(v010, v110, tx);
+    const float c01 = mixf(v001, v101, tx), c11 = mixf(v011, v111, tx);
+    return mixf(mixf(c00, c10, ty), mixf(c01, c11, ty), tz);
+}
+
+/* vbt_smoke_sample.comp:234-305 sampleVbtDensity */
+static float smoke_density(const vo_file* f, const vo_sample_params* p, const uint8_t* bad, float wx, float wy,
+                           float wz)
+{
+    const float px = wx - p->bbox_min[0], py = wy - p->bbox_min[1], pz = wz - p->bbox_min[2];
+    if (px < 0.0f || py < 0.0f || pz < 0.0f || px > (float)(f->width - 1u) || py > (float)(f->height - 1u) ||
+        pz > (float)(f->depth - 1u))
+        return 0.0f;
+    const uint32_t lcx = (f->width + 7u) / 8u, lcy = (f->height + 7u) / 8u, lcz = (f->depth + 7u) / 8u;
+    uint32_t x = (uint32_t)floorf(px), y = (uint32_t)floorf(py), z = (uint32_t)floorf(pz);
+    if (x > f->width - 1u) x = f->width - 1u;
+    if (y > f->height - 1u) y = f->height - 1u;
+    if (z > f->depth - 1u) z = f->depth - 1u;
+    const uint32_t bx = x / 8u < lcx - 1u ? x / 8u : lcx - 1u, by = y / 8u < lcy - 1u ? y / 8u : lcy - 1u,
+                   bz = z / 8u < lcz - 1u ? z / 8u : lcz - 1u;
+    const uint32_t leaf = (bz * lcy + by) * lcx + bx;
+    const uint32_t wb = f->offsets[leaf], we = f->offsets[leaf + 1];
+    if (we <= wb) return 0.0f;
+    const uint32_t hdr = f->payload[wb], mode = hdr & 3u;
+    if (mode == 0u || bad[leaf]) return 0.0f;
+    const uint32_t ccodec = (hdr >> 2) & 3u, fcodec = (hdr >> 4) & 3u, cres = (hdr >> 6) & 7u, fres = (hdr >> 9) & 7u;
+    const uint32_t ckf = rd_u16(f, wb, 4u), fkf = rd_u16(f, wb, 6u);
+    const uint32_t cc = cres * cres * cres;
+    const uint32_t fbase = 8u + cc * 4u + align4u(cc * 8u) + align4u(ckf * (ccodec == 1u ? 8u : 3u));
+    const uint32_t gx = bx * 8u, gy = by * 8u, gz = bz * 8u;
+    const uint32_t w = f->width - gx < 8u ? f->width - gx : 8u, h = f->height - gy < 8u ? f->height - gy : 8u,
+                   d = f->depth - gz < 8u ? f->depth - gz : 8u;
+    const float lx = px - (float)gx, ly = py - (float)gy, lz = pz - (float)gz;
+    float value = smoke_stream(f, p, wb, 8u, ccodec, cres, ckf, w, h, d, lx, ly, lz);
+    if (mode == 3u && fres > 0u) value += smoke_stream(f, p, wb, fbase, fcodec, fres, fkf, w, h, d, lx, ly, lz);
+    return value;
+}
+
+/* vbt_smoke_sample.comp:307-336 main: results[ray] = sum over step_count samples */
+void vo_smoke_sample_rays(const vo_file* f, const vo_sample_params* p, const float* rays, uint32_t n, float* out)
+{
+    uint8_t* bad = (uint8_t*)calloc(f->leaf_count ? f->leaf_count : 1u, 1);
+    for (uint32_t leaf = 0; leaf < f->leaf_count; ++leaf) {
+        const uint32_t wb = f->offsets[leaf], we = f->offsets[leaf + 1];
+        vo_leaf_view v;
+        if (we > wb && vo_parse_leaf((const uint8_t*)(f->payload + wb), (size_t)(we - wb) * 4u, 1, &v) != VO_OK)
+            bad[leaf] = 1;
+    }
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long long i = 0; i < (long long)n; ++i) {
+        const float* r = rays + 8 * i;
+        const float dt = r[7] / maxf((float)p->step_count, 1.0f);
+        float t = r[3] + 0.5f * dt;
+        float acc = 0.0f;
+        for (uint32_t s = 0; s < p->step_count; ++s) {
+            acc += smoke_density(f, p, bad, r[0] + r[4] * t, r[1] + r[5] * t, r[2] + r[6] * t);
+            t += dt;
+        }
+        out[i] = acc;
+    }
     free(bad);
 }

@@ -131,6 +131,7 @@ _sig = {
     "vbt_decode_window": ([_vp, C.c_int, C.c_int, _vp, C.c_uint64, _vp], C.c_int),
     "vbt_selftest_key_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_pack_payload": ([_vp, _vp, C.c_uint32, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64), _vp], C.c_int),
+    "vbt_smoke_sample_rays": ([_vp, C.POINTER(SampleParams), _vp, C.c_uint32, _vp, _vp], C.c_int),
     "vbt_pack_leaves": ([_vp, C.c_uint32, _vp, _vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp, C.c_uint64, _vp, _vp,
                          C.c_uint64, C.POINTER(C.c_uint64), _vp], C.c_int),
     "vbt_detect_keyframes": ([_vp, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, C.POINTER(KeyframeProfile), _vp,
@@ -303,6 +304,13 @@ class Asset:
         n = rays.shape[0]
         _check(_lib.vbt_sample_rays(self._h, _addr(controls), C.byref(params), _addr(rays), n, _addr(out),
                                     _stream(stream)))
+
+    def smoke_sample_rays(self, params, rays, out, stream=None):
+        """The render tree's smoke sampler (vbt_smoke_sample.comp): rays [n, 8] float32 device tensor
+        -> out [n] float32, the sum of params.step_count density samples per ray, decoded straight
+        from the payload."""
+        n = rays.numel() // 8
+        _check(_lib.vbt_smoke_sample_rays(self._h, C.byref(params), _addr(rays), n, _addr(out), _stream(stream)))
 
     def decode_window(self, t0, n, out, frame_stride=None, stream=None):
         """(d) window decode on the tensor cores of frames [t0, t0 + n) into `out` in the cache

@@ -1,6 +1,7 @@
 // sample.cu -- the Studio's ray sampler over the current-frame control cache
 // (VBTStudio/frontend/shaders/vbt_sample.comp), one thread per ray, as plain CUDA with a device
-// buffer for its results (vbt_sample_rays).
+// buffer for its results (vbt_sample_rays); and the render tree's smoke sampler that sums density
+// straight from the payload (render/shaders/vbt_smoke_sample.comp, vbt_smoke_sample_rays).
 //
 // The arithmetic follows the shader operation by operation in single precision with every
 // operation rounded on its own (the library is built without FMA contraction): GLSL mix(a, b, t)
@@ -77,6 +78,7 @@ __device__ float sample_stream(const Sampler& S, uint32_t cl, uint32_t slot_base
                                uint32_t codec, uint32_t res, uint32_t kf, uint32_t w, uint32_t h, uint32_t d, float lx,
                                float ly, float lz)
 {
+    if (res == 0u) return 0.0f;   // no controls (locateCoord would count to 2^32)
     uint32_t x0, x1, y0, y1, z0, z1;
     float tx, ty, tz;
     locate_coord(lx, w, res, x0, x1, tx);
@@ -379,6 +381,144 @@ __global__ void __launch_bounds__(128) sample_rays_kernel(DeviceAsset a, const f
     out[2 * i + 1] = make_float4(res[4], res[5], res[6], res[7]);
 }
 
+// ---- render/shaders/vbt_smoke_sample.comp: density summed straight from the payload -----------
+// Every sample decodes the eight corner controls of the coarse stream (and of the FINE6 stream)
+// with the shader's own decodeTemporalControlValue: the reference search, but the lerp is
+// mix(previous, next, w) with w = float(frame - f0) / float(f1 - f0) (IEEE division).  Mode2
+// leaves contribute their coarse stream only, as in the shader.  Leaves the walker rejected, and
+// streams of resolution 0 (where the shader's locateCoord would count to 2^32), contribute 0.
+
+struct SmokeSampler {
+    const DeviceAsset& a;
+    uint32_t frame, bin;    // clamped frame and its 8-bin time bin
+};
+
+__device__ __forceinline__ uint32_t smoke_key_frame(const uint32_t* pw, uint32_t wb, uint32_t kb, uint32_t codec,
+                                                    uint32_t i)
+{
+    return codec == 1u ? rd_u16(pw, wb, kb + i * 8u) : rd_byte(pw, wb, kb + i * 3u);
+}
+__device__ __forceinline__ float smoke_key_value(const uint32_t* pw, uint32_t wb, uint32_t kb, uint32_t codec,
+                                                 uint32_t i)
+{
+    if (codec == 1u) return __uint_as_float(rd_u32(pw, wb, kb + i * 8u + 4u));
+    return half_bits_to_float(rd_u16(pw, wb, kb + i * 3u + 1u));
+}
+
+// vbt_smoke_sample.comp:124-171 (decodeTemporalControlValue)
+__device__ float smoke_control(const SmokeSampler& S, uint32_t wb, uint32_t sb, uint32_t codec, uint32_t cc,
+                               uint32_t kf, uint32_t ci)
+{
+    if (ci >= cc) return 0.0f;
+    const uint32_t* pw = S.a.payload;
+    const uint32_t kb = sb + cc * 4u + align4(cc * 8u);
+    const uint32_t start = rd_u16(pw, wb, sb + ci * 4u), count = rd_byte(pw, wb, sb + ci * 4u + 2u);
+    if (count == 0u || start + count > kf) return 0.0f;
+    const uint32_t frame = S.frame, bins = sb + cc * 4u + ci * 8u;
+    uint32_t lo = min(rd_byte(pw, wb, bins + S.bin), count - 1u);
+    uint32_t f0 = smoke_key_frame(pw, wb, kb, codec, start + lo);
+    if (f0 > frame) {
+        lo = 0u;
+        f0 = smoke_key_frame(pw, wb, kb, codec, start);
+    }
+    if (f0 >= frame || lo + 1u >= count) return smoke_key_value(pw, wb, kb, codec, start + lo);
+    uint32_t hi = S.bin + 1u < 8u ? min(count - 1u, rd_byte(pw, wb, bins + S.bin + 1u) + 1u) : count - 1u;
+    hi = max(hi, lo + 1u);
+    uint32_t f1 = smoke_key_frame(pw, wb, kb, codec, start + hi);
+    if (f1 < frame) {
+        hi = count - 1u;
+        f1 = smoke_key_frame(pw, wb, kb, codec, start + hi);
+    }
+    if (f1 <= frame) return smoke_key_value(pw, wb, kb, codec, start + hi);
+    while (hi > lo + 1u) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        const uint32_t fm = smoke_key_frame(pw, wb, kb, codec, start + mid);
+        if (fm < frame) {
+            lo = mid;
+            f0 = fm;
+        } else {
+            hi = mid;
+            f1 = fm;
+        }
+    }
+    const float next = smoke_key_value(pw, wb, kb, codec, start + hi);
+    if (f1 == frame) return next;
+    const float prev = smoke_key_value(pw, wb, kb, codec, start + lo);
+    return mixf(prev, next, __fdiv_rn((float)(frame - f0), (float)(f1 - f0)));
+}
+
+// vbt_smoke_sample.comp:195-232 (sampleControlStream)
+__device__ float smoke_stream(const SmokeSampler& S, uint32_t wb, uint32_t sb, uint32_t codec, uint32_t res,
+                              uint32_t kf, uint32_t w, uint32_t h, uint32_t d, float lx, float ly, float lz)
+{
+    if (res == 0u) return 0.0f;
+    uint32_t x0, x1, y0, y1, z0, z1;
+    float tx, ty, tz;
+    locate_coord(lx, w, res, x0, x1, tx);
+    locate_coord(ly, h, res, y0, y1, ty);
+    locate_coord(lz, d, res, z0, z1, tz);
+    const uint32_t cc = res * res * res;
+    auto ctrl = [&](uint32_t x, uint32_t y, uint32_t z) {
+        return smoke_control(S, wb, sb, codec, cc, kf, (z * res + y) * res + x);
+    };
+    const float v000 = ctrl(x0, y0, z0), v100 = ctrl(x1, y0, z0), v010 = ctrl(x0, y1, z0), v110 = ctrl(x1, y1, z0);
+    const float v001 = ctrl(x0, y0, z1), v101 = ctrl(x1, y0, z1), v011 = ctrl(x0, y1, z1), v111 = ctrl(x1, y1, z1);
+    const float c00 = mixf(v000, v100, tx), c10 = mixf(v010, v110, tx);
+    const float c01 = mixf(v001, v101, tx), c11 = mixf(v011, v111, tx);
+    return mixf(mixf(c00, c10, ty), mixf(c01, c11, ty), tz);
+}
+
+// vbt_smoke_sample.comp:234-305 (sampleVbtDensity)
+__device__ float smoke_density(const SmokeSampler& S, const vbt_sample_params& p, float wx, float wy, float wz)
+{
+    const DeviceAsset& a = S.a;
+    const float px = __fsub_rn(wx, p.bbox_min[0]), py = __fsub_rn(wy, p.bbox_min[1]), pz = __fsub_rn(wz, p.bbox_min[2]);
+    if (px < 0.0f || py < 0.0f || pz < 0.0f || px > (float)(a.g.width - 1u) || py > (float)(a.g.height - 1u) ||
+        pz > (float)(a.g.depth - 1u))
+        return 0.0f;
+    const uint32_t x = min(a.g.width - 1u, (uint32_t)floorf(px)), y = min(a.g.height - 1u, (uint32_t)floorf(py)),
+                   z = min(a.g.depth - 1u, (uint32_t)floorf(pz));
+    const uint32_t bx = min(a.g.lcx - 1u, x / 8u), by = min(a.g.lcy - 1u, y / 8u), bz = min(a.g.lcz - 1u, z / 8u);
+    const uint32_t leaf = (bz * a.g.lcy + by) * a.g.lcx + bx;
+    const uint32_t wb = __ldg(a.offsets + leaf), we = __ldg(a.offsets + leaf + 1);
+    if (we <= wb) return 0.0f;
+    const uint32_t hdr = __ldg(a.payload + wb), mode = hdr & 3u;
+    if (mode == kModeEmpty) return 0.0f;
+    if (entry_status(a.entries[leaf]) != kOk) return 0.0f;   // a leaf the walker rejected is not read
+    const uint32_t ccodec = (hdr >> 2) & 3u, fcodec = (hdr >> 4) & 3u;
+    const uint32_t cres = (hdr >> 6) & 7u, fres = (hdr >> 9) & 7u;
+    const uint32_t ckf = rd_u16(a.payload, wb, 4u), fkf = rd_u16(a.payload, wb, 6u);
+    const uint32_t cc = cres * cres * cres;
+    const uint32_t fbase = 8u + cc * 4u + align4(cc * 8u) + align4(ckf * (ccodec == 1u ? 8u : 3u));
+    const uint32_t gx = bx * 8u, gy = by * 8u, gz = bz * 8u;
+    const uint32_t w = min(8u, a.g.width - gx), h = min(8u, a.g.height - gy), d = min(8u, a.g.depth - gz);
+    const float lx = __fsub_rn(px, (float)gx), ly = __fsub_rn(py, (float)gy), lz = __fsub_rn(pz, (float)gz);
+    float value = smoke_stream(S, wb, 8u, ccodec, cres, ckf, w, h, d, lx, ly, lz);
+    if (mode == kModeFine6 && fres > 0u)
+        value = __fadd_rn(value, smoke_stream(S, wb, fbase, fcodec, fres, fkf, w, h, d, lx, ly, lz));
+    return value;
+}
+
+// vbt_smoke_sample.comp:307-336 (main): one thread per ray, the sum of step_count samples.
+__global__ void __launch_bounds__(128) smoke_sample_kernel(DeviceAsset a, vbt_sample_params p,
+                                                           const float4* __restrict__ rays, uint32_t n,
+                                                           float* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int frame = clamp_frame(p.frame_index, (int)a.g.frames);
+    const SmokeSampler S{a, (uint32_t)frame, time_bin(frame, 8u, a.g.frames)};
+    const float4 r0 = rays[2 * i], r1 = rays[2 * i + 1];
+    const float dt = __fdiv_rn(r1.w, gmax((float)p.step_count, 1.0f));
+    float t = __fadd_rn(r0.w, __fmul_rn(0.5f, dt));
+    float acc = 0.0f;
+    for (uint32_t s = 0; s < p.step_count; ++s) {
+        acc = __fadd_rn(acc, smoke_density(S, p, along(r0.x, r1.x, t), along(r0.y, r1.y, t), along(r0.z, r1.z, t)));
+        t = __fadd_rn(t, dt);
+    }
+    out[i] = acc;
+}
+
 }  // namespace
 }  // namespace vbtb
 
@@ -403,4 +543,23 @@ extern "C" int vbt_sample_rays(vbt_asset* a, const float* d_controls, const vbt_
     if (prev >= 0 && prev != a->device) cudaSetDevice(prev);
     return e == cudaSuccess ? VBT_STATUS_OK
                             : set_last_error(VBT_STATUS_CUDA, std::string("sample_rays_kernel: ") + cudaGetErrorString(e));
+}
+
+extern "C" int vbt_smoke_sample_rays(vbt_asset* a, const vbt_sample_params* params, const vbt_ray* d_rays, uint32_t n,
+                                     float* d_out, void* stream)
+{
+    if (!a || !params || (n && (!d_rays || !d_out))) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    if (a->hdr.profile_type == 2u) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "the sampler covers render-temporal assets");
+    if ((reinterpret_cast<uintptr_t>(d_rays) & 15u) != 0u || (reinterpret_cast<uintptr_t>(d_out) & 3u) != 0u)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "rays must be 16-byte and results 4-byte aligned");
+    if (n == 0) return VBT_STATUS_OK;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != a->device) cudaSetDevice(a->device);
+    smoke_sample_kernel<<<(n + 127u) / 128u, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        a->dev, *params, reinterpret_cast<const float4*>(d_rays), n, d_out);
+    const cudaError_t e = cudaGetLastError();
+    if (prev >= 0 && prev != a->device) cudaSetDevice(prev);
+    return e == cudaSuccess ? VBT_STATUS_OK
+                            : set_last_error(VBT_STATUS_CUDA, std::string("smoke_sample_kernel: ") + cudaGetErrorString(e));
 }
