@@ -109,4 +109,49 @@ int vbtref_temporal_pass(const float* values, uint64_t series, int frames, uint6
     return 0;
 }
 
+// The coarse control fitting of the encoder's leaf loop (src/render_temporal_kf_probe_main.cpp:
+// 705-729) for one leaf: the 4^3 controls sampled from the leaf's reconstruction (leafTemporal,
+// voxel (lz*8 + ly)*8 + lx, frames fastest) at controlCoords(4), detectDensityKeyFrames with the
+// control profile, appendControlSequenceToStream (8 time bins) and reconstructFromKeys.  Outputs the
+// stream's descriptor words (keyStart | keyCount << 16 | reserved << 24), bin rows (8 bytes per
+// control), keyframes, requiredMaxBinLocalKeys and the fitted grid [64][frames].  Returns the key
+// count, or -1 when keyCap is too small.
+int vbtref_coarse_fit(const float* leafTemporal, int frames, int width, int height, int depth,
+                      const vr_keyframe_profile* p, uint32_t* desc, uint8_t* bins, uint16_t* keyFrames,
+                      float* keyValues, int keyCap, int* requiredMaxLocal, float* grid)
+{
+    const std::vector<float> lt(leafTemporal, leafTemporal + size_t(512) * size_t(frames));
+    const DensityTemporalProfile prof = to_profile(p);
+    const auto coords = controlCoords(kCoarseRes);
+    BuiltControlStream stream;
+    stream.data.controlCount = uint16_t(kCoarseRes * kCoarseRes * kCoarseRes);
+    stream.data.timeBinCount = 8;
+    std::vector<float> series(static_cast<size_t>(frames)), recon;
+    for (int gz = 0; gz < kCoarseRes; ++gz)
+        for (int gy = 0; gy < kCoarseRes; ++gy)
+            for (int gx = 0; gx < kCoarseRes; ++gx) {
+                const int ctrl = (gz * kCoarseRes + gy) * kCoarseRes + gx;
+                for (int t = 0; t < frames; ++t)
+                    series[size_t(t)] = sampleLeafBufferAtFractional(lt, frames, t, width, height, depth,
+                                                                     coords[size_t(gx)], coords[size_t(gy)],
+                                                                     coords[size_t(gz)]);
+                const auto keys = detectDensityKeyFrames(series, prof, nullptr);
+                appendControlSequenceToStream(stream.data, stream.requiredMaxBinLocalKeys, series, keys, frames, 8);
+                reconstructFromKeys(series, keys, recon);
+                for (int t = 0; t < frames; ++t) grid[size_t(ctrl) * size_t(frames) + size_t(t)] = recon[size_t(t)];
+            }
+    const auto& d = stream.data;
+    if (int(d.keyframes.size()) > keyCap) return -1;
+    for (size_t c = 0; c < d.descriptors.size(); ++c)
+        desc[c] = uint32_t(d.descriptors[c].keyStart) | (uint32_t(d.descriptors[c].keyCount) << 16) |
+                  (uint32_t(d.descriptors[c].reserved) << 24);
+    std::memcpy(bins, d.binIndex.data(), d.binIndex.size());
+    for (size_t k = 0; k < d.keyframes.size(); ++k) {
+        keyFrames[k] = d.keyframes[k].frame;
+        keyValues[k] = d.keyframes[k].value;
+    }
+    *requiredMaxLocal = stream.requiredMaxBinLocalKeys;
+    return int(d.keyframes.size());
+}
+
 }  // extern "C"

@@ -125,6 +125,9 @@ class Oracle:
         i32p = C.POINTER(C.c_int)
         L.vo_detect_keyframes.argtypes = [f32p, C.c_int, C.POINTER(VoKeyframeProfile), i32p, i32p]
         L.vo_reconstruct.argtypes = [f32p, C.c_int, i32p, C.c_int, f32p]
+        L.vo_float_to_half_n.argtypes = [f32p, C.c_uint64, C.POINTER(C.c_uint16)]
+        L.vo_coarse_fit.argtypes = [f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(VoKeyframeProfile), u32p, u8p,
+                                    C.POINTER(C.c_uint16), f32p, C.c_int, C.POINTER(C.c_int), f32p]
         L.vo_keyframe_pass.argtypes = [f32p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(VoKeyframeProfile), u32p,
                                        u32p, u8p, f32p, C.POINTER(C.c_double), C.c_int]
 
@@ -143,6 +146,19 @@ class Oracle:
         out = np.zeros(v.size, np.float32)
         self.lib.vo_reconstruct(_ptr(v, f32p), v.size, _ptr(k, C.POINTER(C.c_int)), k.size, _ptr(out, f32p))
         return out
+
+    def float_to_half(self, values):
+        """renderTemporalFloatToHalfBits of every value (uint16 array)."""
+        v = np.ascontiguousarray(values, np.float32).reshape(-1)
+        out = np.zeros(v.size, np.uint16)
+        self.lib.vo_float_to_half_n(_ptr(v, f32p), v.size, _ptr(out, C.POINTER(C.c_uint16)))
+        return out
+
+    def coarse_fit(self, leaf_recon, extent, profile):
+        """The encoder's coarse control fitting of one leaf: leaf_recon [512, T] (voxel (lz*8+ly)*8+lx,
+        frames fastest) -> dict of desc [64] u32, bins [64, 8] u8, key_frames, key_values,
+        required_max_local and grid [64, T]."""
+        return _coarse_fit(self.lib.vo_coarse_fit, leaf_recon, extent, profile)
 
     def keyframe_pass(self, frames, profile, threads=0):
         """The encoder's per-voxel pass over frames[T, S] (frame-major): dict of key_mask [W, S] u32,
@@ -430,6 +446,24 @@ class Reference:
         return out[:n].copy()
 
 
+def _coarse_fit(fn, leaf_recon, extent, profile):
+    lt = np.ascontiguousarray(leaf_recon, np.float32).reshape(512, -1)
+    T = lt.shape[1]
+    cap = 64 * max(T, 1)
+    desc = np.zeros(64, np.uint32)
+    bins = np.zeros((64, 8), np.uint8)
+    kf = np.zeros(cap, np.uint16)
+    kv = np.zeros(cap, np.float32)
+    grid = np.zeros((64, T), np.float32)
+    req = C.c_int()
+    n = fn(_ptr(lt, f32p), T, *extent, C.byref(profile), _ptr(desc, u32p), _ptr(bins, u8p),
+           _ptr(kf, C.POINTER(C.c_uint16)), _ptr(kv, f32p), cap, C.byref(req), _ptr(grid, f32p))
+    if n < 0:
+        raise RuntimeError("coarse fit: key capacity exceeded")
+    return dict(desc=desc, bins=bins, key_frames=kf[:n].copy(), key_values=kv[:n].copy(),
+                required_max_local=req.value, grid=grid)
+
+
 class KeyframeReference:
     """The reference encoder's detectDensityKeyFrames / reconstructFromKeys, compiled from its source
     (oracle/_ref/libkfref.so, see kf_ref_shim.cpp)."""
@@ -441,6 +475,8 @@ class KeyframeReference:
         i32p = C.POINTER(C.c_int)
         L.vbtref_detect_keyframes.argtypes = [f32p, C.c_int, C.POINTER(VoKeyframeProfile), i32p, i32p]
         L.vbtref_reconstruct.argtypes = [f32p, C.c_int, i32p, C.c_int, f32p]
+        L.vbtref_coarse_fit.argtypes = [f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(VoKeyframeProfile), u32p,
+                                        u8p, C.POINTER(C.c_uint16), f32p, C.c_int, C.POINTER(C.c_int), f32p]
         L.vbtref_temporal_pass.argtypes = [f32p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(VoKeyframeProfile),
                                            u32p, C.POINTER(C.c_double), C.c_int]
 
@@ -458,6 +494,10 @@ class KeyframeReference:
         out = np.zeros(v.size, np.float32)
         self.lib.vbtref_reconstruct(_ptr(v, f32p), v.size, _ptr(k, C.POINTER(C.c_int)), k.size, _ptr(out, f32p))
         return out
+
+    def coarse_fit(self, leaf_recon, extent, profile):
+        """The reference's coarse control fitting of one leaf (see Oracle.coarse_fit)."""
+        return _coarse_fit(self.lib.vbtref_coarse_fit, leaf_recon, extent, profile)
 
     def temporal_pass(self, frames, profile, threads=0, series=None):
         """(key_count [S], err2 [S]) of the encoder's per-voxel loop over frames[T, S] (frame-major);

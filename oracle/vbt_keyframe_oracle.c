@@ -15,6 +15,9 @@
  *   detectDensityKeyFrames   :2080-2167
  *   reconstructFromKeys      :2169-2201
  *   per-voxel leaf loop      :619-659   background test, keys, reconstruction, squared error
+ *   coarse control fitting   :705-729   controlCoords (:189-198), sampleLeafBufferAtFractional
+ *                                       (:2203-2237), buildBinIndexFromKeys (:2288-2305),
+ *                                       appendControlSequenceToStream (:2361-2399)
  * Floating point is kept in the reference's types (float where it computes in float, double
  * where it promotes), with no contraction (built with -ffp-contract=off).  Values are finite.
  */
@@ -278,4 +281,106 @@ void vo_keyframe_pass(const float* values, uint64_t series, int frames, uint64_t
         free(r);
         free(keys);
     }
+}
+
+/* ---- the encoder's coarse control fitting (:705-729) ------------------------------------------ */
+
+/* std::clamp(v, lo, hi) */
+static float clamp_r(float v, float lo, float hi) { return v < lo ? lo : (hi < v ? hi : v); }
+
+/* sampleLeafBufferAtFractional (:2203-2237): trilinear over the leaf's reconstruction lt (voxel
+ * (lz*8 + ly)*8 + lx, frames fastest), the position clamped to the leaf's extent. */
+static float kf_sample_leaf(const float* lt, int frames, int t, int w, int h, int d, float fx, float fy, float fz)
+{
+    const float x = clamp_r(fx, 0.0f, (float)(w - 1 > 0 ? w - 1 : 0));
+    const float y = clamp_r(fy, 0.0f, (float)(h - 1 > 0 ? h - 1 : 0));
+    const float z = clamp_r(fz, 0.0f, (float)(d - 1 > 0 ? d - 1 : 0));
+    const int x0 = (int)floorf(x), y0 = (int)floorf(y), z0 = (int)floorf(z);
+    const int x1 = w - 1 < x0 + 1 ? w - 1 : x0 + 1, y1 = h - 1 < y0 + 1 ? h - 1 : y0 + 1,
+              z1 = d - 1 < z0 + 1 ? d - 1 : z0 + 1;
+    const float tx = x - (float)x0, ty = y - (float)y0, tz = z - (float)z0;
+#define AT(lx, ly, lz) lt[(size_t)((((lz) * 8 + (ly)) * 8 + (lx))) * (size_t)frames + (size_t)t]
+    const float c00 = AT(x0, y0, z0) * (1.0f - tx) + AT(x1, y0, z0) * tx;
+    const float c01 = AT(x0, y0, z1) * (1.0f - tx) + AT(x1, y0, z1) * tx;
+    const float c10 = AT(x0, y1, z0) * (1.0f - tx) + AT(x1, y1, z0) * tx;
+    const float c11 = AT(x0, y1, z1) * (1.0f - tx) + AT(x1, y1, z1) * tx;
+#undef AT
+    const float c0 = c00 * (1.0f - ty) + c10 * ty;
+    const float c1 = c01 * (1.0f - ty) + c11 * ty;
+    return c0 * (1.0f - tz) + c1 * tz;
+}
+
+/* buildBinIndexFromKeys (:2288-2305): per time bin, the index before the first key at or after the
+ * bin's first frame (0 for the first key), else the last key; stored in a byte. */
+static void kf_bin_index(const int* keys, int k, int frames, int bins, uint8_t* out)
+{
+    for (int bin = 0; bin < bins; ++bin) {
+        out[bin] = 0u;
+        if (k == 0) continue;
+        const int start = (int)(((int64_t)bin * (int64_t)frames) / (bins > 1 ? bins : 1));
+        uint8_t local = (uint8_t)(k - 1);
+        for (int i = 0; i < k; ++i)
+            if (keys[i] >= start) {
+                local = (uint8_t)(i > 0 ? i - 1 : 0);
+                break;
+            }
+        out[bin] = local;
+    }
+}
+
+/* controlCoords(4) (:189-198), then for each of the 4^3 controls in (gz, gy, gx) order: the sampled
+ * series, its keys under the control profile, appendControlSequenceToStream (:2361-2399) with 8
+ * time bins, and reconstructFromKeys into grid[ctrl * frames + t].  desc[c] = keyStart |
+ * keyCount << 16 | reserved << 24; bins[c * 8 + b].  Returns the stream's key count (-1 beyond
+ * key_cap); *required_max_local = requiredMaxBinLocalKeys. */
+int vo_coarse_fit(const float* lt, int frames, int w, int h, int d, const vo_keyframe_profile* p, uint32_t* desc,
+                  uint8_t* bins, uint16_t* key_frames, float* key_values, int key_cap, int* required_max_local,
+                  float* grid)
+{
+    const float scale = 7.0f / (float)(4 - 1);
+    float coords[4];
+    for (int i = 0; i < 4; ++i) coords[i] = (float)i * scale;
+    float* series = (float*)malloc((size_t)(frames > 0 ? frames : 1) * sizeof(float));
+    int* keys = (int*)malloc((size_t)(frames > 0 ? frames : 1) * sizeof(int));
+    int nk = 0, overflow = 0;
+    uint8_t required = 1u;
+    for (int gz = 0; gz < 4; ++gz)
+        for (int gy = 0; gy < 4; ++gy)
+            for (int gx = 0; gx < 4; ++gx) {
+                const int ctrl = (gz * 4 + gy) * 4 + gx;
+                for (int t = 0; t < frames; ++t)
+                    series[t] = kf_sample_leaf(lt, frames, t, w, h, d, coords[gx], coords[gy], coords[gz]);
+                const int k = vo_detect_keyframes(series, frames, p, keys, NULL);
+                uint8_t* b = bins + ctrl * 8;
+                kf_bin_index(keys, k, frames, 8, b);
+                int local = 1;
+                for (int bin = 0; bin < 8; ++bin) {
+                    const int next = bin + 1 < 8 ? (int)b[bin + 1] : k;
+                    const int span = next - (int)b[bin] > 1 ? next - (int)b[bin] : 1;
+                    if (span > local) local = span;
+                    if (span > (int)required) required = (uint8_t)span;
+                }
+                desc[ctrl] = (uint32_t)(uint16_t)nk | ((uint32_t)(k < 255 ? k : 255) << 16) |
+                             ((uint32_t)(local < 255 ? local : 255) << 24);
+                for (int i = 0; i < k; ++i) {
+                    if (nk < key_cap) {
+                        key_frames[nk] = (uint16_t)keys[i];
+                        key_values[nk] = series[keys[i]];
+                    } else {
+                        overflow = 1;
+                    }
+                    ++nk;
+                }
+                vo_reconstruct(series, frames, keys, k, grid + (size_t)ctrl * (size_t)frames);
+            }
+    free(series);
+    free(keys);
+    *required_max_local = required;
+    return overflow ? -1 : nk;
+}
+
+/* renderTemporalFloatToHalfBits over an array (vo_float_to_half, element by element). */
+void vo_float_to_half_n(const float* v, uint64_t n, uint16_t* out)
+{
+    for (uint64_t i = 0; i < n; ++i) out[i] = vo_float_to_half(v[i]);
 }

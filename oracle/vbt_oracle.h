@@ -131,6 +131,10 @@ void vo_reconstruct(const float* values, int n, const int* keys, int key_count, 
 void vo_keyframe_pass(const float* values, uint64_t series, int frames, uint64_t frame_stride,
                       const vo_keyframe_profile* p, uint32_t* key_mask, uint32_t* key_count, uint8_t* flags,
                       float* recon, double* err2, int threads);
+int vo_coarse_fit(const float* leaf_recon, int frames, int w, int h, int d, const vo_keyframe_profile* control_profile,
+                  uint32_t* desc, uint8_t* bins, uint16_t* key_frames, float* key_values, int key_cap,
+                  int* required_max_local, float* grid);
+void vo_float_to_half_n(const float* v, uint64_t n, uint16_t* out);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,88 @@
+"""The encoder's coarse control fitting, restated (oracle/vbt_keyframe_oracle.c: vo_coarse_fit), pinned
+on the reference (CPU).
+
+1. Against the reference's own sampleLeafBufferAtFractional, detectDensityKeyFrames,
+   appendControlSequenceToStream and reconstructFromKeys (oracle/_ref/libkfref.so) on seeded leaves
+   of full and cropped extents: descriptors, bin rows, keyframes, requiredMaxBinLocalKeys and the
+   fitted grid, bit for bit.
+2. End to end against a file the reference encoder wrote: config 1's blob field regenerated from its
+   seed (tests/golden/make_assets.py), the per-voxel keyframe pass with the encoder's defaults, each
+   leaf's reconstruction fitted with the control profile (epsilons x 8, the formal default
+   controlEpsScale) -- every leaf's coarse stream equals the one in assets/cfg1_blobs.vbtp
+   (descriptors, bins, key frames, FP16 key values), and the EMPTY leaves are the leaves whose
+   reconstruction stays under the background threshold.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ASSETS, GOLDEN
+
+F32 = np.float32
+
+
+def control_profile():
+    from oracle.oracle import VoKeyframeProfile
+    return VoKeyframeProfile(eps_abs=float(F32(1e-5) * F32(8)), eps_rel=float(F32(0.02) * F32(8)))
+
+
+@pytest.fixture(scope="module")
+def kfref():
+    from oracle.oracle import KFREF_SO, KeyframeReference
+    if not os.path.exists(KFREF_SO):
+        pytest.skip("reference build (oracle/_ref/libkfref.so) not present")
+    return KeyframeReference()
+
+
+def test_coarse_fit_against_reference(oracle, kfref):
+    rng = np.random.default_rng(0)
+    prof = control_profile()
+    for it in range(200):
+        T = int(rng.choice([1, 2, 5, 24, 96]))
+        ext = tuple(int(x) for x in rng.choice([8, 8, 8, 3, 5, 1], 3))
+        t = np.arange(T)[None, :]
+        c = rng.uniform(0, T, (512, 1))
+        amp = rng.uniform(0, 1, (512, 1))
+        lt = (amp * np.exp(-((t - c) / rng.uniform(2, 9)) ** 2) + rng.normal(0, 1e-3, (512, T)) * (it % 2))
+        lt = lt.astype(np.float32)
+        a, b = oracle.coarse_fit(lt, ext, prof), kfref.coarse_fit(lt, ext, prof)
+        for k in ("desc", "bins", "key_frames", "key_values", "grid"):
+            assert np.array_equal(np.asarray(a[k]).view(np.uint8), np.asarray(b[k]).view(np.uint8)), (it, k)
+        assert a["required_max_local"] == b["required_max_local"], it
+
+
+def test_config1_coarse_streams_equal_the_encoders(oracle):
+    path = os.path.join(ASSETS, "cfg1_blobs.vbtp")
+    if not os.path.exists(path):
+        pytest.skip("asset cfg1_blobs not generated (python tests/golden/make_assets.py cfg1_blobs)")
+    from oracle.oracle import VoKeyframeProfile
+    sys.path.insert(0, GOLDEN)
+    from make_assets import blobs
+    from leafstreams import streams_from_file
+    raw = blobs((64, 64, 64), 24, 6, 1)                     # the config-1 field, [T, Z, Y, X]
+    T = raw.shape[0]
+    prof = VoKeyframeProfile()
+    recon = oracle.keyframe_pass(raw.reshape(T, -1), prof)["recon"].reshape(T, 64, 64, 64)
+    leaves, arr, _ = streams_from_file(path)
+    cprof = control_profile()
+    fitted = 0
+    for li in range(leaves.shape[0]):
+        bz, by, bx = li // 64, (li // 8) % 8, li % 8
+        sub = recon[:, 8 * bz:8 * bz + 8, 8 * by:8 * by + 8, 8 * bx:8 * bx + 8]
+        empty = max(0.0, float(sub.max())) < prof.bg_threshold
+        mode = int(leaves[li]["header"]) & 3
+        assert (mode == 0) == empty, li
+        if mode == 0:
+            continue
+        fit = oracle.coarse_fit(np.ascontiguousarray(sub.reshape(T, 512).T), (8, 8, 8), cprof)
+        l = leaves[li]
+        c0, k0, nk = int(l["coarse_control"]), int(l["coarse_key"]), int(l["coarse_kf"])
+        assert np.array_equal(fit["desc"], arr["descriptors"][c0:c0 + 64]), li
+        assert np.array_equal(fit["bins"], arr["bins"].reshape(-1, 8)[c0:c0 + 64]), li
+        assert np.array_equal(fit["key_frames"], arr["key_frames"][k0:k0 + nk]), li
+        want = arr["key_values"][k0:k0 + nk].astype(np.float16).view(np.uint16)
+        assert np.array_equal(oracle.float_to_half(fit["key_values"]), want), li
+        fitted += 1
+    assert fitted > 400
