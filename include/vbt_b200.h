@@ -233,6 +233,24 @@ int vbt_detect_keyframes(const float* d_values, uint64_t series, uint32_t frames
                          uint64_t series_stride, const vbt_keyframe_profile* profile, uint32_t* d_key_mask, uint32_t* d_key_count,
                          uint8_t* d_flags, float* d_recon, double* d_err2, vbt_keyframe_totals* d_totals,
                          void* stream);
+/* The encoder's coarse control fitting (src/render_temporal_kf_probe_main.cpp:705-729) for
+ * leaf_count leaves of a frame-major reconstruction d_recon (the keyframe pass's, value t of voxel
+ * (z*height + y)*width + x at d_recon[t * frame_stride + voxel]): per listed leaf (index
+ * (bz*lcy + by)*lcx + bx of the 8^3 leaf grid), its 4^3 controls sampled at controlCoords(4)
+ * (sampleLeafBufferAtFractional, :2203-2237), keyed with detectDensityKeyFrames under
+ * control_profile (no background test) and appended as appendControlSequenceToStream
+ * (:2361-2399) appends them with 8 time bins.  Outputs per listed leaf i: d_desc[i*64 + c]
+ * (keyStart | keyCount << 16 | reserved << 24), d_bins[(i*64 + c)*8 + b], keyframes from
+ * d_key_frames / d_key_values[i * 64 * frames] on, d_key_count[i] (0xFFFFFFFF for a leaf index
+ * outside the grid), d_required_max_local[i], and optionally the fitted grid
+ * d_grid[(i*64 + c) * frames + t] (reconstructFromKeys).  These are the stream arrays
+ * vbt_pack_leaves reads (bin rows 8 bytes apart).  No reference counterpart as a function: the
+ * reference fits inside its leaf loop. */
+int vbt_coarse_fit(const float* d_recon, uint32_t width, uint32_t height, uint32_t depth, uint32_t frames,
+                   uint64_t frame_stride, const uint32_t* d_leaves, uint32_t leaf_count,
+                   const vbt_keyframe_profile* control_profile, uint32_t* d_desc, uint8_t* d_bins,
+                   uint16_t* d_key_frames, float* d_key_values, uint32_t* d_key_count, uint8_t* d_required_max_local,
+                   float* d_grid, void* stream);
 /* Self-check of the division the keyframe pass uses for alpha = a / b (no reference counterpart):
  * every 1 <= b <= b_max, 0 <= a <= b against the IEEE quotient on `device`; result[0] = mismatches,
  * result[1] = (b << 16 | a) of the first, or all ones. */

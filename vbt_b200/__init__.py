@@ -136,6 +136,8 @@ _sig = {
                          C.c_uint64, C.POINTER(C.c_uint64), _vp], C.c_int),
     "vbt_detect_keyframes": ([_vp, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, C.POINTER(KeyframeProfile), _vp,
                               _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_coarse_fit": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _vp, C.c_uint32,
+                        C.POINTER(KeyframeProfile), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "vbt_selftest_keyframe_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_sample_rays": ([_vp, _vp, C.POINTER(SampleParams), _vp, C.c_uint32, _vp, _vp], C.c_int),
     "vbt_decode_control_cache": ([_vp, C.POINTER(C.c_int), C.c_int, _vp, C.c_uint64, _vp], C.c_int),
@@ -430,6 +432,20 @@ def detect_keyframes(values, profile, key_mask, key_count, flags, recon=None, er
     _check(_lib.vbt_detect_keyframes(_addr(values), n, frames, fs, ss, C.byref(profile), _addr(key_mask),
                                      _addr(key_count), _addr(flags), _addr(recon), _addr(err2), _addr(totals),
                                      _stream(stream)))
+
+
+def coarse_fit(recon, dims, leaves, profile, desc, bins, key_frames, key_values, key_count, required,
+               grid=None, stream=None):
+    """The encoder's coarse control fitting on the GPU over the frame-major reconstruction recon
+    [frames, >= X*Y*Z] (float32 device tensor) of a volume dims = (X, Y, Z), for the leaf indices in
+    leaves (int32 device tensor).  Outputs (device tensors): desc [n, 64] int32, bins [n, 64, 8]
+    uint8, key_frames / key_values [n, 64 * frames] int16 / float32, key_count [n] int32, required
+    [n] uint8, and optionally grid [n, 64, frames] float32."""
+    frames, stride = recon.shape
+    X, Y, Z = dims
+    _check(_lib.vbt_coarse_fit(_addr(recon), X, Y, Z, frames, recon.stride(0), _addr(leaves), leaves.numel(),
+                               C.byref(profile), _addr(desc), _addr(bins), _addr(key_frames), _addr(key_values),
+                               _addr(key_count), _addr(required), _addr(grid), _stream(stream)))
 
 
 def keyframe_totals(buf):

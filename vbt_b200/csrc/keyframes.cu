@@ -435,6 +435,133 @@ __global__ void keyframe_division_check_kernel(uint32_t b_max, unsigned long lon
     if (local) atomicAdd(bad, local);
 }
 
+// ---- the encoder's coarse control fitting (src/render_temporal_kf_probe_main.cpp:705-729) ---------
+// One CTA of 64 threads per leaf, one thread per coarse control c = (gz*4 + gy)*4 + gx: the control's
+// series is sampled from the leaf's reconstruction at controlCoords(4)
+// (sampleLeafBufferAtFractional, :2203-2237) into the same [frame][control] shared column the pass
+// uses, keyed by keyframe_series under the control profile (no background test), and appended to
+// the leaf's stream as appendControlSequenceToStream (:2361-2399) does: descriptor, bin row
+// (buildBinIndexFromKeys, :2288-2305) and keyframes (frame, sampled value).
+
+struct CoarseOut {
+    uint32_t* desc;          // [leaf][64]
+    uint8_t* bins;           // [leaf][64][8]
+    uint16_t* key_frame;     // [leaf][64 * frames]
+    float* key_value;        // [leaf][64 * frames]
+    uint32_t* key_count;     // [leaf]
+    uint8_t* required;       // [leaf] requiredMaxBinLocalKeys
+    float* grid;             // optional [leaf][64][frames]
+};
+
+// std::clamp(v, lo, hi)
+__device__ __forceinline__ float clamp_r(float v, float lo, float hi) { return v < lo ? lo : (hi < v ? hi : v); }
+
+__global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict__ recon, uint32_t X, uint32_t Y,
+                                                        uint32_t Z, int n, unsigned long long fstride,
+                                                        const uint32_t* __restrict__ leaves, uint32_t n_leaves,
+                                                        vbt_keyframe_profile p, int rmax, CoarseOut o)
+{
+    extern __shared__ __align__(16) float cf_smem[];
+    __shared__ int s_count[64], s_start[64], s_span[64 * 8];
+    const int words = (n + 31) >> 5;
+    float* sv = cf_smem;                                               // [n][64]
+    uint32_t* sm = reinterpret_cast<uint32_t*>(sv + n * 64);           // [words][64]
+    float* stop = reinterpret_cast<float*>(sm + words * 64);           // [rmax][64]
+    const int c = threadIdx.x;
+    const uint32_t li = blockIdx.x;
+    if (li >= n_leaves) return;          // uniform per CTA
+    const uint32_t leaf = leaves[li];
+    const uint32_t lcx = (X + 7u) / 8u, lcy = (Y + 7u) / 8u, lcz = (Z + 7u) / 8u;
+    if ((unsigned long long)leaf >= (unsigned long long)lcx * lcy * lcz) {   // uniform per CTA
+        if (c == 0) o.key_count[li] = 0xFFFFFFFFu;
+        return;
+    }
+    const uint32_t bx = leaf % lcx, by = (leaf / lcx) % lcy, bz = leaf / (lcx * lcy);
+    const int w = (int)min(8u, X - 8u * bx), h = (int)min(8u, Y - 8u * by), d = (int)min(8u, Z - 8u * bz);
+    const float scale = __fdiv_rn(7.0f, 3.0f);
+    const int gx = c & 3, gy = (c >> 2) & 3, gz = c >> 4;
+    const float x = clamp_r(__fmul_rn((float)gx, scale), 0.0f, (float)max(0, w - 1));
+    const float y = clamp_r(__fmul_rn((float)gy, scale), 0.0f, (float)max(0, h - 1));
+    const float z = clamp_r(__fmul_rn((float)gz, scale), 0.0f, (float)max(0, d - 1));
+    const int x0 = (int)floorf(x), y0 = (int)floorf(y), z0 = (int)floorf(z);
+    const int x1 = min(w - 1, x0 + 1), y1 = min(h - 1, y0 + 1), z1 = min(d - 1, z0 + 1);
+    const float tx = __fsub_rn(x, (float)x0), ty = __fsub_rn(y, (float)y0), tz = __fsub_rn(z, (float)z0);
+    const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty), uz = __fsub_rn(1.0f, tz);
+    auto vox = [&](int lx, int ly, int lz) {
+        return (unsigned long long)((8u * bz + (uint32_t)lz) * Y + 8u * by + (uint32_t)ly) * X + 8u * bx + (uint32_t)lx;
+    };
+    const unsigned long long v000 = vox(x0, y0, z0), v100 = vox(x1, y0, z0), v001 = vox(x0, y0, z1),
+                             v101 = vox(x1, y0, z1), v010 = vox(x0, y1, z0), v110 = vox(x1, y1, z0),
+                             v011 = vox(x0, y1, z1), v111 = vox(x1, y1, z1);
+    for (int t = 0; t < n; ++t) {
+        const float* f = recon + (unsigned long long)t * fstride;
+        const float c00 = __fadd_rn(__fmul_rn(__ldg(f + v000), ux), __fmul_rn(__ldg(f + v100), tx));
+        const float c01 = __fadd_rn(__fmul_rn(__ldg(f + v001), ux), __fmul_rn(__ldg(f + v101), tx));
+        const float c10 = __fadd_rn(__fmul_rn(__ldg(f + v010), ux), __fmul_rn(__ldg(f + v110), tx));
+        const float c11 = __fadd_rn(__fmul_rn(__ldg(f + v011), ux), __fmul_rn(__ldg(f + v111), tx));
+        const float c0 = __fadd_rn(__fmul_rn(c00, uy), __fmul_rn(c10, ty));
+        const float c1 = __fadd_rn(__fmul_rn(c01, uy), __fmul_rn(c11, ty));
+        sv[t * 64 + c] = __fadd_rn(__fmul_rn(c0, uz), __fmul_rn(c1, tz));
+    }
+    const Column<64> col{sv + c, sm + c};
+    float* grid = o.grid ? o.grid + ((unsigned long long)li * 64u + (unsigned)c) * (unsigned)n : nullptr;
+    const SeriesOut r = keyframe_series<64>(col, stop + c, n, words, p, grid, 1ull);
+    const int count = (int)r.count;
+
+    // buildBinIndexFromKeys: one merge of the sorted keys with the bins' first frames.
+    uint8_t b8[8];
+    {
+        int b = 0, i = 0;
+        for (int wd = 0; wd < words && b < 8; ++wd) {
+            uint32_t bits = col.m[wd * 64];
+            while (bits && b < 8) {
+                const int key = (wd << 5) + __ffs(bits) - 1;
+                bits &= bits - 1u;
+                while (b < 8 && key >= (int)(((long long)b * n) / 8)) b8[b++] = (uint8_t)(i > 0 ? i - 1 : 0);
+                ++i;
+            }
+        }
+        for (; b < 8; ++b) b8[b] = (uint8_t)(count - 1);
+    }
+    int local = 1;
+    for (int b = 0; b < 8; ++b) {
+        const int next = b + 1 < 8 ? (int)b8[b + 1] : count;
+        const int span = max(1, next - (int)b8[b]);
+        s_span[c * 8 + b] = span;
+        local = max(local, span);
+    }
+    s_count[c] = count;
+    __syncthreads();
+    if (c == 0) {            // keyStart: the keys of the controls before, in control order
+        int run = 0, req = 1;
+        for (int k = 0; k < 64; ++k) {
+            s_start[k] = run;
+            run += s_count[k];
+            for (int b = 0; b < 8; ++b) req = (int)(uint8_t)max(req, s_span[k * 8 + b]);
+        }
+        o.key_count[li] = (uint32_t)run;
+        o.required[li] = (uint8_t)req;
+    }
+    __syncthreads();
+    const int start = s_start[c];
+    o.desc[(unsigned long long)li * 64u + (unsigned)c] =
+        (uint32_t)(uint16_t)start | ((uint32_t)min(count, 255) << 16) | ((uint32_t)min(local, 255) << 24);
+    uint8_t* brow = o.bins + ((unsigned long long)li * 64u + (unsigned)c) * 8u;
+    for (int b = 0; b < 8; ++b) brow[b] = b8[b];
+    const unsigned long long kbase = (unsigned long long)li * 64u * (unsigned)n + (unsigned)start;
+    int i = 0;
+    for (int wd = 0; wd < words; ++wd) {
+        uint32_t bits = col.m[wd * 64];
+        while (bits) {
+            const int key = (wd << 5) + __ffs(bits) - 1;
+            bits &= bits - 1u;
+            o.key_frame[kbase + i] = (uint16_t)key;
+            o.key_value[kbase + i] = col.at(key);
+            ++i;
+        }
+    }
+}
+
 template <int NV>
 size_t kf_smem_bytes(int n, int rmax)
 {
@@ -533,4 +660,45 @@ extern "C" int vbt_selftest_keyframe_division(uint32_t b_max, uint64_t* result, 
     result[0] = h[0];
     result[1] = h[1];
     return VBT_STATUS_OK;
+}
+
+extern "C" int vbt_coarse_fit(const float* d_recon, uint32_t width, uint32_t height, uint32_t depth, uint32_t frames,
+                              uint64_t frame_stride, const uint32_t* d_leaves, uint32_t leaf_count,
+                              const vbt_keyframe_profile* control_profile, uint32_t* d_desc, uint8_t* d_bins,
+                              uint16_t* d_key_frames, float* d_key_values, uint32_t* d_key_count,
+                              uint8_t* d_required_max_local, float* d_grid, void* stream)
+{
+    using vbtb::set_last_error;
+    if (!control_profile) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null profile");
+    if (frames == 0 || width == 0 || height == 0 || depth == 0)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "empty volume");
+    if (frames > kKfMaxFrames) return set_last_error(VBT_STATUS_LIMIT, "frames above 1024");
+    const unsigned long long voxels = (unsigned long long)width * height * depth;
+    if (frame_stride < voxels) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "frame_stride smaller than the volume");
+    if (leaf_count == 0) return VBT_STATUS_OK;
+    if (!d_recon || !d_leaves || !d_desc || !d_bins || !d_key_frames || !d_key_values || !d_key_count ||
+        !d_required_max_local)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    const int n = (int)frames;
+    const int m = n - 1;
+    const int rmax = n >= 2 ? m - (m - 1 < (m * 9) / 10 ? m - 1 : (m * 9) / 10) : 1;
+    int dev = 0, smem_max = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t smem = kf_smem_bytes<64>(n, rmax);
+    const size_t static_smem = (64 + 64 + 512) * sizeof(int);
+    if (smem + static_smem > (size_t)smem_max) return set_last_error(VBT_STATUS_LIMIT, "too many frames for one leaf's CTA");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    kf_rcp_init_kernel<<<1, 1024, 0, s>>>();
+    cudaError_t e = cudaFuncSetAttribute(coarse_fit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+        vbt_keyframe_profile prof = *control_profile;
+        prof.bg_threshold = -1.0;          // the control fitting has no background test
+        const CoarseOut o{d_desc, d_bins, d_key_frames, d_key_values, d_key_count, d_required_max_local, d_grid};
+        coarse_fit_kernel<<<leaf_count, 64, smem, s>>>(d_recon, width, height, depth, n, frame_stride, d_leaves,
+                                                       leaf_count, prof, rmax, o);
+        e = cudaGetLastError();
+    }
+    return e == cudaSuccess ? VBT_STATUS_OK
+                            : set_last_error(VBT_STATUS_CUDA, std::string("coarse_fit_kernel: ") + cudaGetErrorString(e));
 }
