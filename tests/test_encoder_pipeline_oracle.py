@@ -86,3 +86,37 @@ def test_config1_coarse_streams_equal_the_encoders(oracle):
         assert np.array_equal(oracle.float_to_half(fit["key_values"]), want), li
         fitted += 1
     assert fitted > 400
+
+
+def test_config1_grid4_leaves_rebuilt_from_the_raw_field(oracle, reference):
+    """The chain the GPU runs (keyframe pass -> coarse fit -> leaf packer), here through the oracle and
+    the reference packer: every GRID4 leaf of cfg1_blobs.vbtp is rebuilt byte for byte from the raw
+    field, with the fit's requiredMaxBinLocalKeys as the stream's maxBinLocalKeys."""
+    path = os.path.join(ASSETS, "cfg1_blobs.vbtp")
+    if not os.path.exists(path):
+        pytest.skip("asset cfg1_blobs not generated (python tests/golden/make_assets.py cfg1_blobs)")
+    from oracle.oracle import VoKeyframeProfile
+    sys.path.insert(0, GOLDEN)
+    from make_assets import blobs
+    from leafstreams import streams_from_file
+    raw = blobs((64, 64, 64), 24, 6, 1)
+    T = raw.shape[0]
+    recon = oracle.keyframe_pass(raw.reshape(T, -1), VoKeyframeProfile())["recon"].reshape(T, 64, 64, 64)
+    leaves, _, blocks = streams_from_file(path)
+    cprof = control_profile()
+    rebuilt = 0
+    for li in range(leaves.shape[0]):
+        word = int(leaves[li]["header"])
+        if word & 3 != 1:
+            continue
+        bz, by, bx = li // 64, (li // 8) % 8, li % 8
+        sub = recon[:, 8 * bz:8 * bz + 8, 8 * by:8 * by + 8, 8 * bx:8 * bx + 8]
+        fit = oracle.coarse_fit(np.ascontiguousarray(sub.reshape(T, 512).T), (8, 8, 8), cprof)
+        d = fit["desc"]
+        triples = np.stack([d & 0xFFFF, (d >> 16) & 0xFF, d >> 24], axis=1).astype(np.uint32).reshape(-1)
+        stream = reference.pack_stream((word >> 2) & 3, triples, fit["bins"].reshape(-1), fit["key_frames"].astype(np.uint32),
+                                       fit["key_values"], 8, max_local=fit["required_max_local"])
+        leaf = reference.build_leaf(word, fit["key_frames"].size, 0, stream, np.zeros(0, np.uint8))
+        assert leaf.tobytes() == blocks[li], li
+        rebuilt += 1
+    assert rebuilt > 400
