@@ -59,3 +59,44 @@ def test_no_gpu_fails_loudly(vbt):
     with pytest.raises(vbt.VbtError) as ei:
         vbt.Asset(os.path.join(GOLDEN, "assets", "tiny_density.vbtp"))
     assert ei.value.status == 42
+
+
+def test_encoder_and_writer_argument_checks(vbt):
+    """The keyframe pass, coarse fit, leaf packer and samplers reject bad scalar arguments on the host,
+    before any device work (the pointers below are never dereferenced)."""
+    L = vbt.lib()
+    fake = C.c_void_p(0x10000)
+    prof = vbt.KeyframeProfile()
+    z = C.c_void_p(None)
+
+    def kf(series, frames, fstride, sstride):
+        return L.vbt_detect_keyframes(fake, series, frames, fstride, sstride, C.byref(prof), fake, fake, fake, z, z,
+                                      z, z)
+    assert kf(10, 0, 10, 1) == 40                      # no frames
+    assert kf(10, 1025, 10, 1) == 43                   # above 1024 frames
+    assert kf(10, 8, 5, 1) == 40                       # frame-major stride shorter than the series
+    assert kf(10, 8, 1, 7) == 40                       # time-fastest stride shorter than the frames
+    assert kf(10, 8, 2, 3) == 40                       # neither layout
+    assert L.vbt_detect_keyframes(fake, 10, 8, 10, 1, None, fake, fake, fake, z, z, z, z) == 40
+
+    def cf(frames, fstride, dims=(16, 16, 16)):
+        return L.vbt_coarse_fit(fake, *dims, frames, fstride, fake, 4, C.byref(prof), fake, fake, fake, fake, fake,
+                                fake, z, z)
+    assert cf(0, 4096) == 40
+    assert cf(2000, 4096) == 43
+    assert cf(8, 100) == 40                            # frame stride shorter than the volume
+    assert cf(8, 4096, (0, 16, 16)) == 40
+
+    total = C.c_uint64()
+    assert L.vbt_pack_leaves(fake, 4, fake, fake, 8, fake, fake, 8, z, 0, None, fake, 64, C.byref(total), z) == 40
+    assert L.vbt_pack_leaves(fake, 4, None, fake, 8, fake, fake, 8, z, 0, fake, fake, 64, C.byref(total), z) == 40
+    assert L.vbt_pack_leaves(fake, 4, fake, C.c_void_p(0x10001), 8, fake, fake, 8, z, 0, fake, fake, 64,
+                             C.byref(total), z) == 40   # bin rows not 4-byte aligned
+    assert L.vbt_pack_payload(fake, None, 4, fake, fake, 64, C.byref(total), z) == 40
+
+    sp = vbt.SampleParams()
+    assert L.vbt_smoke_sample_rays(None, C.byref(sp), fake, 4, fake, z) == 40
+    assert L.vbt_sample_rays(None, fake, C.byref(sp), fake, 4, fake, z) == 40
+    res = (C.c_uint64 * 2)()
+    assert L.vbt_selftest_keyframe_division(0, res, 0) == 40
+    assert L.vbt_selftest_keyframe_division(70000, res, 0) == 40
