@@ -120,3 +120,62 @@ def test_config1_grid4_leaves_rebuilt_from_the_raw_field(oracle, reference):
         assert leaf.tobytes() == blocks[li], li
         rebuilt += 1
     assert rebuilt > 400
+
+
+def levelset_profiles():
+    """The encoder's temporal and control profiles for a level set (render_temporal_kf_probe_main.cpp:
+    430-445 and runRenderTemporalMainline): no cutoff, iso-surface protection at 0 with a band of
+    0.1 voxel in the pass, none in the control fitting."""
+    from oracle.oracle import VoKeyframeProfile
+    common = dict(render_cutoff=0.0, cutoff_band=0.0, cutoff_temporal_protect=0, bg_threshold=-1.0)
+    temporal = VoKeyframeProfile(iso_surface_protect=1, iso_value=0.0, iso_band=float(F32(0.1) * F32(1.0)), **common)
+    control = VoKeyframeProfile(eps_abs=float(F32(1e-5) * F32(8)), eps_rel=float(F32(0.02) * F32(8)), **common)
+    return temporal, control
+
+
+CASES = {   # name: (field recipe of tests/golden/make_assets.py, dims, level set)
+    "tiny_density": (("blobs", ((20, 12, 17), 9, 3, 11)), (20, 12, 17), False),
+    "tiny_levelset": (("sdf_scene", ((24, 20, 28), 12, 12.0, 2.0, 0.3, 3, 2.0, 5.0, 12)), (24, 20, 28), True),
+    "cfg4_sdf_small": (("sdf_scene", ((64, 64, 64), 24, 24.0, 2.0, 0.2, 6, 3.0, 8.0, 4)), (64, 64, 64), True),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_coarse_streams_of_more_files(oracle, name):
+    """As the config-1 check, on a density field with cropped boundary leaves and on two level sets
+    (iso-surface protection in the pass, Mode2 shell leaves in the file: their coarse streams)."""
+    (fn, args), (X, Y, Z), levelset = CASES[name]
+    path = os.path.join(GOLDEN, "assets", name + ".vbtp")
+    if not os.path.exists(path):
+        path = os.path.join(ASSETS, name + ".vbtp")
+    if not os.path.exists(path):
+        pytest.skip(f"asset {name} not generated")
+    from oracle.oracle import VoKeyframeProfile
+    sys.path.insert(0, GOLDEN)
+    import make_assets
+    from leafstreams import streams_from_file
+    raw = getattr(make_assets, fn)(*args)
+    T = raw.shape[0]
+    temporal, control = levelset_profiles() if levelset else (VoKeyframeProfile(), control_profile())
+    recon = oracle.keyframe_pass(raw.reshape(T, -1), temporal)["recon"].reshape(T, Z, Y, X)
+    leaves, arr, _ = streams_from_file(path)
+    lcx, lcy = (X + 7) // 8, (Y + 7) // 8
+    fitted = 0
+    for li in range(leaves.shape[0]):
+        if int(leaves[li]["header"]) & 3 == 0:
+            continue
+        bx, by, bz = li % lcx, (li // lcx) % lcy, li // (lcx * lcy)
+        sub = recon[:, 8 * bz:8 * bz + 8, 8 * by:8 * by + 8, 8 * bx:8 * bx + 8]
+        d, h, w = sub.shape[1:]
+        lt = np.zeros((T, 8, 8, 8), np.float32)
+        lt[:, :d, :h, :w] = sub
+        fit = oracle.coarse_fit(np.ascontiguousarray(lt.reshape(T, 512).T), (w, h, d), control)
+        l = leaves[li]
+        c0, k0, nk = int(l["coarse_control"]), int(l["coarse_key"]), int(l["coarse_kf"])
+        assert np.array_equal(fit["desc"], arr["descriptors"][c0:c0 + 64]), li
+        assert np.array_equal(fit["bins"], arr["bins"].reshape(-1, 8)[c0:c0 + 64]), li
+        assert np.array_equal(fit["key_frames"], arr["key_frames"][k0:k0 + nk]), li
+        want = arr["key_values"][k0:k0 + nk].astype(np.float16).view(np.uint16)
+        assert np.array_equal(oracle.float_to_half(fit["key_values"]), want), li
+        fitted += 1
+    assert fitted >= 10
