@@ -125,6 +125,8 @@ class Oracle:
         i32p = C.POINTER(C.c_int)
         L.vo_detect_keyframes.argtypes = [f32p, C.c_int, C.POINTER(VoKeyframeProfile), i32p, i32p]
         L.vo_reconstruct.argtypes = [f32p, C.c_int, i32p, C.c_int, f32p]
+        L.vo_fine6_fit.argtypes = [f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(VoKeyframeProfile), f32p, u32p,
+                                   u8p, C.POINTER(C.c_uint16), f32p, C.c_int, C.POINTER(C.c_int), f32p]
         L.vo_float_to_half_n.argtypes = [f32p, C.c_uint64, C.POINTER(C.c_uint16)]
         L.vo_coarse_fit.argtypes = [f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(VoKeyframeProfile), u32p, u8p,
                                     C.POINTER(C.c_uint16), f32p, C.c_int, C.POINTER(C.c_int), f32p]
@@ -146,6 +148,25 @@ class Oracle:
         out = np.zeros(v.size, np.float32)
         self.lib.vo_reconstruct(_ptr(v, f32p), v.size, _ptr(k, C.POINTER(C.c_int)), k.size, _ptr(out, f32p))
         return out
+
+    def fine6_fit(self, leaf_recon, extent, profile, coarse_grid):
+        """The FINE6 residual fitting of one leaf over its fitted coarse grid [64, T] (coarse_fit's
+        grid): dict of desc [216], bins [216, 8], key_frames, key_values, required_max_local, grid."""
+        lt = np.ascontiguousarray(leaf_recon, np.float32).reshape(512, -1)
+        T = lt.shape[1]
+        cg = np.ascontiguousarray(coarse_grid, np.float32)
+        cap = 216 * max(T, 1)
+        desc = np.zeros(216, np.uint32)
+        bins = np.zeros((216, 8), np.uint8)
+        kf = np.zeros(cap, np.uint16)
+        kv = np.zeros(cap, np.float32)
+        grid = np.zeros((216, T), np.float32)
+        req = C.c_int()
+        n = self.lib.vo_fine6_fit(_ptr(lt, f32p), T, *extent, C.byref(profile), _ptr(cg, f32p), _ptr(desc, u32p),
+                                  _ptr(bins, u8p), _ptr(kf, C.POINTER(C.c_uint16)), _ptr(kv, f32p), cap, C.byref(req),
+                                  _ptr(grid, f32p))
+        return dict(desc=desc, bins=bins, key_frames=kf[:n].copy(), key_values=kv[:n].copy(),
+                    required_max_local=req.value, grid=grid)
 
     def float_to_half(self, values):
         """renderTemporalFloatToHalfBits of every value (uint16 array)."""

@@ -384,3 +384,91 @@ void vo_float_to_half_n(const float* v, uint64_t n, uint16_t* out)
 {
     for (uint64_t i = 0; i < n; ++i) out[i] = vo_float_to_half(v[i]);
 }
+
+/* sampleControlGridValue (:2240-2286): trilinear over a fitted control grid grid[ctrl * frames + t]
+ * of `res`^3 controls at controlCoords(res), the position clamped to the leaf's extent. */
+static float kf_sample_grid(const float* grid, int res, int frames, int t, int w, int h, int d, float fx, float fy,
+                            float fz)
+{
+    float coords[8];
+    const float scale = res > 1 ? 7.0f / (float)(res - 1) : 0.0f;
+    for (int i = 0; i < res && i < 8; ++i) coords[i] = res > 1 ? (float)i * scale : 0.0f;
+    int i0[3], i1[3];
+    float wt[3];
+    const float pos[3] = {fx, fy, fz};
+    const int ext[3] = {w, h, d};
+    for (int a = 0; a < 3; ++a) {
+        const float p = clamp_r(pos[a], 0.0f, (float)(ext[a] - 1 > 0 ? ext[a] - 1 : 0));
+        int j1 = 1;
+        while (j1 < res - 1 && coords[j1] < p) ++j1;
+        const int j0 = j1 - 1 > 0 ? j1 - 1 : 0;
+        const float c0 = coords[j0], c1 = coords[j1];
+        i0[a] = j0;
+        i1[a] = j1;
+        wt[a] = c1 > c0 ? (p - c0) / (c1 - c0) : 0.0f;
+    }
+#define G(ix, iy, iz) grid[(size_t)(((iz) * res + (iy)) * res + (ix)) * (size_t)frames + (size_t)t]
+    const float tx = wt[0], ty = wt[1], tz = wt[2];
+    const float c00 = G(i0[0], i0[1], i0[2]) * (1.0f - tx) + G(i1[0], i0[1], i0[2]) * tx;
+    const float c01 = G(i0[0], i0[1], i1[2]) * (1.0f - tx) + G(i1[0], i0[1], i1[2]) * tx;
+    const float c10 = G(i0[0], i1[1], i0[2]) * (1.0f - tx) + G(i1[0], i1[1], i0[2]) * tx;
+    const float c11 = G(i0[0], i1[1], i1[2]) * (1.0f - tx) + G(i1[0], i1[1], i1[2]) * tx;
+#undef G
+    const float c0 = c00 * (1.0f - ty) + c10 * ty;
+    const float c1 = c01 * (1.0f - ty) + c11 * ty;
+    return c0 * (1.0f - tz) + c1 * tz;
+}
+
+/* The FINE6 residual fitting (:815-850, the plain fine6 variant): for the 6^3 controls at
+ * controlCoords(6), the series sampled from the reconstruction minus the coarse grid sampled at the
+ * same position, keyed with the control profile and appended with 8 time bins; outputs as
+ * vo_coarse_fit (desc and bins for 216 controls, grid [216][frames]). */
+int vo_fine6_fit(const float* lt, int frames, int w, int h, int d, const vo_keyframe_profile* p,
+                 const float* coarse_grid, uint32_t* desc, uint8_t* bins, uint16_t* key_frames, float* key_values,
+                 int key_cap, int* required_max_local, float* grid)
+{
+    const float scale = 7.0f / (float)(6 - 1);
+    float coords[6];
+    for (int i = 0; i < 6; ++i) coords[i] = (float)i * scale;
+    float* series = (float*)malloc((size_t)(frames > 0 ? frames : 1) * sizeof(float));
+    int* keys = (int*)malloc((size_t)(frames > 0 ? frames : 1) * sizeof(int));
+    int nk = 0, overflow = 0;
+    uint8_t required = 1u;
+    for (int gz = 0; gz < 6; ++gz)
+        for (int gy = 0; gy < 6; ++gy)
+            for (int gx = 0; gx < 6; ++gx) {
+                const int ctrl = (gz * 6 + gy) * 6 + gx;
+                for (int t = 0; t < frames; ++t) {
+                    const float raw_like = kf_sample_leaf(lt, frames, t, w, h, d, coords[gx], coords[gy], coords[gz]);
+                    const float coarse = kf_sample_grid(coarse_grid, 4, frames, t, w, h, d, coords[gx], coords[gy],
+                                                        coords[gz]);
+                    series[t] = raw_like - coarse;
+                }
+                const int k = vo_detect_keyframes(series, frames, p, keys, NULL);
+                uint8_t* b = bins + ctrl * 8;
+                kf_bin_index(keys, k, frames, 8, b);
+                int local = 1;
+                for (int bin = 0; bin < 8; ++bin) {
+                    const int next = bin + 1 < 8 ? (int)b[bin + 1] : k;
+                    const int span = next - (int)b[bin] > 1 ? next - (int)b[bin] : 1;
+                    if (span > local) local = span;
+                    if (span > (int)required) required = (uint8_t)span;
+                }
+                desc[ctrl] = (uint32_t)(uint16_t)nk | ((uint32_t)(k < 255 ? k : 255) << 16) |
+                             ((uint32_t)(local < 255 ? local : 255) << 24);
+                for (int i = 0; i < k; ++i) {
+                    if (nk < key_cap) {
+                        key_frames[nk] = (uint16_t)keys[i];
+                        key_values[nk] = series[keys[i]];
+                    } else {
+                        overflow = 1;
+                    }
+                    ++nk;
+                }
+                if (grid) vo_reconstruct(series, frames, keys, k, grid + (size_t)ctrl * (size_t)frames);
+            }
+    free(series);
+    free(keys);
+    *required_max_local = required;
+    return overflow ? -1 : nk;
+}

@@ -135,6 +135,9 @@ int vo_coarse_fit(const float* leaf_recon, int frames, int w, int h, int d, cons
                   uint32_t* desc, uint8_t* bins, uint16_t* key_frames, float* key_values, int key_cap,
                   int* required_max_local, float* grid);
 void vo_float_to_half_n(const float* v, uint64_t n, uint16_t* out);
+int vo_fine6_fit(const float* leaf_recon, int frames, int w, int h, int d, const vo_keyframe_profile* control_profile,
+                 const float* coarse_grid, uint32_t* desc, uint8_t* bins, uint16_t* key_frames, float* key_values,
+                 int key_cap, int* required_max_local, float* grid);
 
 #ifdef __cplusplus
 }

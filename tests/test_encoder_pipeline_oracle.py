@@ -88,10 +88,12 @@ def test_config1_coarse_streams_equal_the_encoders(oracle):
     assert fitted > 400
 
 
-def test_config1_grid4_leaves_rebuilt_from_the_raw_field(oracle, reference):
-    """The chain the GPU runs (keyframe pass -> coarse fit -> leaf packer), here through the oracle and
-    the reference packer: every GRID4 leaf of cfg1_blobs.vbtp is rebuilt byte for byte from the raw
-    field, with the fit's requiredMaxBinLocalKeys as the stream's maxBinLocalKeys."""
+def test_config1_leaves_rebuilt_from_the_raw_field(oracle, reference):
+    """The encoder chain (keyframe pass -> coarse fit -> FINE6 residual fit -> leaf packer), here
+    through the oracle and the reference packer: every GRID4 and every FINE6 leaf of cfg1_blobs.vbtp
+    is rebuilt byte for byte from the raw field, with each fit's requiredMaxBinLocalKeys as its
+    stream's maxBinLocalKeys (the FINE6 stream: the residual of the reconstruction over the fitted
+    coarse grid, vo_fine6_fit)."""
     path = os.path.join(ASSETS, "cfg1_blobs.vbtp")
     if not os.path.exists(path):
         pytest.skip("asset cfg1_blobs not generated (python tests/golden/make_assets.py cfg1_blobs)")
@@ -104,22 +106,31 @@ def test_config1_grid4_leaves_rebuilt_from_the_raw_field(oracle, reference):
     recon = oracle.keyframe_pass(raw.reshape(T, -1), VoKeyframeProfile())["recon"].reshape(T, 64, 64, 64)
     leaves, _, blocks = streams_from_file(path)
     cprof = control_profile()
-    rebuilt = 0
+    def pack(fit, codec):
+        d = fit["desc"]
+        triples = np.stack([d & 0xFFFF, (d >> 16) & 0xFF, d >> 24], axis=1).astype(np.uint32).reshape(-1)
+        return reference.pack_stream(codec, triples, fit["bins"].reshape(-1), fit["key_frames"].astype(np.uint32),
+                                     fit["key_values"], 8, max_local=fit["required_max_local"])
+
+    rebuilt = {1: 0, 3: 0}
     for li in range(leaves.shape[0]):
         word = int(leaves[li]["header"])
-        if word & 3 != 1:
+        mode = word & 3
+        if mode not in (1, 3):
             continue
         bz, by, bx = li // 64, (li // 8) % 8, li % 8
         sub = recon[:, 8 * bz:8 * bz + 8, 8 * by:8 * by + 8, 8 * bx:8 * bx + 8]
-        fit = oracle.coarse_fit(np.ascontiguousarray(sub.reshape(T, 512).T), (8, 8, 8), cprof)
-        d = fit["desc"]
-        triples = np.stack([d & 0xFFFF, (d >> 16) & 0xFF, d >> 24], axis=1).astype(np.uint32).reshape(-1)
-        stream = reference.pack_stream((word >> 2) & 3, triples, fit["bins"].reshape(-1), fit["key_frames"].astype(np.uint32),
-                                       fit["key_values"], 8, max_local=fit["required_max_local"])
-        leaf = reference.build_leaf(word, fit["key_frames"].size, 0, stream, np.zeros(0, np.uint8))
-        assert leaf.tobytes() == blocks[li], li
-        rebuilt += 1
-    assert rebuilt > 400
+        lt = np.ascontiguousarray(sub.reshape(T, 512).T)
+        fit = oracle.coarse_fit(lt, (8, 8, 8), cprof)
+        coarse = pack(fit, (word >> 2) & 3)
+        fine, nf = np.zeros(0, np.uint8), 0
+        if mode == 3:
+            f6 = oracle.fine6_fit(lt, (8, 8, 8), cprof, fit["grid"])
+            fine, nf = pack(f6, (word >> 4) & 3), f6["key_frames"].size
+        leaf = reference.build_leaf(word, fit["key_frames"].size, nf, coarse, fine)
+        assert leaf.tobytes() == blocks[li], (li, mode)
+        rebuilt[mode] += 1
+    assert rebuilt[1] > 400 and rebuilt[3] > 20, rebuilt
 
 
 def levelset_profiles():
