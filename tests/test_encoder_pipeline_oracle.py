@@ -190,3 +190,79 @@ def test_coarse_streams_of_more_files(oracle, name):
         assert np.array_equal(oracle.float_to_half(fit["key_values"]), want), li
         fitted += 1
     assert fitted >= 10
+
+
+def route_leaf(raw, base, grid_coarse, grid_fine, peak, step=8, cutoff=F32(0.0003), band=F32(0.0001)):
+    """The density route (src/render_temporal_kf_probe_main.cpp:1105-1245 with routeRenderTemporalLeaf,
+    src/render_temporal_route.cpp:27-66, and the thresholds of makeRenderTemporalRouteDefaults): the
+    points of the leaf on the encoder's sampling lattice (every `step`-th frame and voxel; sampleStep
+    8), their truth against the coarse prediction and the coarse + FINE6 prediction sampled from the
+    fitted grids; FINE6 when the coarse fit is too rough, the points are visible and the fine fit gains
+    enough, else GRID4.  Points sit at multiples of 8, so each is a leaf's voxel (0, 0, 0): control 0
+    of either grid."""
+    T = raw.shape[0]
+    bx, by, bz = base
+    lo, hi = float(F32(cutoff - band)), float(F32(cutoff + band))
+    n = vis = bnd = 0
+    ce2 = fe2 = cpk = 0.0
+    for t in range(0, T, step):
+        if bx % step or by % step or bz % step:
+            continue
+        truth = float(raw[t, bz, by, bx])
+        cp, fp = F32(grid_coarse[0, t]), F32(grid_fine[0, t])
+        n += 1
+        vis += truth >= lo
+        bnd += lo <= truth <= hi
+        cd, fd = truth - float(cp), truth - float(F32(cp + fp))
+        ce2 += cd * cd
+        fe2 += fd * fd
+        cpk = max(cpk, abs(cd) / peak)
+    cnt = float(max(1, n))
+    crm, frm = np.sqrt(ce2 / cnt) / peak, np.sqrt(fe2 / cnt) / peak
+    rough = crm > float(F32(0.008)) or cpk > float(F32(0.03))
+    sensitive = vis / cnt >= float(F32(0.005)) or bnd / cnt >= float(F32(0.005))
+    gain = (crm - frm) / max(crm, 1e-12)
+    return 3 if rough and sensitive and gain >= float(F32(0.05)) else 1
+
+
+def test_config1_file_regenerated_from_the_raw_field(oracle, reference):
+    """The whole config-1 VBTPACK4 file from its raw field: per-voxel pass, EMPTY test, coarse fit,
+    FINE6 fit, route, leaf packing (reference packer) and the file layout (52-byte header, word
+    offsets, payload) -- byte for byte the file the reference encoder wrote."""
+    path = os.path.join(ASSETS, "cfg1_blobs.vbtp")
+    if not os.path.exists(path):
+        pytest.skip("asset cfg1_blobs not generated (python tests/golden/make_assets.py cfg1_blobs)")
+    import struct
+    from oracle.oracle import VoKeyframeProfile, pack_payload
+    sys.path.insert(0, GOLDEN)
+    from make_assets import blobs
+    raw = blobs((64, 64, 64), 24, 6, 1)
+    T = raw.shape[0]
+    peak = float(max(F32(1e-6), F32(F32(raw.max()) - F32(raw.min()))))
+    prof = VoKeyframeProfile()
+    recon = oracle.keyframe_pass(raw.reshape(T, -1), prof)["recon"].reshape(T, 64, 64, 64)
+    cprof = control_profile()
+
+    def pack(fit, codec):
+        d = fit["desc"]
+        triples = np.stack([d & 0xFFFF, (d >> 16) & 0xFF, d >> 24], axis=1).astype(np.uint32).reshape(-1)
+        return reference.pack_stream(codec, triples, fit["bins"].reshape(-1), fit["key_frames"].astype(np.uint32),
+                                     fit["key_values"], 8, max_local=fit["required_max_local"])
+
+    blocks = []
+    for li in range(512):
+        bz, by, bx = li // 64, (li // 8) % 8, li % 8
+        sub = recon[:, 8 * bz:8 * bz + 8, 8 * by:8 * by + 8, 8 * bx:8 * bx + 8]
+        if max(0.0, float(sub.max())) < prof.bg_threshold:
+            blocks.append(reference.build_leaf(0, 0, 0, np.zeros(0, np.uint8), np.zeros(0, np.uint8)).tobytes())
+            continue
+        lt = np.ascontiguousarray(sub.reshape(T, 512).T)
+        fit = oracle.coarse_fit(lt, (8, 8, 8), cprof)
+        f6 = oracle.fine6_fit(lt, (8, 8, 8), cprof, fit["grid"])
+        mode = route_leaf(raw, (8 * bx, 8 * by, 8 * bz), fit["grid"], f6["grid"], peak)
+        word = mode | (4 << 6) | ((6 if mode == 3 else 0) << 9)          # FP16 keyframes in both streams
+        fine, nf = (pack(f6, 0), f6["key_frames"].size) if mode == 3 else (np.zeros(0, np.uint8), 0)
+        blocks.append(reference.build_leaf(word, fit["key_frames"].size, nf, pack(fit, 0), fine).tobytes())
+    offsets, payload = pack_payload(blocks)
+    header = b"VBTPACK4" + struct.pack("<11I", 4, 64, 64, 64, T, 8, 4, 0, 512, 1, 0)
+    assert header + offsets.tobytes() + payload.tobytes() == open(path, "rb").read()
