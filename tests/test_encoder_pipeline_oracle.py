@@ -225,22 +225,33 @@ def route_leaf(raw, base, grid_coarse, grid_fine, peak, step=8, cutoff=F32(0.000
     return 3 if rough and sensitive and gain >= float(F32(0.05)) else 1
 
 
-def test_config1_file_regenerated_from_the_raw_field(oracle, reference):
-    """The whole config-1 VBTPACK4 file from its raw field: per-voxel pass, EMPTY test, coarse fit,
-    FINE6 fit, route, leaf packing (reference packer) and the file layout (52-byte header, word
-    offsets, payload) -- byte for byte the file the reference encoder wrote."""
-    path = os.path.join(ASSETS, "cfg1_blobs.vbtp")
+FILES = {   # name: (blobs arguments of tests/golden/make_assets.py, dims)
+    "cfg1_blobs": (((64, 64, 64), 24, 6, 1), (64, 64, 64)),
+    "tiny_density": (((20, 12, 17), 9, 3, 11), (20, 12, 17)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FILES))
+def test_density_file_regenerated_from_the_raw_field(oracle, reference, name):
+    """A whole density VBTPACK4 file from its raw field: per-voxel pass, EMPTY test, coarse fit, FINE6
+    fit, route, leaf packing (reference packer) and the file layout (52-byte header, word offsets,
+    payload) -- byte for byte the file the reference encoder wrote (config 1, and a small field whose
+    boundary leaves are cropped)."""
+    args, (X, Y, Z) = FILES[name]
+    path = os.path.join(GOLDEN, "assets", name + ".vbtp")
     if not os.path.exists(path):
-        pytest.skip("asset cfg1_blobs not generated (python tests/golden/make_assets.py cfg1_blobs)")
+        path = os.path.join(ASSETS, name + ".vbtp")
+    if not os.path.exists(path):
+        pytest.skip(f"asset {name} not generated")
     import struct
     from oracle.oracle import VoKeyframeProfile, pack_payload
     sys.path.insert(0, GOLDEN)
     from make_assets import blobs
-    raw = blobs((64, 64, 64), 24, 6, 1)
+    raw = blobs(*args)
     T = raw.shape[0]
     peak = float(max(F32(1e-6), F32(F32(raw.max()) - F32(raw.min()))))
     prof = VoKeyframeProfile()
-    recon = oracle.keyframe_pass(raw.reshape(T, -1), prof)["recon"].reshape(T, 64, 64, 64)
+    recon = oracle.keyframe_pass(raw.reshape(T, -1), prof)["recon"].reshape(T, Z, Y, X)
     cprof = control_profile()
 
     def pack(fit, codec):
@@ -249,20 +260,25 @@ def test_config1_file_regenerated_from_the_raw_field(oracle, reference):
         return reference.pack_stream(codec, triples, fit["bins"].reshape(-1), fit["key_frames"].astype(np.uint32),
                                      fit["key_values"], 8, max_local=fit["required_max_local"])
 
+    lcx, lcy, lcz = (X + 7) // 8, (Y + 7) // 8, (Z + 7) // 8
+    none = np.zeros(0, np.uint8)
     blocks = []
-    for li in range(512):
-        bz, by, bx = li // 64, (li // 8) % 8, li % 8
+    for li in range(lcx * lcy * lcz):
+        bx, by, bz = li % lcx, (li // lcx) % lcy, li // (lcx * lcy)
         sub = recon[:, 8 * bz:8 * bz + 8, 8 * by:8 * by + 8, 8 * bx:8 * bx + 8]
-        if max(0.0, float(sub.max())) < prof.bg_threshold:
-            blocks.append(reference.build_leaf(0, 0, 0, np.zeros(0, np.uint8), np.zeros(0, np.uint8)).tobytes())
+        if max(0.0, float(sub.max())) < prof.bg_threshold:       # EMPTY: the default header, coarse res 4
+            blocks.append(reference.build_leaf(4 << 6, 0, 0, none, none).tobytes())
             continue
-        lt = np.ascontiguousarray(sub.reshape(T, 512).T)
-        fit = oracle.coarse_fit(lt, (8, 8, 8), cprof)
-        f6 = oracle.fine6_fit(lt, (8, 8, 8), cprof, fit["grid"])
+        d, h, w = sub.shape[1:]
+        lt = np.zeros((T, 8, 8, 8), np.float32)
+        lt[:, :d, :h, :w] = sub
+        lt = np.ascontiguousarray(lt.reshape(T, 512).T)
+        fit = oracle.coarse_fit(lt, (w, h, d), cprof)
+        f6 = oracle.fine6_fit(lt, (w, h, d), cprof, fit["grid"])
         mode = route_leaf(raw, (8 * bx, 8 * by, 8 * bz), fit["grid"], f6["grid"], peak)
         word = mode | (4 << 6) | ((6 if mode == 3 else 0) << 9)          # FP16 keyframes in both streams
-        fine, nf = (pack(f6, 0), f6["key_frames"].size) if mode == 3 else (np.zeros(0, np.uint8), 0)
+        fine, nf = (pack(f6, 0), f6["key_frames"].size) if mode == 3 else (none, 0)
         blocks.append(reference.build_leaf(word, fit["key_frames"].size, nf, pack(fit, 0), fine).tobytes())
     offsets, payload = pack_payload(blocks)
-    header = b"VBTPACK4" + struct.pack("<11I", 4, 64, 64, 64, T, 8, 4, 0, 512, 1, 0)
+    header = b"VBTPACK4" + struct.pack("<11I", 4, X, Y, Z, T, 8, 4, 0, len(blocks), 1, 0)
     assert header + offsets.tobytes() + payload.tobytes() == open(path, "rb").read()
