@@ -127,6 +127,9 @@ class Oracle:
         L.vo_reconstruct.argtypes = [f32p, C.c_int, i32p, C.c_int, f32p]
         L.vo_fine6_fit.argtypes = [f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(VoKeyframeProfile), f32p, u32p,
                                    u8p, C.POINTER(C.c_uint16), f32p, C.c_int, C.POINTER(C.c_int), f32p]
+        L.vo_shell_fit.argtypes = [f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(VoKeyframeProfile), f32p,
+                                   C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, u8p, u32p, u8p,
+                                   C.POINTER(C.c_uint16), f32p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.vo_float_to_half_n.argtypes = [f32p, C.c_uint64, C.POINTER(C.c_uint16)]
         L.vo_coarse_fit.argtypes = [f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(VoKeyframeProfile), u32p, u8p,
                                     C.POINTER(C.c_uint16), f32p, C.c_int, C.POINTER(C.c_int), f32p]
@@ -167,6 +170,28 @@ class Oracle:
                                   _ptr(grid, f32p))
         return dict(desc=desc, bins=bins, key_frames=kf[:n].copy(), key_values=kv[:n].copy(),
                     required_max_local=req.value, grid=grid)
+
+    def shell_fit(self, leaf_recon, extent, profile, coarse_grid, levelset, surface_band, guard_band, temporal_band,
+                  shell_cut):
+        """The Mode2 shell stage of one leaf: dict of occupancy (80 bytes), desc [active], bins
+        [active, 8], key_frames, key_values, active, required_max_local."""
+        lt = np.ascontiguousarray(leaf_recon, np.float32).reshape(512, -1)
+        T = lt.shape[1]
+        cg = np.ascontiguousarray(coarse_grid, np.float32)
+        cap = 512 * max(T, 1)
+        occ = np.zeros(80, np.uint8)
+        desc = np.zeros(512, np.uint32)
+        bins = np.zeros((512, 8), np.uint8)
+        kf = np.zeros(cap, np.uint16)
+        kv = np.zeros(cap, np.float32)
+        act, req = C.c_int(), C.c_int()
+        n = self.lib.vo_shell_fit(_ptr(lt, f32p), T, *extent, C.byref(profile), _ptr(cg, f32p), int(levelset),
+                                  surface_band, guard_band, temporal_band, shell_cut, _ptr(occ, u8p), _ptr(desc, u32p),
+                                  _ptr(bins, u8p), _ptr(kf, C.POINTER(C.c_uint16)), _ptr(kv, f32p), cap, C.byref(act),
+                                  C.byref(req))
+        a = act.value
+        return dict(occupancy=occ, desc=desc[:a].copy(), bins=bins[:a].copy(), key_frames=kf[:n].copy(),
+                    key_values=kv[:n].copy(), active=a, required_max_local=req.value)
 
     def float_to_half(self, values):
         """renderTemporalFloatToHalfBits of every value (uint16 array)."""

@@ -472,3 +472,98 @@ int vo_fine6_fit(const float* lt, int frames, int w, int h, int d, const vo_keyf
     *required_max_local = required;
     return overflow ? -1 : nk;
 }
+
+/* The Mode2 shell stage (:930-1025): the shell voxels of a leaf (inside its extent) and, for each,
+ * the residual of the reconstruction over the fitted coarse grid, keyed with the control profile
+ * (plus, for a level set, addIsoSurfaceKeyFrames on the voxel's own series at 0 +- temporal_band),
+ * reconstructed, and appended to a 4-bin stream with its reconstruction's values at the keys.
+ * A voxel is a shell voxel when, at some frame, (level set) |value| <= surface_band, |coarse| <=
+ * guard_band or their signs differ, or (density) value >= shell_cut.  Writes the 80-byte occupancy
+ * section (8 x u64 voxel masks, 8 x u16 group prefixes), descriptors and 8-byte bin rows (first 4
+ * bytes used) per active voxel; returns the stream's key count (-1 beyond key_cap). */
+int vo_shell_fit(const float* lt, int frames, int w, int h, int d, const vo_keyframe_profile* p,
+                 const float* coarse_grid, int levelset, float surface_band, float guard_band, float temporal_band,
+                 float shell_cut, uint8_t* occupancy, uint32_t* desc, uint8_t* bins, uint16_t* key_frames,
+                 float* key_values, int key_cap, int* active_count, int* required_max_local)
+{
+    float* series = (float*)malloc((size_t)(frames > 0 ? frames : 1) * sizeof(float));
+    float* recon = (float*)malloc((size_t)(frames > 0 ? frames : 1) * sizeof(float));
+    int* keys = (int*)malloc((size_t)(frames > 0 ? frames : 1) * sizeof(int));
+    uint8_t* flag = (uint8_t*)malloc((size_t)(frames > 0 ? frames : 1));
+    int nk = 0, overflow = 0, active = 0;
+    uint8_t required = 1u;
+    memset(occupancy, 0, 80);
+    for (int group = 0; group < 8; ++group) {
+        const uint16_t prefix = (uint16_t)active;
+        memcpy(occupancy + 64 + 2 * group, &prefix, 2);
+        uint64_t word = 0;
+        for (int bit = 0; bit < 64; ++bit) {
+            const int v = group * 64 + bit, lx = v % 8, ly = (v / 8) % 8, lz = v / 64;
+            if (lx >= w || ly >= h || lz >= d) continue;
+            const float* truth = lt + (size_t)v * (size_t)frames;
+            int is_shell = 0;
+            for (int t = 0; t < frames && !is_shell; ++t) {
+                if (levelset) {
+                    const float c = kf_sample_grid(coarse_grid, 4, frames, t, w, h, d, (float)lx, (float)ly, (float)lz);
+                    is_shell = fabsf(truth[t]) <= surface_band || fabsf(c) <= guard_band ||
+                               (truth[t] >= 0.0f) != (c >= 0.0f);
+                } else {
+                    is_shell = truth[t] >= shell_cut;
+                }
+            }
+            if (!is_shell) continue;
+            word |= 1ull << bit;
+            for (int t = 0; t < frames; ++t)
+                series[t] = truth[t] - kf_sample_grid(coarse_grid, 4, frames, t, w, h, d, (float)lx, (float)ly, (float)lz);
+            int k = vo_detect_keyframes(series, frames, p, keys, NULL);
+            if (levelset) {   /* addIsoSurfaceKeyFrames(truth, 0, temporal_band, keys), then sorted and unique */
+                memset(flag, 0, (size_t)frames);
+                for (int i = 0; i < k; ++i) flag[keys[i]] = 1;
+                const float band = fmax_r(0.0f, temporal_band);
+                for (int t = 0; t < frames; ++t) {
+                    const float cur = truth[t] - 0.0f;
+                    if (fabsf(cur) <= band)
+                        for (int u = t - 1; u <= t + 1; ++u)
+                            if (u >= 0 && u < frames) flag[u] = 1;
+                    if (t > 0 && ((truth[t - 1] - 0.0f) >= 0.0f) != (cur >= 0.0f))
+                        for (int u = t - 2; u <= t + 1; ++u)
+                            if (u >= 0 && u < frames) flag[u] = 1;
+                }
+                k = 0;
+                for (int t = 0; t < frames; ++t)
+                    if (flag[t]) keys[k++] = t;
+            }
+            vo_reconstruct(series, frames, keys, k, recon);
+            uint8_t* b = bins + (size_t)active * 8u;
+            memset(b, 0, 8);
+            kf_bin_index(keys, k, frames, 4, b);
+            int local = 1;
+            for (int bin = 0; bin < 4; ++bin) {
+                const int next = bin + 1 < 4 ? (int)b[bin + 1] : k;
+                const int span = next - (int)b[bin] > 1 ? next - (int)b[bin] : 1;
+                if (span > local) local = span;
+                if (span > (int)required) required = (uint8_t)span;
+            }
+            desc[active] = (uint32_t)(uint16_t)nk | ((uint32_t)(k < 255 ? k : 255) << 16) |
+                           ((uint32_t)(local < 255 ? local : 255) << 24);
+            for (int i = 0; i < k; ++i) {
+                if (nk < key_cap) {
+                    key_frames[nk] = (uint16_t)keys[i];
+                    key_values[nk] = recon[keys[i]];
+                } else {
+                    overflow = 1;
+                }
+                ++nk;
+            }
+            ++active;
+        }
+        memcpy(occupancy + 8 * group, &word, 8);
+    }
+    free(series);
+    free(recon);
+    free(keys);
+    free(flag);
+    *active_count = active;
+    *required_max_local = required;
+    return overflow ? -1 : nk;
+}

@@ -135,6 +135,10 @@ int vo_coarse_fit(const float* leaf_recon, int frames, int w, int h, int d, cons
                   uint32_t* desc, uint8_t* bins, uint16_t* key_frames, float* key_values, int key_cap,
                   int* required_max_local, float* grid);
 void vo_float_to_half_n(const float* v, uint64_t n, uint16_t* out);
+int vo_shell_fit(const float* leaf_recon, int frames, int w, int h, int d, const vo_keyframe_profile* control_profile,
+                 const float* coarse_grid, int levelset, float surface_band, float guard_band, float temporal_band,
+                 float shell_cut, uint8_t* occupancy80, uint32_t* desc, uint8_t* bins, uint16_t* key_frames,
+                 float* key_values, int key_cap, int* active_count, int* required_max_local);
 int vo_fine6_fit(const float* leaf_recon, int frames, int w, int h, int d, const vo_keyframe_profile* control_profile,
                  const float* coarse_grid, uint32_t* desc, uint8_t* bins, uint16_t* key_frames, float* key_values,
                  int key_cap, int* required_max_local, float* grid);

@@ -225,19 +225,23 @@ def route_leaf(raw, base, grid_coarse, grid_fine, peak, step=8, cutoff=F32(0.000
     return 3 if rough and sensitive and gain >= float(F32(0.05)) else 1
 
 
-FILES = {   # name: (blobs arguments of tests/golden/make_assets.py, dims)
-    "cfg1_blobs": (((64, 64, 64), 24, 6, 1), (64, 64, 64)),
-    "tiny_density": (((20, 12, 17), 9, 3, 11), (20, 12, 17)),
+FILES = {   # name: (field recipe of tests/golden/make_assets.py, dims, level set)
+    "cfg1_blobs": (("blobs", ((64, 64, 64), 24, 6, 1)), (64, 64, 64), False),
+    "tiny_density": (("blobs", ((20, 12, 17), 9, 3, 11)), (20, 12, 17), False),
+    "tiny_levelset": (("sdf_scene", ((24, 20, 28), 12, 12.0, 2.0, 0.3, 3, 2.0, 5.0, 12)), (24, 20, 28), True),
+    "cfg4_sdf_small": (("sdf_scene", ((64, 64, 64), 24, 24.0, 2.0, 0.2, 6, 3.0, 8.0, 4)), (64, 64, 64), True),
 }
 
 
 @pytest.mark.parametrize("name", sorted(FILES))
-def test_density_file_regenerated_from_the_raw_field(oracle, reference, name):
-    """A whole density VBTPACK4 file from its raw field: per-voxel pass, EMPTY test, coarse fit, FINE6
-    fit, route, leaf packing (reference packer) and the file layout (52-byte header, word offsets,
-    payload) -- byte for byte the file the reference encoder wrote (config 1, and a small field whose
-    boundary leaves are cropped)."""
-    args, (X, Y, Z) = FILES[name]
+def test_file_regenerated_from_the_raw_field(oracle, reference, name):
+    """A whole VBTPACK4 file from its raw field, byte for byte the file the reference encoder wrote:
+    the per-voxel pass, the EMPTY test, the coarse fit, then per leaf either (density) the FINE6 fit
+    and the route between GRID4 and FINE6, or (level set: shell width 3 voxels, coarse guard band
+    1.5, temporal band 0.1) the Mode2 shell stage (vo_shell_fit), a Mode2 leaf wherever it finds shell
+    voxels; leaf packing by the reference packer and the file layout (52-byte header, word offsets,
+    payload).  Config 1, a small density field with cropped boundary leaves, and two level sets."""
+    (fn, args), (X, Y, Z), levelset = FILES[name]
     path = os.path.join(GOLDEN, "assets", name + ".vbtp")
     if not os.path.exists(path):
         path = os.path.join(ASSETS, name + ".vbtp")
@@ -246,19 +250,19 @@ def test_density_file_regenerated_from_the_raw_field(oracle, reference, name):
     import struct
     from oracle.oracle import VoKeyframeProfile, pack_payload
     sys.path.insert(0, GOLDEN)
-    from make_assets import blobs
-    raw = blobs(*args)
+    import make_assets
+    raw = getattr(make_assets, fn)(*args)
     T = raw.shape[0]
     peak = float(max(F32(1e-6), F32(F32(raw.max()) - F32(raw.min()))))
-    prof = VoKeyframeProfile()
+    prof, cprof = levelset_profiles() if levelset else (VoKeyframeProfile(), control_profile())
     recon = oracle.keyframe_pass(raw.reshape(T, -1), prof)["recon"].reshape(T, Z, Y, X)
-    cprof = control_profile()
 
-    def pack(fit, codec):
+    def pack(fit, codec, bins=8):
         d = fit["desc"]
         triples = np.stack([d & 0xFFFF, (d >> 16) & 0xFF, d >> 24], axis=1).astype(np.uint32).reshape(-1)
-        return reference.pack_stream(codec, triples, fit["bins"].reshape(-1), fit["key_frames"].astype(np.uint32),
-                                     fit["key_values"], 8, max_local=fit["required_max_local"])
+        return reference.pack_stream(codec, triples, fit["bins"][:, :bins].reshape(-1),
+                                     fit["key_frames"].astype(np.uint32), fit["key_values"], bins,
+                                     max_local=fit["required_max_local"])
 
     lcx, lcy, lcz = (X + 7) // 8, (Y + 7) // 8, (Z + 7) // 8
     none = np.zeros(0, np.uint8)
@@ -266,19 +270,29 @@ def test_density_file_regenerated_from_the_raw_field(oracle, reference, name):
     for li in range(lcx * lcy * lcz):
         bx, by, bz = li % lcx, (li // lcx) % lcy, li // (lcx * lcy)
         sub = recon[:, 8 * bz:8 * bz + 8, 8 * by:8 * by + 8, 8 * bx:8 * bx + 8]
-        if max(0.0, float(sub.max())) < prof.bg_threshold:       # EMPTY: the default header, coarse res 4
-            blocks.append(reference.build_leaf(4 << 6, 0, 0, none, none).tobytes())
+        if prof.bg_threshold >= 0 and max(0.0, float(sub.max())) < prof.bg_threshold:
+            blocks.append(reference.build_leaf(4 << 6, 0, 0, none, none).tobytes())   # EMPTY, default header
             continue
         d, h, w = sub.shape[1:]
         lt = np.zeros((T, 8, 8, 8), np.float32)
         lt[:, :d, :h, :w] = sub
         lt = np.ascontiguousarray(lt.reshape(T, 512).T)
         fit = oracle.coarse_fit(lt, (w, h, d), cprof)
-        f6 = oracle.fine6_fit(lt, (w, h, d), cprof, fit["grid"])
-        mode = route_leaf(raw, (8 * bx, 8 * by, 8 * bz), fit["grid"], f6["grid"], peak)
-        word = mode | (4 << 6) | ((6 if mode == 3 else 0) << 9)          # FP16 keyframes in both streams
-        fine, nf = (pack(f6, 0), f6["key_frames"].size) if mode == 3 else (none, 0)
-        blocks.append(reference.build_leaf(word, fit["key_frames"].size, nf, pack(fit, 0), fine).tobytes())
+        coarse = pack(fit, 0)
+        if levelset:
+            sh = oracle.shell_fit(lt, (w, h, d), cprof, fit["grid"], True, 3.0, 1.5, float(F32(0.1) * F32(1.0)), 0.0)
+            if sh["active"] > 0:
+                leaf = reference.build_leaf(2 | (4 << 6), fit["key_frames"].size, sh["key_frames"].size, coarse,
+                                            pack(sh, 0, bins=4), sh["occupancy"])
+            else:
+                leaf = reference.build_leaf(1 | (4 << 6), fit["key_frames"].size, 0, coarse, none)
+        else:
+            f6 = oracle.fine6_fit(lt, (w, h, d), cprof, fit["grid"])
+            mode = route_leaf(raw, (8 * bx, 8 * by, 8 * bz), fit["grid"], f6["grid"], peak)
+            word = mode | (4 << 6) | ((6 if mode == 3 else 0) << 9)          # FP16 keyframes in both streams
+            fine, nf = (pack(f6, 0), f6["key_frames"].size) if mode == 3 else (none, 0)
+            leaf = reference.build_leaf(word, fit["key_frames"].size, nf, coarse, fine)
+        blocks.append(leaf.tobytes())
     offsets, payload = pack_payload(blocks)
     header = b"VBTPACK4" + struct.pack("<11I", 4, X, Y, Z, T, 8, 4, 0, len(blocks), 1, 0)
     assert header + offsets.tobytes() + payload.tobytes() == open(path, "rb").read()
