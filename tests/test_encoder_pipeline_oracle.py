@@ -226,6 +226,7 @@ def route_leaf(raw, base, grid_coarse, grid_fine, peak, step=8, cutoff=F32(0.000
 
 
 FILES = {   # name: (field recipe of tests/golden/make_assets.py, dims, level set)
+    "cfg2_plume": (("plume", (256, 96, 2)), (256, 256, 256), False),   # ~2 minutes, 14 GB of host memory
     "cfg1_blobs": (("blobs", ((64, 64, 64), 24, 6, 1)), (64, 64, 64), False),
     "tiny_density": (("blobs", ((20, 12, 17), 9, 3, 11)), (20, 12, 17), False),
     "tiny_levelset": (("sdf_scene", ((24, 20, 28), 12, 12.0, 2.0, 0.3, 3, 2.0, 5.0, 12)), (24, 20, 28), True),
@@ -240,7 +241,8 @@ def test_file_regenerated_from_the_raw_field(oracle, reference, name):
     and the route between GRID4 and FINE6, or (level set: shell width 3 voxels, coarse guard band
     1.5, temporal band 0.1) the Mode2 shell stage (vo_shell_fit), a Mode2 leaf wherever it finds shell
     voxels; leaf packing by the reference packer and the file layout (52-byte header, word offsets,
-    payload).  Config 1, a small density field with cropped boundary leaves, and two level sets."""
+    payload).  The config-2 plume (256^3 x 96, 88 % EMPTY leaves, 72 MB), config 1, a small density field
+    with cropped boundary leaves, and two level sets."""
     (fn, args), (X, Y, Z), levelset = FILES[name]
     path = os.path.join(GOLDEN, "assets", name + ".vbtp")
     if not os.path.exists(path):
