@@ -231,6 +231,8 @@ FILES = {   # name: (field recipe of tests/golden/make_assets.py, dims, level se
     "tiny_density": (("blobs", ((20, 12, 17), 9, 3, 11)), (20, 12, 17), False),
     "tiny_levelset": (("sdf_scene", ((24, 20, 28), 12, 12.0, 2.0, 0.3, 3, 2.0, 5.0, 12)), (24, 20, 28), True),
     "cfg4_sdf_small": (("sdf_scene", ((64, 64, 64), 24, 24.0, 2.0, 0.2, 6, 3.0, 8.0, 4)), (64, 64, 64), True),
+    "mix_fire_temperature": (("fire", ((128, 128, 192), 40, 7), 2), (128, 128, 192), False),   # 300-1800 K
+    "mix_sdf": (("sdf_scene", ((128, 128, 128), 48, 50.0, 12.0, 0.05, 20, 3.0, 12.0, 9)), (128, 128, 128), True),
 }
 
 
@@ -241,9 +243,9 @@ def test_file_regenerated_from_the_raw_field(oracle, reference, name):
     and the route between GRID4 and FINE6, or (level set: shell width 3 voxels, coarse guard band
     1.5, temporal band 0.1) the Mode2 shell stage (vo_shell_fit), a Mode2 leaf wherever it finds shell
     voxels; leaf packing by the reference packer and the file layout (52-byte header, word offsets,
-    payload).  The config-2 plume (256^3 x 96, 88 % EMPTY leaves, 72 MB), config 1, a small density field
-    with cropped boundary leaves, and two level sets."""
-    (fn, args), (X, Y, Z), levelset = FILES[name]
+    payload).  The config-2 plume (256^3 x 96, 88 % EMPTY leaves, 72 MB), config 1, the fire's
+    temperature field, a small density field with cropped boundary leaves, and three level sets."""
+    recipe, (X, Y, Z), levelset = FILES[name]
     path = os.path.join(GOLDEN, "assets", name + ".vbtp")
     if not os.path.exists(path):
         path = os.path.join(ASSETS, name + ".vbtp")
@@ -253,7 +255,9 @@ def test_file_regenerated_from_the_raw_field(oracle, reference, name):
     from oracle.oracle import VoKeyframeProfile, pack_payload
     sys.path.insert(0, GOLDEN)
     import make_assets
-    raw = getattr(make_assets, fn)(*args)
+    raw = getattr(make_assets, recipe[0])(*recipe[1])
+    if len(recipe) > 2:                                     # one field of a multi-field recipe
+        raw = raw[recipe[2]]
     T = raw.shape[0]
     peak = float(max(F32(1e-6), F32(F32(raw.max()) - F32(raw.min()))))
     prof, cprof = levelset_profiles() if levelset else (VoKeyframeProfile(), control_profile())
