@@ -293,8 +293,10 @@ int vbt_decode_control_values(const uint8_t* d_stream, uint32_t stream_bytes, ui
  * the same values as vbt_build_page_table / vbt_get_page_table (0xFFFFFFFF in *active_count means a
  * bounded device-side wait gave up).  Scratch is a fixed 512 KiB array inside the library, held by
  * every GPU that loads it, so leaf_count is limited to 16,777,216 (VBT_STATUS_LIMIT beyond).  The
- * first call on a device looks up that array's device address and should come before any stream
- * capture.  All calls share the array: calls whose kernels overlap on the GPU race. */
+ * first call on a device looks up that array's device address (for the device's primary context;
+ * after cudaDeviceReset the entry point must not be called again on that device) and should come
+ * before any stream capture.  profile_type above 2 is VBT_STATUS_INVALID_ARGUMENT, as the reader
+ * rejects it.  All calls share the array: calls whose kernels overlap on the GPU race. */
 int vbt_build_page_table_noalloc(const uint32_t* d_offsets, const uint32_t* d_payload, uint64_t payload_words,
                                  uint32_t leaf_count, uint32_t profile_type, uint32_t* d_compact,
                                  uint32_t* d_active_list, uint32_t* d_active_count, void* stream);

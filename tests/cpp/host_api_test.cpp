@@ -344,6 +344,33 @@ void stream_tests()
     auto zero = make_stream(20, 8, 0, true);
     zero.maxBinLocalKeys = 0;
     require(!vbt::validateRenderTemporalControlStreamData(zero), "maxBinLocalKeys 0 must not validate");
+
+    // A keyframe count whose byte size wraps the reference's 32-bit extent (2^29 FP32 keys of 8
+    // bytes = 2^32 = 0): the reference's check passes and it would read keys past the stream.
+    // The value decode refuses it on the host, before any device work, with the extent message;
+    // a control without keys still decodes to 0, and an out-of-range descriptor or key range keeps
+    // the reference's own message.
+    {
+        std::vector<uint8_t> st(64, 0u);
+        st[0] = 0u, st[1] = 0u, st[2] = 2u;   // control 0: keyStart 0, keyCount 2
+        const uint32_t wrap_kf = 1u << 29;
+        const auto fp32 = vbt::RenderTemporalSequenceCodec::DP_KEYFRAME_FP32;
+        expect_throw([&] { vbt::decodeRenderTemporalControlValue(st.data(), fp32, 2, 8, 0, wrap_kf, 64, true, 10, 0, 3); },
+                     "render temporal stream decode out of bounds");
+        expect_throw(
+            [&] { vbt::decodeRenderTemporalControlValues(st.data(), fp32, 2, 8, wrap_kf, 64, true, 10, {1, 0}, {0, 3}); },
+            "render temporal stream decode out of bounds");
+        require(vbt::decodeRenderTemporalControlValue(st.data(), fp32, 2, 8, 0, wrap_kf, 64, true, 10, 1, 3) == 0.0f,
+                "a control without keys decodes to 0 without reading keys");
+        st[2] = 0u;
+        const auto zeros = vbt::decodeRenderTemporalControlValues(st.data(), fp32, 2, 8, wrap_kf, 64, true, 10, {0, 1}, {0, 5});
+        require(zeros.size() == 2 && zeros[0] == 0.0f && zeros[1] == 0.0f, "controls without keys decode to 0");
+        st[0] = 1u, st[2] = 1u;   // keyStart 1 + keyCount 1 > keyframeCount 1
+        expect_throw([&] { vbt::decodeRenderTemporalControlValue(st.data(), fp32, 2, 8, 0, 1, 64, true, 10, 0, 3); },
+                     "render temporal keyframe range out of bounds");
+        expect_throw([&] { vbt::decodeRenderTemporalControlValue(st.data(), fp32, 2, 8, 0, 1, 64, true, 10, 2, 3); },
+                     "render temporal control index out of range");
+    }
 }
 
 // ------------------------------------------------ tests/vbt_file_tests.cpp

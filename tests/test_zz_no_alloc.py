@@ -73,3 +73,11 @@ def test_noalloc_rejects_too_many_leaves(vbt, cuda):
     with pytest.raises(vbt.VbtError) as ei:
         vbt.build_page_table_noalloc(d, d, 16, (1 << 24) + 1, 1, d, d, d)
     assert ei.value.status == 43 and "16777216" in ei.value.message
+
+
+def test_noalloc_rejects_unknown_profile(vbt, cuda):
+    d = cuda.zeros(16, dtype=cuda.int32, device="cuda")
+    for profile in (3, 7):
+        with pytest.raises(vbt.VbtError) as ei:
+            vbt.build_page_table_noalloc(d, d, 16, 4, profile, d, d, d)
+        assert ei.value.status == 40 and "profile type" in ei.value.message

@@ -162,6 +162,34 @@ namespace vbtb {
 int set_last_error(int status, const std::string& msg) { return fail(status, msg); }
 }  // namespace vbtb
 
+// Launch-shape facts taken from a render-temporal image's route tags and leaf sizes (nothing is
+// read from the device):
+//  - sparse: fewer than half of the leaves non-EMPTY (the point-query kernel's shape hint);
+//  - the shared-memory leaf stage of the render decode kernel: the largest 16-byte-aligned window
+//    of a non-EMPTY leaf, capped so that two CTAs fit on an SM (232,448 B of shared memory per SM
+//    less 1 KiB per CTA); an asset with bigger leaves gets the kernel variant that decodes those
+//    from global memory.
+// Computed at creation and again for every re-uploaded image, whose leaves may differ in size.
+static void image_shape(const vbt_header& h, const uint8_t* b, uint64_t off_off, uint64_t pay_off, uint64_t words,
+                        AssetGeom& g, bool& sparse)
+{
+    if (h.profile_type == 2u) return;
+    const uint8_t* off = b + off_off;
+    uint64_t active = 0, maxw = 0;
+    for (uint32_t i = 0; i < h.leaf_count; ++i) {
+        const uint64_t w0 = rd32(off + 4ull * i), w1 = rd32(off + 4ull * (i + 1));
+        if (w1 <= w0 || w0 >= words || (rd32(b + pay_off + 4ull * w0) & 3u) == 0u) continue;
+        ++active;
+        const uint64_t a0 = (4ull * w0) & ~15ull, a1 = (4ull * w1 + 15u) & ~15ull;
+        maxw = std::max(maxw, a1 - a0);
+    }
+    sparse = 2u * active < (uint64_t)h.leaf_count;
+    g.sparse = sparse ? 1u : 0u;
+    g.max_window = (uint32_t)std::min<uint64_t>(maxw, 0xFFFFFFFFull);
+    const uint32_t cap = ((233472u / 2u - 1024u - kLeafFixedBytes - 16u) / 1024u) * 1024u;
+    g.stage_bytes = std::min<uint32_t>(std::max<uint32_t>((g.max_window + 1023u) & ~1023u, 4096u), cap);
+}
+
 extern "C" {
 
 const char* vbt_status_string(int s)
@@ -225,15 +253,6 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     const uint64_t scale_off = 52, off_off = scale_off + 4ull * h.coarse_ac_scale_count;
     const uint64_t pay_off = off_off + 4ull * ((uint64_t)h.leaf_count + 1u);
     const uint64_t words = (len - pay_off) / 4u;
-    if (h.profile_type != 2u) {   // route tags of the leaves (word 0 of each non-empty block): a shape hint only
-        uint64_t active = 0;
-        for (uint32_t i = 0; i < h.leaf_count; ++i) {
-            const uint32_t w0 = rd32(b + off_off + 4ull * i), w1 = rd32(b + off_off + 4ull * i + 4u);
-            if (w1 > w0 && w0 < words && (rd32(b + pay_off + 4ull * w0) & 3u) != 0u) ++active;
-        }
-        a->sparse = 2u * active < (uint64_t)h.leaf_count;
-        a->dev.g.sparse = a->sparse ? 1u : 0u;
-    }
     AssetGeom& g = a->dev.g;
     g.width = h.width;
     g.height = h.height;
@@ -246,23 +265,7 @@ int vbt_asset_create(const void* file_bytes, uint64_t len, int device, vbt_asset
     g.profile = h.profile_type;
     g.scale_count = h.coarse_ac_scale_count;
     g.payload_words = words;
-    // Shared-memory leaf stage of the render decode kernel: the largest 16-byte-aligned window of a
-    // non-EMPTY leaf, capped so that two CTAs fit on an SM (232,448 B of shared memory per SM
-    // less 1 KiB per CTA); an asset with bigger leaves gets the kernel variant that decodes those
-    // from global memory.
-    if (h.profile_type != 2u) {
-        const uint8_t* off = b + off_off;
-        uint64_t maxw = 0;
-        for (uint32_t i = 0; i < h.leaf_count; ++i) {
-            const uint64_t w0 = rd32(off + 4ull * i), w1 = rd32(off + 4ull * (i + 1));
-            if ((rd32(b + pay_off + 4ull * w0) & 3u) == 0u) continue;
-            const uint64_t a0 = (4ull * w0) & ~15ull, a1 = (4ull * w1 + 15u) & ~15ull;
-            maxw = std::max(maxw, a1 - a0);
-        }
-        g.max_window = (uint32_t)std::min<uint64_t>(maxw, 0xFFFFFFFFull);
-        const uint32_t cap = ((233472u / 2u - 1024u - kLeafFixedBytes - 16u) / 1024u) * 1024u;
-        g.stage_bytes = std::min<uint32_t>(std::max<uint32_t>((g.max_window + 1023u) & ~1023u, 4096u), cap);
-    }
+    image_shape(h, b, off_off, pay_off, words, g, a->sparse);
     const uint32_t L = h.leaf_count;
     const uint32_t tiles = (L + kWalkTile - 1) / kWalkTile;
     void *d_off, *d_pay, *d_scales, *d_basis, *d_entries, *d_compact, *d_list, *d_counters, *d_err, *d_tiles, *d_sorted,
@@ -366,7 +369,15 @@ int vbt_asset_upload(vbt_asset* a, const void* file_bytes, uint64_t len, void* s
     const uint64_t pay_off = off_off + 4ull * ((uint64_t)h.leaf_count + 1u);
     if (len != pay_off + 4ull * a->dev.g.payload_words)
         return fail(VBT_STATUS_INVALID_ARGUMENT, "image size differs from the asset's");
+    // the new image's leaves may be larger than the old ones: the stage and the kernel variant
+    // follow the image, and timeline graphs captured with the old shape are dropped
+    AssetGeom g = a->dev.g;
+    bool sparse = a->sparse;
+    image_shape(h, b, off_off, pay_off, a->dev.g.payload_words, g, sparse);
     DeviceGuard guard(a->device);
+    if (g.stage_bytes != a->dev.g.stage_bytes || g.max_window != a->dev.g.max_window) release_timeline_graphs(a);
+    a->dev.g = g;
+    a->sparse = sparse;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (h.coarse_ac_scale_count)
         CUDA_TRY(cudaMemcpyAsync((void*)a->dev.scales, b + 52, 4ull * h.coarse_ac_scale_count, cudaMemcpyHostToDevice, s));

@@ -114,9 +114,14 @@ void gpu_decode(const uint8_t* stream, uint32_t bytes, RenderTemporalSequenceCod
 }
 
 // The reference's pre-decode checks of decodeRenderTemporalControlValue
-// (src/render_temporal_decode.cpp:316-327), in its order; returns the stream's real extent.
-uint32_t checked_extent(uint16_t controlCount, uint8_t timeBinCount, uint32_t keyframeCount, uint32_t streamBytes,
-                        bool align, RenderTemporalSequenceCodec codec, uint32_t controlIndex)
+// (src/render_temporal_decode.cpp:316-340), in its order, run on the host bytes: control index,
+// stream extent (32-bit, as the reference computes it), descriptor in bounds, key range.  Returns
+// the bytes the device needs, or 0 when the control has no keys (its value is 0 and no launch is
+// needed).  Where the reference's 32-bit extent wraps (a keyframe count near 2^32 / stride) it
+// would read keys past the stream; here that case is refused with its extent message before any
+// key is read, and the descriptor-only cases keep the reference's results.
+uint32_t checked_extent(const uint8_t* base, uint16_t controlCount, uint8_t timeBinCount, uint32_t keyframeCount,
+                        uint32_t streamBytes, bool align, RenderTemporalSequenceCodec codec, uint32_t controlIndex)
 {
     if (controlIndex >= controlCount) throw_status(VBT_STATUS_CONTROL_INDEX);
     const uint32_t desc = static_cast<uint32_t>(controlCount) * kRenderTemporalControlDescriptorBytes;
@@ -128,6 +133,14 @@ uint32_t checked_extent(uint16_t controlCount, uint8_t timeBinCount, uint32_t ke
     }
     const uint32_t total = desc + bins + keys;
     if (total > streamBytes) throw_status(VBT_STATUS_STREAM_OOB);
+    if (static_cast<uint64_t>(controlIndex) * 4u + 4u > streamBytes) throw_status(VBT_STATUS_DECODE_OOB);
+    const uint8_t* d = base + static_cast<size_t>(controlIndex) * 4u;
+    const uint32_t keyStart = d[0] | (static_cast<uint32_t>(d[1]) << 8), keyCount = d[2];
+    if (keyCount == 0u) return 0u;
+    if (keyStart + keyCount > keyframeCount) throw_status(VBT_STATUS_KEY_RANGE_OOB);
+    const uint64_t keys_wide = static_cast<uint64_t>(keyframeCount) * renderTemporalKeyframeBytes(codec);
+    const uint64_t wide = static_cast<uint64_t>(desc) + bins + (align ? ((keys_wide + 3u) & ~3ull) : keys_wide);
+    if (wide > streamBytes) throw_status(VBT_STATUS_STREAM_OOB);
     return total;
 }
 
@@ -490,7 +503,8 @@ std::vector<float> decodeRenderTemporalControlValues(const uint8_t* base, Render
     if (ci.size() != frames.size()) throw std::invalid_argument("controlIndex and frameIndex sizes differ");
     if (ci.empty()) return {};
     uint32_t extent = 0;
-    for (uint16_t c : ci) extent = checked_extent(cc, bins, kf, streamBytes, align, codec, c);
+    for (uint16_t c : ci) extent = std::max(extent, checked_extent(base, cc, bins, kf, streamBytes, align, codec, c));
+    if (extent == 0u) return std::vector<float>(ci.size(), 0.0f);   // no control has keys
     std::vector<uint32_t> c32(ci.begin(), ci.end());
     std::vector<int32_t> f32(frames.begin(), frames.end());
     std::vector<float> out(ci.size());
@@ -507,7 +521,8 @@ float decodeRenderTemporalControlValue(const uint8_t* base, RenderTemporalSequen
                                        uint32_t kf, uint32_t streamBytes, bool align, int totalFrames,
                                        uint16_t controlIndex, int frameIndex)
 {
-    const uint32_t extent = checked_extent(cc, bins, kf, streamBytes, align, codec, controlIndex);
+    const uint32_t extent = checked_extent(base, cc, bins, kf, streamBytes, align, codec, controlIndex);
+    if (extent == 0u) return 0.0f;   // a control without keys decodes to 0
     const uint32_t c = controlIndex;
     const int32_t f = frameIndex;
     float out = 0.0f;

@@ -105,7 +105,10 @@ __global__ void __launch_bounds__(kTile) page_table_noalloc_kernel(const uint32_
     }
 }
 
-// Device address of the scratch array, looked up once per device with that device current.
+// Device address of the scratch array, looked up once per device with that device current.  The
+// address belongs to the device's primary context, the one the CUDA runtime uses; a process that
+// destroys that context (cudaDeviceReset) must not call the entry point again on that device,
+// because the cached address would then name memory that is no longer mapped.
 std::mutex g_setup_mu;
 unsigned long long* g_scratch_ptr[64] = {};
 
@@ -139,6 +142,8 @@ int vbt_build_page_table_noalloc(const uint32_t* d_offsets, const uint32_t* d_pa
     if (leaf_count == 0 || !d_offsets || !d_compact || !d_active_list || !d_active_count ||
         (profile_type != 2u && !d_payload))
         return vbtb::set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null buffer or zero leaf count");
+    if (profile_type > 2u)
+        return vbtb::set_last_error(VBT_STATUS_INVALID_ARGUMENT, "Invalid VBTPACK4 profile type.");
     if ((uint64_t)leaf_count > kNoAllocMaxLeaves)
         return vbtb::set_last_error(VBT_STATUS_LIMIT, "leaf_count " + std::to_string(leaf_count) +
                                                           " exceeds the allocation-free page table's limit of " +

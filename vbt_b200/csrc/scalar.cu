@@ -36,6 +36,11 @@ __device__ int checked_decode(const CheckedStream& s, uint32_t ci, int frame_ind
     const uint32_t kc = b8(s, 4ull * ci + 2);
     if (kc == 0u) return kOk;
     if (ks + kc > s.kf) return kErrKeyRangeOob;
+    // The check above is the reference's, in 32-bit arithmetic: a keyframe count near 2^32 / stride
+    // wraps it and the reference then reads keys past the stream.  Here no key is read unless the
+    // stream's true extent, in 64 bits, fits.
+    const uint64_t keyb_wide = s.align ? (((uint64_t)s.kf * stride + 3u) & ~3ull) : (uint64_t)s.kf * stride;
+    if ((uint64_t)descb + binb + keyb_wide > s.bytes) return kErrStreamOob;
     const uint64_t kb = descb + binb;
     const uint64_t lb = descb + (uint64_t)ci * s.bins;
     auto kframe = [&](uint32_t i) -> int {
