@@ -75,9 +75,17 @@ class VoLeafView(C.Structure):
                 ("shell_residual_off", C.c_uint32), ("shell_residual_bytes", C.c_uint32)]
 
 
+def reference_tree():
+    """The VBT source tree the _ref targets compile (VBT_REFERENCE_TREE, default: a "reference"
+    directory beside this repository), or None where it is absent."""
+    ref = os.environ.get("VBT_REFERENCE_TREE", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+    return ref if os.path.isdir(os.path.join(ref, "src")) else None
+
+
 def build(ref=False):
     """Build liboracle.so (and, when the reference tree exists, oracle/_ref)."""
-    targets = ["oracle"] + (["ref"] if ref else [])
+    tree = reference_tree() if ref else None
+    targets = ["oracle"] + (["ref", "REF=" + tree] if tree else [])
     subprocess.check_call(["make", "-s", "-C", HERE, "-j8"] + targets)
 
 

@@ -190,7 +190,9 @@ def grf_scientific(shape_xyz, frames, seed, spike_frac=0.001, spike_sigma=10.0):
 def encode(name, data, xyzt, profile, extra_meta=None, time_fastest=False):
     os.makedirs(ASSETS, exist_ok=True)
     if not os.path.exists(ENCODER):
-        subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "ref"])
+        sys.path.insert(0, ROOT)
+        from oracle.oracle import build
+        build(ref=True)
     X, Y, Z, T = xyzt
     with tempfile.TemporaryDirectory(dir=os.environ.get("VBT_ASSET_TMP")) as td:
         raw = os.path.join(td, name + ".raw")

@@ -9,7 +9,7 @@
 //  (c) query_*_kernel       batched (x, y, z, t) point queries and z-slice queries.
 //
 // Render-temporal arithmetic is bit-exact with the reference CPU decoder (every float op is an
-// explicitly rounded _rn intrinsic; see rt_decode.cuh).  Scientific coarse controls are summed in
+// explicitly rounded _rn intrinsic; see rt_search.cuh).  Scientific coarse controls are summed in
 // compensated float-float arithmetic (error-free products and two-sums) to track the reference's
 // double accumulation (render/src/scientific_decode.cpp:82-97) without FP64 on the device.
 #include <cuda/atomic>
@@ -17,7 +17,7 @@
 #include <mutex>
 
 #include "kernels.cuh"
-#include "rt_decode.cuh"
+#include "rt_search.cuh"
 
 namespace vbtb {
 
@@ -30,7 +30,7 @@ __constant__ AxisWeight c_sci_axis[3][8];
 
 #include <cuda_fp16.h>
 
-#include "rt_decode_v3.cuh"
+#include "rt_staged.cuh"
 
 namespace vbtb {
 

@@ -1,4 +1,5 @@
-// rt_decode.cuh -- device-side decode of render-temporal control streams.
+// rt_search.cuh -- device-side decode of render-temporal control streams from the payload
+// (the reference search, one control at one frame).
 //
 // A control stream is [desc u32 x C][bins u8 x C*B, pad 4][keyframes, pad 4].  Decoding one
 // control at one frame follows src/render_temporal_decode.cpp:79-131 (decodeFromSequence):

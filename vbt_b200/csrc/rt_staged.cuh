@@ -1,18 +1,62 @@
-// rt_decode_v3.cuh -- render-temporal decode from a shared-memory copy of the leaf.
+// rt_staged.cuh -- render-temporal leaf decode from a shared-memory copy of the leaf (or, for
+// leaves larger than the stage, straight from the payload through the same word reader).
 //
-// One CTA decodes one leaf for every frame of the launch.  The leaf's bytes are brought into
-// shared memory by a single TMA bulk copy (cp.async.bulk, completion on an mbarrier), so the
-// per-control keyframe walks -- chains of dependent 3-byte reads -- run at shared-memory latency
-// instead of L2 latency.  The copied window is the leaf rounded out to 16-byte boundaries (the
-// payload allocation is 16-byte aligned and padded by 16 bytes, so the window never leaves it).
-// Leaves larger than the stage are decoded the same way straight from global memory.
+// The leaf's bytes are brought into shared memory by one TMA bulk copy (cp.async.bulk,
+// completion on an mbarrier), so the per-control keyframe walks -- chains of dependent 3-byte
+// reads -- run at shared-memory latency instead of L2 latency.  The copied window is the leaf
+// rounded out to 16-byte boundaries (the payload allocation is 16-byte aligned and padded by 16
+// bytes, so the window never leaves it).
 //
-// All decode arithmetic is shared with rt_decode_v2.cuh: cursor walks for leaves whose key frames
-// strictly increase, the reference's hinted bracket search otherwise, and the separable trilinear.
+// Controls: leaves whose key frames strictly increase (checked once per asset) are walked by a
+// cursor that reads each key once -- for such keys the reference's hinted bracket search returns
+// the first key's value before it, the last key's value after it, the key's value on an exact hit
+// and v0 + a (v1 - v0) with a = (t - f0) / (f1 - f0) for the adjacent pair around t, so a cursor
+// k = "first key with frame > t" that only moves forward yields the same bits; other leaves, and
+// frame lists that go backwards, use the reference's search (src/render_temporal_decode.cpp:79-131).
+//
+// Voxels: the reference's trilinear (render/src/render_smoke_vbt_bench_main.cpp:236-267) lerps
+// along x first, then y, then z:  c00 = lerp_x(g[z0][y0][x0], g[z0][y0][x1]), c0 = lerp_y(c00,
+// c10), v = lerp_z(c0, c1).  The x-lerp depends only on (lx, control row y, control row z), and
+// the y-lerp only on (lx, ly, control row z), so they are computed once per leaf and frame
+// (R*R*8 and R*64 lerps) and shared by every voxel that uses them: the same operations on the
+// same operands in the same order, hence the same bits, with 4-6x fewer lerps than per voxel.
 #pragma once
-#include "rt_decode_v2.cuh"
+#include <cuda_fp16.h>
+
+#include "rt_search.cuh"
 
 namespace vbtb {
+
+// Two lerps side by side, each a*(1-t) + b*t rounded after every operation.  Scalar _rn
+// operations on purpose: a packed FP32x2 multiply followed by a packed add is contracted into a
+// packed FMA by this toolkit's assembler even when both carry .rn (measured on sm_100a: every
+// packed multiply and every packed add alone rounds like the scalar one, the pair does not),
+// which would break bit-equality with the reference's separately rounded float arithmetic.
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b)
+{
+    return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+}
+
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t, float2 omt)
+{
+    return make_float2(__fadd_rn(__fmul_rn(a.x, omt.x), __fmul_rn(b.x, t.x)),
+                       __fadd_rn(__fmul_rn(a.y, omt.y), __fmul_rn(b.y, t.y)));
+}
+
+// binary16 -> binary32 with the hardware conversion; NaNs keep their payload bits exactly as
+// src/render_temporal_decode.cpp:167-199 maps them.
+__device__ __forceinline__ float half_to_float_exact(uint32_t h)
+{
+    const float f = __half2float(__ushort_as_half((unsigned short)h));
+    const bool nan = (h & 0x7C00u) == 0x7C00u && (h & 0x3FFu) != 0u;
+    return nan ? __uint_as_float(((h & 0x8000u) << 16) | 0x7F800000u | ((h & 0x3FFu) << 13)) : f;
+}
+
+__device__ __forceinline__ uint32_t row_byte(uint32_t r0, uint32_t r1, uint32_t b)
+{
+    return ((b < 4u ? r0 : r1) >> ((b & 3u) * 8u)) & 0xFFu;
+}
+
 
 // Word readers: global (read-only path) or a shared-memory window that starts at word `w0`.
 struct GlobalWords {
@@ -65,15 +109,15 @@ struct FrameBatch {
     int nb;
 };
 
-// Cursor walk (strictly increasing key frames, non-decreasing frames); see
-// decode_control_cursor in rt_decode_v2.cuh for why it equals the reference's search.
+// Cursor walk (strictly increasing key frames, non-decreasing frames); see the
+// head of this file for why it equals the reference's search.
 template <class M>
 __device__ __forceinline__ void m_control_cursor(const M& m, const StreamRef& s, uint32_t c, const FrameBatch& fb,
                                                  float* dst, int stride)
 {
     const uint32_t desc = m((uint32_t)((s.base + 4ull * c) >> 2));
     const uint32_t kc = (desc >> 16) & 0xFFu;
-    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {   // see decode_control (rt_decode.cuh)
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {   // see decode_control (rt_search.cuh)
         for (int j = 0; j < fb.nb; ++j) dst[j * stride] = 0.0f;
         return;
     }
@@ -157,8 +201,8 @@ __device__ __forceinline__ void m_key_read_nb(const M& m, uint64_t kb, uint32_t 
 // reciprocal RN(1/b) (`rcp`, a table of RN(1/i) for i < 256) and the difference v1 - v0 are
 // formed once; per frame the value is v0 + RN(RN((t - f0) / b) * (v1 - v0)), the quotient by
 // div_small_rn, the first key's value before it, the last key's after it and the key's value on
-// an exact hit -- the bits of the reference's search (see decode_control_cursor in
-// rt_decode_v2.cuh), with selects instead of branches.
+// an exact hit -- the bits of the reference's search (see the head of
+// this file), with selects instead of branches.
 template <class M>
 __device__ __forceinline__ void m_control_stream(const M& m, const StreamRef& s, uint32_t c, const int* fr,
                                                  uint32_t bin0, int n, float* dst, int stride,
@@ -166,7 +210,7 @@ __device__ __forceinline__ void m_control_stream(const M& m, const StreamRef& s,
 {
     const uint32_t desc = m((uint32_t)((s.base + 4ull * c) >> 2));
     const uint32_t kc = (desc >> 16) & 0xFFu;
-    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {   // see decode_control (rt_decode.cuh)
+    if (kc == 0u || (desc & 0xFFFFu) + kc > s.kf) {   // see decode_control (rt_search.cuh)
         for (int j = 0; j < n; ++j) dst[j * stride] = 0.0f;
         return;
     }
@@ -327,6 +371,62 @@ __device__ __forceinline__ double m_control_value_f64(const M& m, const StreamRe
     if (b.kind == 1) return (double)b.v0;
     if (b.kind == 2) return (double)b.v1;
     return (double)b.v0 + (double)(frame - b.f0) / (double)(b.f1 - b.f0) * ((double)b.v1 - (double)b.v0);
+}
+
+// Separable trilinear of one control grid (resolution R >= 2) for one frame.  On return each
+// lane holds its 4 voxel quads: quad i covers voxels 4*(lane + 32 i) .. +3, i.e. lz = 2i +
+// (lane >> 4), ly = (lane >> 1) & 7, lx = 4*(lane & 1) .. +3.
+// w[axis][p] are the axis weights of this grid; x2 (R*R*4 float2) and y4 (R*16 float4) are the
+// warp's scratch rows in shared memory.
+__device__ __forceinline__ void trilinear_quads_ptr(const AxisWeight (*w)[8], float2* x2, float4* y4,
+                                                    const float* __restrict__ g, int R, int lane, float4 q[4])
+{
+    // x-lerps: X[z*R + y][pair] for lx pair (2p, 2p+1)
+    const int nx = R * R * 4;
+    for (int it = lane; it < nx; it += 32) {
+        const int row = it >> 2, p = it & 3;
+        const AxisWeight wa = w[0][2 * p], wb = w[0][2 * p + 1];
+        const float* gr = g + row * R;
+        const float2 A = make_float2(gr[wa.i0], gr[wb.i0]);
+        const float2 B = make_float2(gr[wa.i1], gr[wb.i1]);
+        x2[it] = lerp2(A, B, make_float2(wa.t, wb.t), make_float2(wa.omt, wb.omt));
+    }
+    __syncwarp();
+    // y-lerps: Y[z][ly][quad] for lx quad (4k .. 4k+3), two float2 lerps each
+    const int ny = R * 16;
+    for (int it = lane; it < ny; it += 32) {
+        const int z = it >> 4, ly = (it >> 1) & 7, k = it & 1;
+        const AxisWeight wy = w[1][ly];
+        const float2* xa = x2 + (z * R + wy.i0) * 4 + 2 * k;
+        const float2* xb = x2 + (z * R + wy.i1) * 4 + 2 * k;
+        const float2 t = make_float2(wy.t, wy.t), omt = make_float2(wy.omt, wy.omt);
+        const float2 lo2 = lerp2(xa[0], xb[0], t, omt);
+        const float2 hi2 = lerp2(xa[1], xb[1], t, omt);
+        y4[it] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
+    }
+    __syncwarp();
+    // z-lerps: the lane's four voxel quads
+    const int ly = (lane >> 1) & 7, k = lane & 1;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int lz = 2 * i + (lane >> 4);
+        const AxisWeight wz = w[2][lz];
+        const float4 A = y4[(wz.i0 * 8 + ly) * 2 + k];
+        const float4 B = y4[(wz.i1 * 8 + ly) * 2 + k];
+        const float2 t = make_float2(wz.t, wz.t), omt = make_float2(wz.omt, wz.omt);
+        const float2 lo2 = lerp2(make_float2(A.x, A.y), make_float2(B.x, B.y), t, omt);
+        const float2 hi2 = lerp2(make_float2(A.z, A.w), make_float2(B.z, B.w), t, omt);
+        q[i] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
+    }
+    __syncwarp();
+}
+
+// Grid sample for resolutions 0 and 1 (no interpolation: 0, or the single control).
+__device__ __forceinline__ void constant_quads(const float* __restrict__ g, int R, float4 q[4])
+{
+    const float v = R == 1 ? g[0] : 0.0f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = make_float4(v, v, v, v);
 }
 
 // ---- TMA bulk copy global -> shared with mbarrier completion (sm_90+ PTX, no multicast) ----

@@ -15,7 +15,7 @@
 
 #include "asset.h"
 #include "kernels.cuh"
-#include "rt_decode.cuh"
+#include "rt_search.cuh"
 
 namespace vbtb {
 int set_last_error(int status, const std::string& msg);
