@@ -232,14 +232,17 @@ __device__ LeafEntry walk_rt_leaf(const DeviceAsset& a, uint32_t leaf, int lane)
         }
         if (__any_sync(0xFFFFFFFFu, bad)) status = kErrKeyRangeOob;
     }
-    if (status == kOk && a.key_sorted[leaf]) flags |= kFlagSorted;
+    if (status == kOk && (a.key_sorted[leaf] & 1u)) flags |= kFlagSorted;
+    if (status == kOk && (a.key_sorted[leaf] & 2u)) flags |= kFlagHalfPlain;
     e.info = (active & 0x3FFu) | flags | (status << 16);
     return e;
 }
 
 // Key-order analysis of one leaf (one warp): are the key frames of every control the decoders
-// read strictly increasing?  Controls with an out-of-pool key range are never decoded (see
-// decode_control) and are skipped.
+// read strictly increasing (key_sorted bit 0, kFlagSorted)?  And is no FP16 key value of those
+// controls a NaN (bit 1, kFlagHalfPlain: the hardware half conversion then equals the reference's
+// bit for bit)?  Controls with an out-of-pool key range are never decoded (see decode_control) and
+// are skipped.
 __global__ void __launch_bounds__(256) key_order_kernel(DeviceAsset a)
 {
     const int lane = threadIdx.x & 31;
@@ -248,6 +251,7 @@ __global__ void __launch_bounds__(256) key_order_kernel(DeviceAsset a)
     LeafEntry& e = a.entries[leaf];
     const uint32_t info = e.info;
     bool sorted = entry_status(e) == kOk && (info & kFlagActive) && a.g.profile != 2u;
+    bool plain = sorted;
     if (sorted) {
         const uint32_t* __restrict__ pw = a.payload;
         const uint64_t base = 4ull * e.word_off;
@@ -259,27 +263,36 @@ __global__ void __launch_bounds__(256) key_order_kernel(DeviceAsset a)
             st[ns++] = StreamRef{base + 8u + e.coarse_bytes, fres * fres * fres, 8u, e.kf >> 16, (e.header >> 4) & 3u};
         if (info & kFlagShell)
             st[ns++] = StreamRef{base + e.shell_off, entry_shell_active(e), 4u, e.kf >> 16, (e.header >> 4) & 3u};
-        bool ok = true;
+        bool ok = true, no_nan = true;
         for (int si = 0; si < ns; ++si) {
             const StreamRef& s = st[si];
             const uint64_t kb = stream_key_base(s);
             for (uint32_t c = lane; c < s.controls; c += 32) {
                 const uint32_t desc = ldw(pw, (uint32_t)((s.base + 4ull * c) >> 2));
                 const uint32_t ks = desc & 0xFFFFu, kc = (desc >> 16) & 0xFFu;
-                if (kc < 2u || ks + kc > s.kf) continue;
-                int prev = key_frame(pw, kb, s.codec, ks);
-                for (uint32_t i = 1; i < kc; ++i) {
-                    const int f = key_frame(pw, kb, s.codec, ks + i);
-                    ok &= f > prev;
+                if (kc == 0u || ks + kc > s.kf) continue;
+                int prev = -1;
+                for (uint32_t i = 0; i < kc; ++i) {
+                    int f;
+                    if (s.codec == 1u) {
+                        f = key_frame(pw, kb, s.codec, ks + i);
+                    } else {
+                        const uint32_t k24 = ld_key24(pw, kb + 3ull * (ks + i));
+                        f = (int)(k24 & 0xFFu);
+                        const uint32_t h = k24 >> 8;
+                        no_nan &= !((h & 0x7C00u) == 0x7C00u && (h & 0x3FFu) != 0u);
+                    }
+                    ok &= i == 0u || f > prev;
                     prev = f;
                 }
             }
         }
         sorted = __all_sync(0xFFFFFFFFu, ok);
+        plain = __all_sync(0xFFFFFFFFu, no_nan);
     }
     if (lane == 0) {
-        a.key_sorted[leaf] = sorted ? 1 : 0;
-        if (sorted) e.info = info | kFlagSorted;
+        a.key_sorted[leaf] = (sorted ? 1 : 0) | (plain ? 2 : 0);
+        e.info = info | (sorted ? kFlagSorted : 0u) | (plain ? kFlagHalfPlain : 0u);
     }
 }
 

@@ -30,7 +30,8 @@ struct DeviceAsset {
     uint32_t* counters;          // [0] active count, [1] walk error flags
     unsigned long long* err;     // first failing (leaf << 8 | status), ~0 when none
     unsigned long long* tile_state;  // look-back tile descriptors
-    uint8_t* key_sorted;         // per leaf: 1 when its decoded controls' key frames strictly increase
+    uint8_t* key_sorted;         // per leaf: bit 0 its decoded controls' key frames strictly increase,
+                                 // bit 1 none of their FP16 key values is a NaN
     unsigned long long* work;    // kWorkSlots leaf-work counters [epoch:32 | next index:32]
 };
 
@@ -40,8 +41,9 @@ struct DeviceAsset {
 constexpr uint32_t kWorkSlots = 64;
 
 // Fixed shared memory of the render decode kernel besides its leaf stage (rt_kernel_leaf.cuh:
-// barrier, frame tables, axis weights, 8 warps x (x-lerp + y-lerp rows), 3072-float controls).
-constexpr uint32_t kLeafFixedBytes = 16 + 256 + 128 + 576 + 8 * 196 * 8 + 8 * 112 * 16 + 3072 * 4 + 256 * 4;
+// barrier, frame tables, axis weights, 9 warps x (x-lerp + y-lerp rows), 3072-float controls,
+// reciprocal table, axis weights as 16-byte rows).
+constexpr uint32_t kLeafFixedBytes = 16 + 256 + 128 + 576 + 9 * 196 * 8 + 9 * 112 * 16 + 3072 * 4 + 256 * 4 + 768;
 
 constexpr int kWalkThreads = 256;
 constexpr int kWalkTile = 256;   // leaves per walker CTA (one scan element per thread)
@@ -55,8 +57,9 @@ constexpr int kWarpSlots = 64 + 16 * 64 > kCtrlSlots ? 64 + 16 * 64 : kCtrlSlots
 void launch_walk(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);
 // page table only, from the leaf table the walker built (same predicate, same ranks)
 void launch_page_table(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);
-// Per-asset key-order analysis (after a walk): sets key_sorted[] and the kFlagSorted bit of the
-// leaf table.  Runs at load and after every re-upload; later walks copy the bit from key_sorted.
+// Per-asset key-order analysis (after a walk): sets key_sorted[] and the kFlagSorted /
+// kFlagHalfPlain bits of the leaf table.  Runs at load and after every re-upload; later walks copy
+// the bits from key_sorted.
 void launch_key_order(const DeviceAsset& a, cudaStream_t s);
 // Decode `nframes` frames (frames[] on the host, <= 64) of every active leaf into the cache:
 // out[f * cache_frame_stride + rank * 512 + voxel].

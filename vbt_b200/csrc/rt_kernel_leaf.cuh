@@ -12,13 +12,19 @@
 
 namespace vbtb {
 
-constexpr int kLeafThreads = 256;
+constexpr int kLeafThreads = 256;   // the render window kernel (render_window.cuh)
 constexpr int kLeafWarps = kLeafThreads / 32;
+constexpr int kDecWarps = 9;         // the decode kernel: 288 threads, one per FINE6 control
+constexpr int kDecThreads = 32 * kDecWarps;
 constexpr int kLeafCtrlBudget = 3072;   // floats: frames x controls of one batch
-constexpr uint32_t kLeafFixed =
-    16 + 256 + 128 + 576 + kLeafWarps * 196 * 8 + kLeafWarps * 112 * 16 + kLeafCtrlBudget * 4 + 256 * 4;
+constexpr uint32_t leaf_fixed_bytes(int nw)
+{
+    return 16 + 256 + 128 + 576 + nw * 196 * 8 + nw * 112 * 16 + kLeafCtrlBudget * 4 + 256 * 4 + 768;
+}
+constexpr uint32_t kLeafFixed = leaf_fixed_bytes(kLeafWarps);
+constexpr uint32_t kDecFixed = leaf_fixed_bytes(kDecWarps);
 constexpr uint32_t kStagePad = 16;   // readable bytes past the largest staged window
-static_assert(kLeafFixed == kLeafFixedBytes, "host stage sizing must match the kernel's shared-memory layout");
+static_assert(kDecFixed == kLeafFixedBytes, "host stage sizing must match the kernel's shared-memory layout");
 
 struct LeafSmem {
     uint64_t* bar;
@@ -29,9 +35,12 @@ struct LeafSmem {
     float4* y4;      // [warp][112]
     float* ctrl;     // [kLeafCtrlBudget]
     float* rcp;      // [256] RN(1/i)
+    float4* w16;     // [grid][axis][8] {t, 1 - t, i0, i1}: the axis weights as 16-byte rows
     uint8_t* stage;  // leaf window (16-byte aligned), kStagePad bytes of padding after it
 };
 
+// Shared-memory layout for NW warps (x-lerp and y-lerp rows per warp).
+template <int NW = kLeafWarps>
 __device__ __forceinline__ LeafSmem leaf_layout(uint8_t* dyn)
 {
     LeafSmem s;
@@ -41,10 +50,11 @@ __device__ __forceinline__ LeafSmem leaf_layout(uint8_t* dyn)
     s.b4 = s.b8 + 64;
     s.w = reinterpret_cast<AxisWeight(*)[3][8]>(dyn + 16 + 256 + 128);
     s.x2 = reinterpret_cast<float2*>(dyn + 16 + 256 + 128 + 576);
-    s.y4 = reinterpret_cast<float4*>(reinterpret_cast<uint8_t*>(s.x2) + kLeafWarps * 196 * 8);
-    s.ctrl = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(s.y4) + kLeafWarps * 112 * 16);
+    s.y4 = reinterpret_cast<float4*>(reinterpret_cast<uint8_t*>(s.x2) + NW * 196 * 8);
+    s.ctrl = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(s.y4) + NW * 112 * 16);
     s.rcp = s.ctrl + kLeafCtrlBudget;
-    s.stage = reinterpret_cast<uint8_t*>(s.rcp + 256);
+    s.w16 = reinterpret_cast<float4*>(s.rcp + 256);
+    s.stage = reinterpret_cast<uint8_t*>(s.w16 + 48);
     return s;
 }
 
@@ -52,6 +62,10 @@ struct LeafGeom {
     uint32_t li, bx, by, bz;
     int w, h, d;
 };
+
+}  // namespace vbtb
+#include "rt_leaf_fast.cuh"
+namespace vbtb {
 
 template <bool DENSE>
 __device__ __forceinline__ void store_quad(const DeviceAsset& a, const LeafGeom& G, float* __restrict__ out,
@@ -87,15 +101,16 @@ struct FrameSink {
     }
 };
 
-// Decode one validated, non-EMPTY leaf for all frames of the launch with word reader `m`; each
-// finished quad of 4 voxels goes to `sink(frame index, lane, quad, values)`.  Frame lists that
-// step by 0 or 1 stream each control's keys; other non-decreasing lists (`monotone`) walk a
-// cursor; anything else, or keys that do not strictly increase, uses the reference's search.
-template <class M, class Sink>
+// Decode one validated, non-EMPTY leaf for all frames of the launch with word reader `m` and NW
+// warps; each finished quad of 4 voxels goes to `sink(frame index, lane, quad, values)`.  Frame
+// lists that step by 0 or 1 stream each control's keys; other non-decreasing lists (`monotone`)
+// walk a cursor; anything else, or keys that do not strictly increase, uses the reference's search.
+template <class M, class Sink, int NW = kLeafWarps>
 __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, const LeafSmem& s, const LeafEntry& e,
                                             int nframes, bool steps01, bool monotone, const LeafGeom& G,
                                             const Sink& sink)
 {
+    constexpr int NT = 32 * NW;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t base = 4ull * e.word_off;
     const int cres = (int)((e.header >> 6) & 7u), fres = (int)((e.header >> 9) & 7u);
@@ -111,7 +126,7 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
     // frames per batch: as many as the control buffer holds, rounded down to a multiple of the
     // warp count when that still leaves a full round (each warp reconstructs whole frames)
     int nb_max = min(nframes, kLeafCtrlBudget / max(Ctot, 1));
-    if (nb_max < nframes && nb_max > kLeafWarps) nb_max -= nb_max % kLeafWarps;
+    if (nb_max < nframes && nb_max > NW) nb_max -= nb_max % NW;
     const bool stream = steps01 && (e.info & kFlagSorted) != 0u;
     const bool cursor = !stream && monotone && (e.info & kFlagSorted) != 0u;
     const bool plain = !occ && G.w == 8 && G.h == 8 && G.d == 8;
@@ -148,19 +163,19 @@ __device__ __forceinline__ void leaf_decode(const DeviceAsset& a, const M& m, co
                 else m_control_search(m, st, ci, fb, dst, Ctot);
             }
         };
-        const int c0 = Ctot > kLeafThreads ? kLeafThreads : 0;   // controls [0, c0) are owned whole
+        const int c0 = Ctot > NT ? NT : 0;   // controls [0, c0) are owned whole
         if (c0) run_unit(tid, 0, nb);
         const int rest = Ctot - c0;
-        const int tpc = min(8, max(1, kLeafThreads / rest));
+        const int tpc = min(8, max(1, NT / rest));
         const int part_len = (nb + tpc - 1) / tpc;
-        for (int unit = tid; unit < rest * tpc; unit += kLeafThreads) {
+        for (int unit = tid; unit < rest * tpc; unit += NT) {
             const int c = c0 + unit / tpc, q = unit % tpc;
             const int j0 = q * part_len, j1 = min(nb, j0 + part_len);
             if (j0 < j1) run_unit(c, j0, j1);
         }
         __syncthreads();
         // 2. voxels
-        for (int j = warp; j < nb; j += kLeafWarps) {
+        for (int j = warp; j < nb; j += NW) {
             const float* g = s.ctrl + j * Ctot;
             float4 q[4];
             if (cres >= 2) trilinear_quads_ptr(s.w[0], x2, y4, g, cres, lane, q);
@@ -282,13 +297,29 @@ __global__ void __launch_bounds__(256) zero_empty_kernel(DeviceAsset a, float* _
 // instantiated for assets that have such leaves; it costs registers).
 // Leaves are handed out dynamically (grab_leaf), one at a time per CTA, so that CTAs that drew
 // cheap leaves (few controls, few keys) take more of them.
-template <bool DENSE, bool GLOBAL_FALLBACK>
-__global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsset a, FrameList fl,
-                                                                      float* __restrict__ out, uint64_t frame_stride,
-                                                                      unsigned long long* work, uint32_t epoch)
+// The general decode as a call of its own, so that its registers do not crowd the fast path's
+// (the kernel's shared-memory layout is recomputed from the dynamic shared-memory base).
+template <class M, bool DENSE>
+__device__ __noinline__ void leaf_decode_general(const DeviceAsset& a, M m, LeafEntry e, int nframes, bool steps01,
+                                                 bool monotone, LeafGeom G, float* __restrict__ out,
+                                                 uint64_t frame_stride)
 {
     extern __shared__ __align__(128) uint8_t dyn[];
-    const LeafSmem s = leaf_layout(dyn);
+    const LeafSmem s = leaf_layout<kDecWarps>(dyn);
+    leaf_decode<M, FrameSink<DENSE>, kDecWarps>(a, m, s, e, nframes, steps01, monotone, G,
+                                                FrameSink<DENSE>{a, G, out, frame_stride});
+}
+
+// Staged GRID4 / FINE6 leaves of the common shape take leaf_decode_fast (rt_leaf_fast.cuh), every
+// other leaf the general leaf_decode.
+template <bool DENSE, bool GLOBAL_FALLBACK>
+__global__ void __launch_bounds__(kDecThreads, 2) decode_leaf_kernel(const __grid_constant__ DeviceAsset a,
+                                                                     FrameList fl, float* __restrict__ out,
+                                                                     uint64_t frame_stride, unsigned long long* work,
+                                                                     uint32_t epoch)
+{
+    extern __shared__ __align__(128) uint8_t dyn[];
+    const LeafSmem s = leaf_layout<kDecWarps>(dyn);
     uint32_t* const s_next = reinterpret_cast<uint32_t*>(dyn + 8);   // beside the 8-byte barrier
     const int tid = threadIdx.x;
     const int total = (int)a.g.frames;
@@ -302,7 +333,7 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
         if (to) record_error(a.err, 0u, kErrWaitTimeout);
         *s_next = first;
     }
-    s.rcp[tid] = __frcp_rn((float)tid);
+    if (tid < 256) s.rcp[tid] = __frcp_rn((float)tid);
     if (tid < fl.n) {
         const int fr = clamp_frame(fl.f[tid], total);
         s.fr[tid] = fr;
@@ -340,7 +371,7 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
         }
         if (skip) {
             if (st != kOk && tid == 0) record_error(a.err, leaf, st);
-            for (int idx = tid; idx < fl.n * 128; idx += kLeafThreads)
+            for (int idx = tid; idx < fl.n * 128; idx += kDecThreads)
                 store_quad<DENSE>(a, G, out, frame_stride, idx >> 7, (idx & 127) & 31, (idx & 127) >> 5,
                                   make_float4(0.f, 0.f, 0.f, 0.f));
         } else if (!GLOBAL_FALLBACK && !staged) {   // the launcher never lets this happen
@@ -350,7 +381,9 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
                 const int ws = tid / 24, axis = (tid % 24) >> 3, p = tid & 7;
                 const int R = ws == 0 ? (int)((e.header >> 6) & 7u) : (int)((e.header >> 9) & 7u);
                 const int ext = axis == 0 ? G.w : (axis == 1 ? G.h : G.d);
-                s.w[ws][axis][p] = g_axis[axis_index(R, ext, p)];
+                const AxisWeight aw = g_axis[axis_index(R, ext, p)];
+                s.w[ws][axis][p] = aw;
+                s.w16[tid] = make_float4(aw.t, aw.omt, __int_as_float((int)aw.i0), __int_as_float((int)aw.i1));
             }
             const bool ok = !staged || mbar_wait(s.bar, phase);
             if (__syncthreads_or(!ok)) {   // any thread gave up: the whole CTA stops, together
@@ -359,12 +392,18 @@ __global__ void __launch_bounds__(kLeafThreads, 2) decode_leaf_kernel(DeviceAsse
                 return;
             }
             if (staged) phase ^= 1u;
-            if (staged) {
+            bool fine = false;
+            if (staged && fast_leaf_shape(e, steps01, fine)) {
+                const FrameSink<DENSE> sink{a, G, out, frame_stride};
+                const uint32_t lb = (uint32_t)(b0 - a0);
+                if (fine) leaf_decode_fast<true, kDecWarps>(s.stage, lb, s, e, fl.n, G, sink);
+                else leaf_decode_fast<false, kDecWarps>(s.stage, lb, s, e, fl.n, G, sink);
+            } else if (staged) {
                 const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
-                leaf_decode(a, m, s, e, fl.n, steps01, monotone, G, FrameSink<DENSE>{a, G, out, frame_stride});
+                leaf_decode_general<SharedWords, DENSE>(a, m, e, fl.n, steps01, monotone, G, out, frame_stride);
             } else if (GLOBAL_FALLBACK) {
                 const GlobalWords m{a.payload};
-                leaf_decode(a, m, s, e, fl.n, steps01, monotone, G, FrameSink<DENSE>{a, G, out, frame_stride});
+                leaf_decode_general<GlobalWords, DENSE>(a, m, e, fl.n, steps01, monotone, G, out, frame_stride);
             }
         }
         __syncthreads();   // the next index is visible
@@ -388,7 +427,7 @@ static int leaf_grid(uint32_t smem_bytes)
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_leaf_kernel<DENSE, GF>, kLeafThreads, smem_bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, decode_leaf_kernel<DENSE, GF>, kDecThreads, smem_bytes);
     return sms * (per > 0 ? per : 1);
 }
 
@@ -396,7 +435,7 @@ template <bool DENSE, bool GF>
 static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameList& fl, float* out, uint64_t stride,
                                 int grid, cudaStream_t s)
 {
-    const uint32_t smem = kLeafFixed + a.g.stage_bytes + kStagePad;
+    const uint32_t smem = kDecFixed + a.g.stage_bytes + kStagePad;
     cudaFuncSetAttribute(decode_leaf_kernel<DENSE, GF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int g = grid > 0 ? grid : leaf_grid<DENSE, GF>(smem);
     unsigned long long* slot = a.work + seq % kWorkSlots;
@@ -420,14 +459,14 @@ static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameL
         cudaStreamWaitEvent(side, fork, 0);
         zero_empty_kernel<<<8 * sms, 256, 0, side>>>(a, out, stride, (uint32_t)fl.n);
         cudaEventRecord(join, side);
-        decode_leaf_kernel<DENSE, GF><<<grid > 0 ? grid : sms, kLeafThreads, smem, s>>>(a, fl, out, stride, slot,
+        decode_leaf_kernel<DENSE, GF><<<grid > 0 ? grid : sms, kDecThreads, smem, s>>>(a, fl, out, stride, slot,
                                                                                          seq + 1u);
         cudaStreamWaitEvent(s, join, 0);
         cudaEventDestroy(fork);
         cudaEventDestroy(join);
         return;
     }
-    decode_leaf_kernel<DENSE, GF><<<g, kLeafThreads, smem, s>>>(a, fl, out, stride, slot, seq + 1u);
+    decode_leaf_kernel<DENSE, GF><<<g, kDecThreads, smem, s>>>(a, fl, out, stride, slot, seq + 1u);
 }
 
 static void launch_rt_leaf(const DeviceAsset& a, uint32_t seq, const FrameList& fl, float* out, uint64_t stride,

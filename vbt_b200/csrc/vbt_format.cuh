@@ -66,6 +66,7 @@ constexpr uint32_t kFlagFine = 1u << 11;      // decode the fine stream and add 
 constexpr uint32_t kFlagShell = 1u << 12;     // decode the Mode2 shell residual per occupied voxel
 constexpr uint32_t kFlagOccClamp = 1u << 13;  // Mode2: clamp negatives outside the occupancy to 0
 constexpr uint32_t kFlagSorted = 1u << 14;    // every decoded control's key frames strictly increase
+constexpr uint32_t kFlagHalfPlain = 1u << 15; // no FP16 key value of the leaf is a NaN (the hardware conversion is exact)
 
 VBT_HD uint32_t entry_status(const LeafEntry& e) { return (e.info >> 16) & 0xFFu; }
 VBT_HD uint32_t entry_shell_active(const LeafEntry& e) { return e.info & 0x3FFu; }
