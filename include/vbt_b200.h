@@ -307,10 +307,10 @@ int vbt_build_page_table_noalloc(const uint32_t* d_offsets, const uint32_t* d_pa
  * computed per leaf as one contraction S(512 x 64) . C(64 x n) on tcgen05 tensor cores: S = the
  * coarse trilinear weights (343 S is an integer matrix, exact in BF16), C = the coarse controls at
  * the window's frames (the DCT-II sum of scientific_decode.cpp:82-97, in FP32) split into three
- * BF16 terms; FP32 accumulation in tensor memory; the sparse-event residual is added exactly as
- * the per-frame path does.  Values are not bit-identical to the reference; vbt_window_error gives
- * their error.  CoarseOnly and SparseEvents leaves are covered; DenseGrid leaves record
- * VBT_STATUS_UNSUPPORTED (read by vbt_asset_sync_status) and are written as zeros.
+ * BF16 terms; FP32 accumulation in tensor memory; the sparse-event residual and the DenseGrid
+ * residual (per-frame BFP grid or DCT temporal basis, scientific_decode.cpp:125-233) are added
+ * exactly as the per-frame path does.  Values are not bit-identical to the reference;
+ * vbt_window_error gives their error.  Every generic leaf mode is covered.
  * Render-temporal assets (profile 1): frames [t0, t0 + n), n <= 64, d_out[f * frame_stride +
  * rank * 512 + voxel] over the active leaves of the current page table (vbt_build_page_table
  * first), as vbt_decode_cache, in consecutive windows of 16 frames.  Per leaf and window, the

@@ -16,8 +16,16 @@ Field recipes (shapes are X x Y x Z x T):
   cfg4_sdf_small  64^3 x 24 level set (a scaled-down config-4 scene): sloshing plane
                   z = 24 + 2 sin(0.2 x + 0.1 t) united with 6 ballistic spheres; Mode2 shell.
   tiny_*          small, odd-sized fields (boundary leaves with cropped extents).
-  sci_*           scientific (generic profile, time-fastest RAW) Gaussian random fields with a
-                  k^-5/3 spectrum, phase drift, and 0.1% spikes of 10 sigma.
+  sci_small/_64   scientific (generic profile, time-fastest RAW) Gaussian random fields with a
+                  k^-5/3 spectrum, phase drift, and 0.1% spikes of 10 sigma (SparseEvents leaves).
+  sci_coarse      smooth drifting blobs: every leaf CoarseOnly.
+  sci_dense       blobs + a large-scale pattern with white-noise amplitude: DenseGrid3/4 leaves with
+                  the per-frame BFP residual.
+  sci_dense_tb    blobs + the pattern modulated by DCT frequencies 4..7, encoded with
+                  --generic-dense-temporal-basis --generic-dense-temporal-keep 8: CoarseOnly and
+                  DenseGrid leaves of both residual subtypes (per-frame BFP and DCT temporal basis).
+  sci_modes       64^3 x 32 with regions of each kind: all four generic modes and both dense
+                  subtypes in one asset.
   mix_fire_*      the config-3 fire (density, flames, temperature = 300 + 1500 flames + N(0, 20))
                   at 128 x 128 x 192 x 40: fBm inside a sphere of radius 20 + 2.5 t.
   mix_sdf         the config-4 liquid level set at 128^3 x 48 (sloshing plane, 20 ballistic spheres
@@ -186,8 +194,70 @@ def grf_scientific(shape_xyz, frames, seed, spike_frac=0.001, spike_sigma=10.0):
     return out
 
 
+def _drifting_blobs(shape_xyz, frames, rng, n, sigma_lo, sigma_hi):
+    """[Z, Y, X, T] sum of n Gaussian blobs (amplitude U(0.5, 1.5)) drifting at N(0, 0.3) voxels
+    per frame, and the voxel coordinate grids."""
+    X, Y, Z = shape_xyz
+    zz, yy, xx = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(X), indexing="ij")
+    c0 = rng.uniform(0, 1, (n, 3)) * np.array([X, Y, Z])
+    v = rng.normal(0.0, 0.3, (n, 3))
+    s = rng.uniform(sigma_lo, sigma_hi, n)
+    a = rng.uniform(0.5, 1.5, n)
+    out = np.empty((Z, Y, X, frames), np.float64)
+    for t in range(frames):
+        f = np.zeros((Z, Y, X))
+        for b in range(n):
+            c = c0[b] + v[b] * t
+            f += a[b] * np.exp(-((xx - c[0]) ** 2 + (yy - c[1]) ** 2 + (zz - c[2]) ** 2) / (2.0 * s[b] ** 2))
+        out[..., t] = f
+    return out, (xx, yy, zz)
+
+
+def sci_flicker(shape_xyz, frames, seed, amp, kind):
+    """Scientific fields that steer the generic encoder's leaf modes (time fastest, [Z, Y, X, T]):
+    smooth drifting blobs (every leaf CoarseOnly), plus a large-scale spatial pattern
+    sin(0.35 x + 0.2 y) cos(0.3 z) whose amplitude changes over time -- white noise per frame
+    (kind "white": the DenseGrid per-frame BFP residual) or a sum of the DCT-II frequencies 4..7
+    (kind "mid": with --generic-dense-temporal-basis, also the temporal-basis residual)."""
+    rng = np.random.default_rng(seed)
+    out, (xx, yy, zz) = _drifting_blobs(shape_xyz, frames, rng, 4, 6.0, 12.0)
+    if kind != "none":
+        t = np.arange(frames)
+        if kind == "white":
+            sig = rng.normal(0.0, 1.0, frames)
+        else:
+            sig = sum(rng.normal(0.0, 1.0) * np.cos(np.pi / frames * (t + 0.5) * k) for k in range(4, 8))
+        pat = np.sin(0.35 * xx + 0.2 * yy) * np.cos(0.3 * zz)
+        out += amp * pat[..., None] * sig[None, None, None, :]
+    return out.astype(np.float32)
+
+
+def sci_modes(shape_xyz, frames, seed):
+    """A scientific field whose leaves take all four generic modes: smooth drifting blobs
+    everywhere; x in the middle third adds the pattern of sci_flicker modulated by DCT-II
+    frequencies 4..7 (amplitude 1), the last third by white noise per frame (amplitude 2.5); the
+    upper half of the first third carries 0.2 % spikes of +-4 (SparseEvents), its lower half
+    stays smooth (CoarseOnly).  Time fastest, [Z, Y, X, T]."""
+    X, Y, Z = shape_xyz
+    rng = np.random.default_rng(seed)
+    out, (xx, yy, zz) = _drifting_blobs(shape_xyz, frames, rng, 6, 8.0, 16.0)
+    pat = np.sin(0.35 * xx + 0.2 * yy) * np.cos(0.3 * zz)
+    t = np.arange(frames)
+    mid = sum(rng.normal(0.0, 1.0) * np.cos(np.pi / frames * (t + 0.5) * k) for k in range(4, 8))
+    white = rng.normal(0.0, 1.0, frames)
+    region = (xx * 3) // X
+    out += np.where(region == 1, 1.0 * pat, 0.0)[..., None] * mid[None, None, None, :]
+    out += np.where(region == 2, 2.5 * pat, 0.0)[..., None] * white[None, None, None, :]
+    n = int(0.002 * out.size)
+    idx = rng.choice(out.size, n, replace=False)
+    zi, yi, xi, ti = np.unravel_index(idx, out.shape)
+    keep = (xi < X // 3) & (zi >= Z // 2)
+    out[zi[keep], yi[keep], xi[keep], ti[keep]] += 4.0 * np.sign(rng.normal(size=int(keep.sum())))
+    return out.astype(np.float32)
+
+
 # ----------------------------------------------------------------------------- encode
-def encode(name, data, xyzt, profile, extra_meta=None, time_fastest=False):
+def encode(name, data, xyzt, profile, extra_meta=None, time_fastest=False, args=()):
     os.makedirs(ASSETS, exist_ok=True)
     if not os.path.exists(ENCODER):
         sys.path.insert(0, ROOT)
@@ -207,7 +277,7 @@ def encode(name, data, xyzt, profile, extra_meta=None, time_fastest=False):
             json.dump(m, fh)
         out = os.path.join(ASSETS, name + ".vbtp")
         cmd = [ENCODER, "--input-raw", raw, "--metadata", meta, "--profile", profile,
-               "--save-vbt", out, "--report", os.path.join(td, "report.md"), "--omp-threads", "8"]
+               "--save-vbt", out, "--report", os.path.join(td, "report.md"), "--omp-threads", "8"] + list(args)
         subprocess.check_call(cmd, stdout=subprocess.DEVNULL)
     print(f"{name}: {os.path.getsize(out)} bytes")
     return out
@@ -227,6 +297,18 @@ RECIPES = {
     "sci_64": lambda: encode("sci_64", grf_scientific((64, 64, 64), 32, 6), (64, 64, 64, 32), "generic",
                              time_fastest=True),
     "cfg2_plume": lambda: encode("cfg2_plume", plume(256, 96, 2), (256, 256, 256, 96), "density"),
+    # scientific leaf modes beyond SparseEvents (generic profile): CoarseOnly, DenseGrid3/4 with the
+    # per-frame BFP residual, and the DCT temporal-basis residual
+    "sci_coarse": lambda: encode("sci_coarse", sci_flicker((24, 16, 20), 16, 3, 0.0, "none"), (24, 16, 20, 16),
+                                 "generic", time_fastest=True),
+    "sci_dense": lambda: encode("sci_dense", sci_flicker((24, 16, 20), 16, 3, 1.0, "white"), (24, 16, 20, 16),
+                                "generic", time_fastest=True),
+    "sci_dense_tb": lambda: encode("sci_dense_tb", sci_flicker((24, 16, 20), 16, 3, 0.3, "mid"), (24, 16, 20, 16),
+                                   "generic", time_fastest=True,
+                                   args=("--generic-dense-temporal-basis", "--generic-dense-temporal-keep", "8")),
+    "sci_modes": lambda: encode("sci_modes", sci_modes((64, 64, 64), 32, 21), (64, 64, 64, 32), "generic",
+                                time_fastest=True,
+                                args=("--generic-dense-temporal-basis", "--generic-dense-temporal-keep", "8")),
     # serving-mix assets: the config-3/4/5 scenes at reduced sizes (the full sizes need 36-64 GB
     # of raw float32 input per field, more than this machine's memory, and the encoded fields
     # must stay small enough to travel with the working tree)
@@ -243,7 +325,8 @@ RECIPES = {
 }
 MIX = ["cfg2_plume", "mix_fire_density", "mix_fire_flames", "mix_fire_temperature", "mix_sdf",
        "cfg1_blobs", "cfg4_sdf_small", "mix_sci"]
-DEFAULT = ["tiny_density", "tiny_levelset", "sci_small", "cfg1_blobs", "cfg4_sdf_small", "sci_64", "cfg2_plume"]
+DEFAULT = ["tiny_density", "tiny_levelset", "sci_small", "cfg1_blobs", "cfg4_sdf_small", "sci_64", "cfg2_plume",
+           "sci_modes"]
 
 if __name__ == "__main__":
     names = sys.argv[1:] or DEFAULT

@@ -19,7 +19,8 @@ constructions of the reference's own tests and record the reference's outputs on
                    corruptions (:81-114) with the reference parser's verdicts.
   reader/*.vbtp    the files of tests/vbt_file_tests.cpp:86-131 and the expected message fragments
                    (reader/cases.json).
-  assets/*.vbtp    three small synthetic assets (tests/golden/make_assets.py) and
+  assets/*.vbtp    six small synthetic assets (tests/golden/make_assets.py; the three sci_* beyond
+                   sci_small hold the CoarseOnly, DenseGrid3/4 and temporal-basis leaf modes) and
   assets/*.npz     the reference decoder's frames for every frame index -1 .. T.
 """
 import json
@@ -205,10 +206,13 @@ def gen_reader_cases():
     print("reader cases:", len(cases))
 
 
-def gen_assets(ref):
+GOLDEN_ASSETS = ("tiny_density", "tiny_levelset", "sci_small", "sci_coarse", "sci_dense", "sci_dense_tb")
+
+
+def gen_assets(ref, names=GOLDEN_ASSETS):
     d = os.path.join(HERE, "assets")
     os.makedirs(d, exist_ok=True)
-    for name in ("tiny_density", "tiny_levelset", "sci_small"):
+    for name in names:
         src = os.path.join(ROOT, "assets", name + ".vbtp")
         if not os.path.exists(src):
             import subprocess

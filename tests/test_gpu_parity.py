@@ -17,9 +17,12 @@ pytestmark = pytest.mark.gpu
 SCI_TOL = 1e-6   # relative to the field range
 
 
+GOLDEN_NAMES = ("tiny_density", "tiny_levelset", "sci_small", "sci_coarse", "sci_dense", "sci_dense_tb")
+
+
 def asset_paths(include_large=False):
-    out = [golden_asset(n) for n in ("tiny_density", "tiny_levelset", "sci_small")]
-    names = ["cfg1_blobs", "cfg4_sdf_small", "sci_64"] + (["cfg2_plume"] if include_large else [])
+    out = [golden_asset(n) for n in GOLDEN_NAMES]
+    names = ["cfg1_blobs", "cfg4_sdf_small", "sci_64", "sci_modes"] + (["cfg2_plume"] if include_large else [])
     for n in names:
         p = os.path.join(ASSETS, n + ".vbtp")
         if os.path.exists(p):
@@ -113,8 +116,10 @@ def test_dense_frames(loaded, cuda, path):
 
 
 def test_golden_frames_against_reference_fixtures(vbt, cuda):
-    """The reference's own frames (tests/golden/assets/*.npz), independent of the oracle."""
-    for name in ("tiny_density", "tiny_levelset", "sci_small"):
+    """The reference's own frames (tests/golden/assets/*.npz), independent of the oracle: every
+    render leaf route and every scientific leaf mode (CoarseOnly, SparseEvents, DenseGrid3/4 with
+    the per-frame BFP and the temporal-basis residual)."""
+    for name in GOLDEN_NAMES:
         a = vbt.Asset(golden_asset(name))
         z = np.load(os.path.join(GOLDEN, "assets", name + ".npz"))
         X, Y, Z = a.dims

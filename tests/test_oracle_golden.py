@@ -90,10 +90,14 @@ def test_reader_cases(oracle):
                 oracle.load(path)
 
 
-@pytest.mark.parametrize("name", ["tiny_density", "tiny_levelset", "sci_small"])
+GOLDEN_NAMES = ["tiny_density", "tiny_levelset", "sci_small", "sci_coarse", "sci_dense", "sci_dense_tb"]
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
 def test_golden_asset_frames(oracle, name):
-    """Frames of three small synthetic assets (odd sizes: cropped boundary leaves; Mode2;
-    scientific SparseEvents) equal the reference's frames bit for bit."""
+    """Frames of six small synthetic assets (odd sizes: cropped boundary leaves; Mode2;
+    scientific SparseEvents, CoarseOnly, DenseGrid3/4 with the per-frame BFP residual and with
+    the DCT temporal-basis residual) equal the reference's frames bit for bit."""
     f = oracle.load(golden_asset(name))
     z = np.load(os.path.join(GOLDEN, "assets", name + ".npz"))
     for t, want in zip(z["t"], z["frames"]):
@@ -102,8 +106,8 @@ def test_golden_asset_frames(oracle, name):
 
 
 def _asset_paths():
-    out = [golden_asset(n) for n in ("tiny_density", "tiny_levelset", "sci_small")]
-    for n in ("cfg1_blobs", "cfg4_sdf_small", "sci_64"):
+    out = [golden_asset(n) for n in GOLDEN_NAMES]
+    for n in ("cfg1_blobs", "cfg4_sdf_small", "sci_64", "sci_modes"):
         p = os.path.join(ASSETS, n + ".vbtp")
         if os.path.exists(p):
             out.append(p)

@@ -18,8 +18,8 @@ TOL = 1e-6   # relative to the field range
 
 
 def sci_paths():
-    out = [golden_asset("sci_small")]
-    for n in ("sci_64", "mix_sci"):
+    out = [golden_asset(n) for n in ("sci_small", "sci_coarse", "sci_dense", "sci_dense_tb")]
+    for n in ("sci_64", "mix_sci", "sci_modes"):
         p = os.path.join(ASSETS, n + ".vbtp")
         if os.path.exists(p):
             out.append(p)

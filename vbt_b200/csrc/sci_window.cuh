@@ -14,7 +14,8 @@
 // (S'.c_hi + S'.c_mid + S'.c_lo), accumulated in FP32 in tensor memory: 4 M tiles (128 voxels)
 // x 4 K steps x 3 terms = 48 MMAs of 128 x N x 16 per leaf-window, N = n rounded up to 16.
 // The epilogue reads D from tensor memory, adds the corner terms, scales by 1/343, adds the
-// sparse-event residual (CUDA cores, as the per-frame path) and writes the cache layout.
+// sparse-event or DenseGrid residual (CUDA cores, as the per-frame path) and writes the cache
+// layout.
 //
 // Shared-memory operand layout (canonical K-major, no swizzle): per K step, core matrices of
 // 8 rows x 16 bytes; the two 8-element K halves 128 bytes apart (leading byte offset), 8-row
@@ -170,8 +171,8 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
         const uint32_t st = entry_status(e);
         const uint32_t hdr = e.header, mode = hdr & 3u;
         const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
-        if (st != kOk || mode >= 2u) {   // uniform over the CTA
-            if (tid == 0) record_error(a.err, leaf, st != kOk ? st : kErrUnsupported);
+        if (st != kOk) {   // uniform over the CTA
+            if (tid == 0) record_error(a.err, leaf, st);
             for (int i = tid; i < n * 512; i += kWinThreads)
                 out[(uint64_t)(i >> 9) * frame_stride + (uint64_t)leaf * 512u + (i & 511)] = 0.0f;
             continue;
@@ -241,6 +242,36 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                 }
             win_commit(bar);
         }
+        // DenseGrid leaves, while the products run: the residual grids in place of the coarse
+        // coefficients (no longer read) -- the per-frame BFP grid of every frame of the window,
+        // or the temporal-basis grids (render/src/scientific_decode.cpp:125-233), decoded as the
+        // per-frame path decodes them (sci_decode_controls)
+        const int dres = mode == 2u ? 3 : 4, dper = dres * dres * dres;
+        const int dbits = (int)((hdr >> 8) & 0xFu);
+        const uint32_t dsub = (hdr >> 12) & 7u;
+        const int dtkeep = (int)((hdr >> 15) & 0xFu) + 1;
+        if (mode >= 2u) {
+            const uint64_t scales = base + 4u + (uint64_t)(64 * (keep + 1));
+            if (dsub == 1u) {
+                const int bbytes = (dper * dbits + 7) / 8;
+                const uint64_t data = scales + (uint64_t)(dtkeep * 2);
+                if (dbits > 0)
+                    for (int i = tid; i < dtkeep * dper; i += kWinThreads) {
+                        const int k = i / dper, ci = i % dper;
+                        const float sc = half_bits_to_float(rd.u16(scales + (uint64_t)(k * 2)));
+                        sQ[i] = bfp_sample(rd, data + (uint64_t)(k * bbytes), dres, dbits, sc, ci);
+                    }
+            } else {
+                const int fbytes = (dper * dbits + 7) / 8;
+                for (int i = tid; i < n * dper; i += kWinThreads) {
+                    const int f = i / dper, ci = i % dper;
+                    const uint32_t t = (uint32_t)(t0 + f);
+                    const uint64_t data = scales + (uint64_t)a.g.frames * 2u + (uint64_t)t * fbytes;
+                    const float sc = half_bits_to_float(rd.u16(scales + t * 2u));
+                    sQ[i] = bfp_sample(rd, data, dres, dbits, sc, ci);
+                }
+            }
+        }
         // 4. wait for the products (bounded); a timeout stops the whole CTA after a second wait
         const bool ok = mbar_wait(bar, phase);
         if (__syncthreads_or(!ok)) {
@@ -263,6 +294,9 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
             const int corner = win_corner_of_voxel(v);
             const bool inside = (int)(v & 7u) < ew && (int)((v >> 3) & 7u) < eh && (int)(v >> 6) < ed;
             const bool events = mode == 1u && !scatter && ((s_mask[v >> 5] >> (v & 31u)) & 1u) != 0u;
+            const int dsel = mode == 2u ? 1 : 2;
+            const AxisWeight dx = c_sci_axis[dsel][v & 7u], dy = c_sci_axis[dsel][(v >> 3) & 7u],
+                             dz = c_sci_axis[dsel][v >> 6];
             for (int c0 = (int)half * cols_per_half; c0 < (int)(half + 1) * cols_per_half; c0 += 16) {
                 float d[16];
                 win_ld16(taddr + ((quarter * 32u) << 16) + m * (uint32_t)N + (uint32_t)c0, d);
@@ -273,8 +307,22 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                         float val = d[j];
                         if (corner >= 0) val = __fadd_rn(val, sCorner[corner * kWinMaxN + f]);
                         val = __fmul_rn(val, 1.0f / 343.0f);
-                        if (mode == 1u)
+                        if (mode == 1u) {
                             val = __fadd_rn(val, events ? sparse_at(rd, *s_sparse, v, (uint32_t)(t0 + f)) : 0.0f);
+                        } else if (mode >= 2u) {
+                            float r = 0.0f;
+                            if (dsub == 1u) {
+                                if (dbits > 0) {
+                                    const float* brow = a.basis + (uint64_t)(t0 + f) * 64u;
+                                    for (int k = 0; k < dtkeep; ++k)
+                                        r = __fadd_rn(r, __fmul_rn(tri_small(sQ + k * dper, dres, dx, dy, dz),
+                                                                   __ldg(brow + k)));
+                                }
+                            } else {
+                                r = tri_small(sQ + f * dper, dres, dx, dy, dz);
+                            }
+                            val = __fadd_rn(val, r);
+                        }
                         out[(uint64_t)f * frame_stride + (uint64_t)leaf * 512u + v] = inside ? val : 0.0f;
                     }
                 }
@@ -332,6 +380,47 @@ __device__ __forceinline__ unsigned long long win_ordered(double x)
     return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
 }
 
+// The DenseGrid residual of voxel (lx, ly, lz) at frame t in double without intermediate rounding:
+// the decoded BFP samples and the reference's FP32 axis weights, the per-frame grid or the sum of
+// the temporal-basis grids times the basis values (render/src/scientific_decode.cpp:125-233).
+__device__ double dense_residual_f64(const DeviceAsset& a, SciReader& rd, uint64_t base, uint32_t hdr, int keep,
+                                     uint32_t lx, uint32_t ly, uint32_t lz, uint32_t t)
+{
+    const uint32_t mode = hdr & 3u;
+    const int res = mode == 2u ? 3 : 4, per = res * res * res;
+    const int bits = (int)((hdr >> 8) & 0xFu);
+    const uint32_t sub = (hdr >> 12) & 7u;
+    const int tkeep = (int)((hdr >> 15) & 0xFu) + 1;
+    const int sel = mode == 2u ? 1 : 2;
+    const AxisWeight ax = c_sci_axis[sel][lx], ay = c_sci_axis[sel][ly], az = c_sci_axis[sel][lz];
+    const uint64_t scales = base + 4u + (uint64_t)(64 * (keep + 1));
+    auto tri = [&](uint64_t data, float sc) {
+        double r = 0.0;
+        for (int cz = 0; cz < 2; ++cz)
+            for (int cy = 0; cy < 2; ++cy)
+                for (int cx = 0; cx < 2; ++cx) {
+                    const int ci = ((cz ? az.i1 : az.i0) * res + (cy ? ay.i1 : ay.i0)) * res + (cx ? ax.i1 : ax.i0);
+                    const double w = (double)(cx ? ax.t : ax.omt) * (double)(cy ? ay.t : ay.omt) *
+                                     (double)(cz ? az.t : az.omt);
+                    r += w * (double)bfp_sample(rd, data, res, bits, sc, ci);
+                }
+        return r;
+    };
+    if (sub == 1u) {
+        if (bits <= 0) return 0.0;
+        const int bbytes = (per * bits + 7) / 8;
+        const uint64_t data = scales + (uint64_t)(tkeep * 2);
+        const float* brow = a.basis + (uint64_t)t * 64u;
+        double r = 0.0;
+        for (int k = 0; k < tkeep; ++k)
+            r += tri(data + (uint64_t)(k * bbytes), half_bits_to_float(rd.u16(scales + (uint64_t)(k * 2)))) *
+                 (double)__ldg(brow + k);
+        return r;
+    }
+    const int fbytes = (per * bits + 7) / 8;
+    return tri(scales + (uint64_t)a.g.frames * 2u + (uint64_t)t * fbytes, half_bits_to_float(rd.u16(scales + t * 2u)));
+}
+
 __global__ void __launch_bounds__(256) sci_window_oracle_kernel(DeviceAsset a, int t0, int n,
                                                                 const float* __restrict__ vals, uint64_t frame_stride,
                                                                 unsigned long long* stats)
@@ -346,7 +435,7 @@ __global__ void __launch_bounds__(256) sci_window_oracle_kernel(DeviceAsset a, i
         const uint32_t leaf = (uint32_t)(it >> 9), v = (uint32_t)(it & 511u);
         const LeafEntry e = a.entries[leaf];
         const uint32_t hdr = e.header, mode = hdr & 3u;
-        if (entry_status(e) != kOk || mode >= 2u) continue;
+        if (entry_status(e) != kOk) continue;
         const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
         const uint64_t base = 4ull * e.word_off;
         SciReader rd{a.payload, a.g.payload_words, false};
@@ -379,6 +468,7 @@ __global__ void __launch_bounds__(256) sci_window_oracle_kernel(DeviceAsset a, i
                         ref += w * c;
                     }
             if (mode == 1u) ref += (double)sci_sparse(rd, base, hdr, keep, v, t);
+            else if (mode >= 2u) ref += dense_residual_f64(a, rd, base, hdr, keep, lx, ly, lz, t);
             const double got = (double)vals[(uint64_t)f * frame_stride + (uint64_t)leaf * 512u + v];
             const double err = fabs(got - ref);
             my_max = fmax(my_max, err);
