@@ -21,8 +21,9 @@ LIB_DIR = os.path.join(ROOT, "vbt_b200")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 
 
-def compile_program(name, out_dir):
-    """g++ the test program against libvbt_b200.so and liboracle.so (both built by build())."""
+def compile_program(name, out_dir, cuda_runtime=False):
+    """g++ the test program against libvbt_b200.so and liboracle.so (both built by build()), and
+    the CUDA runtime when the program calls it itself."""
     for lib in (os.path.join(LIB_DIR, "libvbt_b200.so"), os.path.join(ORACLE_DIR, "liboracle.so")):
         if not os.path.exists(lib):
             pytest.skip(f"{os.path.basename(lib)} not built (run __graft_entry__.build())")
@@ -30,6 +31,9 @@ def compile_program(name, out_dir):
     cmd = ["/usr/bin/g++", "-std=c++17", "-O1", "-Wall", "-I", os.path.join(ROOT, "include"), "-I", ORACLE_DIR,
            "-I", CPP, os.path.join(CPP, name + ".cpp"), "-o", exe, "-L", LIB_DIR, "-lvbt_b200", "-L", ORACLE_DIR,
            "-loracle", f"-Wl,-rpath,{LIB_DIR}:{ORACLE_DIR}"]
+    if cuda_runtime:
+        cmd += ["-I", "/usr/local/cuda/include", "-L", "/usr/local/cuda/lib64", "-lcudart",
+                "-Wl,-rpath,/usr/local/cuda/lib64"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     return exe
 
@@ -149,3 +153,16 @@ def test_decode_api_program(tmp_path, cuda):
     r = subprocess.run([exe] + render + ["--sci", golden_asset("sci_small")], capture_output=True, text=True,
                        timeout=900)
     assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_facade_copies_and_latency(tmp_path, cuda):
+    """Device copies of VbtFile objects: bounded without releaseDeviceCopy, never stale after an
+    in-place change or a reload into the same object; and the scalar calls' latency."""
+    exe = compile_program("facade_test", str(tmp_path), cuda_runtime=True)
+    r = subprocess.run([exe, golden_asset("tiny_density"), golden_asset("sci_small")], capture_output=True, text=True,
+                       timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
+    lat = {ln.split()[1]: float(ln.split()[2]) for ln in r.stdout.splitlines() if ln.startswith("LATENCY")}
+    assert set(lat) == {"decodeRenderTemporalLeafControlValue", "decodeScientificValueAtCpu"}

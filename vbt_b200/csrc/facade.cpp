@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <random>
 #include <stdexcept>
@@ -54,25 +55,33 @@ RenderTemporalStreamLayout stream_layout(uint32_t start, uint32_t controls, uint
     throw std::runtime_error(vbt_status_string(status));
 }
 
-// Per-thread device staging for the scalar decode calls.
-struct Staging {
-    uint8_t* d_stream = nullptr;
-    size_t stream_cap = 0;
-    std::vector<uint8_t> last;   // host copy of the bytes currently in d_stream
-    void* d_io = nullptr;
-    size_t io_cap = 0;
-    ~Staging()
-    {
-        if (d_stream) cudaFree(d_stream);
-        if (d_io) cudaFree(d_io);
-    }
-};
-thread_local Staging g_stage;
-
 void cuda_check(cudaError_t e, const char* what)
 {
     if (e != cudaSuccess) throw std::runtime_error(std::string("no usable CUDA device (") + what + "): " + cudaGetErrorString(e));
 }
+
+// Per-thread device staging for the scalar decode calls: a non-blocking stream of the thread's
+// own (threads that decode at the same time do not queue behind one another on the legacy default
+// stream), the last stream bytes uploaded, and one pinned host block and one device block for the
+// (control, frame) pairs in and the (value, status) pairs out, so that a call is one copy in, one
+// launch, one copy out and one stream synchronisation.
+struct Staging {
+    cudaStream_t stream = nullptr;
+    uint8_t* d_stream = nullptr;
+    size_t stream_cap = 0;
+    std::vector<uint8_t> last;   // host copy of the bytes currently in d_stream
+    void* d_io = nullptr;
+    void* h_io = nullptr;        // pinned
+    size_t io_cap = 0;
+    ~Staging()
+    {
+        if (stream) cudaStreamDestroy(stream);
+        if (d_stream) cudaFree(d_stream);
+        if (d_io) cudaFree(d_io);
+        if (h_io) cudaFreeHost(h_io);
+    }
+};
+thread_local Staging g_stage;
 
 // Decode n (control, frame) pairs of one stream on the GPU; statuses per pair.
 void gpu_decode(const uint8_t* stream, uint32_t bytes, RenderTemporalSequenceCodec codec, uint32_t cc, uint32_t bins,
@@ -80,6 +89,7 @@ void gpu_decode(const uint8_t* stream, uint32_t bytes, RenderTemporalSequenceCod
                 int32_t* status)
 {
     Staging& s = g_stage;
+    if (!s.stream) cuda_check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (bytes > s.stream_cap) {
         if (s.d_stream) cudaFree(s.d_stream);
         s.d_stream = nullptr;
@@ -89,28 +99,35 @@ void gpu_decode(const uint8_t* stream, uint32_t bytes, RenderTemporalSequenceCod
         s.stream_cap = bytes;
     }
     if (bytes && (s.last.size() != bytes || std::memcmp(s.last.data(), stream, bytes) != 0)) {
-        cuda_check(cudaMemcpy(s.d_stream, stream, bytes, cudaMemcpyHostToDevice), "cudaMemcpy");
+        cuda_check(cudaMemcpyAsync(s.d_stream, stream, bytes, cudaMemcpyHostToDevice, s.stream), "cudaMemcpyAsync");
         s.last.assign(stream, stream + bytes);
     }
-    const size_t io = n * (4 + 4 + 4 + 4);
+    const size_t io = n * 16;
     if (io > s.io_cap) {
         if (s.d_io) cudaFree(s.d_io);
-        s.d_io = nullptr;
+        if (s.h_io) cudaFreeHost(s.h_io);
+        s.d_io = s.h_io = nullptr;
         s.io_cap = 0;
         cuda_check(cudaMalloc(&s.d_io, io), "cudaMalloc");
+        cuda_check(cudaHostAlloc(&s.h_io, io, cudaHostAllocDefault), "cudaHostAlloc");
         s.io_cap = io;
     }
-    auto* d_ci = static_cast<uint32_t*>(s.d_io);
-    auto* d_fr = reinterpret_cast<int32_t*>(d_ci + n);
-    auto* d_out = reinterpret_cast<float*>(d_fr + n);
-    auto* d_st = reinterpret_cast<int32_t*>(d_out + n);
-    cuda_check(cudaMemcpy(d_ci, ci, 4 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
-    cuda_check(cudaMemcpy(d_fr, fr, 4 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+    // [control indices][frames] in, [values][statuses] out, adjacent in both blocks
+    auto* h = static_cast<uint8_t*>(s.h_io);
+    std::memcpy(h, ci, 4 * n);
+    std::memcpy(h + 4 * n, fr, 4 * n);
+    auto* d = static_cast<uint8_t*>(s.d_io);
+    cuda_check(cudaMemcpyAsync(d, h, 8 * n, cudaMemcpyHostToDevice, s.stream), "cudaMemcpyAsync");
     const int st = vbt_decode_control_values(s.d_stream, bytes, static_cast<uint32_t>(codec), cc, bins, kf, align ? 1 : 0,
-                                             total, d_ci, d_fr, n, d_out, d_st, nullptr);
+                                             total, reinterpret_cast<const uint32_t*>(d),
+                                             reinterpret_cast<const int32_t*>(d + 4 * n), n,
+                                             reinterpret_cast<float*>(d + 8 * n), reinterpret_cast<int32_t*>(d + 12 * n),
+                                             s.stream);
     if (st) throw std::runtime_error(vbt_last_error());
-    cuda_check(cudaMemcpy(out, d_out, 4 * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
-    cuda_check(cudaMemcpy(status, d_st, 4 * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    cuda_check(cudaMemcpyAsync(h + 8 * n, d + 8 * n, 8 * n, cudaMemcpyDeviceToHost, s.stream), "cudaMemcpyAsync");
+    cuda_check(cudaStreamSynchronize(s.stream), "cudaStreamSynchronize");
+    std::memcpy(out, h + 8 * n, 4 * n);
+    std::memcpy(status, h + 12 * n, 4 * n);
 }
 
 // The reference's pre-decode checks of decodeRenderTemporalControlValue
@@ -685,34 +702,109 @@ std::vector<uint8_t> image_of(const VbtFile& f)
     return img;
 }
 
-struct CacheEntry {
-    const void *scales, *offsets, *payload;
-    size_t ns, no, np;
-    vbt_asset* asset;
+// Device copies of VbtFile objects for the GPU-backed calls.  The reference's decoders read the
+// VbtFile's vectors on every call, so a copy made earlier must never decode bytes the caller has
+// since changed: each call compares, against the image it last uploaded, exactly the bytes it is
+// about to decode -- the header, the AC scales and, per leaf it reads, that leaf's two offsets and
+// its payload words -- and uploads the file again when any of them differ.  A different file that
+// reuses a freed VbtFile's address is caught the same way.  Copies are kept for the most recently
+// used files only (kMaxCopies, and at most kMaxCopyBytes of device memory in all), so files that
+// are destroyed without releaseDeviceCopy hold no device memory beyond those bounds.
+constexpr size_t kMaxCopies = 8;
+constexpr uint64_t kMaxCopyBytes = 2ull << 30;
+
+struct DeviceCopy {
+    std::mutex mu;               // one call at a time on a copy (a call may upload it again)
+    vbt_asset* asset = nullptr;
+    std::vector<uint8_t> image;  // the bytes last uploaded
+    uint64_t device_bytes = 0;
+    uint64_t tick = 0;
+    ~DeviceCopy()
+    {
+        if (asset) vbt_asset_destroy(asset);
+    }
 };
 std::mutex g_cache_mu;
-std::map<const VbtFile*, CacheEntry> g_cache;
+std::map<const VbtFile*, std::shared_ptr<DeviceCopy>> g_cache;
+uint64_t g_tick = 0;
 
-vbt_asset* device_copy(const VbtFile& f)
+// The copy of `f` (created empty when absent), most recently used; older copies beyond the
+// bounds are dropped from the cache (a call still using one keeps it alive until it returns).
+std::shared_ptr<DeviceCopy> cache_entry(const VbtFile& f)
 {
+    std::vector<std::shared_ptr<DeviceCopy>> dropped;   // destroyed after the lock is released
     std::lock_guard<std::mutex> lock(g_cache_mu);
-    auto it = g_cache.find(&f);
-    if (it != g_cache.end()) {
-        const CacheEntry& c = it->second;
-        if (c.scales == f.coarseAcScales.data() && c.offsets == f.offsetsWords.data() &&
-            c.payload == f.payloadWords.data() && c.ns == f.coarseAcScales.size() && c.no == f.offsetsWords.size() &&
-            c.np == f.payloadWords.size())
-            return c.asset;
-        vbt_asset_destroy(c.asset);
-        g_cache.erase(it);
+    auto& slot = g_cache[&f];
+    if (!slot) slot = std::make_shared<DeviceCopy>();
+    slot->tick = ++g_tick;
+    std::shared_ptr<DeviceCopy> mine = slot;
+    for (;;) {
+        uint64_t bytes = 0;
+        auto oldest = g_cache.end();
+        for (auto it = g_cache.begin(); it != g_cache.end(); ++it) {
+            bytes += it->second->device_bytes;
+            if (it->second != mine && (oldest == g_cache.end() || it->second->tick < oldest->second->tick)) oldest = it;
+        }
+        if (oldest == g_cache.end() || (g_cache.size() <= kMaxCopies && bytes <= kMaxCopyBytes)) break;
+        dropped.push_back(std::move(oldest->second));
+        g_cache.erase(oldest);
     }
-    const auto img = image_of(f);
-    vbt_asset* a = nullptr;
-    const int st = vbt_asset_create(img.data(), img.size(), 0, &a);
-    if (st) throw std::runtime_error(vbt_last_error());
-    g_cache[&f] = CacheEntry{f.coarseAcScales.data(), f.offsetsWords.data(), f.payloadWords.data(),
-                             f.coarseAcScales.size(), f.offsetsWords.size(), f.payloadWords.size(), a};
-    return a;
+    return mine;
+}
+
+bool same_words(const uint8_t* a, const void* b, size_t words) { return std::memcmp(a, b, 4 * words) == 0; }
+
+// Make c->asset decode `f`: compare the header, the scales and the payload of the leaves in
+// `leaves` (every leaf when `all`) with the uploaded image, and upload `f` again when they differ.
+// Called with c->mu held.
+vbt_asset* synced(DeviceCopy& c, const VbtFile& f, const std::vector<uint32_t>& leaves, bool all)
+{
+    const size_t ns = f.coarseAcScales.size(), no = f.offsetsWords.size(), np = f.payloadWords.size();
+    const size_t bytes = 52 + 4 * (ns + no + np);
+    bool fresh = c.asset != nullptr && c.image.size() == bytes;
+    if (fresh) {
+        uint8_t head[52];
+        std::memcpy(head, f.header.magic, 8);
+        const uint32_t w[11] = {f.header.version, f.header.width, f.header.height, f.header.depth, f.header.frames,
+                                f.header.leafSize, f.header.coarseResolution, f.header.maxCoarseKeep,
+                                f.header.leafCount, f.header.profileType, f.header.coarseAcScaleCount};
+        std::memcpy(head + 8, w, 44);
+        const uint8_t* img = c.image.data();
+        const uint8_t* off = img + 52 + 4 * ns;
+        const uint8_t* pay = off + 4 * no;
+        fresh = std::memcmp(img, head, 52) == 0 && same_words(img + 52, f.coarseAcScales.data(), ns);
+        if (fresh && all) {
+            fresh = same_words(off, f.offsetsWords.data(), no) && same_words(pay, f.payloadWords.data(), np);
+        } else if (fresh) {
+            fresh = no > 0 && same_words(off + 4 * (no - 1), &f.offsetsWords[no - 1], 1);
+            for (size_t i = 0; fresh && i < leaves.size(); ++i) {
+                const uint32_t l = leaves[i];
+                if (l + 1u >= no) continue;   // the decode reads no such leaf
+                fresh = same_words(off + 4ull * l, &f.offsetsWords[l], 2);
+                const uint32_t w0 = f.offsetsWords[l], w1 = f.offsetsWords[l + 1];
+                if (fresh && w0 < w1 && w1 <= np) fresh = same_words(pay + 4ull * w0, &f.payloadWords[w0], w1 - w0);
+            }
+        }
+    }
+    if (fresh) return c.asset;
+    std::vector<uint8_t> img = image_of(f);
+    if (c.asset && c.image.size() == img.size() && std::memcmp(c.image.data(), img.data(), 52) == 0) {
+        // same header and sizes: into the resident buffers
+        int st = vbt_asset_upload(c.asset, img.data(), img.size(), nullptr);
+        if (st == VBT_STATUS_OK && cudaDeviceSynchronize() != cudaSuccess) st = VBT_STATUS_CUDA;
+        if (st) throw std::runtime_error(vbt_last_error());
+    } else {
+        if (c.asset) vbt_asset_destroy(c.asset);
+        c.asset = nullptr;
+        c.device_bytes = 0;
+        vbt_asset* a = nullptr;
+        if (vbt_asset_create(img.data(), img.size(), 0, &a)) throw std::runtime_error(vbt_last_error());
+        c.asset = a;
+        vbt_asset_info info{};
+        if (vbt_asset_get_info(a, &info) == VBT_STATUS_OK) c.device_bytes = info.device_bytes;
+    }
+    c.image = std::move(img);
+    return c.asset;
 }
 
 }  // namespace
@@ -886,19 +978,43 @@ void sortQueriesByLeaf(std::vector<Query4D>& queries)
 
 std::vector<float> decodeValuesGpu(const VbtFile& file, const std::vector<Query4D>& queries)
 {
-    vbt_asset* a = device_copy(file);
     std::vector<uint32_t> q(queries.size() * 4);
+    std::vector<uint32_t> leaves;
+    leaves.reserve(queries.size());
+    const VbtFileHeader& h = file.header;
     for (size_t i = 0; i < queries.size(); ++i) {
         q[4 * i] = queries[i].x;
         q[4 * i + 1] = queries[i].y;
         q[4 * i + 2] = queries[i].z;
         q[4 * i + 3] = queries[i].t;
+        if (queries[i].x < h.width && queries[i].y < h.height && queries[i].z < h.depth)
+            leaves.push_back(leafIndexForVoxel(h, queries[i].x, queries[i].y, queries[i].z));
     }
+    std::sort(leaves.begin(), leaves.end());
+    leaves.erase(std::unique(leaves.begin(), leaves.end()), leaves.end());
+    const bool all = leaves.size() * 4 >= h.leafCount;   // most leaves: compare the file in one pass
     std::vector<float> out(queries.size());
+    const std::shared_ptr<DeviceCopy> c = cache_entry(file);
+    std::lock_guard<std::mutex> lock(c->mu);
+    vbt_asset* a = synced(*c, file, leaves, all);
     const int st = vbt_query_points_host(a, q.data(), queries.size(), out.data(), nullptr);
     if (st) throw std::runtime_error(vbt_last_error());
     return out;
 }
+
+namespace {
+// A dense frame of `file` through its device copy (every leaf is read).
+std::vector<float> frames_of(const VbtFile& file, int frameIndex)
+{
+    std::vector<float> out(size_t(file.header.width) * file.header.height * file.header.depth);
+    const std::shared_ptr<DeviceCopy> c = cache_entry(file);
+    std::lock_guard<std::mutex> lock(c->mu);
+    vbt_asset* a = synced(*c, file, {}, true);
+    const int st = vbt_decode_frames_host(a, &frameIndex, 1, out.data(), nullptr);
+    if (st) throw std::runtime_error(vbt_last_error());
+    return out;
+}
+}  // namespace
 
 float decodeScientificValueAtCpu(const VbtFile& file, const Query4D& query)
 {
@@ -911,31 +1027,29 @@ float decodeScientificValueAtCpu(const VbtFile& file, const Query4D& query)
 std::vector<float> reconstructScientificFrameCpu(const VbtFile& file, uint32_t frameIndex)
 {
     if (frameIndex >= file.header.frames) throw std::out_of_range("frame outside the asset's frames");
-    vbt_asset* a = device_copy(file);
-    std::vector<float> out(size_t(file.header.width) * file.header.height * file.header.depth);
-    const int f = static_cast<int>(frameIndex);
-    const int st = vbt_decode_frames_host(a, &f, 1, out.data(), nullptr);
-    if (st) throw std::runtime_error(vbt_last_error());
-    return out;
+    return frames_of(file, static_cast<int>(frameIndex));
 }
 
 std::vector<float> decodeRenderTemporalFrame(const VbtFile& file, int frameIndex)
 {
-    vbt_asset* a = device_copy(file);
-    std::vector<float> out(size_t(file.header.width) * file.header.height * file.header.depth);
-    const int st = vbt_decode_frames_host(a, &frameIndex, 1, out.data(), nullptr);
-    if (st) throw std::runtime_error(vbt_last_error());
-    return out;
+    return frames_of(file, frameIndex);
 }
 
 void releaseDeviceCopy(const VbtFile& file)
 {
+    std::shared_ptr<DeviceCopy> dropped;   // destroyed after the lock, once no call uses it
     std::lock_guard<std::mutex> lock(g_cache_mu);
     auto it = g_cache.find(&file);
     if (it != g_cache.end()) {
-        vbt_asset_destroy(it->second.asset);
+        dropped = std::move(it->second);
         g_cache.erase(it);
     }
+}
+
+size_t deviceCopyCount()
+{
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    return g_cache.size();
 }
 
 }  // namespace vbt::render
