@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--no-keyframes", action="store_true")
     p.add_argument("--no-writer", action="store_true")
     p.add_argument("--serve-requests", type=int, default=300)
+    p.add_argument("--no-ref-queries", action="store_true")
     return p.parse_args()
 
 
@@ -290,6 +291,29 @@ def serve_once(vbt, assets, reqs, pinned, plain, arrivals):
             "launches": int(st.launches), "units": int(st.units), "arena_peak_bytes": int(st.arena_peak_bytes)}
 
 
+def equal_p99_sweep(vbt, assets, reqs, inputs, at_rate, plain_capacity, served_capacity):
+    """Throughput of served and plain at equal p99: the target p99 is plain's own at 0.8x its
+    closed-loop capacity; each path is swept over Poisson arrival rates (multiples of plain's
+    capacity up to 1.2x its own) and the highest rate whose p99 stays within the target is that
+    path's sustained throughput at equal p99."""
+    target = serve_once(vbt, assets, reqs, inputs, True, at_rate(0.8 * plain_capacity))["p99_ms"]
+    rows = {"plain": [], "served": []}
+    best = {"plain": 0.0, "served": 0.0}
+    for name, plain, cap in (("plain", True, plain_capacity), ("served", False, served_capacity)):
+        for m in (0.5, 0.8, 1.0, 1.25, 1.5, 2.0, 2.5, 3.0, 4.0, 5.0, 6.0, 8.0):
+            rate = m * plain_capacity
+            if rate > 1.2 * cap:
+                break
+            r = serve_once(vbt, assets, reqs, inputs, plain, at_rate(rate))
+            rows[name].append({"rate_req_per_s": rate, "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
+                               "achieved_req_per_s": r["requests_per_s"]})
+            if r["p99_ms"] <= target:
+                best[name] = max(best[name], r["requests_per_s"])
+    return {"target_p99_ms": target, "sweep": rows, "plain_req_per_s_at_target": best["plain"],
+            "served_req_per_s_at_target": best["served"],
+            "throughput_ratio_at_equal_p99": best["served"] / best["plain"] if best["plain"] > 0 else None}
+
+
 def run_serving(args, local_rank):
     """The serving mix over the resident assets: served (4 streams, HBM-budget admission, point
     requests merged across assets) against plain (one request per launch, one launch in flight),
@@ -341,6 +365,10 @@ def run_serving(args, local_rank):
     d_open_s_p = serve_once(vbt, assets, reqs, dev, False, at_rate(d_lam_p))
     d_open_p_p = serve_once(vbt, assets, reqs, dev, True, at_rate(d_lam_p))
     d_open_s_s = serve_once(vbt, assets, reqs, dev, False, at_rate(d_lam_s))
+    equal_host = equal_p99_sweep(vbt, assets, reqs, pinned, at_rate, closed_p["requests_per_s"],
+                                 closed_s["requests_per_s"])
+    equal_dev = equal_p99_sweep(vbt, assets, reqs, dev, at_rate, d_closed_p["requests_per_s"],
+                                d_closed_s["requests_per_s"])
     for a in assets:
         a.close()
     return {"workload": "serving mix: 70% point batches of 1e3-1e6 uniform (x,y,z,t), 20% z-slices over 1-16 "
@@ -353,6 +381,7 @@ def run_serving(args, local_rank):
                        "poisson_at_0.8x_served_capacity": open_s_s},
             "plain": {"closed_loop": closed_p, "poisson_at_0.8x_plain_capacity": open_p_p},
             "throughput_ratio_closed_loop": closed_s["decoded_values_per_s"] / closed_p["decoded_values_per_s"],
+            "equal_p99": equal_host,
             "arrival_rates_req_per_s": {"0.8x_plain": lam_p, "0.8x_served": lam_s},
             "device_resident": {
                 "workload": "the same requests with point inputs in device memory and every result device-resident",
@@ -360,6 +389,7 @@ def run_serving(args, local_rank):
                            "poisson_at_0.8x_served_capacity": d_open_s_s},
                 "plain": {"closed_loop": d_closed_p, "poisson_at_0.8x_plain_capacity": d_open_p_p},
                 "throughput_ratio_closed_loop": d_closed_s["decoded_values_per_s"] / d_closed_p["decoded_values_per_s"],
+                "equal_p99": equal_dev,
                 "arrival_rates_req_per_s": {"0.8x_plain": d_lam_p, "0.8x_served": d_lam_s}}}
 
 
@@ -743,6 +773,81 @@ def run_keyframes(args, local_rank, reps=3, work=None):
     return out
 
 
+# ------------------------------------------------------------------------------ reference CUDA queries
+REF_QUERY_BENCH = os.path.join(ROOT, "oracle", "_ref", "vbt_cuda_query_bench")
+REF_QUERY_ASSETS = ["mix_sci", "sci_modes", "cfg5_sci"]
+
+
+def run_reference_queries(args, local_rank, n=1_000_000, repeats=100):
+    """Scientific point queries on one B200: the reference's own CUDA benchmark
+    (render/src/vbt_cuda_query_bench.cu, vbtQueryKernel on the queries as drawn and
+    vbtGroupedLeafQueryKernel on them sorted by leaf; built unmodified for sm_100a by
+    oracle/Makefile) beside this library's point-query kernel, on the same asset, the same number
+    of uniform random (x, y, z, t) queries (the reference's generator and seed on its side, numpy's
+    on this one), the same repeat count, device time by CUDA events over the repeats on both
+    sides, inputs resident."""
+    import tempfile
+
+    import torch
+    import vbt_b200 as vbt
+    if not os.path.exists(REF_QUERY_BENCH):
+        return {"skipped": "oracle/_ref/vbt_cuda_query_bench not built (the reference tree is absent)"}
+    out = {}
+    dev = f"cuda:{local_rank}"
+    for name in REF_QUERY_ASSETS:
+        path = os.path.join(ROOT, "assets", name + ".vbtp")
+        if not os.path.exists(path):
+            continue
+        with tempfile.TemporaryDirectory() as td:
+            js = os.path.join(td, "ref.json")
+            cmd = [REF_QUERY_BENCH, "--input-vbt", path, "--query-count", str(n), "--pattern", "random",
+                   "--fixed-frame", "0", "--seed", "7", "--repeats", str(repeats), "--json-out", js]
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            if r.returncode != 0 or not os.path.exists(js):
+                out[name] = {"reference_failed": (r.stderr or r.stdout)[-300:]}
+                continue
+            ref = json.load(open(js))
+        a = vbt.Asset(path, device=local_rank)
+        X, Y, Z = a.dims
+        T = a.frames
+        rng = np.random.default_rng(7)
+        q = np.stack([rng.integers(0, X, n), rng.integers(0, Y, n), rng.integers(0, Z, n), rng.integers(0, T, n)],
+                     1).astype(np.uint32)
+        leaf = ((q[:, 2] // 8) * ((Y + 7) // 8) + q[:, 1] // 8) * ((X + 7) // 8) + q[:, 0] // 8
+        q_sorted = q[np.lexsort((q[:, 0], q[:, 1], q[:, 2], q[:, 3], leaf))]
+        res = {}
+        for label, qq in (("unsorted", q), ("sorted", q_sorted)):
+            dq = torch.from_numpy(np.ascontiguousarray(qq).view(np.int32)).to(dev)
+            o = torch.empty(n, dtype=torch.float32, device=dev)
+            s = torch.cuda.Stream(device=dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s):
+                for _ in range(3):
+                    a.query_points(dq, o, stream=s)
+                e0.record(s)
+                for _ in range(repeats):
+                    a.query_points(dq, o, stream=s)
+                e1.record(s)
+            s.synchronize()
+            a.sync_status(s)
+            ms = e0.elapsed_time(e1)
+            res[label] = {"kernel_ms": ms, "queries_per_s": n * repeats / (ms * 1e-3)}
+        a.close()
+        best_ref = max(ref["unsorted"]["queries_per_sec"], ref["sorted"]["queries_per_sec"])
+        out[name] = {"queries": n, "repeats": repeats, "pattern": "uniform random (x, y, z, t)",
+                     "reference_cuda": {"unsorted_queries_per_s": ref["unsorted"]["queries_per_sec"],
+                                        "sorted_grouped_queries_per_s": ref["sorted"]["queries_per_sec"],
+                                        "max_abs_diff_vs_reference_cpu": max(ref["unsorted"]["max_abs_diff"],
+                                                                            ref["sorted"]["max_abs_diff"])},
+                     "ours": {"unsorted_queries_per_s": res["unsorted"]["queries_per_s"],
+                              "sorted_queries_per_s": res["sorted"]["queries_per_s"]},
+                     "speedup_unsorted": res["unsorted"]["queries_per_s"] / ref["unsorted"]["queries_per_sec"],
+                     "speedup_sorted": res["sorted"]["queries_per_s"] / ref["sorted"]["queries_per_sec"],
+                     "speedup_best_vs_best": max(res["unsorted"]["queries_per_s"], res["sorted"]["queries_per_s"]) /
+                     best_ref}
+    return out or {"skipped": "no scientific asset generated"}
+
+
 # ------------------------------------------------------------------------------ writer
 def run_writer(args, local_rank, reps=5):
     """The VBTPACK4 writer on one B200 (vbt_pack_leaves: every leaf's control streams packed and the
@@ -991,6 +1096,10 @@ def run_ours(args, rank, local_rank, world):
     if rank == 0 and world == 1 and not args.no_writer:
         writer = run_writer(args, local_rank)
 
+    ref_queries = None
+    if rank == 0 and world == 1 and not args.no_ref_queries:
+        ref_queries = run_reference_queries(args, local_rank)
+
     window = window_render = None
     if rank == 0 and world == 1 and not args.no_window:
         window = run_window(args, local_rank)
@@ -1016,6 +1125,9 @@ def run_ours(args, rank, local_rank, world):
                            "cache_ring_bytes": int(cache.numel() * 4), "parallelism": f"replicas x{world}"},
                 "roofline": {"bound": "hbm", "kernel": "decode_leaf_kernel<cache>", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                             "traffic_source": "profiles/decode_leaf_cfg2.md: dram bytes of one ncu capture of "
+                                               "this kernel on this workload (not measured by this run)"
+                             if traffic is not None else None,
                              "algorithmic_bytes_per_launch": int(statistics.mean(alg_per_launch)),
                              "launch_ms": statistics.mean(dec_ms), "peak_source": peak_src},
                 "kernels_ms": {"page_table": statistics.mean(pt_ms), "decode_per_launch": statistics.mean(dec_ms)},
@@ -1028,7 +1140,7 @@ def run_ours(args, rank, local_rank, world):
                           "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
                 "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "precision_window": window,
                 "precision_window_render": window_render, "full_frame": full_frame, "ray_sampler": sampler,
-                "keyframe_pass": keyframes, "writer": writer,
+                "keyframe_pass": keyframes, "writer": writer, "point_queries_vs_reference_cuda": ref_queries,
                 "gpu_launches": args.steps * (1 + len(chunks)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
