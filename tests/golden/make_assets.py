@@ -26,6 +26,8 @@ Field recipes (shapes are X x Y x Z x T):
                   DenseGrid leaves of both residual subtypes (per-frame BFP and DCT temporal basis).
   sci_modes       64^3 x 32 with regions of each kind: all four generic modes and both dense
                   subtypes in one asset.
+  cfg5_sci        the config-5 scientific field at its stated size, 512^3 x 64 (generated to disk
+                  frame by frame and encoded from there).
   mix_fire_*      the config-3 fire (density, flames, temperature = 300 + 1500 flames + N(0, 20))
                   at 128 x 128 x 192 x 40: fBm inside a sphere of radius 20 + 2.5 t.
   mix_sdf         the config-4 liquid level set at 128^3 x 48 (sloshing plane, 20 ballistic spheres
@@ -194,6 +196,60 @@ def grf_scientific(shape_xyz, frames, seed, spike_frac=0.001, spike_sigma=10.0):
     return out
 
 
+def grf_scientific_to_file(shape_xyz, frames, seed, raw_path, spike_frac=0.001, spike_sigma=10.0):
+    """grf_scientific's recipe for fields too large to hold in memory (configuration 5: 512^3 x 64
+    float32, 34 GB), written straight to a time-fastest RAW file ([Z, Y, X, T]).  Frames are made
+    one at a time by a float32 inverse FFT into a frame-major scratch file beside raw_path, then
+    transposed slab by slab; the field is divided by its standard deviation over all frames and
+    0.1% of its values get spikes of +-10 sigma, as in grf_scientific (the random draws differ, so
+    the field is not grf_scientific's for the same seed).  Returns the field's min and max."""
+    import scipy.fft
+    rng = np.random.default_rng(seed)
+    X, Y, Z = shape_xyz
+    kz = np.fft.fftfreq(Z).astype(np.float32)[:, None, None]
+    ky = np.fft.fftfreq(Y).astype(np.float32)[None, :, None]
+    kx = np.fft.fftfreq(X).astype(np.float32)[None, None, :]
+    k = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    k[0, 0, 0] = 1.0
+    amp = (k ** np.float32(-5.0 / 6.0)).astype(np.float32)
+    amp[0, 0, 0] = 0.0
+    del k
+    phase0 = rng.uniform(0, 2 * np.pi, amp.shape).astype(np.float32)
+    omega = rng.normal(0.0, 0.08, amp.shape).astype(np.float32)
+    scratch = raw_path + ".frames"
+    fm = np.memmap(scratch, np.float32, "w+", shape=(frames, Z, Y, X))
+    sq = 0.0
+    for t in range(frames):
+        spec = amp * np.exp(1j * (phase0 + omega * np.float32(t))).astype(np.complex64)
+        f = scipy.fft.ifftn(spec, workers=os.cpu_count()).real.astype(np.float32)
+        del spec
+        fm[t] = f
+        sq += float(np.square(f, dtype=np.float64).sum())
+        del f
+    fm.flush()
+    del amp, phase0, omega
+    n = frames * X * Y * Z
+    sigma = np.float32(max(np.sqrt(sq / n), 1e-12))
+    n_spk = max(1, int(spike_frac * n))
+    idx = np.sort(rng.choice(n, n_spk, replace=False))
+    sgn = np.sign(rng.normal(size=n_spk)).astype(np.float32)
+    out = np.memmap(raw_path, np.float32, "w+", shape=(Z, Y, X, frames))
+    slab = max(1, (256 << 20) // (Y * X * frames * 4))
+    lo_v, hi_v = float("inf"), float("-inf")
+    for z0 in range(0, Z, slab):
+        z1 = min(Z, z0 + slab)
+        block = np.ascontiguousarray(np.moveaxis(np.asarray(fm[:, z0:z1]), 0, -1)) / sigma
+        lo, hi = np.searchsorted(idx, [z0 * Y * X * frames, z1 * Y * X * frames])
+        flat = block.reshape(-1)
+        flat[idx[lo:hi] - z0 * Y * X * frames] += np.float32(spike_sigma) * sgn[lo:hi]
+        out[z0:z1] = block
+        lo_v, hi_v = min(lo_v, float(block.min())), max(hi_v, float(block.max()))
+    out.flush()
+    del fm, out
+    os.remove(scratch)
+    return lo_v, hi_v
+
+
 def _drifting_blobs(shape_xyz, frames, rng, n, sigma_lo, sigma_hi):
     """[Z, Y, X, T] sum of n Gaussian blobs (amplitude U(0.5, 1.5)) drifting at N(0, 0.3) voxels
     per frame, and the voxel coordinate grids."""
@@ -283,6 +339,32 @@ def encode(name, data, xyzt, profile, extra_meta=None, time_fastest=False, args=
     return out
 
 
+def encode_large_scientific(name, shape_xyz, frames, seed):
+    """A scientific field written to disk by grf_scientific_to_file and encoded from there (the
+    encoder reads the RAW file itself); the scratch files go under VBT_ASSET_TMP (default: the
+    system temporary directory) and need about twice the RAW size."""
+    os.makedirs(ASSETS, exist_ok=True)
+    if not os.path.exists(ENCODER):
+        sys.path.insert(0, ROOT)
+        from oracle.oracle import build
+        build(ref=True)
+    X, Y, Z = shape_xyz
+    with tempfile.TemporaryDirectory(dir=os.environ.get("VBT_ASSET_TMP")) as td:
+        raw = os.path.join(td, name + ".raw")
+        lo, hi = grf_scientific_to_file(shape_xyz, frames, seed, raw)
+        meta = os.path.join(td, name + ".metadata.json")
+        with open(meta, "w") as fh:
+            json.dump({"dimensions": [X, Y, Z, frames], "axis_order": ["X", "Y", "Z", "T"],
+                       "time_is_fastest_dimension": True, "data_type": "float32", "data_min": lo,
+                       "data_max": hi}, fh)
+        out = os.path.join(ASSETS, name + ".vbtp")
+        cmd = [ENCODER, "--input-raw", raw, "--metadata", meta, "--profile", "generic", "--save-vbt", out,
+               "--report", os.path.join(td, "report.md"), "--omp-threads", str(os.cpu_count())]
+        subprocess.check_call(cmd, stdout=subprocess.DEVNULL)
+    print(f"{name}: {os.path.getsize(out)} bytes")
+    return out
+
+
 LEVELSET = {"conversion_mode": "levelset", "shell_width_voxels": 3.0, "voxel_size": 1.0}
 
 RECIPES = {
@@ -306,6 +388,8 @@ RECIPES = {
     "sci_dense_tb": lambda: encode("sci_dense_tb", sci_flicker((24, 16, 20), 16, 3, 0.3, "mid"), (24, 16, 20, 16),
                                    "generic", time_fastest=True,
                                    args=("--generic-dense-temporal-basis", "--generic-dense-temporal-keep", "8")),
+    # configuration 5's scientific field at its stated size (512^3 x 64, time fastest, 34 GB of RAW)
+    "cfg5_sci": lambda: encode_large_scientific("cfg5_sci", (512, 512, 512), 64, 8),
     "sci_modes": lambda: encode("sci_modes", sci_modes((64, 64, 64), 32, 21), (64, 64, 64, 32), "generic",
                                 time_fastest=True,
                                 args=("--generic-dense-temporal-basis", "--generic-dense-temporal-keep", "8")),
