@@ -310,6 +310,17 @@ __device__ __noinline__ void leaf_decode_general(const DeviceAsset& a, M m, Leaf
                                                 FrameSink<DENSE>{a, G, out, frame_stride});
 }
 
+// The specialised decode (rt_leaf_fast.cuh) as a call of its own too: each path gets the whole
+// register budget of the 288-thread launch.
+template <bool FINE, bool DENSE>
+__device__ __noinline__ void leaf_decode_fast_call(const DeviceAsset& a, LeafEntry e, uint32_t lb, int nframes,
+                                                   LeafGeom G, float* __restrict__ out, uint64_t frame_stride)
+{
+    extern __shared__ __align__(128) uint8_t dyn[];
+    const LeafSmem s = leaf_layout<kDecWarps>(dyn);
+    leaf_decode_fast<FINE, kDecWarps>(s.stage, lb, s, e, nframes, G, FrameSink<DENSE>{a, G, out, frame_stride});
+}
+
 // Staged GRID4 / FINE6 leaves of the common shape take leaf_decode_fast (rt_leaf_fast.cuh), every
 // other leaf the general leaf_decode.
 template <bool DENSE, bool GLOBAL_FALLBACK>
@@ -394,10 +405,9 @@ __global__ void __launch_bounds__(kDecThreads, 2) decode_leaf_kernel(const __gri
             if (staged) phase ^= 1u;
             bool fine = false;
             if (staged && fast_leaf_shape(e, steps01, fine)) {
-                const FrameSink<DENSE> sink{a, G, out, frame_stride};
                 const uint32_t lb = (uint32_t)(b0 - a0);
-                if (fine) leaf_decode_fast<true, kDecWarps>(s.stage, lb, s, e, fl.n, G, sink);
-                else leaf_decode_fast<false, kDecWarps>(s.stage, lb, s, e, fl.n, G, sink);
+                if (fine) leaf_decode_fast_call<true, DENSE>(a, e, lb, fl.n, G, out, frame_stride);
+                else leaf_decode_fast_call<false, DENSE>(a, e, lb, fl.n, G, out, frame_stride);
             } else if (staged) {
                 const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
                 leaf_decode_general<SharedWords, DENSE>(a, m, e, fl.n, steps01, monotone, G, out, frame_stride);

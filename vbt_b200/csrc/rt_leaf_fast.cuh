@@ -119,14 +119,15 @@ __device__ __forceinline__ void axis_row(const float4* __restrict__ w16, int axi
     i1 = __float_as_int(r.w);
 }
 
-// trilinear_quads_ptr (rt_staged.cuh) for a compile-time even resolution R: the same lerps on the
-// same operands in the same order, with the item loops unrolled.
+// The x- and y-phases of trilinear_quads_ptr (rt_staged.cuh) for a compile-time even resolution R:
+// the same lerps on the same operands in the same order, item loops unrolled.  x-lerps go to x2
+// ([control row z*R + y][lx pair]), y-lerps to y4 ([control row z][ly][lx quad]).
 template <int R>
-__device__ __forceinline__ void trilinear_fixed(const float4* __restrict__ w16, float2* x2, float4* y4,
-                                                const float* __restrict__ g, int lane, float4 q[4])
+__device__ __forceinline__ void trilinear_xy(const float4* __restrict__ w16, float2* x2, float4* y4,
+                                             const float* __restrict__ g, int lane)
 {
     static_assert(R % 2 == 0 && R >= 2 && R <= 6, "even resolutions up to 6");
-    constexpr int NX = R * R * 4;   // x items: [control row z*R + y][lx pair]
+    constexpr int NX = R * R * 4;
     {
         const int p = lane & 3;
         float ta, oa, tb, ob;
@@ -146,36 +147,35 @@ __device__ __forceinline__ void trilinear_fixed(const float4* __restrict__ w16, 
     }
     __syncwarp();
     const int k = lane & 1;
-    {
-        float t, o;
-        int i0, i1;
-        axis_row(w16, 1, (lane >> 1) & 7, t, o, i0, i1);
-        const float2 ty = make_float2(t, t), oy = make_float2(o, o);
+    float t, o;
+    int i0, i1;
+    axis_row(w16, 1, (lane >> 1) & 7, t, o, i0, i1);
+    const float2 ty = make_float2(t, t), oy = make_float2(o, o);
 #pragma unroll
-        for (int m = 0; m < R / 2; ++m) {   // y items: [control row z][ly][lx quad], R * 16 of them
-            const int z = (lane >> 4) + 2 * m;
-            const float4 a = *reinterpret_cast<const float4*>(x2 + (z * R + i0) * 4 + 2 * k);
-            const float4 b = *reinterpret_cast<const float4*>(x2 + (z * R + i1) * 4 + 2 * k);
-            const float2 lo2 = lerp2(make_float2(a.x, a.y), make_float2(b.x, b.y), ty, oy);
-            const float2 hi2 = lerp2(make_float2(a.z, a.w), make_float2(b.z, b.w), ty, oy);
-            y4[lane + 32 * m] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
-        }
+    for (int m = 0; m < R / 2; ++m) {   // R * 16 y items
+        const int z = (lane >> 4) + 2 * m;
+        const float4 a = *reinterpret_cast<const float4*>(x2 + (z * R + i0) * 4 + 2 * k);
+        const float4 b = *reinterpret_cast<const float4*>(x2 + (z * R + i1) * 4 + 2 * k);
+        const float2 lo2 = lerp2(make_float2(a.x, a.y), make_float2(b.x, b.y), ty, oy);
+        const float2 hi2 = lerp2(make_float2(a.z, a.w), make_float2(b.z, b.w), ty, oy);
+        y4[lane + 32 * m] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
     }
     __syncwarp();
-    const int ly = (lane >> 1) & 7;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        float tz, oz;
-        int i0, i1;
-        axis_row(w16, 2, 2 * i + (lane >> 4), tz, oz, i0, i1);
-        const float4 A = y4[(i0 * 8 + ly) * 2 + k];
-        const float4 B = y4[(i1 * 8 + ly) * 2 + k];
-        const float2 t = make_float2(tz, tz), omt = make_float2(oz, oz);
-        const float2 lo2 = lerp2(make_float2(A.x, A.y), make_float2(B.x, B.y), t, omt);
-        const float2 hi2 = lerp2(make_float2(A.z, A.w), make_float2(B.z, B.w), t, omt);
-        q[i] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
-    }
-    __syncwarp();
+}
+
+// The z-phase of trilinear_quads_ptr for the lane's quad i (voxels 4 (lane + 32 i) .. + 3).
+__device__ __forceinline__ float4 trilinear_z(const float4* __restrict__ w16, const float4* y4, int lane, int i)
+{
+    const int k = lane & 1, ly = (lane >> 1) & 7;
+    float tz, oz;
+    int i0, i1;
+    axis_row(w16, 2, 2 * i + (lane >> 4), tz, oz, i0, i1);
+    const float4 A = y4[(i0 * 8 + ly) * 2 + k];
+    const float4 B = y4[(i1 * 8 + ly) * 2 + k];
+    const float2 t = make_float2(tz, tz), omt = make_float2(oz, oz);
+    const float2 lo2 = lerp2(make_float2(A.x, A.y), make_float2(B.x, B.y), t, omt);
+    const float2 hi2 = lerp2(make_float2(A.z, A.w), make_float2(B.z, B.w), t, omt);
+    return make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
 }
 
 // Can leaf_decode_fast take this leaf?  (Staged, timeline frames, strictly increasing FP16 keys
@@ -192,6 +192,7 @@ __device__ __forceinline__ bool fast_leaf_shape(const LeafEntry& e, bool steps01
 
 // Decode one staged leaf of the fast shape for all nframes frames of the launch (NW warps; the
 // leaf's bytes start at stage offset lb).  Quads go to sink(frame index, lane, quad, values).
+// Per lane and slot the voxel phase holds one quad at a time.
 template <bool FINE, int NW, class Sink>
 __device__ __forceinline__ void leaf_decode_fast(const uint8_t* __restrict__ st, uint32_t lb, const LeafSmem& s,
                                                  const LeafEntry& e, int nframes, const LeafGeom& G,
@@ -240,35 +241,31 @@ __device__ __forceinline__ void leaf_decode_fast(const uint8_t* __restrict__ st,
             const int fi = pp * Lp + b0 + j;
             if (fi >= min(nframes, (pp + 1) * Lp)) continue;
             const float* g = s.ctrl + slot * CT;
-            float4 q[4];
-            trilinear_fixed<4>(s.w16, x2, y4, g, lane, q);
-            if (FINE) {
-                float4 qf[4];
-                trilinear_fixed<6>(s.w16 + 24, x2, y4, g + CC, lane, qf);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const float2 lo2 = add2_rn(make_float2(q[i].x, q[i].y), make_float2(qf[i].x, qf[i].y));
-                    const float2 hi2 = add2_rn(make_float2(q[i].z, q[i].w), make_float2(qf[i].z, qf[i].w));
-                    q[i] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
-                }
-            }
-            if (plain) {
-#pragma unroll
-                for (int i = 0; i < 4; ++i) sink(fi, lane, i, q[i]);
-                continue;
-            }
+            // FINE6: the fine grid's x/y tables first (y4 region), then the coarse grid's into the
+            // x2 region ([x2: 64 float2][y: 64 float4]); each quad is then coarse + fine, rounded
+            // once (the reference's sum; addition is commutative) and stored at once
+            float4* yc = FINE ? reinterpret_cast<float4*>(x2 + 64) : y4;
+            if (FINE) trilinear_xy<6>(s.w16 + 24, x2, y4, g + CC, lane);
+            trilinear_xy<4>(s.w16, x2, yc, g, lane);
             const int ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const int lz = 2 * i + (lane >> 4);
-                const bool row_in = ly < G.h && lz < G.d;
-                float4 v = q[i];
-                if (!row_in || lx0 >= G.w) v.x = 0.0f;
-                if (!row_in || lx0 + 1 >= G.w) v.y = 0.0f;
-                if (!row_in || lx0 + 2 >= G.w) v.z = 0.0f;
-                if (!row_in || lx0 + 3 >= G.w) v.w = 0.0f;
+                float4 v = trilinear_z(s.w16, yc, lane, i);
+                if (FINE) {
+                    const float4 f = trilinear_z(s.w16 + 24, y4, lane, i);
+                    v = make_float4(__fadd_rn(v.x, f.x), __fadd_rn(v.y, f.y), __fadd_rn(v.z, f.z), __fadd_rn(v.w, f.w));
+                }
+                if (!plain) {
+                    const int lz = 2 * i + (lane >> 4);
+                    const bool row_in = ly < G.h && lz < G.d;
+                    if (!row_in || lx0 >= G.w) v.x = 0.0f;
+                    if (!row_in || lx0 + 1 >= G.w) v.y = 0.0f;
+                    if (!row_in || lx0 + 2 >= G.w) v.z = 0.0f;
+                    if (!row_in || lx0 + 3 >= G.w) v.w = 0.0f;
+                }
                 sink(fi, lane, i, v);
             }
+            __syncwarp();   // the tables are read before the next slot overwrites them
         }
         __syncthreads();
     }
