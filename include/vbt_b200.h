@@ -251,6 +251,41 @@ int vbt_coarse_fit(const float* d_recon, uint32_t width, uint32_t height, uint32
                    const vbt_keyframe_profile* control_profile, uint32_t* d_desc, uint8_t* d_bins,
                    uint16_t* d_key_frames, float* d_key_values, uint32_t* d_key_count, uint8_t* d_required_max_local,
                    float* d_grid, void* stream);
+/* The encoder's FINE6 residual fitting (src/render_temporal_kf_probe_main.cpp:815-850) for the
+ * listed leaves: as vbt_coarse_fit for the 6^3 controls at controlCoords(6), each series the leaf's
+ * sampled reconstruction minus the fitted coarse grid (d_coarse_grid[(i*64 + c) * frames + t],
+ * vbt_coarse_fit's d_grid for the same leaves) sampled at the same position
+ * (sampleControlGridValue, :2240-2286).  Outputs per listed leaf i: d_desc[i*216 + c],
+ * d_bins[(i*216 + c)*8 + b], keyframes from d_key_frames / d_key_values[i * 216 * frames] on,
+ * d_key_count[i], d_required_max_local[i] and optionally d_grid[(i*216 + c) * frames + t]. */
+int vbt_fine6_fit(const float* d_recon, uint32_t width, uint32_t height, uint32_t depth, uint32_t frames,
+                  uint64_t frame_stride, const uint32_t* d_leaves, uint32_t leaf_count,
+                  const vbt_keyframe_profile* control_profile, const float* d_coarse_grid, uint32_t* d_desc,
+                  uint8_t* d_bins, uint16_t* d_key_frames, float* d_key_values, uint32_t* d_key_count,
+                  uint8_t* d_required_max_local, float* d_grid, void* stream);
+/* The encoder's Mode2 shell stage (src/render_temporal_kf_probe_main.cpp:930-1025) for the listed
+ * leaves: the shell voxels (level set: |value| <= surface_band, |coarse| <= guard_band or a sign
+ * change at some frame; otherwise value >= shell_cut), each one's residual over the fitted coarse
+ * grid keyed under control_profile (level sets add addIsoSurfaceKeyFrames at 0 +- temporal_band,
+ * :2051-2078) and appended in voxel order to a 4-bin stream with its reconstructFromKeys values.
+ * Outputs per listed leaf i: the 80-byte occupancy section d_occupancy[i*80], d_desc[i*512 + a],
+ * d_bins[(i*512 + a)*8 + b] (first 4 bytes), keyframes from d_key_frames / d_key_values
+ * [i * 512 * frames] on, d_key_count[i], d_active[i] (shell voxels) and d_required_max_local[i]. */
+int vbt_shell_fit(const float* d_recon, uint32_t width, uint32_t height, uint32_t depth, uint32_t frames,
+                  uint64_t frame_stride, const uint32_t* d_leaves, uint32_t leaf_count,
+                  const vbt_keyframe_profile* control_profile, const float* d_coarse_grid, int levelset,
+                  float surface_band, float guard_band, float temporal_band, float shell_cut, uint8_t* d_occupancy,
+                  uint32_t* d_desc, uint8_t* d_bins, uint16_t* d_key_frames, float* d_key_values,
+                  uint32_t* d_key_count, uint32_t* d_active, uint8_t* d_required_max_local, void* stream);
+/* The encoder's density route (src/render_temporal_kf_probe_main.cpp:1105-1245 with
+ * routeRenderTemporalLeaf, src/render_temporal_route.cpp:27-66) per listed leaf: d_mode[i] = 3
+ * (FINE6) or 1 (GRID4) from the raw field d_raw (frame-major) on the encoder's sampling lattice and
+ * the fitted coarse and FINE6 grids (d_grid of vbt_coarse_fit / vbt_fine6_fit); peak = the field's
+ * max - min (at least 1e-6), visible_lo / visible_hi = render cutoff -/+ its band. */
+int vbt_route_density(const float* d_raw, uint32_t width, uint32_t height, uint32_t depth, uint32_t frames,
+                      uint64_t frame_stride, const uint32_t* d_leaves, uint32_t leaf_count, const float* d_coarse_grid,
+                      const float* d_fine_grid, double peak, double visible_lo, double visible_hi, uint8_t* d_mode,
+                      void* stream);
 /* Self-check of the division the keyframe pass uses for alpha = a / b (no reference counterpart):
  * every 1 <= b <= b_max, 0 <= a <= b against the IEEE quotient on `device`; result[0] = mismatches,
  * result[1] = (b << 16 | a) of the first, or all ones. */

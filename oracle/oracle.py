@@ -108,6 +108,7 @@ class Oracle:
             build()
         L = self.lib = C.CDLL(ORACLE_SO)
         L.vo_load_file.argtypes = [C.c_char_p, C.POINTER(VoFile), C.c_char_p, C.c_size_t]
+        L.vo_load_image.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(VoFile), C.c_char_p, C.c_size_t]
         L.vo_free_file.argtypes = [C.POINTER(VoFile)]
         L.vo_decode_frame.argtypes = [C.POINTER(VoFile), C.c_int, f32p, C.c_int, u32p]
         L.vo_build_page_table.argtypes = [C.POINTER(VoFile), u32p]
@@ -227,8 +228,8 @@ class Oracle:
                                   _ptr(out["err2"], C.POINTER(C.c_double)), threads if threads else os.cpu_count())
         return out
 
-    def load(self, path):
-        return OracleFile(self, path)
+    def load(self, path=None, image=None):
+        return OracleFile(self, path, image)
 
     def decode_control(self, stream, codec, cc, bins, kf, stream_bytes, total, ci, frame, align=True):
         s = np.ascontiguousarray(stream, np.uint8)
@@ -260,11 +261,23 @@ class Oracle:
 
 
 class OracleFile:
-    def __init__(self, oracle, path):
+    """A VBTPACK4 file in the oracle: from a path, or from a file image held in memory (bytes, a
+    numpy array or a host torch tensor)."""
+
+    def __init__(self, oracle, path=None, image=None):
         self.o = oracle
         self.f = VoFile()
         err = C.create_string_buffer(512)
-        if oracle.lib.vo_load_file(path.encode(), C.byref(self.f), err, 512) != 0:
+        if path is not None:
+            st = oracle.lib.vo_load_file(os.fspath(path).encode(), C.byref(self.f), err, 512)
+        elif isinstance(image, (bytes, bytearray)):
+            buf = (C.c_uint8 * len(image)).from_buffer_copy(image)
+            st = oracle.lib.vo_load_image(C.cast(buf, C.c_void_p), len(image), C.byref(self.f), err, 512)
+        else:
+            ptr = image.data_ptr() if hasattr(image, "data_ptr") else image.ctypes.data
+            n = image.numel() * image.element_size() if hasattr(image, "data_ptr") else image.nbytes
+            st = oracle.lib.vo_load_image(C.c_void_p(ptr), n, C.byref(self.f), err, 512)
+        if st != 0:
             raise RuntimeError(err.value.decode())
         self.dims = (self.f.width, self.f.height, self.f.depth)
         self.frames = self.f.frames

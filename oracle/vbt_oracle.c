@@ -6,6 +6,7 @@
  * the reference's does (the reference is compiled for baseline x86-64, which
  * has no FMA).  All file:line citations are paths inside the VBT project.
  */
+#define _POSIX_C_SOURCE 200809L /* fmemopen */
 #include "vbt_oracle.h"
 
 #include <math.h>
@@ -435,6 +436,8 @@ static void set_err(char* err, size_t n, const char* msg)
     if (err && n) snprintf(err, n, "%s", msg);
 }
 
+static int load_stream(FILE* fp, vo_file* out, char* err, size_t n);
+
 int vo_load_file(const char* path, vo_file* out, char* err, size_t n)
 {
     memset(out, 0, sizeof *out);
@@ -445,6 +448,23 @@ int vo_load_file(const char* path, vo_file* out, char* err, size_t n)
         set_err(err, n, b);
         return -1;
     }
+    return load_stream(fp, out, err, n);
+}
+
+/* The same checks and copies over a file image held in memory (read through fmemopen). */
+int vo_load_image(const uint8_t* bytes, uint64_t len, vo_file* out, char* err, size_t n)
+{
+    memset(out, 0, sizeof *out);
+    FILE* fp = (bytes && len) ? fmemopen((void*)bytes, (size_t)len, "rb") : NULL;
+    if (!fp) {
+        set_err(err, n, "Invalid VBTPACK4 file size.");
+        return -1;
+    }
+    return load_stream(fp, out, err, n);
+}
+
+static int load_stream(FILE* fp, vo_file* out, char* err, size_t n)
+{
     fseek(fp, 0, SEEK_END);
     const uint64_t file_bytes = (uint64_t)ftell(fp);
     fseek(fp, 0, SEEK_SET);

@@ -83,6 +83,7 @@ int vo_decode_leaf_frame(const uint8_t* leaf, size_t bytes, int total_frames, in
                          int w, int h, int d, float* out);
 
 int vo_load_file(const char* path, vo_file* out, char* err, size_t err_len);
+int vo_load_image(const uint8_t* bytes, uint64_t len, vo_file* out, char* err, size_t err_len);
 void vo_free_file(vo_file* f);
 
 /* Render-temporal family (profileType 0/1). */

@@ -35,7 +35,8 @@ Field recipes (shapes are X x Y x Z x T):
   mix_sci         the config-5 scientific field at 128^3 x 64, time fastest.
   The mix_* assets, cfg2_plume, cfg1_blobs and cfg4_sdf_small are the serving mix (MIX).
 
-Usage: python tests/golden/make_assets.py [names...]   (default: the small set + cfg1 + cfg2)
+Usage: python tests/golden/make_assets.py [names...]   (default: the small set + cfg1 + cfg2;
+       the name "digests" writes tests/golden/asset_digests.json for the assets present)
 """
 import json
 import os
@@ -412,7 +413,49 @@ MIX = ["cfg2_plume", "mix_fire_density", "mix_fire_flames", "mix_fire_temperatur
 DEFAULT = ["tiny_density", "tiny_levelset", "sci_small", "cfg1_blobs", "cfg4_sdf_small", "sci_64", "cfg2_plume",
            "sci_modes"]
 
+# the raw fields of the render-temporal assets: name -> (recipe, arguments, field of a multi-field
+# recipe or None, (X, Y, Z), level set)
+FIELDS = {
+    "tiny_density": ("blobs", ((20, 12, 17), 9, 3, 11), None, (20, 12, 17), False),
+    "tiny_levelset": ("sdf_scene", ((24, 20, 28), 12, 12.0, 2.0, 0.3, 3, 2.0, 5.0, 12), None, (24, 20, 28), True),
+    "cfg1_blobs": ("blobs", ((64, 64, 64), 24, 6, 1), None, (64, 64, 64), False),
+    "cfg4_sdf_small": ("sdf_scene", ((64, 64, 64), 24, 24.0, 2.0, 0.2, 6, 3.0, 8.0, 4), None, (64, 64, 64), True),
+    "cfg2_plume": ("plume", (256, 96, 2), None, (256, 256, 256), False),
+    "mix_fire_density": ("fire", ((128, 128, 192), 40, 7), 0, (128, 128, 192), False),
+    "mix_fire_flames": ("fire", ((128, 128, 192), 40, 7), 1, (128, 128, 192), False),
+    "mix_fire_temperature": ("fire", ((128, 128, 192), 40, 7), 2, (128, 128, 192), False),
+    "mix_sdf": ("sdf_scene", ((128, 128, 128), 48, 50.0, 12.0, 0.05, 20, 3.0, 12.0, 9), None, (128, 128, 128), True),
+}
+
+
+def field_of(name):
+    """(raw [T, Z, Y, X] float32, (X, Y, Z), level set) of a render-temporal asset's field."""
+    fn, args, index, dims, levelset = FIELDS[name]
+    raw = globals()[fn](*args)
+    return (raw if index is None else raw[index]), dims, levelset
+
+
+DIGESTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "asset_digests.json")
+
+
+def write_digests():
+    """SHA-256 and size of every asset present, so a machine that holds only some of the files can
+    still check a file regenerated there against the one the reference encoder wrote."""
+    import hashlib
+    out = {}
+    for f in sorted(os.listdir(ASSETS)):
+        if f.endswith(".vbtp"):
+            data = open(os.path.join(ASSETS, f), "rb").read()
+            out[f[:-5]] = {"sha256": hashlib.sha256(data).hexdigest(), "bytes": len(data)}
+    with open(DIGESTS, "w") as fh:
+        json.dump(out, fh, indent=1, sort_keys=True)
+        fh.write("\n")
+
+
 if __name__ == "__main__":
     names = sys.argv[1:] or DEFAULT
     for n in names:
-        RECIPES[n]()
+        if n == "digests":
+            write_digests()
+        else:
+            RECIPES[n]()

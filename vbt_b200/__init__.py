@@ -138,6 +138,13 @@ _sig = {
                               _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "vbt_coarse_fit": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _vp, C.c_uint32,
                         C.POINTER(KeyframeProfile), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_fine6_fit": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _vp, C.c_uint32,
+                       C.POINTER(KeyframeProfile), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_shell_fit": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _vp, C.c_uint32,
+                       C.POINTER(KeyframeProfile), _vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                       _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "vbt_route_density": ([_vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _vp, C.c_uint32,
+                           _vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp], C.c_int),
     "vbt_selftest_keyframe_division": ([C.c_uint32, C.POINTER(C.c_uint64), C.c_int], C.c_int),
     "vbt_sample_rays": ([_vp, _vp, C.POINTER(SampleParams), _vp, C.c_uint32, _vp, _vp], C.c_int),
     "vbt_decode_control_cache": ([_vp, C.POINTER(C.c_int), C.c_int, _vp, C.c_uint64, _vp], C.c_int),
@@ -225,6 +232,10 @@ class Asset:
         self._h = _vp()
         if path is not None:
             _check(_lib.vbt_asset_open(os.fspath(path).encode(), device, C.byref(self._h)))
+        elif hasattr(data, "data_ptr") or hasattr(data, "ctypes"):   # a host torch tensor or numpy array
+            ptr = data.data_ptr() if hasattr(data, "data_ptr") else data.ctypes.data
+            n = data.numel() * data.element_size() if hasattr(data, "data_ptr") else data.nbytes
+            _check(_lib.vbt_asset_create(C.c_void_p(ptr), n, device, C.byref(self._h)))
         else:
             buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
             _check(_lib.vbt_asset_create(C.cast(buf, _vp), len(data), device, C.byref(self._h)))
@@ -446,6 +457,43 @@ def coarse_fit(recon, dims, leaves, profile, desc, bins, key_frames, key_values,
     _check(_lib.vbt_coarse_fit(_addr(recon), X, Y, Z, frames, recon.stride(0), _addr(leaves), leaves.numel(),
                                C.byref(profile), _addr(desc), _addr(bins), _addr(key_frames), _addr(key_values),
                                _addr(key_count), _addr(required), _addr(grid), _stream(stream)))
+
+
+def fine6_fit(recon, dims, leaves, profile, coarse_grid, desc, bins, key_frames, key_values, key_count, required,
+              grid=None, stream=None):
+    """The encoder's FINE6 residual fitting on the GPU: as coarse_fit for the 6^3 controls at
+    controlCoords(6), each series the sampled reconstruction minus coarse_grid ([n, 64, frames],
+    coarse_fit's grid of the same leaves) sampled at the same position.  Outputs desc [n, 216],
+    bins [n, 216, 8], key_frames / key_values [n, 216 * frames], key_count [n], required [n] and
+    optionally grid [n, 216, frames]."""
+    frames = recon.shape[0]
+    X, Y, Z = dims
+    _check(_lib.vbt_fine6_fit(_addr(recon), X, Y, Z, frames, recon.stride(0), _addr(leaves), leaves.numel(),
+                              C.byref(profile), _addr(coarse_grid), _addr(desc), _addr(bins), _addr(key_frames),
+                              _addr(key_values), _addr(key_count), _addr(required), _addr(grid), _stream(stream)))
+
+
+def shell_fit(recon, dims, leaves, profile, coarse_grid, levelset, surface_band, guard_band, temporal_band, shell_cut,
+              occupancy, desc, bins, key_frames, key_values, key_count, active, required, stream=None):
+    """The encoder's Mode2 shell stage on the GPU for the listed leaves: occupancy [n, 80] uint8, desc
+    [n, 512], bins [n, 512, 8], key_frames / key_values [n, 512 * frames], key_count [n], active [n]
+    (shell voxels) and required [n]."""
+    frames = recon.shape[0]
+    X, Y, Z = dims
+    _check(_lib.vbt_shell_fit(_addr(recon), X, Y, Z, frames, recon.stride(0), _addr(leaves), leaves.numel(),
+                              C.byref(profile), _addr(coarse_grid), int(levelset), surface_band, guard_band,
+                              temporal_band, shell_cut, _addr(occupancy), _addr(desc), _addr(bins), _addr(key_frames),
+                              _addr(key_values), _addr(key_count), _addr(active), _addr(required), _stream(stream)))
+
+
+def route_density(raw, dims, leaves, coarse_grid, fine_grid, peak, visible_lo, visible_hi, mode, stream=None):
+    """The encoder's density route per listed leaf (mode [n] uint8: 3 FINE6, 1 GRID4) from the raw
+    field raw [frames, >= X*Y*Z] and the fitted coarse and fine grids."""
+    frames = raw.shape[0]
+    X, Y, Z = dims
+    _check(_lib.vbt_route_density(_addr(raw), X, Y, Z, frames, raw.stride(0), _addr(leaves), leaves.numel(),
+                                  _addr(coarse_grid), _addr(fine_grid), float(peak), float(visible_lo),
+                                  float(visible_hi), _addr(mode), _stream(stream)))
 
 
 def keyframe_totals(buf):

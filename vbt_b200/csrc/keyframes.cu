@@ -444,29 +444,77 @@ __global__ void keyframe_division_check_kernel(uint32_t b_max, unsigned long lon
 // (buildBinIndexFromKeys, :2288-2305) and keyframes (frame, sampled value).
 
 struct CoarseOut {
-    uint32_t* desc;          // [leaf][64]
-    uint8_t* bins;           // [leaf][64][8]
-    uint16_t* key_frame;     // [leaf][64 * frames]
-    float* key_value;        // [leaf][64 * frames]
+    uint32_t* desc;          // [leaf][C]
+    uint8_t* bins;           // [leaf][C][8]
+    uint16_t* key_frame;     // [leaf][C * frames]
+    float* key_value;        // [leaf][C * frames]
     uint32_t* key_count;     // [leaf]
     uint8_t* required;       // [leaf] requiredMaxBinLocalKeys
-    float* grid;             // optional [leaf][64][frames]
+    float* grid;             // optional [leaf][C][frames]
 };
 
 // std::clamp(v, lo, hi)
 __device__ __forceinline__ float clamp_r(float v, float lo, float hi) { return v < lo ? lo : (hi < v ? hi : v); }
 
-__global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict__ recon, uint32_t X, uint32_t Y,
-                                                        uint32_t Z, int n, unsigned long long fstride,
-                                                        const uint32_t* __restrict__ leaves, uint32_t n_leaves,
-                                                        vbt_keyframe_profile p, int rmax, CoarseOut o)
+// One axis of sampleControlGridValue (:2240-2286) on a fitted 4^3 grid at controlCoords(4): the
+// position clamped to the extent, the first coordinate at or above it (from the second on), the
+// weight (p - c0) / (c1 - c0).
+__device__ __forceinline__ void grid4_axis(float pos, int ext, int& j0, int& j1, float& w)
 {
+    const float scale = __fdiv_rn(7.0f, 3.0f);
+    const float p = clamp_r(pos, 0.0f, (float)max(0, ext - 1));
+    int k = 1;
+    while (k < 3 && __fmul_rn((float)k, scale) < p) ++k;
+    j1 = k;
+    j0 = k - 1 > 0 ? k - 1 : 0;
+    const float c0 = __fmul_rn((float)j0, scale), c1 = __fmul_rn((float)j1, scale);
+    w = c1 > c0 ? __fdiv_rn(__fsub_rn(p, c0), __fsub_rn(c1, c0)) : 0.0f;
+}
+
+// The fitted 4^3 grid g[ctrl * n + t] sampled at frame t with the axes of grid4_axis, in the
+// encoder's lerp order (x, then y, then z).
+struct Grid4Sample {
+    int x0, x1, y0, y1, z0, z1;
+    float tx, ty, tz;
+    __device__ __forceinline__ void init(float fx, float fy, float fz, int w, int h, int d)
+    {
+        grid4_axis(fx, w, x0, x1, tx);
+        grid4_axis(fy, h, y0, y1, ty);
+        grid4_axis(fz, d, z0, z1, tz);
+    }
+    __device__ __forceinline__ float at(const float* __restrict__ g, int n, int t) const
+    {
+        auto G = [&](int ix, int iy, int iz) { return __ldg(g + (unsigned)(((iz * 4 + iy) * 4 + ix) * n + t)); };
+        const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty), uz = __fsub_rn(1.0f, tz);
+        const float c00 = __fadd_rn(__fmul_rn(G(x0, y0, z0), ux), __fmul_rn(G(x1, y0, z0), tx));
+        const float c01 = __fadd_rn(__fmul_rn(G(x0, y0, z1), ux), __fmul_rn(G(x1, y0, z1), tx));
+        const float c10 = __fadd_rn(__fmul_rn(G(x0, y1, z0), ux), __fmul_rn(G(x1, y1, z0), tx));
+        const float c11 = __fadd_rn(__fmul_rn(G(x0, y1, z1), ux), __fmul_rn(G(x1, y1, z1), tx));
+        const float c0 = __fadd_rn(__fmul_rn(c00, uy), __fmul_rn(c10, ty));
+        const float c1 = __fadd_rn(__fmul_rn(c01, uy), __fmul_rn(c11, ty));
+        return __fadd_rn(__fmul_rn(c0, uz), __fmul_rn(c1, tz));
+    }
+};
+
+// The control fitting of one leaf per CTA, one thread per control of an R^3 grid at
+// controlCoords(R): R = 4 is the coarse fit (:705-729); R = 6 with RESID the FINE6 residual fit
+// (:815-850), whose series is the sampled reconstruction minus the fitted coarse grid
+// (cgrid[leaf][64][frames], from the coarse fit) sampled at the same position.
+template <int R, bool RESID>
+__global__ void __launch_bounds__(R * R * R) control_fit_kernel(const float* __restrict__ recon, uint32_t X,
+                                                                uint32_t Y, uint32_t Z, int n,
+                                                                unsigned long long fstride,
+                                                                const uint32_t* __restrict__ leaves,
+                                                                uint32_t n_leaves, vbt_keyframe_profile p, int rmax,
+                                                                const float* __restrict__ cgrid, CoarseOut o)
+{
+    constexpr int NV = R * R * R;
     extern __shared__ __align__(16) float cf_smem[];
-    __shared__ int s_count[64], s_start[64], s_span[64 * 8];
+    __shared__ int s_count[NV], s_start[NV], s_span[NV * 8];
     const int words = (n + 31) >> 5;
-    float* sv = cf_smem;                                               // [n][64]
-    uint32_t* sm = reinterpret_cast<uint32_t*>(sv + n * 64);           // [words][64]
-    float* stop = reinterpret_cast<float*>(sm + words * 64);           // [rmax][64]
+    float* sv = cf_smem;                                               // [n][NV]
+    uint32_t* sm = reinterpret_cast<uint32_t*>(sv + n * NV);           // [words][NV]
+    float* stop = reinterpret_cast<float*>(sm + words * NV);           // [rmax][NV]
     const int c = threadIdx.x;
     const uint32_t li = blockIdx.x;
     if (li >= n_leaves) return;          // uniform per CTA
@@ -478,11 +526,12 @@ __global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict_
     }
     const uint32_t bx = leaf % lcx, by = (leaf / lcx) % lcy, bz = leaf / (lcx * lcy);
     const int w = (int)min(8u, X - 8u * bx), h = (int)min(8u, Y - 8u * by), d = (int)min(8u, Z - 8u * bz);
-    const float scale = __fdiv_rn(7.0f, 3.0f);
-    const int gx = c & 3, gy = (c >> 2) & 3, gz = c >> 4;
-    const float x = clamp_r(__fmul_rn((float)gx, scale), 0.0f, (float)max(0, w - 1));
-    const float y = clamp_r(__fmul_rn((float)gy, scale), 0.0f, (float)max(0, h - 1));
-    const float z = clamp_r(__fmul_rn((float)gz, scale), 0.0f, (float)max(0, d - 1));
+    const float scale = __fdiv_rn(7.0f, (float)(R - 1));
+    const int gx = c % R, gy = (c / R) % R, gz = c / (R * R);
+    const float px = __fmul_rn((float)gx, scale), py = __fmul_rn((float)gy, scale), pz = __fmul_rn((float)gz, scale);
+    const float x = clamp_r(px, 0.0f, (float)max(0, w - 1));
+    const float y = clamp_r(py, 0.0f, (float)max(0, h - 1));
+    const float z = clamp_r(pz, 0.0f, (float)max(0, d - 1));
     const int x0 = (int)floorf(x), y0 = (int)floorf(y), z0 = (int)floorf(z);
     const int x1 = min(w - 1, x0 + 1), y1 = min(h - 1, y0 + 1), z1 = min(d - 1, z0 + 1);
     const float tx = __fsub_rn(x, (float)x0), ty = __fsub_rn(y, (float)y0), tz = __fsub_rn(z, (float)z0);
@@ -493,6 +542,9 @@ __global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict_
     const unsigned long long v000 = vox(x0, y0, z0), v100 = vox(x1, y0, z0), v001 = vox(x0, y0, z1),
                              v101 = vox(x1, y0, z1), v010 = vox(x0, y1, z0), v110 = vox(x1, y1, z0),
                              v011 = vox(x0, y1, z1), v111 = vox(x1, y1, z1);
+    Grid4Sample cs{};
+    const float* cg = RESID ? cgrid + (unsigned long long)li * 64u * (unsigned)n : nullptr;
+    if (RESID) cs.init(px, py, pz, w, h, d);
     for (int t = 0; t < n; ++t) {
         const float* f = recon + (unsigned long long)t * fstride;
         const float c00 = __fadd_rn(__fmul_rn(__ldg(f + v000), ux), __fmul_rn(__ldg(f + v100), tx));
@@ -501,11 +553,13 @@ __global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict_
         const float c11 = __fadd_rn(__fmul_rn(__ldg(f + v011), ux), __fmul_rn(__ldg(f + v111), tx));
         const float c0 = __fadd_rn(__fmul_rn(c00, uy), __fmul_rn(c10, ty));
         const float c1 = __fadd_rn(__fmul_rn(c01, uy), __fmul_rn(c11, ty));
-        sv[t * 64 + c] = __fadd_rn(__fmul_rn(c0, uz), __fmul_rn(c1, tz));
+        float v = __fadd_rn(__fmul_rn(c0, uz), __fmul_rn(c1, tz));
+        if (RESID) v = __fsub_rn(v, cs.at(cg, n, t));
+        sv[t * NV + c] = v;
     }
-    const Column<64> col{sv + c, sm + c};
-    float* grid = o.grid ? o.grid + ((unsigned long long)li * 64u + (unsigned)c) * (unsigned)n : nullptr;
-    const SeriesOut r = keyframe_series<64>(col, stop + c, n, words, p, grid, 1ull);
+    const Column<NV> col{sv + c, sm + c};
+    float* grid = o.grid ? o.grid + ((unsigned long long)li * NV + (unsigned)c) * (unsigned)n : nullptr;
+    const SeriesOut r = keyframe_series<NV>(col, stop + c, n, words, p, grid, 1ull);
     const int count = (int)r.count;
 
     // buildBinIndexFromKeys: one merge of the sorted keys with the bins' first frames.
@@ -513,7 +567,7 @@ __global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict_
     {
         int b = 0, i = 0;
         for (int wd = 0; wd < words && b < 8; ++wd) {
-            uint32_t bits = col.m[wd * 64];
+            uint32_t bits = col.m[wd * NV];
             while (bits && b < 8) {
                 const int key = (wd << 5) + __ffs(bits) - 1;
                 bits &= bits - 1u;
@@ -534,7 +588,7 @@ __global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict_
     __syncthreads();
     if (c == 0) {            // keyStart: the keys of the controls before, in control order
         int run = 0, req = 1;
-        for (int k = 0; k < 64; ++k) {
+        for (int k = 0; k < NV; ++k) {
             s_start[k] = run;
             run += s_count[k];
             for (int b = 0; b < 8; ++b) req = (int)(uint8_t)max(req, s_span[k * 8 + b]);
@@ -544,14 +598,14 @@ __global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict_
     }
     __syncthreads();
     const int start = s_start[c];
-    o.desc[(unsigned long long)li * 64u + (unsigned)c] =
+    o.desc[(unsigned long long)li * NV + (unsigned)c] =
         (uint32_t)(uint16_t)start | ((uint32_t)min(count, 255) << 16) | ((uint32_t)min(local, 255) << 24);
-    uint8_t* brow = o.bins + ((unsigned long long)li * 64u + (unsigned)c) * 8u;
+    uint8_t* brow = o.bins + ((unsigned long long)li * NV + (unsigned)c) * 8u;
     for (int b = 0; b < 8; ++b) brow[b] = b8[b];
-    const unsigned long long kbase = (unsigned long long)li * 64u * (unsigned)n + (unsigned)start;
+    const unsigned long long kbase = (unsigned long long)li * NV * (unsigned)n + (unsigned)start;
     int i = 0;
     for (int wd = 0; wd < words; ++wd) {
-        uint32_t bits = col.m[wd * 64];
+        uint32_t bits = col.m[wd * NV];
         while (bits) {
             const int key = (wd << 5) + __ffs(bits) - 1;
             bits &= bits - 1u;
@@ -560,6 +614,247 @@ __global__ void __launch_bounds__(64) coarse_fit_kernel(const float* __restrict_
             ++i;
         }
     }
+}
+
+// ---- the Mode2 shell stage (:930-1025) ------------------------------------------------------
+// One leaf per CTA, 128 threads, the 512 voxels in four rounds.  A voxel inside the leaf's extent
+// is a shell voxel when at some frame (level set) |value| <= surface_band, |coarse| <= guard_band
+// or their signs differ, or (density) value >= shell_cut -- value the pass's reconstruction,
+// coarse the fitted coarse grid sampled at the voxel.  Its residual series (value - coarse) is
+// keyed under the control profile, for a level set joined with addIsoSurfaceKeyFrames (:2051-2078)
+// on the voxel's own series at 0 +- temporal_band, and appended to a 4-bin stream with its
+// reconstructFromKeys values at the keys (:2169-2201).  Streams follow the voxel order; the
+// occupancy section holds the 8 x u64 voxel masks and the 8 x u16 group prefixes.
+
+struct ShellOut {
+    uint8_t* occupancy;      // [leaf][80]
+    uint32_t* desc;          // [leaf][512]
+    uint8_t* bins;           // [leaf][512][8] (first 4 bytes used)
+    uint16_t* key_frame;     // [leaf][512 * frames]
+    float* key_value;        // [leaf][512 * frames]
+    uint32_t* key_count;     // [leaf]
+    uint32_t* active;        // [leaf]
+    uint8_t* required;       // [leaf]
+};
+
+constexpr int kShellThreads = 128;
+
+__global__ void __launch_bounds__(kShellThreads) shell_fit_kernel(
+    const float* __restrict__ recon, uint32_t X, uint32_t Y, uint32_t Z, int n, unsigned long long fstride,
+    const uint32_t* __restrict__ leaves, uint32_t n_leaves, vbt_keyframe_profile p, int rmax,
+    const float* __restrict__ cgrid, int levelset, float surface_band, float guard_band, float temporal_band,
+    float shell_cut, ShellOut o)
+{
+    constexpr int NT = kShellThreads;
+    extern __shared__ __align__(16) float sh_smem[];
+    __shared__ uint32_t s_mask[16];            // voxel bits, 32 per word
+    __shared__ int s_wc[NT / 32], s_wk[NT / 32];
+    __shared__ int s_run_active, s_run_keys, s_req;
+    const int words = (n + 31) >> 5;
+    float* sv = sh_smem;                                               // [n][NT]
+    uint32_t* sm = reinterpret_cast<uint32_t*>(sv + n * NT);           // [words][NT]
+    float* stop = reinterpret_cast<float*>(sm + words * NT);           // [rmax][NT]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t li = blockIdx.x;
+    if (li >= n_leaves) return;
+    const uint32_t leaf = leaves[li];
+    const uint32_t lcx = (X + 7u) / 8u, lcy = (Y + 7u) / 8u, lcz = (Z + 7u) / 8u;
+    if ((unsigned long long)leaf >= (unsigned long long)lcx * lcy * lcz) {
+        if (tid == 0) o.key_count[li] = 0xFFFFFFFFu;
+        return;
+    }
+    const uint32_t bx = leaf % lcx, by = (leaf / lcx) % lcy, bz = leaf / (lcx * lcy);
+    const int w = (int)min(8u, X - 8u * bx), h = (int)min(8u, Y - 8u * by), d = (int)min(8u, Z - 8u * bz);
+    const float* cg = cgrid + (unsigned long long)li * 64u * (unsigned)n;
+    if (tid == 0) {
+        s_run_active = 0;
+        s_run_keys = 0;
+        s_req = 1;
+    }
+    if (tid < 16) s_mask[tid] = 0u;
+    __syncthreads();
+    const Column<NT> col{sv + tid, sm + tid};
+    for (int round = 0; round < 512 / NT; ++round) {
+        const int v = round * NT + tid;
+        const int lx = v & 7, ly = (v >> 3) & 7, lz = v >> 6;
+        const bool inside = lx < w && ly < h && lz < d;
+        const unsigned long long vo =
+            (unsigned long long)((8u * bz + (uint32_t)lz) * Y + 8u * by + (uint32_t)ly) * X + 8u * bx + (uint32_t)lx;
+        Grid4Sample gs{};
+        gs.init((float)lx, (float)ly, (float)lz, w, h, d);
+        bool shell = false;
+        if (inside) {
+            for (int t = 0; t < n && !shell; ++t) {
+                const float truth = __ldg(recon + (unsigned long long)t * fstride + vo);
+                if (levelset) {
+                    const float c = gs.at(cg, n, t);
+                    shell = fabsf(truth) <= surface_band || fabsf(c) <= guard_band || (truth >= 0.0f) != (c >= 0.0f);
+                } else {
+                    shell = truth >= shell_cut;
+                }
+            }
+        }
+        int count = 0, local = 1;
+        uint8_t b4[4] = {0, 0, 0, 0};
+        if (shell) {
+            for (int t = 0; t < n; ++t)
+                sv[t * NT + tid] = __fsub_rn(__ldg(recon + (unsigned long long)t * fstride + vo), gs.at(cg, n, t));
+            keyframe_series<NT>(col, stop + tid, n, words, p, nullptr, 1ull);
+            if (levelset) {   // addIsoSurfaceKeyFrames(value, 0, temporal_band), sorted and unique
+                const float band = fmax_r(0.0f, temporal_band);
+                float prev = 0.0f;
+                for (int t = 0; t < n; ++t) {
+                    const float cur = __ldg(recon + (unsigned long long)t * fstride + vo);
+                    if (fabsf(cur) <= band) {
+                        if (t > 0) col.set(t - 1);
+                        col.set(t);
+                        if (t + 1 < n) col.set(t + 1);
+                    }
+                    if (t > 0 && (prev >= 0.0f) != (cur >= 0.0f)) {
+                        if (t > 1) col.set(t - 2);
+                        col.set(t - 1);
+                        col.set(t);
+                        if (t + 1 < n) col.set(t + 1);
+                    }
+                    prev = cur;
+                }
+            }
+            for (int wd = 0; wd < words; ++wd) count += __popc(col.m[wd * NT]);
+            // buildBinIndexFromKeys with 4 bins
+            int b = 0, i = 0;
+            for (int wd = 0; wd < words && b < 4; ++wd) {
+                uint32_t bits = col.m[wd * NT];
+                while (bits && b < 4) {
+                    const int key = (wd << 5) + __ffs(bits) - 1;
+                    bits &= bits - 1u;
+                    while (b < 4 && key >= (int)(((long long)b * n) / 4)) b4[b++] = (uint8_t)(i > 0 ? i - 1 : 0);
+                    ++i;
+                }
+            }
+            for (; b < 4; ++b) b4[b] = (uint8_t)(count - 1);
+            for (int bb = 0; bb < 4; ++bb) {
+                const int next = bb + 1 < 4 ? (int)b4[bb + 1] : count;
+                local = max(local, max(1, next - (int)b4[bb]));
+            }
+        }
+        // voxel-order ranks of this round's shell voxels and key starts
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, shell);
+        int kincl = count;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, kincl, off);
+            if (lane >= off) kincl += y;
+        }
+        if (lane == 31) {
+            s_wc[warp] = __popc(bal);
+            s_wk[warp] = kincl;
+        }
+        if (lane == 0) s_mask[(round * NT + warp * 32) >> 5] = bal;
+        __syncthreads();
+        int abase = s_run_active, kbase = s_run_keys;
+        for (int q = 0; q < warp; ++q) {
+            abase += s_wc[q];
+            kbase += s_wk[q];
+        }
+        if (shell) {
+            const int a = abase + __popc(bal & ((1u << lane) - 1u));
+            const int start = kbase + kincl - count;
+            o.desc[(unsigned long long)li * 512u + (unsigned)a] =
+                (uint32_t)(uint16_t)start | ((uint32_t)min(count, 255) << 16) | ((uint32_t)min(local, 255) << 24);
+            uint8_t* brow = o.bins + ((unsigned long long)li * 512u + (unsigned)a) * 8u;
+            for (int bb = 0; bb < 8; ++bb) brow[bb] = bb < 4 ? b4[bb] : 0u;
+            // the reconstruction at each key: the first key's value, then per key
+            // value(a) + 1 x (value(b) - value(a)) over the interval (a, b] that ends at it
+            const unsigned long long kb = (unsigned long long)li * 512u * (unsigned)n + (unsigned)start;
+            int i = 0, prev_key = -1;
+            for (int wd = 0; wd < words; ++wd) {
+                uint32_t bits = col.m[wd * NT];
+                while (bits) {
+                    const int key = (wd << 5) + __ffs(bits) - 1;
+                    bits &= bits - 1u;
+                    float val = col.at(key);
+                    if (prev_key >= 0) {
+                        const float va = col.at(prev_key);
+                        val = __double2float_rn(__dadd_rn((double)va, (double)__fsub_rn(val, va)));
+                    }
+                    o.key_frame[kb + i] = (uint16_t)key;
+                    o.key_value[kb + i] = val;
+                    prev_key = key;
+                    ++i;
+                }
+            }
+            atomicMax(&s_req, local);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int q = 0; q < NT / 32; ++q) {
+                s_run_active += s_wc[q];
+                s_run_keys += s_wk[q];
+            }
+        }
+        __syncthreads();
+    }
+    // occupancy: 8 x u64 masks, then 8 x u16 prefixes (shell voxels before the group)
+    if (tid < 8) {
+        uint32_t pre = 0;
+        for (int g = 0; g < tid; ++g) pre += __popc(s_mask[2 * g]) + __popc(s_mask[2 * g + 1]);
+        uint8_t* occ = o.occupancy + (unsigned long long)li * 80u;
+        const uint32_t lo = s_mask[2 * tid], hi = s_mask[2 * tid + 1];
+        for (int k = 0; k < 4; ++k) {
+            occ[8 * tid + k] = (uint8_t)(lo >> (8 * k));
+            occ[8 * tid + 4 + k] = (uint8_t)(hi >> (8 * k));
+        }
+        occ[64 + 2 * tid] = (uint8_t)pre;
+        occ[64 + 2 * tid + 1] = (uint8_t)(pre >> 8);
+    }
+    if (tid == 0) {
+        o.key_count[li] = (uint32_t)s_run_keys;
+        o.active[li] = (uint32_t)s_run_active;
+        o.required[li] = (uint8_t)min(s_req, 255);
+    }
+}
+
+// ---- the density route (:1105-1245, routeRenderTemporalLeaf :27-66) --------------------------
+// Per listed leaf, the encoder's sampling lattice (every 8th frame, the leaf's voxel (0, 0, 0) --
+// control 0 of either fitted grid): the raw value against the coarse prediction and against coarse
+// + FINE6, in double as the encoder accumulates them; FINE6 (mode 3) when the coarse fit is too
+// rough, the points are visible and the fine fit gains enough, else GRID4 (mode 1).
+__global__ void route_kernel(const float* __restrict__ raw, uint32_t X, uint32_t Y, uint32_t Z, int n,
+                             unsigned long long fstride, const uint32_t* __restrict__ leaves, uint32_t n_leaves,
+                             const float* __restrict__ cgrid, const float* __restrict__ fgrid, double peak, double lo,
+                             double hi, uint8_t* __restrict__ mode)
+{
+    const uint32_t li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= n_leaves) return;
+    const uint32_t leaf = leaves[li];
+    const uint32_t lcx = (X + 7u) / 8u, lcy = (Y + 7u) / 8u, lcz = (Z + 7u) / 8u;
+    if ((unsigned long long)leaf >= (unsigned long long)lcx * lcy * lcz) {
+        mode[li] = 0;
+        return;
+    }
+    const uint32_t bx = leaf % lcx, by = (leaf / lcx) % lcy, bz = leaf / (lcx * lcy);
+    const unsigned long long vo = (unsigned long long)(8u * bz * Y + 8u * by) * X + 8u * bx;
+    const float* cg = cgrid + (unsigned long long)li * 64u * (unsigned)n;
+    const float* fg = fgrid + (unsigned long long)li * 216u * (unsigned)n;
+    int cnt = 0, vis = 0, bnd = 0;
+    double ce2 = 0.0, fe2 = 0.0, cpk = 0.0;
+    for (int t = 0; t < n; t += 8) {
+        const double truth = (double)__ldg(raw + (unsigned long long)t * fstride + vo);
+        const float cp = __ldg(cg + t), fp = __ldg(fg + t);
+        ++cnt;
+        vis += truth >= lo;
+        bnd += lo <= truth && truth <= hi;
+        const double cd = __dsub_rn(truth, (double)cp), fd = __dsub_rn(truth, (double)__fadd_rn(cp, fp));
+        ce2 = __dadd_rn(ce2, __dmul_rn(cd, cd));
+        fe2 = __dadd_rn(fe2, __dmul_rn(fd, fd));
+        cpk = dmax_r(cpk, __ddiv_rn(fabs(cd), peak));
+    }
+    const double c = (double)(cnt > 1 ? cnt : 1);
+    const double crm = __ddiv_rn(__dsqrt_rn(__ddiv_rn(ce2, c)), peak);
+    const double frm = __ddiv_rn(__dsqrt_rn(__ddiv_rn(fe2, c)), peak);
+    const bool rough = crm > (double)0.008f || cpk > (double)0.03f;
+    const bool sensitive = __ddiv_rn((double)vis, c) >= (double)0.005f || __ddiv_rn((double)bnd, c) >= (double)0.005f;
+    const double gain = __ddiv_rn(__dsub_rn(crm, frm), dmax_r(crm, 1e-12));
+    mode[li] = (rough && sensitive && gain >= (double)0.05f) ? 3 : 1;
 }
 
 template <int NV>
@@ -690,15 +985,124 @@ extern "C" int vbt_coarse_fit(const float* d_recon, uint32_t width, uint32_t hei
     if (smem + static_smem > (size_t)smem_max) return set_last_error(VBT_STATUS_LIMIT, "too many frames for one leaf's CTA");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     kf_rcp_init_kernel<<<1, 1024, 0, s>>>();
-    cudaError_t e = cudaFuncSetAttribute(coarse_fit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(control_fit_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e == cudaSuccess) {
         vbt_keyframe_profile prof = *control_profile;
         prof.bg_threshold = -1.0;          // the control fitting has no background test
         const CoarseOut o{d_desc, d_bins, d_key_frames, d_key_values, d_key_count, d_required_max_local, d_grid};
-        coarse_fit_kernel<<<leaf_count, 64, smem, s>>>(d_recon, width, height, depth, n, frame_stride, d_leaves,
-                                                       leaf_count, prof, rmax, o);
+        control_fit_kernel<4, false><<<leaf_count, 64, smem, s>>>(d_recon, width, height, depth, n, frame_stride,
+                                                                  d_leaves, leaf_count, prof, rmax, nullptr, o);
         e = cudaGetLastError();
     }
     return e == cudaSuccess ? VBT_STATUS_OK
-                            : set_last_error(VBT_STATUS_CUDA, std::string("coarse_fit_kernel: ") + cudaGetErrorString(e));
+                            : set_last_error(VBT_STATUS_CUDA, std::string("control_fit_kernel<4>: ") + cudaGetErrorString(e));
+}
+
+extern "C" int vbt_fine6_fit(const float* d_recon, uint32_t width, uint32_t height, uint32_t depth, uint32_t frames,
+                             uint64_t frame_stride, const uint32_t* d_leaves, uint32_t leaf_count,
+                             const vbt_keyframe_profile* control_profile, const float* d_coarse_grid, uint32_t* d_desc,
+                             uint8_t* d_bins, uint16_t* d_key_frames, float* d_key_values, uint32_t* d_key_count,
+                             uint8_t* d_required_max_local, float* d_grid, void* stream)
+{
+    using vbtb::set_last_error;
+    if (!control_profile) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null profile");
+    if (frames == 0 || width == 0 || height == 0 || depth == 0)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "empty volume");
+    if (frames > kKfMaxFrames) return set_last_error(VBT_STATUS_LIMIT, "frames above 1024");
+    const unsigned long long voxels = (unsigned long long)width * height * depth;
+    if (frame_stride < voxels) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "frame_stride smaller than the volume");
+    if (leaf_count == 0) return VBT_STATUS_OK;
+    if (!d_recon || !d_leaves || !d_coarse_grid || !d_desc || !d_bins || !d_key_frames || !d_key_values ||
+        !d_key_count || !d_required_max_local)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    const int n = (int)frames;
+    const int m = n - 1;
+    const int rmax = n >= 2 ? m - (m - 1 < (m * 9) / 10 ? m - 1 : (m * 9) / 10) : 1;
+    int dev = 0, smem_max = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t smem = kf_smem_bytes<216>(n, rmax);
+    const size_t static_smem = (216 + 216 + 216 * 8) * sizeof(int);
+    if (smem + static_smem > (size_t)smem_max) return set_last_error(VBT_STATUS_LIMIT, "too many frames for one leaf's CTA");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    kf_rcp_init_kernel<<<1, 1024, 0, s>>>();
+    cudaError_t e = cudaFuncSetAttribute(control_fit_kernel<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess) {
+        vbt_keyframe_profile prof = *control_profile;
+        prof.bg_threshold = -1.0;
+        const CoarseOut o{d_desc, d_bins, d_key_frames, d_key_values, d_key_count, d_required_max_local, d_grid};
+        control_fit_kernel<6, true><<<leaf_count, 216, smem, s>>>(d_recon, width, height, depth, n, frame_stride,
+                                                                  d_leaves, leaf_count, prof, rmax, d_coarse_grid, o);
+        e = cudaGetLastError();
+    }
+    return e == cudaSuccess ? VBT_STATUS_OK
+                            : set_last_error(VBT_STATUS_CUDA, std::string("control_fit_kernel<6>: ") + cudaGetErrorString(e));
+}
+
+extern "C" int vbt_shell_fit(const float* d_recon, uint32_t width, uint32_t height, uint32_t depth, uint32_t frames,
+                             uint64_t frame_stride, const uint32_t* d_leaves, uint32_t leaf_count,
+                             const vbt_keyframe_profile* control_profile, const float* d_coarse_grid, int levelset,
+                             float surface_band, float guard_band, float temporal_band, float shell_cut,
+                             uint8_t* d_occupancy, uint32_t* d_desc, uint8_t* d_bins, uint16_t* d_key_frames,
+                             float* d_key_values, uint32_t* d_key_count, uint32_t* d_active,
+                             uint8_t* d_required_max_local, void* stream)
+{
+    using vbtb::set_last_error;
+    if (!control_profile) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null profile");
+    if (frames == 0 || width == 0 || height == 0 || depth == 0)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "empty volume");
+    if (frames > kKfMaxFrames) return set_last_error(VBT_STATUS_LIMIT, "frames above 1024");
+    const unsigned long long voxels = (unsigned long long)width * height * depth;
+    if (frame_stride < voxels) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "frame_stride smaller than the volume");
+    if (leaf_count == 0) return VBT_STATUS_OK;
+    if (!d_recon || !d_leaves || !d_coarse_grid || !d_occupancy || !d_desc || !d_bins || !d_key_frames ||
+        !d_key_values || !d_key_count || !d_active || !d_required_max_local)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    const int n = (int)frames;
+    const int m = n - 1;
+    const int rmax = n >= 2 ? m - (m - 1 < (m * 9) / 10 ? m - 1 : (m * 9) / 10) : 1;
+    int dev = 0, smem_max = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t smem = kf_smem_bytes<kShellThreads>(n, rmax);
+    if (smem + 1024 > (size_t)smem_max) return set_last_error(VBT_STATUS_LIMIT, "too many frames for one leaf's CTA");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    kf_rcp_init_kernel<<<1, 1024, 0, s>>>();
+    cudaError_t e = cudaFuncSetAttribute(shell_fit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+        vbt_keyframe_profile prof = *control_profile;
+        prof.bg_threshold = -1.0;
+        const ShellOut o{d_occupancy, d_desc, d_bins, d_key_frames, d_key_values, d_key_count, d_active,
+                         d_required_max_local};
+        shell_fit_kernel<<<leaf_count, kShellThreads, smem, s>>>(d_recon, width, height, depth, n, frame_stride,
+                                                                  d_leaves, leaf_count, prof, rmax, d_coarse_grid,
+                                                                  levelset, surface_band, guard_band, temporal_band,
+                                                                  shell_cut, o);
+        e = cudaGetLastError();
+    }
+    return e == cudaSuccess ? VBT_STATUS_OK
+                            : set_last_error(VBT_STATUS_CUDA, std::string("shell_fit_kernel: ") + cudaGetErrorString(e));
+}
+
+extern "C" int vbt_route_density(const float* d_raw, uint32_t width, uint32_t height, uint32_t depth, uint32_t frames,
+                                 uint64_t frame_stride, const uint32_t* d_leaves, uint32_t leaf_count,
+                                 const float* d_coarse_grid, const float* d_fine_grid, double peak, double visible_lo,
+                                 double visible_hi, uint8_t* d_mode, void* stream)
+{
+    using vbtb::set_last_error;
+    if (frames == 0 || width == 0 || height == 0 || depth == 0)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "empty volume");
+    if (leaf_count == 0) return VBT_STATUS_OK;
+    if (!d_raw || !d_leaves || !d_coarse_grid || !d_fine_grid || !d_mode)
+        return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
+    if (!(peak > 0.0)) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "peak must be positive");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    route_kernel<<<(leaf_count + 127) / 128, 128, 0, s>>>(d_raw, width, height, depth, (int)frames, frame_stride,
+                                                          d_leaves, leaf_count, d_coarse_grid, d_fine_grid, peak,
+                                                          visible_lo, visible_hi, d_mode);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VBT_STATUS_OK
+                            : set_last_error(VBT_STATUS_CUDA, std::string("route_kernel: ") + cudaGetErrorString(e));
 }

@@ -101,6 +101,34 @@ struct FrameSink {
     }
 };
 
+// The same stores from values held by the sink itself (no references to the launch's asset or the
+// leaf's geometry), for the specialised path.
+template <bool DENSE>
+struct QuadSink {
+    float* __restrict__ out;
+    uint64_t frame_stride;
+    uint32_t li, width, height, bx, by, bz;
+    int w, h, d;
+    __device__ __forceinline__ void operator()(int fi, int lane, int i, float4 v) const
+    {
+        const int lz = 2 * i + (lane >> 4), ly = (lane >> 1) & 7, lx0 = 4 * (lane & 1);
+        if (DENSE) {
+            if (ly < h && lz < d) {
+                float* dst = out + (uint64_t)fi * frame_stride +
+                             ((uint64_t)(bz * 8 + lz) * height + (by * 8 + ly)) * width + bx * 8 + lx0;
+                if (lx0 + 4 <= w && (((uintptr_t)dst) & 15u) == 0u) {
+                    *reinterpret_cast<float4*>(dst) = v;
+                } else {
+                    const float vv[4] = {v.x, v.y, v.z, v.w};
+                    for (int k = 0; k < 4 && lx0 + k < w; ++k) dst[k] = vv[k];
+                }
+            }
+        } else {
+            reinterpret_cast<float4*>(out + (uint64_t)fi * frame_stride + (uint64_t)li * 512u)[lane + 32 * i] = v;
+        }
+    }
+};
+
 // Decode one validated, non-EMPTY leaf for all frames of the launch with word reader `m` and NW
 // warps; each finished quad of 4 voxels goes to `sink(frame index, lane, quad, values)`.  Frame
 // lists that step by 0 or 1 stream each control's keys; other non-decreasing lists (`monotone`)
@@ -318,7 +346,8 @@ __device__ __noinline__ void leaf_decode_fast_call(const DeviceAsset& a, LeafEnt
 {
     extern __shared__ __align__(128) uint8_t dyn[];
     const LeafSmem s = leaf_layout<kDecWarps>(dyn);
-    leaf_decode_fast<FINE, kDecWarps>(s.stage, lb, s, e, nframes, G, FrameSink<DENSE>{a, G, out, frame_stride});
+    const QuadSink<DENSE> sink{out, frame_stride, G.li, a.g.width, a.g.height, G.bx, G.by, G.bz, G.w, G.h, G.d};
+    leaf_decode_fast<FINE, kDecWarps>(s.stage, lb, s, e, nframes, G, sink);
 }
 
 // Staged GRID4 / FINE6 leaves of the common shape take leaf_decode_fast (rt_leaf_fast.cuh), every
