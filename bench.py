@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--no-writer", action="store_true")
     p.add_argument("--serve-requests", type=int, default=300)
     p.add_argument("--no-ref-queries", action="store_true")
+    p.add_argument("--full-size", action="store_true",
+                   help="also encode and decode configurations 3 and 4 at their stated sizes (several minutes)")
     return p.parse_args()
 
 
@@ -314,23 +316,33 @@ def equal_p99_sweep(vbt, assets, reqs, inputs, at_rate, plain_capacity, served_c
             "throughput_ratio_at_equal_p99": best["served"] / best["plain"] if best["plain"] > 0 else None}
 
 
-def run_serving(args, local_rank):
-    """The serving mix over the resident assets: served (4 streams, HBM-budget admission, point
-    requests merged across assets) against plain (one request per launch, one launch in flight),
-    closed loop (all requests at once) and open loop (Poisson arrivals at a common rate)."""
-    import torch
-    import vbt_b200 as vbt
-    assets, names, skipped = [], [], []
-    for n in SERVE_ASSETS:
+def open_assets(vbt, names, local_rank):
+    """The named assets of assets/ that exist (and the names skipped, with the reason)."""
+    assets, opened, skipped = [], [], []
+    for n in names:
         p = os.path.join(ROOT, "assets", n + ".vbtp")
         if not os.path.exists(p):
             skipped.append(f"{n}: not generated")
             continue
         try:
             assets.append(vbt.Asset(p, device=local_rank))
-            names.append(n)
+            opened.append(n)
         except vbt.VbtError as e:
             skipped.append(f"{n}: {e}")
+    return assets, opened, skipped
+
+
+def run_serving(args, local_rank, assets=None, names=None):
+    """The serving mix over the resident assets: served (4 streams, HBM-budget admission, point
+    requests merged across assets) against plain (one request per launch, one launch in flight),
+    closed loop (all requests at once) and open loop (Poisson arrivals at a common rate).  By
+    default the reduced-size mix of assets/; `assets` (open, with their names) replaces it."""
+    import torch
+    import vbt_b200 as vbt
+    own = assets is None
+    skipped = []
+    if own:
+        assets, names, skipped = open_assets(vbt, SERVE_ASSETS, local_rank)
     if len(assets) < 2:
         return {"skipped": "serving-mix assets not generated (tests/golden/make_assets.py)"}
     reqs = serving_requests(assets, args.serve_requests)
@@ -369,8 +381,9 @@ def run_serving(args, local_rank):
                                  closed_s["requests_per_s"])
     equal_dev = equal_p99_sweep(vbt, assets, reqs, dev, at_rate, d_closed_p["requests_per_s"],
                                 d_closed_s["requests_per_s"])
-    for a in assets:
-        a.close()
+    if own:
+        for a in assets:
+            a.close()
     return {"workload": "serving mix: 70% point batches of 1e3-1e6 uniform (x,y,z,t), 20% z-slices over 1-16 "
                         "frames, 10% dense frames, uniform over the assets; point inputs and outputs in pinned host "
                         "memory, slice and frame results device-resident (released when done)",
@@ -848,6 +861,171 @@ def run_reference_queries(args, local_rank, n=1_000_000, repeats=100):
     return out or {"skipped": "no scientific asset generated"}
 
 
+# ------------------------------------------------------------------------------ configs 3 and 4 at full size
+def timed_ms(torch, s, fn, reps, flush=None):
+    """Mean device time (CUDA events on stream s) of fn over reps runs after one untimed run."""
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    with torch.cuda.stream(s):
+        fn()
+        for e0, e1 in ev:
+            if flush is not None:
+                flush.zero_()
+            e0.record(s)
+            fn()
+            e1.record(s)
+    s.synchronize()
+    return statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+
+
+def encode_on_gpu(torch, slab, dims, levelset):
+    """A field produced slab by slab on the GPU, encoded there (vbt_b200.encode) and brought into a
+    pinned host file image; (image, seconds)."""
+    from vbt_b200.encode import encode_render_temporal, file_image
+    t0 = time.time()
+    h, off, pay = encode_render_temporal(slab, dims, levelset=levelset)
+    torch.cuda.synchronize()
+    img = file_image(h, off, pay, pinned=True)
+    return img, time.time() - t0
+
+
+def cache_timeline(torch, a, dev, W=16, reps=2):
+    """The whole timeline as W-frame cache launches into one W-frame ring: device ms per timeline,
+    voxels/s and the fraction of measured HBM peak of the algorithmic bytes."""
+    T, A = a.frames, a.active_count
+    ring = torch.empty((W, A, 512), dtype=torch.float32, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    chunks = [list(range(t, min(T, t + W))) for t in range(0, T, W)]
+    ms = timed_ms(torch, s, lambda: [a.decode_cache(ch, ring, frame_stride=A * 512, stream=s) for ch in chunks], reps)
+    a.sync_status(s)
+    per_frame, _ = algorithmic_bytes_per_frame(a.leaf_table())
+    peak, _ = measured_peak()
+    gbs = per_frame * T / (ms * 1e-3) / 1e9
+    del ring
+    return {"frames_per_launch": W, "ms_per_timeline": ms, "voxels_per_s": A * 512 * T / (ms * 1e-3),
+            "algorithmic_bytes_per_frame": per_frame, "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak}
+
+
+def window_vs_exact(torch, a, dev, W=16):
+    """(d) over the whole timeline in W-frame windows per active leaf: the tensor-core window
+    (vbt_decode_window) and the exact per-frame decode (vbt_decode_cache), device time of each,
+    and the error of each against the FP64 oracle relative to the field's range."""
+    T, A = a.frames, a.active_count
+    starts = list(range(0, T - W + 1, W))
+    win = torch.empty((W, A, 512), dtype=torch.float32, device=dev)
+    ref = torch.empty_like(win)
+    s = torch.cuda.Stream(device=dev)
+    win_ms = timed_ms(torch, s, lambda: [a.decode_window(t, W, win, frame_stride=A * 512, stream=s) for t in starts], 2)
+    ref_ms = timed_ms(torch, s, lambda: [a.decode_cache(list(range(t, t + W)), ref, frame_stride=A * 512, stream=s)
+                                         for t in starts], 2)
+    stats = {"window": [0.0, 0.0], "exact": [0.0, 0.0]}
+    lo, hi = float("inf"), float("-inf")
+    for t in starts:
+        with torch.cuda.stream(s):
+            a.decode_window(t, W, win, frame_stride=A * 512, stream=s)
+            a.decode_cache(list(range(t, t + W)), ref, frame_stride=A * 512, stream=s)
+        for key, buf in (("window", win), ("exact", ref)):
+            mx, rms, l, h = a.window_error(t, W, buf, frame_stride=A * 512, stream=s)
+            stats[key][0] = max(stats[key][0], mx)
+            stats[key][1] += rms * rms
+            lo, hi = min(lo, l), max(hi, h)
+    a.sync_status(s)
+    rng = hi - lo
+    vox = A * 512 * W * len(starts)
+    del win, ref
+    return {"windows": len(starts), "frames": W * len(starts), "oracle_range": [lo, hi],
+            "tensor_core_window": {"ms": win_ms, "voxels_per_s": vox / (win_ms * 1e-3),
+                                   "max_abs_err_rel_range": stats["window"][0] / rng,
+                                   "rms_err_rel_range": (stats["window"][1] / len(starts)) ** 0.5 / rng},
+            "fp32_per_frame": {"ms": ref_ms, "voxels_per_s": vox / (ref_ms * 1e-3),
+                               "max_abs_err_rel_range": stats["exact"][0] / rng,
+                               "rms_err_rel_range": (stats["exact"][1] / len(starts)) ** 0.5 / rng},
+            "speedup": ref_ms / win_ms}
+
+
+def dense_timeline(torch, a, dev, W=16, reps=2):
+    """Dense full frames (vbt_decode_frames) over the whole timeline, W frames per launch into one
+    W-frame buffer: device ms, voxels/s, and the fraction of measured HBM peak of the algorithmic
+    bytes (active leaves' decode bytes, less the cache write, plus 4 bytes per voxel written)."""
+    X, Y, Z = a.dims
+    T, vox = a.frames, a.dims[0] * a.dims[1] * a.dims[2]
+    out = torch.empty((W, vox), dtype=torch.float32, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    chunks = [list(range(t, min(T, t + W))) for t in range(0, T, W)]
+    ms = timed_ms(torch, s, lambda: [a.decode_frames(ch, out, stream=s) for ch in chunks], reps)
+    a.sync_status(s)
+    bytes_cache, n_act = algorithmic_bytes_per_frame(a.leaf_table())
+    per_frame = bytes_cache - 2048 * n_act + 4 * vox
+    peak, _ = measured_peak()
+    gbs = per_frame * T / (ms * 1e-3) / 1e9
+    del out
+    return {"frames_per_launch": W, "ms_per_timeline": ms, "voxels_per_s": vox * T / (ms * 1e-3),
+            "algorithmic_bytes_per_frame": per_frame, "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak}
+
+
+def run_full_size(args, local_rank):
+    """Configurations 3 and 4 at their stated sizes.  The raw fields (36-64 GB of float32 each) are
+    generated on the GPU from their seeds (tests/golden/gpu_fields.py), slab by slab, and encoded
+    there by this library's encoder chain (vbt_b200.encode; byte-exact against the reference encoder
+    on the reduced assets), so no raw field or large asset leaves the box.
+      config 3: the fire's three aligned fields, 384 x 384 x 512 x 120: the cache timeline and the
+                (d) window decode against the exact decode, with the error against the FP64 oracle;
+      config 4: the liquid level set, 512^3 x 120, Mode2 shell: dense full frames over the timeline;
+      config 5: the serving mix over eight resident assets of the stated sizes (the five above, the
+                plume, the 512^3 x 64 scientific field, and the two small scenes).
+    Decoded values are checked against the oracle in tests/test_full_size.py."""
+    import torch
+    import vbt_b200 as vbt
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import gpu_fields as gf
+    dev = f"cuda:{local_rank}"
+    out = {}
+    resident, names = [], []
+    fire = gf.Fire(torch, **gf.FIRE_FULL, device=dev)
+    dims = gf.FIRE_FULL["shape_xyz"]
+    for i, name in enumerate(("density", "flames", "temperature")):
+        img, enc_s = encode_on_gpu(torch, lambda z0, z1: fire.slab(i, z0, z1), dims, False)
+        a = vbt.Asset(data=img, device=local_rank)
+        a.build_page_table()
+        out["config3_fire_" + name] = {
+            "dims": list(dims) + [a.frames], "leaves": a.leaf_count, "active_leaves": a.active_count,
+            "file_bytes": int(img.numel()), "encode_s": enc_s,
+            "cache_timeline": cache_timeline(torch, a, dev), "precision_window": window_vs_exact(torch, a, dev)}
+        resident.append(a)
+        names.append("config3_fire_" + name)
+        del img
+    del fire
+    torch.cuda.empty_cache()
+    lv = gf.LevelSet(torch, **gf.LEVELSET_FULL, device=dev)
+    dims = gf.LEVELSET_FULL["shape_xyz"]
+    img, enc_s = encode_on_gpu(torch, lv.slab, dims, True)
+    a = vbt.Asset(data=img, device=local_rank)
+    a.build_page_table()
+    rows = a.leaf_table()
+    modes = np.bincount(rows[:, 1] & 3, minlength=4)
+    out["config4_levelset"] = {"dims": list(dims) + [a.frames], "leaves": a.leaf_count,
+                               "active_leaves": a.active_count, "grid4_leaves": int(modes[1]),
+                               "mode2_leaves": int(modes[2]), "file_bytes": int(img.numel()), "encode_s": enc_s,
+                               "full_frames": dense_timeline(torch, a, dev)}
+    resident.append(a)
+    names.append("config4_levelset")
+    del img
+    torch.cuda.empty_cache()
+    # config 5: the serving mix over eight resident assets of the stated sizes -- the plume (config 2),
+    # the fire's three fields (config 3), the level set (config 4), the scientific field 512^3 x 64
+    # (config 5's own field, reference-encoded) and the two small scenes of configs 1 and 4
+    more, more_names, skipped = open_assets(vbt, ["cfg2_plume", "cfg5_sci", "cfg1_blobs", "cfg4_sdf_small"],
+                                            local_rank)
+    if not args.no_serve:
+        out["config5_serving"] = run_serving(args, local_rank, resident + more, names + more_names)
+        out["config5_serving"]["assets_skipped"] = skipped
+        out["config5_serving"]["resident_file_bytes"] = int(sum(x.info.payload_words * 4 for x in resident + more))
+    for x in resident + more:
+        x.close()
+    out["note"] = ("fields generated and encoded on the GPU from their seeds; timings are device time with "
+                   "the asset resident; encode_s is wall time of generation + encode + copy to host")
+    return out
+
+
 # ------------------------------------------------------------------------------ writer
 def run_writer(args, local_rank, reps=5):
     """The VBTPACK4 writer on one B200 (vbt_pack_leaves: every leaf's control streams packed and the
@@ -1105,6 +1283,10 @@ def run_ours(args, rank, local_rank, world):
         window = run_window(args, local_rank)
         window_render = run_window_render(args, local_rank)
 
+    full_size = None
+    if rank == 0 and world == 1 and args.full_size:
+        full_size = run_full_size(args, local_rank)
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         serving = run_serving(args, local_rank)
@@ -1140,7 +1322,7 @@ def run_ours(args, rank, local_rank, world):
                           "launches_per_step": 2 * T, "speedup_batched_vs_plain": value / world / plain_value},
                 "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "precision_window": window,
                 "precision_window_render": window_render, "full_frame": full_frame, "ray_sampler": sampler,
-                "keyframe_pass": keyframes, "writer": writer, "point_queries_vs_reference_cuda": ref_queries,
+                "keyframe_pass": keyframes, "writer": writer, "full_size": full_size, "point_queries_vs_reference_cuda": ref_queries,
                 "gpu_launches": args.steps * (1 + len(chunks)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
