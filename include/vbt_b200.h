@@ -408,11 +408,12 @@ int vbt_decode_cache_timeline(vbt_asset* asset, int t0, int n, float* d_out, uin
 /* ---- Serving loop -----------------------------------------------------------------------------
  * No counterpart in the reference (its decoders are one call per value or per frame).  A server
  * keeps several resident assets, accepts point, slice and frame requests from any thread, admits
- * them while an HBM budget for their inputs and results has room, merges the point requests that
- * are admitted together into one multi-asset launch, and runs launches on `slots` streams so
- * that requests arriving while others are on the GPU overlap with them (continuous batching).
- * One scheduler thread per server issues all GPU work.  Results are identical to the one-asset
- * calls above (the same kernels; tested alone versus in a mix). */
+ * them while an HBM budget for their inputs and results has room, and runs the requests admitted
+ * together -- points, slices and frames of any assets, mixed -- as one persistent launch whose
+ * warps take tiles of all of them from a work counter (a CUDA graph per stream, its parameters
+ * updated each step).  Launches run on `slots` streams, so that requests arriving while others are
+ * on the GPU overlap with them (continuous batching).  One scheduler thread per server issues all
+ * GPU work.  Results are identical to the one-asset calls above (tested alone versus in a mix). */
 typedef struct vbt_server vbt_server;
 
 typedef struct {
@@ -420,8 +421,12 @@ typedef struct {
     uint64_t hbm_budget_bytes;   /* device memory for in-flight inputs and not yet released results */
     uint64_t host_staging_bytes; /* pinned host memory for requests with pageable host buffers */
     uint32_t slots;              /* launch streams, 1 .. 32 (units in flight at once) */
-    uint32_t max_batch_queries;  /* point queries merged into one launch, 0 = 4,194,304 */
-    uint32_t plain;              /* 1: one request per launch, one launch in flight, FIFO (baseline) */
+    uint32_t max_batch_queries;  /* values (points, slice and frame voxels) merged into one launch,
+                                  * 0 = 4,194,304; a larger request runs alone */
+    uint32_t plain;              /* 1: one request per launch, one launch in flight, FIFO, each kind
+                                  * on its own kernel (the baseline) */
+    uint32_t separate_kinds;     /* 1: merge only point requests (one multi-asset point launch);
+                                  * slices and frames each on their own kernel */
 } vbt_server_config;
 
 #define VBT_REQ_POINTS 1u   /* points[n_points] = (x, y, z, t) quads -> n_points floats */

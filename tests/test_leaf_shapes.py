@@ -124,3 +124,43 @@ def test_bench_asset_takes_the_specialised_path(vbt):
     fast, fine = fast_leaves(rows)
     active = (rows[:, 7] & (1 << 10)) != 0
     assert fast.sum() == active.sum() and fine.sum() > 0
+
+
+def test_leaves_larger_than_the_stage(vbt, cuda, oracle):
+    """Leaves bigger than the shared-memory stage: FINE6 leaves of a noisy field over 120 frames
+    (the fire's temperature recipe at 24 x 16 x 40, generated and encoded on the GPU), up to ~100 KB
+    each; the specialised path reads those from global memory (and, when more than a quarter of
+    the leaves are that big, every leaf).
+    Timeline caches of several launch shapes and dense frames, bit for bit against the oracle."""
+    import sys
+    from conftest import GOLDEN
+    sys.path.insert(0, GOLDEN)
+    import gpu_fields as gf
+    from vbt_b200.encode import encode_render_temporal, file_image
+    fire = gf.Fire(cuda, (24, 16, 40), 120, 7, device="cuda")
+    h, off, pay = encode_render_temporal(lambda z0, z1: fire.slab(2, z0, z1), (24, 16, 40))
+    img = file_image(h, off, pay)
+    a = vbt.Asset(data=img)
+    f = oracle.load(image=img)
+    try:
+        rows = a.leaf_table()
+        offs = f.offsets().astype(np.int64)
+        windows = ((4 * offs[1:] + 15) & ~15) - ((4 * offs[:-1]) & ~15)
+        fast, fine = fast_leaves(rows)
+        stage_cap = 69632                                  # the stage's cap at two CTAs per SM
+        assert fast.all() and fine.any()
+        assert (windows > stage_cap).any(), windows.max()
+        a.build_page_table()
+        T = f.frames
+        lists = [list(range(0, 48)), list(range(48, 112)), list(range(T - 5, T + 2)), [7], [T // 2, 3]]
+        check_cache(cuda, a, f, lists, "large leaves")
+        X, Y, Z = f.dims
+        frames = [0, 1, 59, 118, 119]
+        out = cuda.empty((len(frames), Z, Y, X), dtype=cuda.float32, device="cuda")
+        a.decode_frames(frames, out)
+        a.sync_status()
+        got = out.cpu().numpy()
+        for i, t in enumerate(frames):
+            assert np.array_equal(got[i].view(np.uint32), f.frame(t, threads=8).view(np.uint32)), t
+    finally:
+        a.close()

@@ -288,3 +288,37 @@ def test_device_resident_requests(vbt, cuda, assets):
         got = keep[j][-1][:len(ref[j])].cpu().numpy()
         assert np.array_equal(got.view(np.uint32), ref[j].view(np.uint32)), (j, reqs[j][0])
     srv.close()
+
+
+@pytest.mark.parametrize("separate", [False, True], ids=["mixed", "separate_kinds"])
+def test_mixed_launch_equals_alone(vbt, cuda, assets, separate):
+    """Points, slices and frames over several assets, pending together behind a long request, go
+    out as one persistent mixed launch (serve_mixed_kernel, replayed from the stream's graph): far
+    fewer units than requests, one launch per unit.  Every result equals the plain server's (each
+    request on its own kind's kernel) bit for bit; so does the schedule that merges only points."""
+    reqs = make_requests(assets, seed=21, n=40)
+    alone = run_alone(vbt, cuda, assets, reqs)
+    srv = vbt.Server(hbm_budget_bytes=512 << 20, slots=1, separate_kinds=separate)
+    ids = [srv.add_asset(a) for a in assets]
+    big = assets[0]
+    X, Y, Z = big.dims
+    n = 1 << 21
+    r0 = np.random.default_rng(5)
+    hq = np.stack([r0.integers(0, X, n), r0.integers(0, Y, n), r0.integers(0, Z, n),
+                   r0.integers(0, big.frames, n)], axis=1).astype(np.uint32)
+    hold = srv.submit_points(ids[0], hq, np.empty(n, np.float32))   # pageable: staged by the scheduler
+    bufs = [pinned_empty(cuda, out_size(assets[r[1]], r)) for r in reqs]
+    tickets = [submit(srv, ids, r, bufs[j][1]) for j, r in enumerate(reqs)]
+    assert srv.wait(hold).status == 0
+    srv.release(hold)
+    for j, t in enumerate(tickets):
+        res = srv.wait(t)
+        assert res.status == 0, (reqs[j][0], res.status)
+        srv.release(t)
+    st = srv.stats()
+    srv.close()
+    for j, r in enumerate(reqs):
+        assert np.array_equal(bufs[j][1].view(np.uint32), alone[j].view(np.uint32)), (j, r[0])
+    if not separate:
+        assert st.units < len(reqs) // 2, st.units
+        assert st.launches <= st.units, (st.launches, st.units)

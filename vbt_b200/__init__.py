@@ -41,7 +41,8 @@ class VbtAssetInfo(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_uint64), ("host_staging_bytes", C.c_uint64),
-                ("slots", C.c_uint32), ("max_batch_queries", C.c_uint32), ("plain", C.c_uint32)]
+                ("slots", C.c_uint32), ("max_batch_queries", C.c_uint32), ("plain", C.c_uint32),
+                ("separate_kinds", C.c_uint32)]
 
 
 class Request(C.Structure):
@@ -536,14 +537,16 @@ def decode_control_values(d_stream, stream_bytes, codec, control_count, bins, kf
 
 class Server:
     """The serving loop (vbt_server_* in include/vbt_b200.h): resident assets, requests admitted
-    by an HBM budget, point requests merged across assets, launches overlapped on `slots` streams.
+    by an HBM budget, the requests admitted together run as one mixed persistent launch (or, with
+    separate_kinds, only point requests merged), launches overlapped on `slots` streams.
 
     Host buffers handed to submit_*() (numpy arrays) must stay alive until the request is done;
     the object keeps references to them until release()."""
 
     def __init__(self, hbm_budget_bytes=1 << 30, slots=4, max_batch_queries=0, plain=False, device=0,
-                 host_staging_bytes=256 << 20):
-        cfg = ServerConfig(device, hbm_budget_bytes, host_staging_bytes, slots, max_batch_queries, int(plain))
+                 host_staging_bytes=256 << 20, separate_kinds=False):
+        cfg = ServerConfig(device, hbm_budget_bytes, host_staging_bytes, slots, max_batch_queries, int(plain),
+                           int(separate_kinds))
         self._h = _vp()
         _check(_lib.vbt_server_create(C.byref(cfg), C.byref(self._h)))
         self._keep = {}

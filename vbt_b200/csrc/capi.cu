@@ -168,26 +168,29 @@ int set_last_error(int status, const std::string& msg) { return fail(status, msg
 //  - the shared-memory leaf stage of the render decode kernel: the largest 16-byte-aligned window
 //    of a non-EMPTY leaf, capped so that two CTAs fit on an SM (232,448 B of shared memory per SM
 //    less 1 KiB per CTA); an asset with bigger leaves gets the kernel variant that decodes those
-//    from global memory.
+//    from global memory.  When more than a quarter of the non-EMPTY leaves exceed the cap, no leaf
+//    is staged: the kernel then reads every leaf through L1, which the unused stage leaves free.
 // Computed at creation and again for every re-uploaded image, whose leaves may differ in size.
 static void image_shape(const vbt_header& h, const uint8_t* b, uint64_t off_off, uint64_t pay_off, uint64_t words,
                         AssetGeom& g, bool& sparse)
 {
     if (h.profile_type == 2u) return;
     const uint8_t* off = b + off_off;
-    uint64_t active = 0, maxw = 0;
+    const uint32_t cap = ((233472u / 2u - 1024u - kLeafFixedBytes - 16u) / 1024u) * 1024u;
+    uint64_t active = 0, maxw = 0, fits = 0;
     for (uint32_t i = 0; i < h.leaf_count; ++i) {
         const uint64_t w0 = rd32(off + 4ull * i), w1 = rd32(off + 4ull * (i + 1));
         if (w1 <= w0 || w0 >= words || (rd32(b + pay_off + 4ull * w0) & 3u) == 0u) continue;
         ++active;
         const uint64_t a0 = (4ull * w0) & ~15ull, a1 = (4ull * w1 + 15u) & ~15ull;
         maxw = std::max(maxw, a1 - a0);
+        fits += a1 - a0 <= cap ? 1u : 0u;
     }
     sparse = 2u * active < (uint64_t)h.leaf_count;
     g.sparse = sparse ? 1u : 0u;
     g.max_window = (uint32_t)std::min<uint64_t>(maxw, 0xFFFFFFFFull);
-    const uint32_t cap = ((233472u / 2u - 1024u - kLeafFixedBytes - 16u) / 1024u) * 1024u;
     g.stage_bytes = std::min<uint32_t>(std::max<uint32_t>((g.max_window + 1023u) & ~1023u, 4096u), cap);
+    if (4u * fits < 3u * active) g.stage_bytes = 0u;
 }
 
 extern "C" {

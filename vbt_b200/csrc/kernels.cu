@@ -1511,6 +1511,59 @@ void launch_query_slice(const DeviceAsset& a, uint32_t z, int t0, int t1, float*
     query_slice_kernel<<<default_grid(), kDecodeWarps * 32, 0, s>>>(a, z, t0, t1, out);
 }
 
+}  // namespace vbtb
+#include "serve_mixed.cuh"
+namespace vbtb {
+
+uint64_t mixed_request_tiles(const MixedReq& r, const AssetGeom& g) { return mixed_tiles(r, g); }
+
+int launch_serve_mixed(const DeviceAsset* assets, const MixedReq* reqs, uint32_t k, uint64_t n_tiles,
+                       unsigned long long* counter, unsigned long long* errs, MixedStepGraph* graph, cudaStream_t s)
+{
+    if (k == 0 || n_tiles == 0) return 0;
+    if (k > kMaxMixedReqs) return (int)cudaErrorInvalidValue;
+    int grid = mixed_grid(n_tiles);
+    if (!graph) {
+        cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+        serve_mixed_kernel<<<grid, kMixedWarps * 32, 0, s>>>(assets, reqs, k, n_tiles, counter, errs);
+        return (int)cudaGetLastError();
+    }
+    void* args[] = {(void*)&assets, (void*)&reqs, (void*)&k, (void*)&n_tiles, (void*)&counter, (void*)&errs};
+    cudaKernelNodeParams kp{};
+    kp.func = (void*)serve_mixed_kernel;
+    kp.gridDim = dim3((unsigned)grid);
+    kp.blockDim = dim3(kMixedWarps * 32);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = args;
+    cudaError_t e = cudaSuccess;
+    if (!graph->exec) {
+        cudaMemsetParams mp{};
+        mp.dst = counter;
+        mp.value = 0;
+        mp.elementSize = 4;
+        mp.width = 2;
+        mp.height = 1;
+        cudaGraphNode_t memset_node = nullptr;
+        if ((e = cudaGraphCreate(&graph->graph, 0)) != cudaSuccess ||
+            (e = cudaGraphAddMemsetNode(&memset_node, graph->graph, nullptr, 0, &mp)) != cudaSuccess ||
+            (e = cudaGraphAddKernelNode(&graph->kernel, graph->graph, &memset_node, 1, &kp)) != cudaSuccess ||
+            (e = cudaGraphInstantiate(&graph->exec, graph->graph, 0)) != cudaSuccess) {
+            release_mixed_graph(*graph);
+            return (int)e;
+        }
+    } else if ((e = cudaGraphExecKernelNodeSetParams(graph->exec, graph->kernel, &kp)) != cudaSuccess) {
+        return (int)e;
+    }
+    return (int)cudaGraphLaunch(graph->exec, s);
+}
+
+void release_mixed_graph(MixedStepGraph& g)
+{
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = MixedStepGraph{};
+}
+
 // Exhaustive check of div_small_rn (the render decode's interval quotient) against IEEE division:
 // every pair 0 < a < b <= b_max, with RN(1/b) as the decode forms it.  Counts mismatches and keeps
 // the smallest failing (b << 16 | a).

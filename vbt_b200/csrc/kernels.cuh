@@ -54,6 +54,35 @@ constexpr int kCtrlSlots = 343 + 512;   // coarse (<= 7^3) + fine (<= 7^3) or sh
 // per-warp shared slots: max(render controls, scientific 64 controls + 16 basis grids of 4^3)
 constexpr int kWarpSlots = 64 + 16 * 64 > kCtrlSlots ? 64 + 16 * 64 : kCtrlSlots;
 
+// One request of a mixed serving step (serve_mixed_kernel, serve_mixed.cuh): the kind, the asset
+// (an index into the step's DeviceAsset array), its running tile offset and its device buffers.
+constexpr uint32_t kMixedPoints = 0, kMixedSlice = 1, kMixedFrames = 2;
+constexpr uint32_t kMaxMixedReqs = 256;
+struct MixedReq {
+    uint32_t kind, asset;
+    uint32_t n;       // points: queries; frames: frames
+    uint32_t a0;      // slice: z
+    int32_t t0, t1;   // slice: frames [t0, t1)
+    uint64_t first;   // tiles of the step before this request's
+    uint64_t in;      // points: device address of its queries (16 B each); frames: of its int32 frame list
+    uint64_t out;     // device address of its result
+};
+// Tiles of one request of a mixed step (host and device agree on this count).
+uint64_t mixed_request_tiles(const MixedReq& r, const AssetGeom& g);
+// A mixed step as a CUDA graph (work-counter reset, then the persistent kernel), built on first
+// use and relaunched with the next step's parameters.
+struct MixedStepGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNode_t kernel = nullptr;
+};
+// Launch one mixed step: reqs[k] (device) with running tile offsets summing to n_tiles; errs[k]
+// receive each request's first failing (leaf << 8 | status).  counter: an 8-byte device word of
+// the caller's (reset by the step).  With a graph, the step replays it (its parameters updated).
+int launch_serve_mixed(const DeviceAsset* assets, const MixedReq* reqs, uint32_t k, uint64_t n_tiles,
+                       unsigned long long* counter, unsigned long long* errs, MixedStepGraph* graph, cudaStream_t s);
+void release_mixed_graph(MixedStepGraph& g);
+
 void launch_walk(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);
 // page table only, from the leaf table the walker built (same predicate, same ranks)
 void launch_page_table(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);

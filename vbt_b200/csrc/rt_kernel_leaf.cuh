@@ -339,19 +339,24 @@ __device__ __noinline__ void leaf_decode_general(const DeviceAsset& a, M m, Leaf
 }
 
 // The specialised decode (rt_leaf_fast.cuh) as a call of its own too: each path gets the whole
-// register budget of the 288-thread launch.
-template <bool FINE, bool DENSE>
-__device__ __noinline__ void leaf_decode_fast_call(const DeviceAsset& a, LeafEntry e, uint32_t lb, int nframes,
-                                                   LeafGeom G, float* __restrict__ out, uint64_t frame_stride)
+// register budget of the 288-thread launch.  The leaf's bytes are read from the shared-memory
+// stage, or (GLOBAL_KEYS: a leaf larger than the stage) straight from the payload through L1 --
+// the same byte offsets from the 16-byte-aligned window start a0; the payload's 16-byte tail
+// padding keeps the second word of the last key read inside the allocation.
+template <bool FINE, bool DENSE, bool GLOBAL_KEYS>
+__device__ __noinline__ void leaf_decode_fast_call(const DeviceAsset& a, LeafEntry e, uint32_t lb, uint64_t a0,
+                                                   int nframes, LeafGeom G, float* __restrict__ out,
+                                                   uint64_t frame_stride)
 {
     extern __shared__ __align__(128) uint8_t dyn[];
     const LeafSmem s = leaf_layout<kDecWarps>(dyn);
     const QuadSink<DENSE> sink{out, frame_stride, G.li, a.g.width, a.g.height, G.bx, G.by, G.bz, G.w, G.h, G.d};
-    leaf_decode_fast<FINE, kDecWarps>(s.stage, lb, s, e, nframes, G, sink);
+    const uint8_t* st = GLOBAL_KEYS ? reinterpret_cast<const uint8_t*>(a.payload) + a0 : s.stage;
+    leaf_decode_fast<FINE, kDecWarps>(st, lb, s, e, nframes, G, sink);
 }
 
-// Staged GRID4 / FINE6 leaves of the common shape take leaf_decode_fast (rt_leaf_fast.cuh), every
-// other leaf the general leaf_decode.
+// GRID4 / FINE6 leaves of the common shape take leaf_decode_fast (rt_leaf_fast.cuh), staged or
+// (GLOBAL_FALLBACK) from global memory; every other leaf the general leaf_decode.
 template <bool DENSE, bool GLOBAL_FALLBACK>
 __global__ void __launch_bounds__(kDecThreads, 2) decode_leaf_kernel(const __grid_constant__ DeviceAsset a,
                                                                      FrameList fl, float* __restrict__ out,
@@ -433,10 +438,15 @@ __global__ void __launch_bounds__(kDecThreads, 2) decode_leaf_kernel(const __gri
             }
             if (staged) phase ^= 1u;
             bool fine = false;
-            if (staged && fast_leaf_shape(e, steps01, fine)) {
+            if (fast_leaf_shape(e, steps01, fine) && (staged || GLOBAL_FALLBACK)) {
                 const uint32_t lb = (uint32_t)(b0 - a0);
-                if (fine) leaf_decode_fast_call<true, DENSE>(a, e, lb, fl.n, G, out, frame_stride);
-                else leaf_decode_fast_call<false, DENSE>(a, e, lb, fl.n, G, out, frame_stride);
+                if (staged) {
+                    if (fine) leaf_decode_fast_call<true, DENSE, false>(a, e, lb, a0, fl.n, G, out, frame_stride);
+                    else leaf_decode_fast_call<false, DENSE, false>(a, e, lb, a0, fl.n, G, out, frame_stride);
+                } else if constexpr (GLOBAL_FALLBACK) {
+                    if (fine) leaf_decode_fast_call<true, DENSE, true>(a, e, lb, a0, fl.n, G, out, frame_stride);
+                    else leaf_decode_fast_call<false, DENSE, true>(a, e, lb, a0, fl.n, G, out, frame_stride);
+                }
             } else if (staged) {
                 const SharedWords m{reinterpret_cast<const uint32_t*>(s.stage), (uint32_t)(a0 >> 2)};
                 leaf_decode_general<SharedWords, DENSE>(a, m, e, fl.n, steps01, monotone, G, out, frame_stride);
@@ -485,8 +495,9 @@ static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameL
         cudaMemsetAsync(slot, 0, sizeof(unsigned long long), s);
     if (DENSE) {
         // The zero fill (bandwidth-bound, small CTAs) runs beside the leaf decode (latency-bound)
-        // on a side stream: fork and join through events on the caller's stream, the decode given
-        // one CTA per SM so that zero-fill CTAs fit beside it.  The two write disjoint segments.
+        // on a side stream: fork and join through events on the caller's stream, the decode of a
+        // mostly EMPTY volume given one CTA per SM so that zero-fill CTAs fit beside it.  The two
+        // write disjoint segments.
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -498,8 +509,9 @@ static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameL
         cudaStreamWaitEvent(side, fork, 0);
         zero_empty_kernel<<<8 * sms, 256, 0, side>>>(a, out, stride, (uint32_t)fl.n);
         cudaEventRecord(join, side);
-        decode_leaf_kernel<DENSE, GF><<<grid > 0 ? grid : sms, kDecThreads, smem, s>>>(a, fl, out, stride, slot,
-                                                                                         seq + 1u);
+        // a volume with few EMPTY leaves has little to zero: the decode takes the whole GPU
+        const int dg = grid > 0 ? grid : (a.g.sparse ? sms : leaf_grid<DENSE, GF>(smem));
+        decode_leaf_kernel<DENSE, GF><<<dg, kDecThreads, smem, s>>>(a, fl, out, stride, slot, seq + 1u);
         cudaStreamWaitEvent(s, join, 0);
         cudaEventDestroy(fork);
         cudaEventDestroy(join);

@@ -8,10 +8,15 @@
 //      the device arena (the HBM budget) has room for their inputs and results.  A request that
 //      does not fit may be passed over by later ones at most kMaxBypass times; after that the
 //      server admits nothing behind it until it fits;
-//   3. batching: the point requests admitted in one pass become one multi-asset launch; slice and
-//      frame requests get a unit each.
+//   3. batching: the requests admitted in one pass -- points, slices and frames of any assets --
+//      become units of up to max_batch_queries values each (a larger request is a unit of its own),
+//      and a unit is ONE persistent launch (serve_mixed_kernel) whose warps take tiles of all its
+//      requests from a work counter, replayed from a per-stream CUDA graph with the unit's
+//      parameters.  With separate_kinds, only point requests merge (one multi-asset point launch)
+//      and slices and frames run on their own kernels, a unit each.
 // Units run on `slots` streams, so requests that arrive while others are on the GPU overlap
-// with them.  In plain mode the server admits one request per unit and keeps one unit in flight.
+// with them.  In plain mode the server admits one request per unit, keeps one unit in flight, and
+// runs each on its kind's own kernel.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,7 +46,8 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr uint32_t kMaxAssets = 64;
-constexpr uint32_t kMaxUnitRequests = 256;   // requests merged into one point launch
+constexpr uint32_t kMaxUnitRequests = 256;   // requests merged into one launch
+static_assert(kMaxUnitRequests <= kMaxMixedReqs, "a unit's requests fit the mixed kernel's table");
 constexpr uint32_t kMaxSlots = 32;
 constexpr int kMaxBypass = 64;
 constexpr uint64_t kAlign = 256;
@@ -123,9 +129,11 @@ struct Req {
 
 struct Unit {
     std::vector<Req*> reqs;
-    Block dev_in;     // error words, segment table, point inputs
-    Block stage_in;   // pinned staging of the segment table and pageable point inputs
+    Block dev_in;     // error words, segment or request table, point inputs
+    Block stage_in;   // pinned staging of the table and pageable point inputs
     uint64_t points = 0;
+    uint64_t frames = 0;   // frame indices of the unit's frame requests (mixed units)
+    bool mixed = false;    // one serve_mixed_kernel launch over all of its requests
 };
 
 // Memory the copy engines reach directly: pinned host memory, or device (or managed) memory of
@@ -149,6 +157,12 @@ uint64_t err_bytes(uint32_t k) { return (8ull * k + 15) & ~15ull; }
 // Device input block of a point unit: [errs][segment table][queries 16N], each part 16-byte
 // aligned (the queries are read as uint4, the output addresses as 64-bit words).
 uint64_t points_in_bytes(uint32_t k, uint64_t n) { return err_bytes(k) + ((seg_bytes(k) + 15) & ~15ull) + 16ull * n; }
+uint64_t a16(uint64_t b) { return (b + 15) & ~15ull; }
+// Request table of a k-request mixed unit with nf frame indices in all: [MixedReq k][int32 nf],
+// staged on the host and copied as one block.
+uint64_t mixed_table_bytes(uint32_t k, uint64_t nf) { return a16(sizeof(MixedReq) * k) + a16(4ull * nf); }
+// Device input block of a mixed unit: [errs][request table][queries 16N], each part 16-byte aligned.
+uint64_t mixed_in_bytes(uint32_t k, uint64_t nf, uint64_t n) { return err_bytes(k) + mixed_table_bytes(k, nf) + 16ull * n; }
 
 }  // namespace
 
@@ -168,6 +182,8 @@ struct vbt_server {
     cudaStream_t streams[kMaxSlots]{};
     cudaEvent_t events[kMaxSlots]{};
     Unit* busy[kMaxSlots]{};
+    unsigned long long* d_counters = nullptr;   // the mixed launch's work counter, one per stream
+    MixedStepGraph graphs[kMaxSlots];           // the mixed step as a graph, one per stream
     // requests
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -188,6 +204,7 @@ struct vbt_server {
     bool reserve_result(Req* r);
     void unreserve_result(Req* r);
     bool fill_points(Unit* u);
+    bool fill_mixed(Unit* u);
     void admit(std::vector<Unit*>& out, int free_slots);
     void launch(Unit* u, int slot);
     void finalize(Unit* u, int slot);
@@ -268,13 +285,52 @@ bool vbt_server::fill_points(Unit* u)
     return false;
 }
 
+// Reserve a mixed unit's input blocks, returning requests from the back to the queue until they fit.
+bool vbt_server::fill_mixed(Unit* u)
+{
+    while (!u->reqs.empty()) {
+        const uint32_t k = (uint32_t)u->reqs.size();
+        uint64_t n = 0, nf = 0, pageable = 0;
+        for (Req* r : u->reqs) {
+            if (r->r.kind == VBT_REQ_POINTS) {
+                n += r->r.n_points;
+                if (!r->pinned_in) pageable += 16ull * r->r.n_points;
+            } else if (r->r.kind == VBT_REQ_FRAMES) {
+                nf += r->frames.size();
+            }
+        }
+        Block d, h;
+        d.bytes = mixed_in_bytes(k, nf, n);
+        h.bytes = mixed_table_bytes(k, nf) + pageable;
+        if (arena.alloc(d.bytes, &d.off)) {
+            d.valid = true;
+            if (stage.alloc(h.bytes, &h.off)) {
+                h.valid = true;
+                u->dev_in = d;
+                u->stage_in = h;
+                u->points = n;
+                u->frames = nf;
+                u->mixed = true;
+                return true;
+            }
+            arena.release(d.off, d.bytes);
+        }
+        Req* last = u->reqs.back();
+        u->reqs.pop_back();
+        unreserve_result(last);
+        last->state = 0;
+    }
+    return false;
+}
+
 // Build the units of this pass (called with mu held).
 void vbt_server::admit(std::vector<Unit*>& out, int free_slots)
 {
+    const bool mixed = !cfg.plain && !cfg.separate_kinds;
     while (free_slots > 0 && !pending.empty()) {
         Unit* u = new Unit();
         bool points_unit = false;
-        uint64_t points = 0;
+        uint64_t points = 0, values = 0;
         size_t scanned = 0;
         Req* blocked = nullptr;   // the oldest request of this pass that did not fit
         for (auto it = pending.begin(); it != pending.end(); ++it, ++scanned) {
@@ -283,8 +339,13 @@ void vbt_server::admit(std::vector<Unit*>& out, int free_slots)
             if (cfg.plain && scanned > 0) break;
             const bool pts = r->r.kind == VBT_REQ_POINTS;
             if (!u->reqs.empty()) {
-                if (!points_unit || !pts) continue;   // only point requests merge
-                if (u->reqs.size() >= kMaxUnitRequests || points + r->r.n_points > cfg.max_batch_queries) continue;
+                if (u->reqs.size() >= kMaxUnitRequests) continue;
+                if (mixed) {
+                    if (values + r->result_floats > cfg.max_batch_queries) continue;
+                } else {
+                    if (!points_unit || !pts) continue;   // only point requests merge
+                    if (points + r->r.n_points > cfg.max_batch_queries) continue;
+                }
             }
             if (blocked && blocked->bypassed >= kMaxBypass) break;   // hold the line for it
             if (pts) r->pinned_in = is_pinned(r->r.points);
@@ -295,13 +356,19 @@ void vbt_server::admit(std::vector<Unit*>& out, int free_slots)
             if (blocked) ++blocked->bypassed;
             r->state = 1;
             u->reqs.push_back(r);
-            if (!pts) break;   // slices and frames run alone
-            points_unit = true;
-            points += r->r.n_points;
+            values += r->result_floats;
+            if (pts) {
+                points_unit = true;
+                points += r->r.n_points;
+            }
             if (cfg.plain) break;
+            if (mixed) continue;
+            if (!pts) break;   // slices and frames run alone
         }
         bool ok = !u->reqs.empty();
-        if (ok && points_unit) {
+        if (ok && mixed) {
+            ok = fill_mixed(u);
+        } else if (ok && points_unit) {
             ok = fill_points(u);
         } else if (ok) {
             Block d;
@@ -340,7 +407,58 @@ void vbt_server::launch(Unit* u, int slot)
     cudaMemsetAsync(d_err, 0xFF, 8ull * k, st);
     uint64_t nl = 0;
     Req* r0 = u->reqs[0];
-    if (r0->r.kind == VBT_REQ_POINTS) {
+    int launch_err = 0;
+    if (u->mixed) {
+        // request table (+ frame lists) staged and copied as one block, point inputs after it
+        uint8_t* hs = h_stage + u->stage_in.off;
+        MixedReq* tab = reinterpret_cast<MixedReq*>(hs);
+        int32_t* hfr = reinterpret_cast<int32_t*>(hs + a16(sizeof(MixedReq) * k));
+        uint8_t* dtab = din + err_bytes(k);
+        uint8_t* dfr = dtab + a16(sizeof(MixedReq) * k);
+        uint8_t* dq = dtab + mixed_table_bytes(k, u->frames);
+        uint8_t* hpage = hs + mixed_table_bytes(k, u->frames);
+        uint64_t q = 0, f = 0, tiles = 0;
+        for (uint32_t i = 0; i < k; ++i) {
+            Req* r = u->reqs[i];
+            MixedReq m{};
+            m.asset = r->r.asset;
+            m.first = tiles;
+            m.out = reinterpret_cast<uint64_t>(d_arena + r->dev_result.off);
+            if (r->r.kind == VBT_REQ_POINTS) {
+                m.kind = kMixedPoints;
+                m.n = (uint32_t)r->r.n_points;
+                m.in = reinterpret_cast<uint64_t>(dq + 16ull * q);
+                const uint64_t b = 16ull * r->r.n_points;
+                if (b) {
+                    if (r->pinned_in) {
+                        cudaMemcpyAsync(dq + 16ull * q, r->r.points, b, cudaMemcpyDefault, st);
+                    } else {
+                        std::memcpy(hpage, r->r.points, b);
+                        cudaMemcpyAsync(dq + 16ull * q, hpage, b, cudaMemcpyHostToDevice, st);
+                        hpage += b;
+                    }
+                }
+                q += r->r.n_points;
+            } else if (r->r.kind == VBT_REQ_SLICE) {
+                m.kind = kMixedSlice;
+                m.a0 = r->r.z;
+                m.t0 = r->r.t0;
+                m.t1 = r->r.t1;
+            } else {
+                m.kind = kMixedFrames;
+                m.n = (uint32_t)r->frames.size();
+                m.in = reinterpret_cast<uint64_t>(dfr + 4ull * f);
+                if (m.n) std::memcpy(hfr + f, r->frames.data(), 4ull * m.n);
+                f += m.n;
+            }
+            tab[i] = m;
+            tiles += mixed_request_tiles(m, assets[r->r.asset]->dev.g);
+        }
+        cudaMemcpyAsync(dtab, hs, mixed_table_bytes(k, u->frames), cudaMemcpyHostToDevice, st);
+        launch_err = launch_serve_mixed(d_assets, reinterpret_cast<const MixedReq*>(dtab), k, tiles, d_counters + slot,
+                                        d_err, &graphs[slot], st);
+        nl = tiles ? 1 : 0;
+    } else if (r0->r.kind == VBT_REQ_POINTS) {
         uint8_t* hseg = h_stage + u->stage_in.off;
         uint32_t* starts = reinterpret_cast<uint32_t*>(hseg);
         uint64_t* outs = reinterpret_cast<uint64_t*>(hseg + ((4ull * (2 * k + 1) + 7) & ~7ull));
@@ -410,7 +528,7 @@ void vbt_server::launch(Unit* u, int slot)
     std::lock_guard<std::mutex> lk(mu);
     launches += nl;
     ++units;
-    if (e != cudaSuccess)
+    if (e != cudaSuccess || launch_err != 0)
         for (Req* r : u->reqs) r->status = VBT_STATUS_CUDA;
 }
 
@@ -557,6 +675,7 @@ int vbt_server_create(const vbt_server_config* config, vbt_server** out)
     if (e == cudaSuccess) e = cudaMalloc(&s->d_assets, sizeof(DeviceAsset) * kMaxAssets);
     if (e == cudaSuccess) e = cudaHostAlloc(&s->h_stage, c.host_staging_bytes, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(&s->h_err, 8ull * kMaxSlots * kMaxUnitRequests, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_counters, 8ull * kMaxSlots);
     for (uint32_t i = 0; e == cudaSuccess && i < c.slots; ++i) {
         e = cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->events[i], cudaEventDisableTiming);
@@ -570,6 +689,7 @@ int vbt_server_create(const vbt_server_config* config, vbt_server** out)
         }
         cudaFree(s->d_arena);
         cudaFree(s->d_assets);
+        cudaFree(s->d_counters);
         cudaFreeHost(s->h_stage);
         cudaFreeHost(s->h_err);
         delete s;
@@ -637,11 +757,12 @@ int vbt_serve_submit(vbt_server* s, const vbt_request* rq, uint64_t* ticket)
     }
     if (st == VBT_STATUS_OK) {
         r->result_floats = result_floats(r->r, a);
+        const uint64_t np = rq->kind == VBT_REQ_POINTS ? rq->n_points : 0, nf = r->frames.size();
         const uint64_t need = Arena::round(4ull * r->result_floats) +
-                              Arena::round(rq->kind == VBT_REQ_POINTS ? points_in_bytes(1, rq->n_points) : 8);
+                              Arena::round(std::max(points_in_bytes(1, np), mixed_in_bytes(1, nf, np)));
         const uint64_t staged = (rq->host_out && !is_pinned(rq->host_out) ? 4ull * r->result_floats : 0) +
                                 (rq->kind == VBT_REQ_POINTS && !is_pinned(rq->points) ? 16ull * rq->n_points : 0) +
-                                seg_bytes(1);
+                                std::max(seg_bytes(1), mixed_table_bytes(1, nf));
         if (need > s->cfg.hbm_budget_bytes)
             st = VBT_STATUS_LIMIT, msg = "request needs more device memory than the server's budget";
         else if (Arena::round(staged) + kAlign > s->cfg.host_staging_bytes)
@@ -756,12 +877,14 @@ int vbt_server_destroy(vbt_server* s)
     cudaSetDevice(s->cfg.device);
     for (uint32_t i = 0; i < s->cfg.slots; ++i) {
         cudaStreamSynchronize(s->streams[i]);
+        release_mixed_graph(s->graphs[i]);
         cudaStreamDestroy(s->streams[i]);
         cudaEventDestroy(s->events[i]);
     }
     for (auto& kv : s->tickets) delete kv.second;
     cudaFree(s->d_arena);
     cudaFree(s->d_assets);
+    cudaFree(s->d_counters);
     cudaFreeHost(s->h_stage);
     cudaFreeHost(s->h_err);
     cudaSetDevice(prev);
