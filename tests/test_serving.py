@@ -293,8 +293,9 @@ def test_device_resident_requests(vbt, cuda, assets):
 @pytest.mark.parametrize("separate", [False, True], ids=["mixed", "separate_kinds"])
 def test_mixed_launch_equals_alone(vbt, cuda, assets, separate):
     """Points, slices and frames over several assets, pending together behind a long request, go
-    out as one persistent mixed launch (serve_mixed_kernel, replayed from the stream's graph): far
-    fewer units than requests, one launch per unit.  Every result equals the plain server's (each
+    out together: the points in one multi-asset point launch, the slices and frames in one
+    persistent mixed launch (serve_mixed_kernel, replayed from the stream's graph) -- far fewer
+    units than requests, at most two launches per unit.  Every result equals the plain server's (each
     request on its own kind's kernel) bit for bit; so does the schedule that merges only points."""
     reqs = make_requests(assets, seed=21, n=40)
     alone = run_alone(vbt, cuda, assets, reqs)
@@ -321,4 +322,4 @@ def test_mixed_launch_equals_alone(vbt, cuda, assets, separate):
         assert np.array_equal(bufs[j][1].view(np.uint32), alone[j].view(np.uint32)), (j, r[0])
     if not separate:
         assert st.units < len(reqs) // 2, st.units
-        assert st.launches <= st.units, (st.launches, st.units)
+        assert st.launches <= 2 * st.units, (st.launches, st.units)   # points + one mixed launch

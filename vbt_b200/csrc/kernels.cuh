@@ -54,17 +54,18 @@ constexpr int kCtrlSlots = 343 + 512;   // coarse (<= 7^3) + fine (<= 7^3) or sh
 // per-warp shared slots: max(render controls, scientific 64 controls + 16 basis grids of 4^3)
 constexpr int kWarpSlots = 64 + 16 * 64 > kCtrlSlots ? 64 + 16 * 64 : kCtrlSlots;
 
-// One request of a mixed serving step (serve_mixed_kernel, serve_mixed.cuh): the kind, the asset
-// (an index into the step's DeviceAsset array), its running tile offset and its device buffers.
-constexpr uint32_t kMixedPoints = 0, kMixedSlice = 1, kMixedFrames = 2;
+// One slice or frame request of a mixed serving step (serve_mixed_kernel, serve_mixed.cuh): the
+// kind, the asset (an index into the step's DeviceAsset array), its running tile offset and its
+// device buffers.
+constexpr uint32_t kMixedSlice = 1, kMixedFrames = 2;
 constexpr uint32_t kMaxMixedReqs = 256;
 struct MixedReq {
     uint32_t kind, asset;
-    uint32_t n;       // points: queries; frames: frames
+    uint32_t n;       // frames: frames
     uint32_t a0;      // slice: z
     int32_t t0, t1;   // slice: frames [t0, t1)
     uint64_t first;   // tiles of the step before this request's
-    uint64_t in;      // points: device address of its queries (16 B each); frames: of its int32 frame list
+    uint64_t in;      // frames: device address of its int32 frame list
     uint64_t out;     // device address of its result
 };
 // Tiles of one request of a mixed step (host and device agree on this count).

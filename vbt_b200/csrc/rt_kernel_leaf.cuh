@@ -270,52 +270,47 @@ __device__ __forceinline__ uint32_t grab_leaf(unsigned long long* slot, uint32_t
     return 0xFFFFFFFFu;
 }
 
-// Dense frames, EMPTY leaves: zero their segments of every output row (row = (frame, z, y), y
-// fastest), one row per group of per_row threads, rows grid-strided.  This runs as its own
-// full-occupancy launch before the leaf decode, which then visits only the active leaves: the
-// stores of the zero fill are bandwidth-bound and need many warps in flight, the leaf decode is
-// latency-bound with 16 warps per SM.  An inactive leaf with a walker status records it (once).
-__global__ void __launch_bounds__(256) zero_empty_kernel(DeviceAsset a, float* __restrict__ out,
-                                                         uint64_t frame_stride, uint32_t nframes)
+// Dense frames, EMPTY leaves: zero their segments of the eight lines of y-band `by` in z-plane zz,
+// in every frame of the launch, the whole CTA.  The band's inactive leaves are a 64-bit mask per 64
+// leaves along x (a ballot over the page table, the same for every line and frame); the warps take
+// (line, frame) pairs and the lanes store consecutive 16-byte chunks (a chunk never straddles two
+// leaves).  Inactive leaves with a walker status record it once (the leaf's first plane).  vec:
+// rows 16-byte aligned (X % 4 == 0, 16-byte aligned output and frame stride); otherwise one float
+// per store.
+template <int NW>
+__device__ __forceinline__ void zero_band(const DeviceAsset& a, float* __restrict__ out, uint64_t frame_stride,
+                                          int nframes, uint32_t zz, uint32_t by, bool vec)
 {
-    const uint32_t X = a.g.width, Y = a.g.height, Z = a.g.depth;
-    const uint64_t rows = (uint64_t)nframes * Z * Y;
-    const bool vec = (X & 3u) == 0u && (reinterpret_cast<uintptr_t>(out) & 15u) == 0u && (frame_stride & 3u) == 0u;
-    const uint32_t per_row = vec ? X >> 2 : X;
-    const uint32_t group = per_row >= 256u ? 1u : 256u / per_row;
-    const uint32_t k = threadIdx.x / per_row;
-    if (k >= group) return;
-    const uint32_t u0 = threadIdx.x - k * per_row, ustep = group == 1u ? 256u : per_row;
-    // a contiguous block of rows per CTA: one division to place the thread's first row, then the
-    // (frame, z, y) coordinates are carried forward
-    const uint64_t per_cta = (rows + gridDim.x - 1) / gridDim.x;
-    const uint64_t rb = (uint64_t)blockIdx.x * per_cta;
-    const uint64_t re = rows < rb + per_cta ? rows : rb + per_cta;
-    if (rb + k >= re) return;
-    const uint64_t zy_n = (uint64_t)Z * Y;
-    uint32_t fi = (uint32_t)((rb + k) / zy_n);
-    const uint32_t zy = (uint32_t)(rb + k - (uint64_t)fi * zy_n);
-    uint32_t z = zy / Y, y = zy - z * Y;
-    for (uint64_t r = rb + k; r < re; r += group) {
-        const uint32_t lrow = ((z >> 3) * a.g.lcy + (y >> 3)) * a.g.lcx;
-        float* row = out + (uint64_t)fi * frame_stride + ((uint64_t)z * Y + y) * X;
-        for (uint32_t u = u0; u < per_row; u += ustep) {
-            const uint32_t x = vec ? 4u * u : u;
-            const uint32_t leaf = lrow + (x >> 3);
-            if (__ldg(a.compact + leaf) != kNoRank) continue;
-            if (fi == 0u && ((x | y | z) & 7u) == 0u) {
-                const uint32_t st = entry_status(a.entries[leaf]);
-                if (st != kOk) record_error(a.err, leaf, st);
+    const uint32_t X = a.g.width, Y = a.g.height;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lrow = ((zz >> 3) * a.g.lcy + by) * a.g.lcx;
+    const uint32_t lines = min(8u, Y - 8u * by);
+    for (uint32_t b0 = 0; b0 < a.g.lcx; b0 += 64u) {
+        const uint32_t bx0 = b0 + (uint32_t)lane, bx1 = bx0 + 32u;
+        const bool e0 = bx0 < a.g.lcx && __ldg(a.compact + lrow + bx0) == kNoRank;
+        const bool e1 = bx1 < a.g.lcx && __ldg(a.compact + lrow + bx1) == kNoRank;
+        if (warp == 0 && (zz & 7u) == 0u) {
+            if (e0) {
+                const uint32_t st = entry_status(a.entries[lrow + bx0]);
+                if (st != kOk) record_error(a.err, lrow + bx0, st);
             }
-            if (vec) *reinterpret_cast<float4*>(row + x) = make_float4(0.f, 0.f, 0.f, 0.f);
-            else row[x] = 0.0f;
+            if (e1) {
+                const uint32_t st = entry_status(a.entries[lrow + bx1]);
+                if (st != kOk) record_error(a.err, lrow + bx1, st);
+            }
         }
-        y += group;
-        while (y >= Y) {
-            y -= Y;
-            if (++z == Z) {
-                z = 0;
-                ++fi;
+        const uint64_t mask = (uint64_t)__ballot_sync(0xFFFFFFFFu, e0) | ((uint64_t)__ballot_sync(0xFFFFFFFFu, e1) << 32);
+        if (mask == 0ull) continue;
+        const uint32_t x_end = min(X, 8u * (b0 + 64u));
+        for (uint32_t pr = (uint32_t)warp; pr < lines * (uint32_t)nframes; pr += NW) {
+            const uint32_t fi = pr / lines, y = 8u * by + (pr - fi * lines);
+            float* row = out + (uint64_t)fi * frame_stride + ((uint64_t)zz * Y + y) * X;
+            if (vec) {
+                for (uint32_t x = 8u * b0 + 4u * (uint32_t)lane; x < x_end; x += 128u)
+                    if ((mask >> ((x >> 3) - b0)) & 1ull) *reinterpret_cast<float4*>(row + x) = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                for (uint32_t x = 8u * b0 + (uint32_t)lane; x < x_end; x += 32u)
+                    if ((mask >> ((x >> 3) - b0)) & 1ull) row[x] = 0.0f;
             }
         }
     }
@@ -368,8 +363,17 @@ __global__ void __launch_bounds__(kDecThreads, 2) decode_leaf_kernel(const __gri
     uint32_t* const s_next = reinterpret_cast<uint32_t*>(dyn + 8);   // beside the 8-byte barrier
     const int tid = threadIdx.x;
     const int total = (int)a.g.frames;
-    // the active leaves by rank (dense frames: EMPTY leaves are zeroed by zero_empty_kernel)
+    // work items: the active leaves by rank and, for dense frames of a volume with inactive leaves,
+    // one item per (z-plane, y-band of leaves) that zeroes the inactive leaves' segments of that
+    // band in every frame.  The two kinds are interleaved in proportion (item i is leaf
+    // floor(i A / N) when that value steps at i, else zero band i - floor(i A / N)), so
+    // bandwidth-bound zeroing and latency-bound decoding share the GPU throughout the launch.
     const uint32_t n_leaves = *(volatile const uint32_t*)a.counters;
+    const uint32_t n_zero = DENSE && n_leaves < a.g.leaf_count ? a.g.depth * a.g.lcy : 0u;
+    const uint64_t n_items = (uint64_t)n_leaves + n_zero;
+    const bool vec = (a.g.width & 3u) == 0u && (reinterpret_cast<uintptr_t>(out) & 15u) == 0u &&
+                     (frame_stride & 3u) == 0u;
+
     if (tid == 0) {
         mbar_init(s.bar, 1);
         mbar_init_fence();
@@ -392,10 +396,27 @@ __global__ void __launch_bounds__(kDecThreads, 2) decode_leaf_kernel(const __gri
     const uint8_t* pay_bytes = reinterpret_cast<const uint8_t*>(a.payload);
     uint32_t phase = 0;
     uint32_t li = *s_next;
-    while (li < n_leaves) {
+    while (li < n_items) {
         // every thread has read li, and the previous leaf's shared-memory reads are complete
         __syncthreads();
-        const uint32_t rank = li;
+        uint32_t rank = li;
+        if (DENSE && n_zero) {
+            const uint32_t d = (uint32_t)((uint64_t)li * n_leaves / n_items);
+            const uint32_t d1 = (uint32_t)((uint64_t)(li + 1u) * n_leaves / n_items);
+            if (d1 == d) {   // a zero band
+                if (tid == 0) {
+                    bool to = false;
+                    *s_next = grab_leaf(work, epoch, to);
+                    if (to) record_error(a.err, 0u, kErrWaitTimeout);
+                }
+                const uint32_t zi = li - d;
+                zero_band<kDecWarps>(a, out, frame_stride, fl.n, zi / a.g.lcy, zi % a.g.lcy, vec);
+                __syncthreads();   // the next index is visible
+                li = *s_next;
+                continue;
+            }
+            rank = d;
+        }
         const uint32_t leaf = __ldg(a.active_list + rank);
         const LeafEntry e = a.entries[leaf];
         LeafGeom G;
@@ -460,16 +481,6 @@ __global__ void __launch_bounds__(kDecThreads, 2) decode_leaf_kernel(const __gri
     }
 }
 
-// One non-blocking side stream per device for the dense zero fill (created on first use, with
-// the device current; kept for the process).
-static cudaStream_t dense_side_stream(int dev)
-{
-    static std::once_flag once[64];
-    static cudaStream_t streams[64];
-    std::call_once(once[dev & 63], [&] { cudaStreamCreateWithFlags(&streams[dev & 63], cudaStreamNonBlocking); });
-    return streams[dev & 63];
-}
-
 template <bool DENSE, bool GF>
 static int leaf_grid(uint32_t smem_bytes)
 {
@@ -493,30 +504,6 @@ static void launch_leaf_variant(const DeviceAsset& a, uint32_t seq, const FrameL
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
         cudaMemsetAsync(slot, 0, sizeof(unsigned long long), s);
-    if (DENSE) {
-        // The zero fill (bandwidth-bound, small CTAs) runs beside the leaf decode (latency-bound)
-        // on a side stream: fork and join through events on the caller's stream, the decode of a
-        // mostly EMPTY volume given one CTA per SM so that zero-fill CTAs fit beside it.  The two
-        // write disjoint segments.
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaStream_t side = dense_side_stream(dev);
-        cudaEvent_t fork = nullptr, join = nullptr;
-        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
-        cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
-        cudaEventRecord(fork, s);
-        cudaStreamWaitEvent(side, fork, 0);
-        zero_empty_kernel<<<8 * sms, 256, 0, side>>>(a, out, stride, (uint32_t)fl.n);
-        cudaEventRecord(join, side);
-        // a volume with few EMPTY leaves has little to zero: the decode takes the whole GPU
-        const int dg = grid > 0 ? grid : (a.g.sparse ? sms : leaf_grid<DENSE, GF>(smem));
-        decode_leaf_kernel<DENSE, GF><<<dg, kDecThreads, smem, s>>>(a, fl, out, stride, slot, seq + 1u);
-        cudaStreamWaitEvent(s, join, 0);
-        cudaEventDestroy(fork);
-        cudaEventDestroy(join);
-        return;
-    }
     decode_leaf_kernel<DENSE, GF><<<g, kDecThreads, smem, s>>>(a, fl, out, stride, slot, seq + 1u);
 }
 

@@ -9,11 +9,12 @@
 //      does not fit may be passed over by later ones at most kMaxBypass times; after that the
 //      server admits nothing behind it until it fits;
 //   3. batching: the requests admitted in one pass -- points, slices and frames of any assets --
-//      become units of up to max_batch_queries values each (a larger request is a unit of its own),
-//      and a unit is ONE persistent launch (serve_mixed_kernel) whose warps take tiles of all its
-//      requests from a work counter, replayed from a per-stream CUDA graph with the unit's
-//      parameters.  With separate_kinds, only point requests merge (one multi-asset point launch)
-//      and slices and frames run on their own kernels, a unit each.
+//      become units of up to max_batch_queries values each (a larger request is a unit of its own).
+//      A unit is at most two launches: its point requests, across assets, in one multi-asset point
+//      launch, and its slices and frames in ONE persistent launch (serve_mixed_kernel) whose warps
+//      take tiles of all of them from a work counter, replayed from a per-stream CUDA graph with
+//      the unit's parameters.  With separate_kinds, only point requests merge and slices and
+//      frames run on their own kernels, a unit each.
 // Units run on `slots` streams, so requests that arrive while others are on the GPU overlap
 // with them.  In plain mode the server admits one request per unit, keeps one unit in flight, and
 // runs each on its kind's own kernel.
@@ -158,11 +159,18 @@ uint64_t err_bytes(uint32_t k) { return (8ull * k + 15) & ~15ull; }
 // aligned (the queries are read as uint4, the output addresses as 64-bit words).
 uint64_t points_in_bytes(uint32_t k, uint64_t n) { return err_bytes(k) + ((seg_bytes(k) + 15) & ~15ull) + 16ull * n; }
 uint64_t a16(uint64_t b) { return (b + 15) & ~15ull; }
-// Request table of a k-request mixed unit with nf frame indices in all: [MixedReq k][int32 nf],
-// staged on the host and copied as one block.
-uint64_t mixed_table_bytes(uint32_t k, uint64_t nf) { return a16(sizeof(MixedReq) * k) + a16(4ull * nf); }
-// Device input block of a mixed unit: [errs][request table][queries 16N], each part 16-byte aligned.
-uint64_t mixed_in_bytes(uint32_t k, uint64_t nf, uint64_t n) { return err_bytes(k) + mixed_table_bytes(k, nf) + 16ull * n; }
+// Tables of a mixed unit with kp point requests and km slice / frame requests holding nf frame
+// indices in all: [point segment table][MixedReq km][int32 nf], staged on the host and copied as
+// one block.
+uint64_t mixed_table_bytes(uint32_t kp, uint32_t km, uint64_t nf)
+{
+    return a16(seg_bytes(kp)) + a16(sizeof(MixedReq) * km) + a16(4ull * nf);
+}
+// Device input block of a mixed unit: [errs][tables][queries 16N], each part 16-byte aligned.
+uint64_t mixed_in_bytes(uint32_t kp, uint32_t km, uint64_t nf, uint64_t n)
+{
+    return err_bytes(kp + km) + mixed_table_bytes(kp, km, nf) + 16ull * n;
+}
 
 }  // namespace
 
@@ -289,19 +297,21 @@ bool vbt_server::fill_points(Unit* u)
 bool vbt_server::fill_mixed(Unit* u)
 {
     while (!u->reqs.empty()) {
-        const uint32_t k = (uint32_t)u->reqs.size();
+        uint32_t kp = 0;
         uint64_t n = 0, nf = 0, pageable = 0;
         for (Req* r : u->reqs) {
             if (r->r.kind == VBT_REQ_POINTS) {
+                ++kp;
                 n += r->r.n_points;
                 if (!r->pinned_in) pageable += 16ull * r->r.n_points;
             } else if (r->r.kind == VBT_REQ_FRAMES) {
                 nf += r->frames.size();
             }
         }
+        const uint32_t km = (uint32_t)u->reqs.size() - kp;
         Block d, h;
-        d.bytes = mixed_in_bytes(k, nf, n);
-        h.bytes = mixed_table_bytes(k, nf) + pageable;
+        d.bytes = mixed_in_bytes(kp, km, nf, n);
+        h.bytes = mixed_table_bytes(kp, km, nf) + pageable;
         if (arena.alloc(d.bytes, &d.off)) {
             d.valid = true;
             if (stage.alloc(h.bytes, &h.off)) {
@@ -311,6 +321,10 @@ bool vbt_server::fill_mixed(Unit* u)
                 u->points = n;
                 u->frames = nf;
                 u->mixed = true;
+                // point requests first: the point launch reports into errs[0, kp), the mixed one
+                // into errs[kp, k)
+                std::stable_partition(u->reqs.begin(), u->reqs.end(),
+                                      [](const Req* r) { return r->r.kind == VBT_REQ_POINTS; });
                 return true;
             }
             arena.release(d.off, d.bytes);
@@ -409,37 +423,49 @@ void vbt_server::launch(Unit* u, int slot)
     Req* r0 = u->reqs[0];
     int launch_err = 0;
     if (u->mixed) {
-        // request table (+ frame lists) staged and copied as one block, point inputs after it
+        // tables staged and copied as one block: [point segment table][MixedReq][frame lists];
+        // the point inputs after them
+        uint32_t kp = 0;
+        while (kp < k && u->reqs[kp]->r.kind == VBT_REQ_POINTS) ++kp;
+        const uint32_t km = k - kp;
         uint8_t* hs = h_stage + u->stage_in.off;
-        MixedReq* tab = reinterpret_cast<MixedReq*>(hs);
-        int32_t* hfr = reinterpret_cast<int32_t*>(hs + a16(sizeof(MixedReq) * k));
-        uint8_t* dtab = din + err_bytes(k);
-        uint8_t* dfr = dtab + a16(sizeof(MixedReq) * k);
-        uint8_t* dq = dtab + mixed_table_bytes(k, u->frames);
-        uint8_t* hpage = hs + mixed_table_bytes(k, u->frames);
-        uint64_t q = 0, f = 0, tiles = 0;
-        for (uint32_t i = 0; i < k; ++i) {
+        uint32_t* starts = reinterpret_cast<uint32_t*>(hs);
+        uint64_t* outs = reinterpret_cast<uint64_t*>(hs + ((4ull * (2 * kp + 1) + 7) & ~7ull));
+        MixedReq* tab = reinterpret_cast<MixedReq*>(hs + a16(seg_bytes(kp)));
+        int32_t* hfr = reinterpret_cast<int32_t*>(reinterpret_cast<uint8_t*>(tab) + a16(sizeof(MixedReq) * km));
+        uint8_t* dseg = din + err_bytes(k);
+        uint8_t* dtab = dseg + a16(seg_bytes(kp));
+        uint8_t* dfr = dtab + a16(sizeof(MixedReq) * km);
+        const uint64_t tables = mixed_table_bytes(kp, km, u->frames);
+        uint8_t* dq = dseg + tables;
+        uint8_t* hpage = hs + tables;
+        uint64_t q = 0, f = 0, tiles = 0, sparse_points = 0;
+        for (uint32_t i = 0; i < kp; ++i) {
             Req* r = u->reqs[i];
+            starts[i] = (uint32_t)q;
+            starts[kp + 1 + i] = r->r.asset;
+            outs[i] = reinterpret_cast<uint64_t>(d_arena + r->dev_result.off);
+            const uint64_t b = 16ull * r->r.n_points;
+            if (b) {
+                if (r->pinned_in) {
+                    cudaMemcpyAsync(dq + 16ull * q, r->r.points, b, cudaMemcpyDefault, st);
+                } else {
+                    std::memcpy(hpage, r->r.points, b);
+                    cudaMemcpyAsync(dq + 16ull * q, hpage, b, cudaMemcpyHostToDevice, st);
+                    hpage += b;
+                }
+            }
+            if (assets[r->r.asset]->sparse) sparse_points += r->r.n_points;
+            q += r->r.n_points;
+        }
+        starts[kp] = (uint32_t)q;
+        for (uint32_t i = 0; i < km; ++i) {
+            Req* r = u->reqs[kp + i];
             MixedReq m{};
             m.asset = r->r.asset;
             m.first = tiles;
             m.out = reinterpret_cast<uint64_t>(d_arena + r->dev_result.off);
-            if (r->r.kind == VBT_REQ_POINTS) {
-                m.kind = kMixedPoints;
-                m.n = (uint32_t)r->r.n_points;
-                m.in = reinterpret_cast<uint64_t>(dq + 16ull * q);
-                const uint64_t b = 16ull * r->r.n_points;
-                if (b) {
-                    if (r->pinned_in) {
-                        cudaMemcpyAsync(dq + 16ull * q, r->r.points, b, cudaMemcpyDefault, st);
-                    } else {
-                        std::memcpy(hpage, r->r.points, b);
-                        cudaMemcpyAsync(dq + 16ull * q, hpage, b, cudaMemcpyHostToDevice, st);
-                        hpage += b;
-                    }
-                }
-                q += r->r.n_points;
-            } else if (r->r.kind == VBT_REQ_SLICE) {
+            if (r->r.kind == VBT_REQ_SLICE) {
                 m.kind = kMixedSlice;
                 m.a0 = r->r.z;
                 m.t0 = r->r.t0;
@@ -454,10 +480,18 @@ void vbt_server::launch(Unit* u, int slot)
             tab[i] = m;
             tiles += mixed_request_tiles(m, assets[r->r.asset]->dev.g);
         }
-        cudaMemcpyAsync(dtab, hs, mixed_table_bytes(k, u->frames), cudaMemcpyHostToDevice, st);
-        launch_err = launch_serve_mixed(d_assets, reinterpret_cast<const MixedReq*>(dtab), k, tiles, d_counters + slot,
-                                        d_err, &graphs[slot], st);
-        nl = tiles ? 1 : 0;
+        cudaMemcpyAsync(dseg, hs, tables, cudaMemcpyHostToDevice, st);
+        if (q) {
+            launch_query_points_batch(d_assets, reinterpret_cast<const uint32_t*>(dseg), kp,
+                                      reinterpret_cast<const uint4*>(dq), q, d_err,
+                                      sparse_points == 0u ? 0 : (sparse_points == q ? 2 : 1), st);
+            ++nl;
+        }
+        if (tiles) {
+            launch_err = launch_serve_mixed(d_assets, reinterpret_cast<const MixedReq*>(dtab), km, tiles,
+                                            d_counters + slot, d_err + kp, &graphs[slot], st);
+            ++nl;
+        }
     } else if (r0->r.kind == VBT_REQ_POINTS) {
         uint8_t* hseg = h_stage + u->stage_in.off;
         uint32_t* starts = reinterpret_cast<uint32_t*>(hseg);
@@ -758,11 +792,12 @@ int vbt_serve_submit(vbt_server* s, const vbt_request* rq, uint64_t* ticket)
     if (st == VBT_STATUS_OK) {
         r->result_floats = result_floats(r->r, a);
         const uint64_t np = rq->kind == VBT_REQ_POINTS ? rq->n_points : 0, nf = r->frames.size();
+        const uint32_t kp = rq->kind == VBT_REQ_POINTS ? 1u : 0u;
         const uint64_t need = Arena::round(4ull * r->result_floats) +
-                              Arena::round(std::max(points_in_bytes(1, np), mixed_in_bytes(1, nf, np)));
+                              Arena::round(std::max(points_in_bytes(1, np), mixed_in_bytes(kp, 1u - kp, nf, np)));
         const uint64_t staged = (rq->host_out && !is_pinned(rq->host_out) ? 4ull * r->result_floats : 0) +
                                 (rq->kind == VBT_REQ_POINTS && !is_pinned(rq->points) ? 16ull * rq->n_points : 0) +
-                                std::max(seg_bytes(1), mixed_table_bytes(1, nf));
+                                std::max(seg_bytes(1), mixed_table_bytes(kp, 1u - kp, nf));
         if (need > s->cfg.hbm_budget_bytes)
             st = VBT_STATUS_LIMIT, msg = "request needs more device memory than the server's budget";
         else if (Arena::round(staged) + kAlign > s->cfg.host_staging_bytes)

@@ -1,34 +1,28 @@
-// serve_mixed.cuh -- one persistent launch over every request a serving step admitted: point
-// batches, z-slices and dense frames of any resident assets, mixed.  Included by kernels.cu (it
-// uses that file's decode helpers).
+// serve_mixed.cuh -- one persistent launch over the slice and frame requests a serving step
+// admitted, of any resident assets, mixed.  Included by kernels.cu (it uses that file's decode
+// helpers).  (The step's point requests go to the multi-asset point kernel beside it: a point is a
+// chain of dependent loads that wants every thread an SM can hold in flight, while a leaf tile
+// needs this kernel's 128 registers per thread.)
 //
-// The step's requests form a table (MixedReq, in device memory) with a running count of tiles.  A
-// tile is one warp's piece of work:
-//   points  kPtTile queries (a lane per query, kPtPerLane rounds): point_value, as the point kernels;
+// The requests form a table (MixedReq, in device memory) with a running count of tiles.  A tile is
+// one warp's piece of work:
 //   slice   one (leaf of the z layer, frame): the leaf's controls at the frame, then its rows of
 //           the layer -- the body of query_slice_kernel;
 //   frames  one (leaf, frame) of a dense frame: controls, then all 64 rows of the leaf (zeros for
 //           an EMPTY leaf) -- the body of the warp-per-leaf decode_kernel<DENSE>.
-// Warps take tiles kTileGrab at a time from a work counter (zeroed before the launch), so cheap
-// and expensive tiles of different requests spread over the GPU as they come.  Each request has
-// its own result array and error word; the values are those of the per-request kernels, bit for
-// bit.
+// Warps take tiles kTileGrab at a time from a work counter (zeroed before the launch), so the
+// tiles of large and small requests spread over the GPU as they come.  Each request has its own
+// result array and error word; the values are those of the per-request kernels, bit for bit.
 #pragma once
 
 namespace vbtb {
 
-constexpr int kPtPerLane = 4;
-constexpr uint32_t kPtTile = 32u * kPtPerLane;
 constexpr uint32_t kTileGrab = 4;
 
 // Tiles of one request (the host's count: same arithmetic).
 __host__ __device__ __forceinline__ uint64_t mixed_tiles(const MixedReq& r, const AssetGeom& g)
 {
-    switch (r.kind) {
-    case kMixedPoints: return ((uint64_t)r.n + kPtTile - 1u) / kPtTile;
-    case kMixedSlice: return (uint64_t)g.lcx * g.lcy * (uint64_t)(r.t1 - r.t0);
-    default: return (uint64_t)g.leaf_count * r.n;
-    }
+    return r.kind == kMixedSlice ? (uint64_t)g.lcx * g.lcy * (uint64_t)(r.t1 - r.t0) : (uint64_t)g.leaf_count * r.n;
 }
 
 // Slice tile: rows of leaf `li` of the z layer at frame t into the request's [t - t0][y][x] output.
@@ -156,15 +150,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32) serve_mixed_kernel(const Dev
             const DeviceAsset& a = assets[rq.asset];
             const uint64_t u = tile - rq.first;
             unsigned long long* err = errs + lo;
-            if (rq.kind == kMixedPoints) {
-                const uint4* q = reinterpret_cast<const uint4*>(rq.in);
-                float* out = reinterpret_cast<float*>(rq.out);
-#pragma unroll
-                for (int p = 0; p < kPtPerLane; ++p) {
-                    const uint64_t i = u * kPtTile + (uint64_t)(p * 32 + lane);
-                    if (i < rq.n) out[i] = point_value(a, q[i], err);
-                }
-            } else if (rq.kind == kMixedSlice) {
+            if (rq.kind == kMixedSlice) {
                 const uint32_t layer = a.g.lcx * a.g.lcy;
                 mixed_slice_tile(a, rq, (uint32_t)(u % layer), rq.t0 + (int)(u / layer), s_ctrl, err, lane);
             } else {
