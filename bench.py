@@ -927,17 +927,25 @@ def run_reference_queries(args, local_rank, n=1_000_000, repeats=100):
             ms = e0.elapsed_time(e1)
             res[label] = {"kernel_ms": ms, "queries_per_s": n * repeats / (ms * 1e-3)}
         a.close()
-        best_ref = max(ref["unsorted"]["queries_per_sec"], ref["sorted"]["queries_per_sec"])
+        # the grouped kernel decodes a leaf's controls once, at its first query's frame, for every
+        # query of the leaf: on random-t queries it is not the reference's decode (its own check
+        # against the reference CPU decoder reports the difference), so the fair best of the
+        # reference is its best run whose values agree with the CPU decoder
+        tol = 1e-4   # absolute; the fields span about +-15 (the grouped kernel misses by up to ~5)
+        ok = {k: ref[k]["max_abs_diff"] <= tol for k in ("unsorted", "sorted")}
+        valid = [ref[k]["queries_per_sec"] for k in ("unsorted", "sorted") if ok[k]]
+        best_ref = max(valid) if valid else max(ref["unsorted"]["queries_per_sec"], ref["sorted"]["queries_per_sec"])
         out[name] = {"queries": n, "repeats": repeats, "pattern": "uniform random (x, y, z, t)",
                      "reference_cuda": {"unsorted_queries_per_s": ref["unsorted"]["queries_per_sec"],
                                         "sorted_grouped_queries_per_s": ref["sorted"]["queries_per_sec"],
-                                        "max_abs_diff_vs_reference_cpu": max(ref["unsorted"]["max_abs_diff"],
-                                                                            ref["sorted"]["max_abs_diff"])},
+                                        "unsorted_max_abs_diff_vs_reference_cpu": ref["unsorted"]["max_abs_diff"],
+                                        "sorted_grouped_max_abs_diff_vs_reference_cpu": ref["sorted"]["max_abs_diff"],
+                                        "agrees_with_reference_cpu": ok},
                      "ours": {"unsorted_queries_per_s": res["unsorted"]["queries_per_s"],
                               "sorted_queries_per_s": res["sorted"]["queries_per_s"]},
                      "speedup_unsorted": res["unsorted"]["queries_per_s"] / ref["unsorted"]["queries_per_sec"],
                      "speedup_sorted": res["sorted"]["queries_per_s"] / ref["sorted"]["queries_per_sec"],
-                     "speedup_best_vs_best": max(res["unsorted"]["queries_per_s"], res["sorted"]["queries_per_s"]) /
+                     "speedup_best_vs_best_agreeing": max(res["unsorted"]["queries_per_s"], res["sorted"]["queries_per_s"]) /
                      best_ref}
     return out or {"skipped": "no scientific asset generated"}
 

@@ -1172,6 +1172,100 @@ __device__ __forceinline__ float rt_point(const DeviceAsset& a, const LeafEntry&
     return v;
 }
 
+// 32 bits of the payload from byte b, b unaligned (two word reads; the payload's 16-byte tail
+// padding keeps the second word inside the allocation).
+__device__ __forceinline__ uint32_t pay_u32(const uint32_t* __restrict__ pw, uint64_t b)
+{
+    const uint32_t w = (uint32_t)(b >> 2);
+    return __funnelshift_r(ldw(pw, w), ldw(pw, w + 1u), (uint32_t)(b & 3u) * 8u);
+}
+
+// The point decode of a scientific leaf whose coarse block and sparse-event section lie inside the
+// payload (so none of the SciReader's per-byte checks can fire) and whose keep is at most 8: the
+// same arithmetic as sci_point's coarse part and sci_sparse, in the same order, with each
+// control's record (at most 8 bytes: keep <= 7) read as two 32-bit windows, the basis row and AC
+// scales read once per query, and the event keys as 32-bit windows.  Returns false (nothing
+// decoded) when the leaf is not of that shape; sci_point then decodes it.
+__device__ __forceinline__ bool sci_point_fast(const DeviceAsset& a, const LeafEntry& e, uint32_t lx, uint32_t ly,
+                                               uint32_t lz, uint32_t t, float& value)
+{
+    const uint32_t hdr = e.header;
+    const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
+    const uint32_t mode = hdr & 3u;
+    const uint64_t base = 4ull * e.word_off;
+    const uint64_t bytes = 4ull * a.g.payload_words;
+    const uint64_t sb = base + 4u + (uint64_t)(64 * (keep + 1));
+    if (keep > 7 || mode >= 2u || sb + 4u > bytes) return false;
+    const uint32_t* __restrict__ pw = a.payload;
+    const float* brow = a.basis + (uint64_t)t * 64u;
+    float b[7], sc[6];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) b[k] = k < keep ? __ldg(brow + k) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sc[k] = k + 1 < keep ? __ldg(a.scales + k) : 0.0f;
+    auto at = [&](int ci) {
+        const uint64_t cb = base + 4u + (uint64_t)ci * (keep + 1);
+        const uint32_t w0 = pay_u32(pw, cb), w1 = keep > 3 ? pay_u32(pw, cb + 4u) : 0u;
+        float hi, lo;
+        two_prod(half_bits_to_float(w0 & 0xFFFFu), b[0], hi, lo);
+#pragma unroll
+        for (int k = 1; k < 7; ++k) {
+            if (k < keep) {   // AC byte k at cb + k + 1: bytes 2, 3 of w0, then bytes 0..3 of w1
+                const uint32_t byte = k + 1 < 4 ? (w0 >> (8 * (k + 1))) : (w1 >> (8 * (k - 3)));
+                const float coeff = __fmul_rn((float)(int8_t)(byte & 0xFFu), sc[k - 1]);
+                float ph, pl;
+                two_prod(coeff, b[k], ph, pl);
+                ff_add(hi, lo, ph, pl);
+            }
+        }
+        return __fadd_rn(hi, lo);
+    };
+    const AxisWeight ax = c_sci_axis[0][lx], ay = c_sci_axis[0][ly], az = c_sci_axis[0][lz];
+    auto ci = [&](int cx, int cy, int cz) { return at((cz * 4 + cy) * 4 + cx); };
+    const float c00 = lerp_ref(ci(ax.i0, ay.i0, az.i0), ci(ax.i1, ay.i0, az.i0), ax.t, ax.omt);
+    const float c01 = lerp_ref(ci(ax.i0, ay.i0, az.i1), ci(ax.i1, ay.i0, az.i1), ax.t, ax.omt);
+    const float c10 = lerp_ref(ci(ax.i0, ay.i1, az.i0), ci(ax.i1, ay.i1, az.i0), ax.t, ax.omt);
+    const float c11 = lerp_ref(ci(ax.i0, ay.i1, az.i1), ci(ax.i1, ay.i1, az.i1), ax.t, ax.omt);
+    const float coarse = lerp_ref(lerp_ref(c00, c10, ay.t, ay.omt), lerp_ref(c01, c11, ay.t, ay.omt), az.t, az.omt);
+    float r = 0.0f;
+    const uint32_t count = (hdr >> 16) & 0x0FFFu;
+    if (mode == 1u && count != 0u) {   // sci_sparse
+        const uint32_t tier = (hdr >> 8) & 3u;
+        const uint32_t cap = tier == 0u ? 64u : tier == 1u ? 256u : tier == 2u ? 768u : 1024u;
+        if (sb + 100u + 2u * cap + cap / 2u + 4u > bytes) return false;   // the section's extent
+        const uint32_t li = (lz * 8u + ly) * 8u + lx;
+        const uint32_t fpb = ((hdr >> 10) & 0xFu) + 1u;
+        const uint32_t bin = t / fpb < 15u ? t / fpb : 15u;
+        const uint32_t lt = (t - bin * fpb) & 0xFFu;
+        const float es = __uint_as_float(pay_u32(pw, sb));
+        const uint32_t mw = pay_u32(pw, sb + 4u + (li >> 5) * 4u);
+        if (es > 0.0f && (mw & (1u << (li & 31u))) != 0u) {
+            const uint64_t bb = sb + 68u;
+            const uint32_t se = pay_u32(pw, bb + bin * 2u);
+            const uint32_t start = se & 0xFFFFu;
+            const uint32_t end = bin + 1u < 16u ? se >> 16 : (count & 0xFFFFu);
+            const uint64_t cb = bb + 32u, rb = cb + cap * 2u;
+            const uint32_t target = ((lt << 9) | (li & 0x1FFu)) & 0xFFFFu;
+            int left = (int)start, right = (int)end - 1;
+            while (left <= right) {
+                const int mid = (left + right) >> 1;
+                const uint32_t key = pay_u32(pw, cb + (uint32_t)mid * 2u) & 0xFFFFu;
+                if (key == target) {
+                    const uint32_t byte = pay_u32(pw, rb + (uint32_t)(mid >> 1)) & 0xFFu;
+                    int q = (int)((mid & 1) == 0 ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
+                    if (q & 8) q -= 16;
+                    r = __fmul_rn((float)q, es);
+                    break;
+                }
+                if (key < target) left = mid + 1;
+                else right = mid - 1;
+            }
+        }
+    }
+    value = __fadd_rn(coarse, r);
+    return true;
+}
+
 __device__ __forceinline__ float sci_point(const DeviceAsset& a, const LeafEntry& e, uint32_t lx, uint32_t ly, uint32_t lz, uint32_t t,
                            bool& oob)
 {
@@ -1245,6 +1339,8 @@ __device__ __forceinline__ float point_value(const DeviceAsset& a, uint4 qq, uns
             record_error(err, leaf, kErrDecodeOob);
             return 0.0f;
         }
+        float fv;
+        if (sci_point_fast(a, e, x & 7u, y & 7u, z & 7u, t, fv)) return fv;
         bool oob = false;
         const float v = sci_point(a, e, x & 7u, y & 7u, z & 7u, t, oob);
         if (oob) record_error(err, leaf, kErrDecodeOob);
