@@ -572,6 +572,49 @@ __device__ __forceinline__ void ff_add(float& hi, float& lo, float ph, float pl)
     lo = __fsub_rn(t, __fsub_rn(hi, s));
 }
 
+// 32 bits of the payload from byte b, b unaligned (two word reads; the payload's 16-byte tail
+// padding keeps the second word inside the allocation).
+__device__ __forceinline__ uint32_t pay_u32(const uint32_t* __restrict__ pw, uint64_t b)
+{
+    const uint32_t w = (uint32_t)(b >> 2);
+    return __funnelshift_r(ldw(pw, w), ldw(pw, w + 1u), (uint32_t)(b & 3u) * 8u);
+}
+
+// The basis row b_k(t) and the AC scales of a leaf with keep <= 7, read once for several controls.
+struct SciTerms {
+    float b[7], sc[6];
+    __device__ __forceinline__ SciTerms(const DeviceAsset& a, uint32_t t, int keep)
+    {
+        const float* brow = a.basis + (uint64_t)t * 64u;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) b[k] = k < keep ? __ldg(brow + k) : 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sc[k] = k + 1 < keep ? __ldg(a.scales + k) : 0.0f;
+    }
+};
+
+// sci_control for a control record at byte cb of at most 8 bytes (keep <= 7) that lies inside the
+// payload: the same products and compensated sum in the same order, the record read as two 32-bit
+// windows (DC half in bytes 0-1, AC byte k at byte k + 1).
+__device__ __forceinline__ float sci_control_fast(const uint32_t* __restrict__ pw, uint64_t cb, int keep,
+                                                  const SciTerms& tm)
+{
+    const uint32_t w0 = pay_u32(pw, cb), w1 = keep > 3 ? pay_u32(pw, cb + 4u) : 0u;
+    float hi, lo;
+    two_prod(half_bits_to_float(w0 & 0xFFFFu), tm.b[0], hi, lo);
+#pragma unroll
+    for (int k = 1; k < 7; ++k) {
+        if (k < keep) {
+            const uint32_t byte = k + 1 < 4 ? (w0 >> (8 * (k + 1))) : (w1 >> (8 * (k - 3)));
+            const float coeff = __fmul_rn((float)(int8_t)(byte & 0xFFu), tm.sc[k - 1]);
+            float ph, pl;
+            two_prod(coeff, tm.b[k], ph, pl);
+            ff_add(hi, lo, ph, pl);
+        }
+    }
+    return __fadd_rn(hi, lo);
+}
+
 // Coarse control ci at frame t: DC * b0(t) + sum_k (i8 * acScale[k-1]) * bk(t).
 __device__ __forceinline__ float sci_control(const DeviceAsset& a, SciReader& rd, uint64_t base, int keep, int ci,
                                              const float* __restrict__ brow)
@@ -664,6 +707,7 @@ struct SparseLeaf {
     uint64_t sb, bb;        // section base, bin table
     float es;               // event scale (residuals are 0 unless es > 0)
     uint32_t count, cap, fpb;
+    bool inside;            // the whole section lies inside the payload: reads need no checks
 };
 
 __device__ __forceinline__ SparseLeaf sparse_leaf(SciReader& rd, uint64_t base, uint32_t hdr, int keep)
@@ -676,6 +720,8 @@ __device__ __forceinline__ SparseLeaf sparse_leaf(SciReader& rd, uint64_t base, 
     s.sb = base + 4u + (uint64_t)(64 * (keep + 1));
     s.bb = s.sb + 68u;
     s.es = s.count ? __uint_as_float(rd.u32(s.sb)) : 0.0f;
+    // es, mask, bins, 16-bit keys, 4-bit residuals (and the 4 bytes a 32-bit window reads past)
+    s.inside = s.sb + 100u + 2u * s.cap + s.cap / 2u + 4u <= 4ull * rd.words;
     return s;
 }
 
@@ -691,17 +737,21 @@ __device__ __forceinline__ float sparse_at(SciReader& rd, const SparseLeaf& s, u
 {
     const uint32_t bin = t / s.fpb < 15u ? t / s.fpb : 15u;
     const uint32_t lt = (t - bin * s.fpb) & 0xFFu;
-    const uint32_t start = rd.u16(s.bb + bin * 2u);
-    const uint32_t end = bin + 1u < 16u ? rd.u16(s.bb + (bin + 1u) * 2u) : (s.count & 0xFFFFu);
+    // inside the payload, the 16-bit fields are read as 32-bit windows (one or two word reads
+    // instead of two checked byte reads); the values are the same
+    auto u16 = [&](uint64_t b) { return s.inside ? (pay_u32(rd.pw, b) & 0xFFFFu) : rd.u16(b); };
+    const uint32_t start = u16(s.bb + bin * 2u);
+    const uint32_t end = bin + 1u < 16u ? u16(s.bb + (bin + 1u) * 2u) : (s.count & 0xFFFFu);
     if (start >= end) return 0.0f;
     const uint64_t cb = s.bb + 32u, rb = cb + s.cap * 2u;
     const uint32_t target = ((lt << 9) | (li & 0x1FFu)) & 0xFFFFu;
     int left = (int)start, right = (int)end - 1;
     while (left <= right) {
         const int mid = (left + right) >> 1;
-        const uint32_t key = rd.u16(cb + (uint32_t)mid * 2u);
+        const uint32_t key = u16(cb + (uint32_t)mid * 2u);
         if (key == target) {
-            const uint32_t byte = rd.byte(rb + (uint32_t)(mid >> 1));
+            const uint32_t byte = s.inside ? (pay_u32(rd.pw, rb + (uint32_t)(mid >> 1)) & 0xFFu)
+                                           : rd.byte(rb + (uint32_t)(mid >> 1));
             int q = (int)((mid & 1) == 0 ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
             if (q & 8) q -= 16;
             return __fmul_rn((float)q, s.es);
@@ -766,15 +816,16 @@ __device__ __forceinline__ void sci_scatter_frame(const DeviceAsset& a, const Le
     if (sp.count && sp.es > 0.0f) {
         const uint32_t bin = t / sp.fpb < 15u ? t / sp.fpb : 15u;
         const uint32_t lt7 = (t - bin * sp.fpb) & 0x7Fu;   // the search key keeps 7 bits of it
-        const uint32_t st0 = rd.u16(sp.bb + bin * 2u);
-        const uint32_t en = bin + 1u < 16u ? rd.u16(sp.bb + (bin + 1u) * 2u) : (sp.count & 0xFFFFu);
+        auto u16 = [&](uint64_t b) { return sp.inside ? (pay_u32(rd.pw, b) & 0xFFFFu) : rd.u16(b); };
+        const uint32_t st0 = u16(sp.bb + bin * 2u);
+        const uint32_t en = bin + 1u < 16u ? u16(sp.bb + (bin + 1u) * 2u) : (sp.count & 0xFFFFu);
         const uint64_t cb = sp.bb + 32u, rb = cb + sp.cap * 2u;
         for (uint32_t i = st0 + (uint32_t)lane; i < en; i += 32u) {
-            const uint32_t key = rd.u16(cb + 2u * i);
+            const uint32_t key = u16(cb + 2u * i);
             if ((key >> 9) != lt7) continue;
             const uint32_t li = key & 511u;
             if ((int)(li & 7u) >= w || (int)((li >> 3) & 7u) >= h || (int)(li >> 6) >= d) continue;
-            const uint32_t byte = rd.byte(rb + (i >> 1));
+            const uint32_t byte = sp.inside ? (pay_u32(rd.pw, rb + (i >> 1)) & 0xFFu) : rd.byte(rb + (i >> 1));
             int q = (int)((i & 1u) == 0u ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
             if (q & 8) q -= 16;
             float* o = dst(li);
@@ -794,7 +845,13 @@ __device__ void sci_decode_controls(const DeviceAsset& a, const LeafEntry& e, ui
     const uint32_t hdr = e.header;
     const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
     const float* brow = a.basis + (uint64_t)t * 64u;
-    for (int c = lane; c < 64; c += nl) s_ctrl[c] = sci_control(a, rd, base, keep, c, brow);
+    if (keep <= 7 && base + 4u + (uint64_t)(64 * (keep + 1)) + 4u <= 4ull * a.g.payload_words) {
+        // the coarse block lies inside the payload: word-window reads, terms read once per lane
+        const SciTerms tm(a, t, keep);
+        for (int c = lane; c < 64; c += nl) s_ctrl[c] = sci_control_fast(a.payload, base + 4u + (uint64_t)c * (keep + 1), keep, tm);
+    } else {
+        for (int c = lane; c < 64; c += nl) s_ctrl[c] = sci_control(a, rd, base, keep, c, brow);
+    }
     const uint32_t mode = hdr & 3u;
     if (mode >= 2u) {
         const int res = mode == 2u ? 3 : 4;
@@ -1172,14 +1229,6 @@ __device__ __forceinline__ float rt_point(const DeviceAsset& a, const LeafEntry&
     return v;
 }
 
-// 32 bits of the payload from byte b, b unaligned (two word reads; the payload's 16-byte tail
-// padding keeps the second word inside the allocation).
-__device__ __forceinline__ uint32_t pay_u32(const uint32_t* __restrict__ pw, uint64_t b)
-{
-    const uint32_t w = (uint32_t)(b >> 2);
-    return __funnelshift_r(ldw(pw, w), ldw(pw, w + 1u), (uint32_t)(b & 3u) * 8u);
-}
-
 // The point decode of a scientific leaf whose coarse block and sparse-event section lie inside the
 // payload (so none of the SciReader's per-byte checks can fire) and whose keep is at most 8: the
 // same arithmetic as sci_point's coarse part and sci_sparse, in the same order, with each
@@ -1197,29 +1246,8 @@ __device__ __forceinline__ bool sci_point_fast(const DeviceAsset& a, const LeafE
     const uint64_t sb = base + 4u + (uint64_t)(64 * (keep + 1));
     if (keep > 7 || mode >= 2u || sb + 4u > bytes) return false;
     const uint32_t* __restrict__ pw = a.payload;
-    const float* brow = a.basis + (uint64_t)t * 64u;
-    float b[7], sc[6];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) b[k] = k < keep ? __ldg(brow + k) : 0.0f;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) sc[k] = k + 1 < keep ? __ldg(a.scales + k) : 0.0f;
-    auto at = [&](int ci) {
-        const uint64_t cb = base + 4u + (uint64_t)ci * (keep + 1);
-        const uint32_t w0 = pay_u32(pw, cb), w1 = keep > 3 ? pay_u32(pw, cb + 4u) : 0u;
-        float hi, lo;
-        two_prod(half_bits_to_float(w0 & 0xFFFFu), b[0], hi, lo);
-#pragma unroll
-        for (int k = 1; k < 7; ++k) {
-            if (k < keep) {   // AC byte k at cb + k + 1: bytes 2, 3 of w0, then bytes 0..3 of w1
-                const uint32_t byte = k + 1 < 4 ? (w0 >> (8 * (k + 1))) : (w1 >> (8 * (k - 3)));
-                const float coeff = __fmul_rn((float)(int8_t)(byte & 0xFFu), sc[k - 1]);
-                float ph, pl;
-                two_prod(coeff, b[k], ph, pl);
-                ff_add(hi, lo, ph, pl);
-            }
-        }
-        return __fadd_rn(hi, lo);
-    };
+    const SciTerms tm(a, t, keep);
+    auto at = [&](int ci) { return sci_control_fast(pw, base + 4u + (uint64_t)ci * (keep + 1), keep, tm); };
     const AxisWeight ax = c_sci_axis[0][lx], ay = c_sci_axis[0][ly], az = c_sci_axis[0][lz];
     auto ci = [&](int cx, int cy, int cz) { return at((cz * 4 + cy) * 4 + cx); };
     const float c00 = lerp_ref(ci(ax.i0, ay.i0, az.i0), ci(ax.i1, ay.i0, az.i0), ax.t, ax.omt);
