@@ -150,10 +150,15 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
         mbar_init(bar, 1);
         mbar_init_fence();
     }
-    // A = S' (343 entered as 342), one exact BF16 per entry
+    // A = S' (343 entered as 342), one exact BF16 per entry; the 32 axis weights 7 w(x, c) come
+    // from a table in shared memory (in the Q region, not yet in use)
+    uint32_t* s_w7 = reinterpret_cast<uint32_t*>(sQ);
+    if (tid < 32) s_w7[tid] = win_w7((uint32_t)tid >> 2, (uint32_t)tid & 3u);
+    __syncthreads();
     for (uint32_t idx = tid; idx < 512u * 64u; idx += kWinThreads) {
         const uint32_t v = idx >> 6, ci = idx & 63u;
-        uint32_t w = win_w7(v & 7u, ci & 3u) * win_w7((v >> 3) & 7u, (ci >> 2) & 3u) * win_w7(v >> 6, ci >> 4);
+        uint32_t w = s_w7[((v & 7u) << 2) | (ci & 3u)] * s_w7[(((v >> 3) & 7u) << 2) | ((ci >> 2) & 3u)] *
+                     s_w7[((v >> 6) << 2) | (ci >> 4)];
         if (w == 343u) w = 342u;
         const uint32_t m = v >> 7, s = ci >> 4;
         *reinterpret_cast<uint16_t*>(sA + (m * 4u + s) * 4096u + win_off(v & 127u, ci & 15u)) = win_bf16_bits((float)w);
@@ -180,11 +185,19 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
         const uint64_t base = 4ull * e.word_off;
         // 1. coefficients q[ci][k]: DC (fp16) for k = 0, int8 x acScale[k-1] otherwise
         SciReader rd{a.payload, a.g.payload_words, false};
+        // the coarse block inside the payload: 32-bit windows instead of checked byte reads
+        const bool block_in = base + 4u + (uint64_t)(64 * (keep + 1)) + 4u <= 4ull * a.g.payload_words;
         for (int i = tid; i < 64 * keep; i += kWinThreads) {
             const int ci = i / keep, k = i % keep;
             const uint64_t cb = base + 4u + (uint64_t)ci * (keep + 1);
-            sQ[i] = k == 0 ? half_bits_to_float(rd.u16(cb))
-                           : __fmul_rn((float)(int8_t)rd.byte(cb + 2u + (k - 1)), __ldg(a.scales + k - 1));
+            if (block_in) {
+                const uint32_t w = pay_u32(a.payload, k == 0 ? cb : cb + 2u + (k - 1));
+                sQ[i] = k == 0 ? half_bits_to_float(w & 0xFFFFu)
+                               : __fmul_rn((float)(int8_t)(w & 0xFFu), __ldg(a.scales + k - 1));
+            } else {
+                sQ[i] = k == 0 ? half_bits_to_float(rd.u16(cb))
+                               : __fmul_rn((float)(int8_t)rd.byte(cb + 2u + (k - 1)), __ldg(a.scales + k - 1));
+            }
         }
         // the sparse section's header and occupancy mask, once per leaf
         if (mode == 1u && tid < 16) {
@@ -294,6 +307,26 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
             const int corner = win_corner_of_voxel(v);
             const bool inside = (int)(v & 7u) < ew && (int)((v >> 3) & 7u) < eh && (int)(v >> 6) < ed;
             const bool events = mode == 1u && !scatter && ((s_mask[v >> 5] >> (v & 31u)) & 1u) != 0u;
+            if (mode <= 1u && !events) {
+                // no residual at this voxel (CoarseOnly, or events added by the scatter below, or
+                // none here): D (+ the corner term) / 343, the same operations as the general case
+                for (int c0 = (int)half * cols_per_half; c0 < (int)(half + 1) * cols_per_half; c0 += 16) {
+                    float d[16];
+                    win_ld16(taddr + ((quarter * 32u) << 16) + m * (uint32_t)N + (uint32_t)c0, d);
+                    float* o = out + (uint64_t)c0 * frame_stride + (uint64_t)leaf * 512u + v;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        if (c0 + j < n) {
+                            float val = d[j];
+                            if (corner >= 0) val = __fadd_rn(val, sCorner[corner * kWinMaxN + c0 + j]);
+                            val = __fmul_rn(val, 1.0f / 343.0f);
+                            if (mode == 1u) val = __fadd_rn(val, 0.0f);
+                            o[(uint64_t)j * frame_stride] = inside ? val : 0.0f;
+                        }
+                    }
+                }
+                continue;
+            }
             const int dsel = mode == 2u ? 1 : 2;
             const AxisWeight dx = c_sci_axis[dsel][v & 7u], dy = c_sci_axis[dsel][(v >> 3) & 7u],
                              dz = c_sci_axis[dsel][v >> 6];
@@ -338,10 +371,10 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
             for (uint32_t b = 0; b < 16u; ++b) {
                 const uint32_t st0 = s_bin[b], en = b < 15u ? s_bin[b + 1] : (sp.count & 0xFFFFu);
                 for (uint32_t e = st0 + (uint32_t)tid; e < en; e += kWinThreads) {
-                    const uint32_t key = rd.u16(cb + 2u * e);
+                    const uint32_t key = sp.inside ? (pay_u32(a.payload, cb + 2u * e) & 0xFFFFu) : rd.u16(cb + 2u * e);
                     const uint32_t lt = key >> 9, li = key & 511u;
                     if ((int)(li & 7u) >= ew || (int)((li >> 3) & 7u) >= eh || (int)(li >> 6) >= ed) continue;
-                    const uint32_t byte = rd.byte(rb + (e >> 1));
+                    const uint32_t byte = sp.inside ? (pay_u32(a.payload, rb + (e >> 1)) & 0xFFu) : rd.byte(rb + (e >> 1));
                     int q = (int)((e & 1u) == 0u ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
                     if (q & 8) q -= 16;
                     const float r = __fmul_rn((float)q, sp.es);
