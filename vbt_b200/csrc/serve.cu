@@ -9,7 +9,10 @@
 //      does not fit may be passed over by later ones at most kMaxBypass times; after that the
 //      server admits nothing behind it until it fits;
 //   3. batching: the requests admitted in one pass -- points, slices and frames of any assets --
-//      become units of up to max_batch_queries values each (a larger request is a unit of its own).
+//      become units of up to max_batch_queries values each (a larger request is a unit of its own:
+//      measured, a single frame of a large volume decodes faster as the mixed launch's leaf tiles,
+//      which read only the keys the frame needs, than on the dense frame kernel, which stages
+//      each whole leaf).
 //      A unit is at most two launches: its point requests, across assets, in one multi-asset point
 //      launch, and its slices and frames in ONE persistent launch (serve_mixed_kernel) whose warps
 //      take tiles of all of them from a work counter, replayed from a per-stream CUDA graph with
