@@ -321,6 +321,54 @@ def test_unsorted_keys_and_descending_frames(vbt, cuda, oracle, tmp_path):
     a.close()
 
 
+def test_event_on_masked_out_voxel(vbt, cuda, oracle, tmp_path):
+    """A SparseEvents leaf with an event on a voxel whose mask bit is clear: the reference's mask
+    test hides that event, so the leaf loses the sorted flag (no scatter of its events) and the
+    per-frame, cache and window decodes still agree with the oracle."""
+    path = golden_asset("sci_small")
+    raw = bytearray(open(path, "rb").read())
+    f = oracle.load(path)
+    off, pay = f.offsets(), f.payload()
+    p0 = bytes(raw).find(pay.tobytes())
+    hdr = pay[off[:-1]]
+    leaf = int(np.flatnonzero(((hdr & 3) == 1) & (((hdr >> 16) & 0xFFF) > 0))[0])
+    h = int(hdr[leaf])
+    keep = ((h >> 2) & 0x3F) + 1
+    sb = p0 + 4 * int(off[leaf]) + 4 + 64 * (keep + 1)
+    bins = np.frombuffer(bytes(raw[sb + 68:sb + 100]), np.uint16)
+    e0 = int(bins[int(np.flatnonzero(np.append(bins[1:], (h >> 16) & 0xFFF) > bins)[0])])
+    key = int(np.frombuffer(bytes(raw[sb + 100 + 2 * e0:sb + 102 + 2 * e0]), np.uint16)[0])
+    li = key & 511
+    mw = sb + 4 + 4 * (li >> 5)
+    word = int(np.frombuffer(bytes(raw[mw:mw + 4]), np.uint32)[0]) & ~(1 << (li & 31))
+    raw[mw:mw + 4] = np.uint32(word).tobytes()
+    path2 = str(tmp_path / "masked_event.vbtp")
+    open(path2, "wb").write(raw)
+    a = vbt.Asset(data=bytes(raw))
+    f2 = oracle.load(path2)
+    rows = a.leaf_table()
+    assert (rows[leaf, 7] & (1 << 14)) == 0
+    X, Y, Z = a.dims
+    ts = list(range(a.frames))
+    out = cuda.empty((len(ts), Z, Y, X), dtype=cuda.float32, device="cuda")
+    a.decode_frames(ts, out)
+    a.sync_status()
+    got = out.cpu().numpy()
+    for i, t in enumerate(ts):
+        assert same_bits(got[i], f2.frame(t)), t
+    L = a.leaf_count
+    exact = cuda.empty((len(ts), L, 512), dtype=cuda.float32, device="cuda")
+    a.decode_cache(ts, exact, frame_stride=L * 512)
+    win = cuda.empty((len(ts), L, 512), dtype=cuda.float32, device="cuda")
+    a.decode_window(0, len(ts), win)
+    a.sync_status()
+    e, w = exact.cpu().numpy(), win.cpu().numpy()
+    mx, _, lo, hi = a.window_error(0, len(ts), win)
+    assert np.abs(w.astype(np.float64) - e).max() <= 1e-6 * (hi - lo)
+    assert mx <= 1e-6 * (hi - lo)
+    a.close()
+
+
 @pytest.mark.parametrize("name", ["cfg2_plume", "mix_fire_flames"])
 def test_point_queries_sparse_volume(oracle, cuda, vbt, name):
     """Volumes whose leaves are mostly EMPTY take the compacting point-query kernel (trivial

@@ -762,10 +762,11 @@ __device__ __forceinline__ float sparse_at(SciReader& rd, const SparseLeaf& s, u
     return 0.0f;
 }
 
-// Scientific leaves: kFlagSorted marks a SparseEvents leaf whose event keys strictly increase
-// within every bin range (and whose ranges stay inside the key table).  The reference finds an
-// event by binary search per voxel and frame (render/src/scientific_decode.cpp:235-295); on such a
-// leaf the search finds a key exactly when it is present, so decoders may instead visit the
+// Scientific leaves: kFlagSorted marks a SparseEvents leaf whose bin ranges follow one another
+// (start <= end, inside the key table), whose event keys strictly increase within every range and
+// whose events all sit on voxels with their mask bit set.  The reference finds an event by binary
+// search per voxel and frame, after the mask test (render/src/scientific_decode.cpp:235-295); on
+// such a leaf the search finds a key exactly when it is present, so decoders may instead visit the
 // events of a frame's bin and add each to its voxel.  One warp per leaf, at load and upload.
 __global__ void __launch_bounds__(256) sci_event_order_kernel(DeviceAsset a)
 {
@@ -784,10 +785,14 @@ __global__ void __launch_bounds__(256) sci_event_order_kernel(DeviceAsset a)
             for (uint32_t b = 0; b < 16u; ++b) {
                 const uint32_t st0 = rd.u16(sp.bb + 2u * b);
                 const uint32_t en = b < 15u ? rd.u16(sp.bb + 2u * (b + 1u)) : (sp.count & 0xFFFFu);
+                if (st0 > en) ok = false;
                 if (st0 >= en) continue;
                 if (en > sp.cap) ok = false;
-                for (uint32_t i = st0 + (uint32_t)lane; i + 1u < en && ok; i += 32u)
-                    ok = rd.u16(sp.bb + 32u + 2u * i) < rd.u16(sp.bb + 32u + 2u * (i + 1u));
+                for (uint32_t i = st0 + (uint32_t)lane; i < en && ok; i += 32u) {
+                    const uint32_t key = rd.u16(sp.bb + 32u + 2u * i);
+                    if (i + 1u < en) ok = key < rd.u16(sp.bb + 32u + 2u * (i + 1u));
+                    ok = ok && ((sparse_mask_word(rd, sp, (key & 511u) >> 5) >> (key & 31u)) & 1u) != 0u;
+                }
             }
         }
         sorted = __all_sync(0xFFFFFFFFu, ok && !rd.oob);

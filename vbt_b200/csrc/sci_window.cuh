@@ -210,9 +210,10 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
         if (rd.oob) record_error(a.err, leaf, kErrDecodeOob);
         __syncthreads();
         // Events are scattered onto their (frame, voxel) on leaves whose keys strictly increase
-        // within every bin (kFlagSorted, set at load); otherwise each voxel with events searches
-        // per frame, as the reference does.
-        const bool scatter = mode == 1u && (e.info & kFlagSorted) != 0u && s_sparse->count && s_sparse->es > 0.0f;
+        // within every bin (kFlagSorted, set at load) and whose event scale is finite; otherwise
+        // each voxel with events searches per frame, as the reference does.
+        const bool scatter = mode == 1u && (e.info & kFlagSorted) != 0u && s_sparse->count &&
+                             s_sparse->es > 0.0f && s_sparse->es <= 3.40282347e38f;
         // 2. C[f][ci] (compensated FP32 sum), split into three BF16 terms, B tiles and corners
         for (int i = tid; i < 64 * N; i += kWinThreads) {
             const int ci = i & 63, f = i >> 6;
@@ -285,6 +286,39 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                 }
             }
         }
+        // SparseEvents leaves with scattered events, while the products run: the 4-bit residual
+        // code q of every event that a window frame's search would find, as nibble f & 7 of word
+        // (f >> 3) * 512 + voxel of a table in place of the coefficients (all zeros elsewhere).
+        // An event key (lt << 9 | voxel) of bin b belongs to the frames b * fpb + lt for b < 15
+        // (lt < fpb), and for the last bin to every frame 15 * fpb + lt + 128 j (the search key
+        // keeps 7 bits of the local time).  The bin ranges follow one another (kFlagSorted), so the
+        // events of the window's bins are one run and each event finds its bin among 16 starts.
+        uint32_t* s_ev = reinterpret_cast<uint32_t*>(sQ);
+        if (scatter) {
+            for (int i = tid; i < (int)(kWinQ / 16u); i += kWinThreads)
+                reinterpret_cast<uint4*>(s_ev)[i] = make_uint4(0u, 0u, 0u, 0u);
+            __syncthreads();
+            const SparseLeaf sp = *s_sparse;
+            const uint64_t cb = sp.bb + 32u, rb = cb + sp.cap * 2u;
+            const uint32_t t1 = (uint32_t)(t0 + n);
+            const uint32_t b_lo = min(15u, (uint32_t)t0 / sp.fpb), b_hi = min(15u, (t1 - 1u) / sp.fpb);
+            const uint32_t e_lo = s_bin[b_lo], e_hi = b_hi < 15u ? s_bin[b_hi + 1u] : (sp.count & 0xFFFFu);
+            for (uint32_t ev = e_lo + (uint32_t)tid; ev < e_hi; ev += kWinThreads) {
+                uint32_t b = b_lo;
+                while (b < b_hi && s_bin[b + 1u] <= ev) ++b;
+                const uint32_t key = sp.inside ? (pay_u32(a.payload, cb + 2u * ev) & 0xFFFFu) : rd.u16(cb + 2u * ev);
+                const uint32_t lt = key >> 9, li = key & 511u;
+                if (b < 15u && lt >= sp.fpb) continue;
+                const uint32_t byte = sp.inside ? (pay_u32(a.payload, rb + (ev >> 1)) & 0xFFu) : rd.byte(rb + (ev >> 1));
+                const uint32_t nib = (ev & 1u) == 0u ? (byte & 0xFu) : ((byte >> 4) & 0xFu);
+                const uint32_t tend = b < 15u ? min((b + 1u) * sp.fpb, a.g.frames) : a.g.frames;
+                for (uint32_t t = b * sp.fpb + lt; t < tend && t < t1; t += 128u)
+                    if (t >= (uint32_t)t0) {
+                        const uint32_t f = t - (uint32_t)t0;
+                        atomicOr(s_ev + (f >> 3) * 512u + li, nib << ((f & 7u) * 4u));
+                    }
+            }
+        }
         // 4. wait for the products (bounded); a timeout stops the whole CTA after a second wait
         const bool ok = mbar_wait(bar, phase);
         if (__syncthreads_or(!ok)) {
@@ -307,12 +341,22 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
             const int corner = win_corner_of_voxel(v);
             const bool inside = (int)(v & 7u) < ew && (int)((v >> 3) & 7u) < eh && (int)(v >> 6) < ed;
             const bool events = mode == 1u && !scatter && ((s_mask[v >> 5] >> (v & 31u)) & 1u) != 0u;
-            if (mode <= 1u && !events) {
-                // no residual at this voxel (CoarseOnly, or events added by the scatter below, or
-                // none here): D (+ the corner term) / 343, the same operations as the general case
+            // the branch is taken by whole warps: tcgen05.ld is a warp-wide instruction that every
+            // lane must issue together (a warp with any searched voxel takes the general case,
+            // whose operations for the others are the same as here)
+            if (mode <= 1u && !__any_sync(0xFFFFFFFFu, events)) {
+                // no residual at this voxel (CoarseOnly, or none here), or the scattered events of
+                // the table: D (+ the corner term) / 343 (+ q * es), the same operations as the
+                // general case (an absent event is q = 0, which adds +0 as the search's 0 does)
                 for (int c0 = (int)half * cols_per_half; c0 < (int)(half + 1) * cols_per_half; c0 += 16) {
                     float d[16];
                     win_ld16(taddr + ((quarter * 32u) << 16) + m * (uint32_t)N + (uint32_t)c0, d);
+                    uint32_t q0 = 0u, q1 = 0u;
+                    if (scatter) {
+                        q0 = s_ev[(uint32_t)(c0 >> 3) * 512u + v];
+                        q1 = s_ev[(uint32_t)((c0 >> 3) + 1) * 512u + v];
+                    }
+                    const float es = scatter ? s_sparse->es : 0.0f;
                     float* o = out + (uint64_t)c0 * frame_stride + (uint64_t)leaf * 512u + v;
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
@@ -320,7 +364,10 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                             float val = d[j];
                             if (corner >= 0) val = __fadd_rn(val, sCorner[corner * kWinMaxN + c0 + j]);
                             val = __fmul_rn(val, 1.0f / 343.0f);
-                            if (mode == 1u) val = __fadd_rn(val, 0.0f);
+                            if (mode == 1u) {
+                                const int q = ((int)((j < 8 ? q0 : q1) << (28 - 4 * (j & 7)))) >> 28;
+                                val = __fadd_rn(val, scatter ? __fmul_rn((float)q, es) : 0.0f);
+                            }
                             o[(uint64_t)j * frame_stride] = inside ? val : 0.0f;
                         }
                     }
@@ -357,33 +404,6 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                             val = __fadd_rn(val, r);
                         }
                         out[(uint64_t)f * frame_stride + (uint64_t)leaf * 512u + v] = inside ? val : 0.0f;
-                    }
-                }
-            }
-        }
-        // 6. scattered events: each event key (lt << 9 | voxel) of bin b adds q * es to the frames
-        //    whose search would find it -- b * fpb + lt for b < 15 (lt < fpb), and for the last
-        //    bin every frame 15 * fpb + lt + 128 j (the search key keeps 7 bits of the local time)
-        if (scatter) {
-            __syncthreads();   // this leaf's coarse values are written
-            const SparseLeaf sp = *s_sparse;
-            const uint64_t cb = sp.bb + 32u, rb = cb + sp.cap * 2u;
-            for (uint32_t b = 0; b < 16u; ++b) {
-                const uint32_t st0 = s_bin[b], en = b < 15u ? s_bin[b + 1] : (sp.count & 0xFFFFu);
-                for (uint32_t e = st0 + (uint32_t)tid; e < en; e += kWinThreads) {
-                    const uint32_t key = sp.inside ? (pay_u32(a.payload, cb + 2u * e) & 0xFFFFu) : rd.u16(cb + 2u * e);
-                    const uint32_t lt = key >> 9, li = key & 511u;
-                    if ((int)(li & 7u) >= ew || (int)((li >> 3) & 7u) >= eh || (int)(li >> 6) >= ed) continue;
-                    const uint32_t byte = sp.inside ? (pay_u32(a.payload, rb + (e >> 1)) & 0xFFu) : rd.byte(rb + (e >> 1));
-                    int q = (int)((e & 1u) == 0u ? (byte & 0xFu) : ((byte >> 4) & 0xFu));
-                    if (q & 8) q -= 16;
-                    const float r = __fmul_rn((float)q, sp.es);
-                    uint32_t t = b * sp.fpb + lt;
-                    if (b < 15u && lt >= sp.fpb) continue;
-                    for (; t < a.g.frames; t += (b < 15u ? a.g.frames : 128u)) {
-                        if (t < (uint32_t)t0 || t >= (uint32_t)(t0 + n)) continue;
-                        float* o = out + (uint64_t)(t - (uint32_t)t0) * frame_stride + (uint64_t)leaf * 512u + li;
-                        *o = __fadd_rn(*o, r);
                     }
                 }
             }
