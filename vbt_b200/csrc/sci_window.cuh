@@ -31,7 +31,9 @@ constexpr uint32_t kWinA = 4u * 4u * 4096u;             // 4 M tiles x 4 K steps
 constexpr uint32_t kWinB = 4u * 3u * (kWinMaxN * 32u);  // 4 K steps x 3 terms x (64 rows x 32 B)
 constexpr uint32_t kWinCorner = 8u * kWinMaxN * 4u;     // corner controls x frames, FP32
 constexpr uint32_t kWinQ = 64u * 64u * 4u;              // 64 controls x keep (<= 64) coefficients
-constexpr uint32_t kWinSmem = kWinA + kWinB + kWinCorner + kWinQ + 256u;   // + barrier, TMEM address, sparse header
+constexpr int kWinBasisK = 8;                            // basis terms held in FP64 per frame
+constexpr uint32_t kWinBd = kWinMaxN * kWinBasisK * 8u;  // b_k(t0 + f), k < 8, FP64
+constexpr uint32_t kWinSmem = kWinA + kWinB + kWinCorner + kWinQ + kWinBd + 256u;   // + barrier, TMEM address, sparse header
 
 __device__ __forceinline__ uint32_t win_smem_u32(const void* p)
 {
@@ -122,6 +124,28 @@ __device__ __forceinline__ void win_ld16(uint32_t taddr, float (&v)[16])
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// L2 prefetch of a scientific leaf's payload, one 128-byte line per thread: the coefficient block
+// with the sparse section's header, mask, bins and the keys of its events (or 512 bytes past the
+// block for other modes), and the events' 4-bit codes.  Only lines that start inside the payload.
+__device__ __forceinline__ void win_prefetch_leaf(const DeviceAsset& a, const LeafEntry& e, int tid)
+{
+    const uint32_t hdr = e.header, mode = hdr & 3u;
+    const uint32_t keep = ((hdr >> 2) & 0x3Fu) + 1u, count = (hdr >> 16) & 0x0FFFu;
+    const uint64_t base = 4ull * e.word_off, sb = base + 4u + 64u * (keep + 1u);
+    const uint64_t end = mode == 1u ? sb + 100u + 2u * count : sb + 512u;
+    const uint32_t tier = (hdr >> 8) & 3u;
+    const uint32_t cap = tier == 0u ? 64u : tier == 1u ? 256u : tier == 2u ? 768u : 1024u;
+    const uint64_t rb = sb + 100u + 2u * cap;
+    const uint64_t lim = 4ull * a.g.payload_words;
+    const uint64_t l0 = base & ~127ull, n0 = (end - l0 + 127u) / 128u;
+    uint64_t at = ~0ull;
+    if ((uint64_t)tid < n0) at = l0 + 128u * (uint64_t)tid;
+    else if (mode == 1u && count && (uint64_t)tid >= 128u && (uint64_t)tid < 128u + (count / 2u + 128u) / 128u + 1u)
+        at = (rb & ~127ull) + 128u * (uint64_t)(tid - 128);
+    if (at < lim)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const uint8_t*>(a.payload) + at));
+}
+
 // One CTA per leaf at a time (grid-stride), 256 threads, 2 CTAs per SM (shared memory and the
 // 256 tensor-memory columns each).  out[f * frame_stride + leaf * 512 + voxel] for f < n.
 __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset a, int t0, int n,
@@ -132,7 +156,8 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
     uint8_t* sB = wdyn + kWinA;
     float* sCorner = reinterpret_cast<float*>(wdyn + kWinA + kWinB);
     float* sQ = reinterpret_cast<float*>(wdyn + kWinA + kWinB + kWinCorner);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(wdyn + kWinA + kWinB + kWinCorner + kWinQ);
+    double* sBd = reinterpret_cast<double*>(wdyn + kWinA + kWinB + kWinCorner + kWinQ);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wdyn + kWinA + kWinB + kWinCorner + kWinQ + kWinBd);
     uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
     SparseLeaf* s_sparse = reinterpret_cast<SparseLeaf*>(bar + 2);                 // 40 bytes
     uint32_t* s_mask = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(bar) + 64);   // 16 words
@@ -154,6 +179,11 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
     // from a table in shared memory (in the Q region, not yet in use)
     uint32_t* s_w7 = reinterpret_cast<uint32_t*>(sQ);
     if (tid < 32) s_w7[tid] = win_w7((uint32_t)tid >> 2, (uint32_t)tid & 3u);
+    // the window's first basis values in FP64 (the same for every leaf)
+    for (int i = tid; i < kWinMaxN * kWinBasisK; i += kWinThreads) {
+        const int f = i / kWinBasisK, k = i % kWinBasisK;
+        sBd[i] = f < n ? (double)__ldg(a.basis + (uint64_t)(t0 + f) * 64u + k) : 0.0;
+    }
     __syncthreads();
     for (uint32_t idx = tid; idx < 512u * 64u; idx += kWinThreads) {
         const uint32_t v = idx >> 6, ci = idx & 63u;
@@ -171,8 +201,17 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
     uint32_t phase = 0;
 
-    for (uint32_t leaf = blockIdx.x; leaf < a.g.leaf_count; leaf += gridDim.x) {
-        const LeafEntry e = a.entries[leaf];
+    // leaf table entries are read two leaves ahead; the next leaf's payload is prefetched into
+    // L2 while this one decodes (its coefficient block and, for SparseEvents, the event keys and
+    // codes), so the leaf's first reads are L2 hits
+    const uint32_t L = a.g.leaf_count, G = gridDim.x;
+    LeafEntry e_n1 = blockIdx.x < L ? a.entries[blockIdx.x] : LeafEntry{};
+    LeafEntry e_n2 = blockIdx.x + G < L ? a.entries[blockIdx.x + G] : LeafEntry{};
+    for (uint32_t leaf = blockIdx.x; leaf < L; leaf += G) {
+        const LeafEntry e = e_n1;
+        e_n1 = e_n2;
+        if (leaf + 2u * G < L) e_n2 = a.entries[leaf + 2u * G];
+        if (leaf + G < L && entry_status(e_n1) == kOk) win_prefetch_leaf(a, e_n1, tid);
         const uint32_t st = entry_status(e);
         const uint32_t hdr = e.header, mode = hdr & 3u;
         const int keep = (int)((hdr >> 2) & 0x3Fu) + 1;
@@ -214,31 +253,47 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
         // each voxel with events searches per frame, as the reference does.
         const bool scatter = mode == 1u && (e.info & kFlagSorted) != 0u && s_sparse->count &&
                              s_sparse->es > 0.0f && s_sparse->es <= 3.40282347e38f;
-        // 2. C[f][ci] (compensated FP32 sum), split into three BF16 terms, B tiles and corners
-        for (int i = tid; i < 64 * N; i += kWinThreads) {
-            const int ci = i & 63, f = i >> 6;
-            float c = 0.0f;
-            if (f < n) {
-                const float* brow = a.basis + (uint64_t)(t0 + f) * 64u;
-                float hi, lo;
-                two_prod(sQ[ci * keep], __ldg(brow), hi, lo);
-                for (int k = 1; k < keep; ++k) {
-                    float ph, pl;
-                    two_prod(sQ[ci * keep + k], __ldg(brow + k), ph, pl);
-                    ff_add(hi, lo, ph, pl);
-                }
-                c = __fadd_rn(hi, lo);
-            }
-            const uint16_t b0 = win_bf16_bits(c);
-            const float r1 = __fsub_rn(c, win_bf16_val(b0));
-            const uint16_t b1 = win_bf16_bits(r1);
-            const uint16_t b2 = win_bf16_bits(__fsub_rn(r1, win_bf16_val(b1)));
-            const uint32_t s = (uint32_t)ci >> 4, off = win_off((uint32_t)f, (uint32_t)ci & 15u);
-            *reinterpret_cast<uint16_t*>(sB + (s * 3u + 0u) * (uint32_t)(N * 32) + off) = b0;
-            *reinterpret_cast<uint16_t*>(sB + (s * 3u + 1u) * (uint32_t)(N * 32) + off) = b1;
-            *reinterpret_cast<uint16_t*>(sB + (s * 3u + 2u) * (uint32_t)(N * 32) + off) = b2;
+        // 2. C[f][ci] = sum_k q[ci][k] b_k(t0 + f) in FP64 (exact products, one rounding per
+        //    term) rounded once to FP32, split into three BF16 terms, B tiles and corners.  Thread
+        //    tid owns control ci = tid % 64 (its coefficients in registers) and frames tid / 64 + 4 j.
+        {
+            const int ci = tid & 63;
+            double qd[kWinBasisK];
+#pragma unroll
+            for (int k = 0; k < kWinBasisK; ++k) qd[k] = k < keep ? (double)sQ[ci * keep + k] : 0.0;
+            const uint32_t s = (uint32_t)ci >> 4;
             const int corner = win_corner_of_control((uint32_t)ci);
-            if (corner >= 0) sCorner[corner * kWinMaxN + f] = c;
+            for (int f = tid >> 6; f < N; f += kWinThreads / 64) {
+                float c = 0.0f;
+                if (f < n) {
+                    const double* bd = sBd + f * kWinBasisK;
+                    double acc = 0.0;
+                    if (keep <= 4) {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (k < keep) acc = __fma_rn(qd[k], bd[k], acc);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < kWinBasisK; ++k)
+                            if (k < keep) acc = __fma_rn(qd[k], bd[k], acc);
+                    }
+                    if (keep > kWinBasisK) {
+                        const float* brow = a.basis + (uint64_t)(t0 + f) * 64u;
+                        for (int k = kWinBasisK; k < keep; ++k)
+                            acc = __fma_rn((double)sQ[ci * keep + k], (double)__ldg(brow + k), acc);
+                    }
+                    c = __double2float_rn(acc);
+                }
+                const uint16_t b0 = win_bf16_bits(c);
+                const float r1 = __fsub_rn(c, win_bf16_val(b0));
+                const uint16_t b1 = win_bf16_bits(r1);
+                const uint16_t b2 = win_bf16_bits(__fsub_rn(r1, win_bf16_val(b1)));
+                const uint32_t off = win_off((uint32_t)f, (uint32_t)ci & 15u);
+                *reinterpret_cast<uint16_t*>(sB + (s * 3u + 0u) * (uint32_t)(N * 32) + off) = b0;
+                *reinterpret_cast<uint16_t*>(sB + (s * 3u + 1u) * (uint32_t)(N * 32) + off) = b1;
+                *reinterpret_cast<uint16_t*>(sB + (s * 3u + 2u) * (uint32_t)(N * 32) + off) = b2;
+                if (corner >= 0) sCorner[corner * kWinMaxN + f] = c;
+            }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         win_tc_fence_before();
@@ -319,11 +374,16 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                     }
             }
         }
-        // 4. wait for the products (bounded); a timeout stops the whole CTA after a second wait
-        const bool ok = mbar_wait(bar, phase);
+        // 4. wait for the products (bounded): one thread polls the barrier while the others sleep
+        //    in the CTA barrier (no issue slots spent spinning); a timeout stops the whole CTA
+        //    after a second wait
+        bool ok = true;
+        if (tid == 0) ok = mbar_wait(bar, phase);
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) record_error(a.err, leaf, kErrWaitTimeout);
-            mbar_wait(bar, phase);
+            if (tid == 0) {
+                record_error(a.err, leaf, kErrWaitTimeout);
+                mbar_wait(bar, phase);
+            }
             break;
         }
         phase ^= 1u;
@@ -336,6 +396,7 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
         const uint32_t quarter = (uint32_t)(warp & 3), half = (uint32_t)(warp >> 2);
         const uint32_t row = quarter * 32u + (uint32_t)lane;
         const int cols_per_half = N / 2;
+        const bool full_leaf = ew == 8 && eh == 8 && ed == 8;
         for (uint32_t m = 0; m < 4u; ++m) {
             const uint32_t v = m * 128u + row;
             const int corner = win_corner_of_voxel(v);
@@ -348,6 +409,8 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                 // no residual at this voxel (CoarseOnly, or none here), or the scattered events of
                 // the table: D (+ the corner term) / 343 (+ q * es), the same operations as the
                 // general case (an absent event is q = 0, which adds +0 as the search's 0 does)
+                const bool wcorner = __any_sync(0xFFFFFFFFu, corner >= 0);
+                const float es = scatter ? s_sparse->es : 0.0f;
                 for (int c0 = (int)half * cols_per_half; c0 < (int)(half + 1) * cols_per_half; c0 += 16) {
                     float d[16];
                     win_ld16(taddr + ((quarter * 32u) << 16) + m * (uint32_t)N + (uint32_t)c0, d);
@@ -356,8 +419,22 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                         q0 = s_ev[(uint32_t)(c0 >> 3) * 512u + v];
                         q1 = s_ev[(uint32_t)((c0 >> 3) + 1) * 512u + v];
                     }
-                    const float es = scatter ? s_sparse->es : 0.0f;
                     float* o = out + (uint64_t)c0 * frame_stride + (uint64_t)leaf * 512u + v;
+                    // the common chunk -- 16 frames inside the window, a full leaf, no corner voxel
+                    // in the warp -- without the per-output tests (same operations)
+                    if (!wcorner && full_leaf && c0 + 16 <= n) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            float val = __fmul_rn(d[j], 1.0f / 343.0f);
+                            if (mode == 1u) {
+                                const int q = ((int)((j < 8 ? q0 : q1) << (28 - 4 * (j & 7)))) >> 28;
+                                val = __fadd_rn(val, scatter ? __fmul_rn((float)q, es) : 0.0f);
+                            }
+                            *o = val;
+                            o += frame_stride;
+                        }
+                        continue;
+                    }
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
                         if (c0 + j < n) {
