@@ -31,8 +31,9 @@ constexpr uint32_t kWinA = 4u * 4u * 4096u;             // 4 M tiles x 4 K steps
 constexpr uint32_t kWinB = 4u * 3u * (kWinMaxN * 32u);  // 4 K steps x 3 terms x (64 rows x 32 B)
 constexpr uint32_t kWinCorner = 8u * kWinMaxN * 4u;     // corner controls x frames, FP32
 constexpr uint32_t kWinQ = 64u * 64u * 4u;              // 64 controls x keep (<= 64) coefficients
-constexpr int kWinBasisK = 8;                            // basis terms held in FP64 per frame
-constexpr uint32_t kWinBd = kWinMaxN * kWinBasisK * 8u;  // b_k(t0 + f), k < 8, FP64
+constexpr int kWinBasisK = 4;                            // basis terms held in FP64 per frame
+constexpr int kWinBdStride = kWinBasisK + 1;             // doubles per frame row (8 rows: 8 bank pairs)
+constexpr uint32_t kWinBd = kWinMaxN * kWinBdStride * 8u;   // b_k(t0 + f), k < 4, FP64
 constexpr uint32_t kWinSmem = kWinA + kWinB + kWinCorner + kWinQ + kWinBd + 256u;   // + barrier, TMEM address, sparse header
 
 __device__ __forceinline__ uint32_t win_smem_u32(const void* p)
@@ -182,16 +183,21 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
     // the window's first basis values in FP64 (the same for every leaf)
     for (int i = tid; i < kWinMaxN * kWinBasisK; i += kWinThreads) {
         const int f = i / kWinBasisK, k = i % kWinBasisK;
-        sBd[i] = f < n ? (double)__ldg(a.basis + (uint64_t)(t0 + f) * 64u + k) : 0.0;
+        sBd[f * kWinBdStride + k] = f < n ? (double)__ldg(a.basis + (uint64_t)(t0 + f) * 64u + k) : 0.0;
     }
     __syncthreads();
-    for (uint32_t idx = tid; idx < 512u * 64u; idx += kWinThreads) {
-        const uint32_t v = idx >> 6, ci = idx & 63u;
-        uint32_t w = s_w7[((v & 7u) << 2) | (ci & 3u)] * s_w7[(((v >> 3) & 7u) << 2) | ((ci >> 2) & 3u)] *
-                     s_w7[((v >> 6) << 2) | (ci >> 4)];
-        if (w == 343u) w = 342u;
-        const uint32_t m = v >> 7, s = ci >> 4;
-        *reinterpret_cast<uint16_t*>(sA + (m * 4u + s) * 4096u + win_off(v & 127u, ci & 15u)) = win_bf16_bits((float)w);
+    // two adjacent controls per 32-bit store; a warp's 32 stores cover 8 rows x 4 words of one
+    // 8-row core group: 32 distinct banks
+    for (uint32_t P = tid; P < 512u * 32u; P += kWinThreads) {
+        const uint32_t v = (P & 7u) | (((P >> 5) & 63u) << 3);
+        const uint32_t ci = 2u * (((P >> 3) & 3u) | ((P >> 11) << 2));
+        const uint32_t yz = s_w7[(((v >> 3) & 7u) << 2) | ((ci >> 2) & 3u)] * s_w7[((v >> 6) << 2) | (ci >> 4)];
+        uint32_t w0 = s_w7[((v & 7u) << 2) | (ci & 3u)] * yz, w1 = s_w7[((v & 7u) << 2) | ((ci & 3u) | 1u)] * yz;
+        if (w0 == 343u) w0 = 342u;
+        if (w1 == 343u) w1 = 342u;
+        const uint32_t m = v >> 7, sk = ci >> 4;
+        *reinterpret_cast<uint32_t*>(sA + (m * 4u + sk) * 4096u + win_off(v & 127u, ci & 15u)) =
+            (uint32_t)win_bf16_bits((float)w0) | ((uint32_t)win_bf16_bits((float)w1) << 16);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     win_tc_fence_before();
@@ -255,44 +261,52 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                              s_sparse->es > 0.0f && s_sparse->es <= 3.40282347e38f;
         // 2. C[f][ci] = sum_k q[ci][k] b_k(t0 + f) in FP64 (exact products, one rounding per
         //    term) rounded once to FP32, split into three BF16 terms, B tiles and corners.  Thread
-        //    tid owns control ci = tid % 64 (its coefficients in registers) and frames tid / 64 + 4 j.
+        //    owns controls ci0 = 8 warp + 2 (lane / 8) and ci0 + 1 (coefficients in registers) and
+        //    frames lane % 8 + 8 j; its three 32-bit stores per frame hit 32 distinct banks per warp.
         {
-            const int ci = tid & 63;
-            double qd[kWinBasisK];
+            const int ci0 = 8 * warp + 2 * (lane >> 3);
+            double qa[kWinBasisK], qb[kWinBasisK];
 #pragma unroll
-            for (int k = 0; k < kWinBasisK; ++k) qd[k] = k < keep ? (double)sQ[ci * keep + k] : 0.0;
-            const uint32_t s = (uint32_t)ci >> 4;
-            const int corner = win_corner_of_control((uint32_t)ci);
-            for (int f = tid >> 6; f < N; f += kWinThreads / 64) {
-                float c = 0.0f;
+            for (int k = 0; k < kWinBasisK; ++k) {
+                qa[k] = k < keep ? (double)sQ[ci0 * keep + k] : 0.0;
+                qb[k] = k < keep ? (double)sQ[(ci0 + 1) * keep + k] : 0.0;
+            }
+            const uint32_t sk = (uint32_t)ci0 >> 4, kk = (uint32_t)ci0 & 15u;
+            const int cora = win_corner_of_control((uint32_t)ci0), corb = win_corner_of_control((uint32_t)ci0 + 1u);
+            for (int f = lane & 7; f < N; f += 8) {
+                float ca = 0.0f, cb = 0.0f;
                 if (f < n) {
-                    const double* bd = sBd + f * kWinBasisK;
-                    double acc = 0.0;
-                    if (keep <= 4) {
+                    const double* bd = sBd + f * kWinBdStride;
+                    double xa = 0.0, xb = 0.0;
 #pragma unroll
-                        for (int k = 0; k < 4; ++k)
-                            if (k < keep) acc = __fma_rn(qd[k], bd[k], acc);
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < kWinBasisK; ++k)
-                            if (k < keep) acc = __fma_rn(qd[k], bd[k], acc);
-                    }
+                    for (int k = 0; k < kWinBasisK; ++k)
+                        if (k < keep) {
+                            const double b = bd[k];
+                            xa = __fma_rn(qa[k], b, xa);
+                            xb = __fma_rn(qb[k], b, xb);
+                        }
                     if (keep > kWinBasisK) {
                         const float* brow = a.basis + (uint64_t)(t0 + f) * 64u;
-                        for (int k = kWinBasisK; k < keep; ++k)
-                            acc = __fma_rn((double)sQ[ci * keep + k], (double)__ldg(brow + k), acc);
+                        for (int k = kWinBasisK; k < keep; ++k) {
+                            const double b = (double)__ldg(brow + k);
+                            xa = __fma_rn((double)sQ[ci0 * keep + k], b, xa);
+                            xb = __fma_rn((double)sQ[(ci0 + 1) * keep + k], b, xb);
+                        }
                     }
-                    c = __double2float_rn(acc);
+                    ca = __double2float_rn(xa);
+                    cb = __double2float_rn(xb);
                 }
-                const uint16_t b0 = win_bf16_bits(c);
-                const float r1 = __fsub_rn(c, win_bf16_val(b0));
-                const uint16_t b1 = win_bf16_bits(r1);
-                const uint16_t b2 = win_bf16_bits(__fsub_rn(r1, win_bf16_val(b1)));
-                const uint32_t off = win_off((uint32_t)f, (uint32_t)ci & 15u);
-                *reinterpret_cast<uint16_t*>(sB + (s * 3u + 0u) * (uint32_t)(N * 32) + off) = b0;
-                *reinterpret_cast<uint16_t*>(sB + (s * 3u + 1u) * (uint32_t)(N * 32) + off) = b1;
-                *reinterpret_cast<uint16_t*>(sB + (s * 3u + 2u) * (uint32_t)(N * 32) + off) = b2;
-                if (corner >= 0) sCorner[corner * kWinMaxN + f] = c;
+                const uint16_t a0 = win_bf16_bits(ca), b0 = win_bf16_bits(cb);
+                const float ra = __fsub_rn(ca, win_bf16_val(a0)), rb = __fsub_rn(cb, win_bf16_val(b0));
+                const uint16_t a1 = win_bf16_bits(ra), b1 = win_bf16_bits(rb);
+                const uint16_t a2 = win_bf16_bits(__fsub_rn(ra, win_bf16_val(a1)));
+                const uint16_t b2 = win_bf16_bits(__fsub_rn(rb, win_bf16_val(b1)));
+                uint8_t* dst = sB + sk * 3u * (uint32_t)(N * 32) + win_off((uint32_t)f, kk);
+                *reinterpret_cast<uint32_t*>(dst) = (uint32_t)a0 | ((uint32_t)b0 << 16);
+                *reinterpret_cast<uint32_t*>(dst + (uint32_t)(N * 32)) = (uint32_t)a1 | ((uint32_t)b1 << 16);
+                *reinterpret_cast<uint32_t*>(dst + 2u * (uint32_t)(N * 32)) = (uint32_t)a2 | ((uint32_t)b2 << 16);
+                if (cora >= 0) sCorner[cora * kWinMaxN + f] = ca;
+                if (corb >= 0) sCorner[corb * kWinMaxN + f] = cb;
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -423,15 +437,29 @@ __global__ void __launch_bounds__(kWinThreads, 2) sci_window_kernel(DeviceAsset 
                     // the common chunk -- 16 frames inside the window, a full leaf, no corner voxel
                     // in the warp -- without the per-output tests (same operations)
                     if (!wcorner && full_leaf && c0 + 16 <= n) {
+                        if (scatter) {
+                            // q as a float without a conversion: the code's bits (sign bit
+                            // flipped) in the mantissa of 1.5 * 2^23, minus 1.5 * 2^23 + 8 (exact)
+                            const uint32_t x0 = q0 ^ 0x88888888u, x1 = q1 ^ 0x88888888u;
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            float val = __fmul_rn(d[j], 1.0f / 343.0f);
-                            if (mode == 1u) {
-                                const int q = ((int)((j < 8 ? q0 : q1) << (28 - 4 * (j & 7)))) >> 28;
-                                val = __fadd_rn(val, scatter ? __fmul_rn((float)q, es) : 0.0f);
+                            for (int j = 0; j < 16; ++j) {
+                                const uint32_t u = ((j < 8 ? x0 : x1) >> (4 * (j & 7))) & 0xFu;
+                                const float qf = __fsub_rn(__uint_as_float(0x4B400000u | u), 12582920.0f);
+                                *o = __fadd_rn(__fmul_rn(d[j], 1.0f / 343.0f), __fmul_rn(qf, es));
+                                o += frame_stride;
                             }
-                            *o = val;
-                            o += frame_stride;
+                        } else if (mode == 1u) {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) {
+                                *o = __fadd_rn(__fmul_rn(d[j], 1.0f / 343.0f), 0.0f);
+                                o += frame_stride;
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) {
+                                *o = __fmul_rn(d[j], 1.0f / 343.0f);
+                                o += frame_stride;
+                            }
                         }
                         continue;
                     }
