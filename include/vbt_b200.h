@@ -96,7 +96,7 @@ int vbt_get_page_table(vbt_asset* asset, uint32_t* compact, uint32_t* active_cou
 /* Synchronous host copy of the 32-byte leaf-table rows (8 uint32 per leaf). */
 int vbt_get_leaf_table(vbt_asset* asset, uint32_t* rows);
 
-/* Kernel (b): current-frame voxel cache for `nframes` (<= 64) frames in one launch:
+/* Kernel (b): current-frame voxel cache for `nframes` (<= 128) frames in one launch:
  * d_out[f * frame_stride + rank * 512 + (lz*8 + ly)*8 + lx].  Voxels outside a boundary leaf's
  * extent are 0.  Values equal decodeFrameToDense (render/src/render_smoke_vbt_bench_main.cpp:
  * 389-452) voxel for voxel; the Studio cache it replaces is vbt_cache.comp:176-294.
@@ -106,7 +106,7 @@ int vbt_decode_cache(vbt_asset* asset, const int* frames, int nframes, float* d_
 /* The reference Studio's control cache (VBTStudio/frontend/shaders/vbt_cache.comp:168-236), for
  * consumers written against it: d_out[f * frame_stride + rank * 576 + slot] over the active leaves
  * of the current page table (vbt_build_page_table first) and frames[0..nframes) (clamped as the
- * reference clamps, 1..64 frames).  Slot s < 64 holds coarse control s; from slot 64 on, the fine
+ * reference clamps, 1..128 frames).  Slot s < 64 holds coarse control s; from slot 64 on, the fine
  * grid's controls (FINE6) or the Mode2 shell residual controls; other slots hold 0.  Values are
  * the reference CPU decoder's (decodeRenderTemporalControlValue, src/render_temporal_decode.cpp:
  * 304-356); render-temporal assets only. */

@@ -3,7 +3,7 @@
 decode_leaf_kernel takes GRID4 and FINE6 leaves of the common shape (coarse resolution 4, fine 6,
 FP16 keys that strictly increase and hold no NaN) through its specialised path whenever the
 frames of a launch step by 0 or 1, and every other leaf, or any other frame list, through the
-general path.  Here every launch shape the specialised path distinguishes -- 1 to 64 frames (one
+general path.  Here every launch shape the specialised path distinguishes -- 1 to 128 frames (one
 or several frame batches, GRID4 frame parts of unequal length), repeated frames at the clamped
 ends, boundary leaves with cropped extents, cache and dense outputs -- is checked against the
 oracle on every frame, and frame lists that step back or skip (the general path) likewise.
@@ -75,7 +75,7 @@ def test_timeline_launch_shapes(loaded, cuda, path):
     a.build_page_table()
     T = f.frames
     big = "cfg2" in path or "mix_fire" in path
-    counts = [5, 48, 64] if big else [1, 2, 3, 4, 5, 9, 13, 17, 48, 64]
+    counts = [5, 48, 64, 96, 128] if big else [1, 2, 3, 4, 5, 9, 13, 17, 48, 64, 96, 128]
     lists = []
     for k in counts:
         for start in ([-1] if big else [-1, T // 3]):

@@ -460,7 +460,8 @@ int vbt_get_leaf_table(vbt_asset* a, uint32_t* rows)
 
 static int check_frames(vbt_asset* a, const int* frames, int nframes)
 {
-    if (!frames || nframes <= 0 || nframes > 64) return fail(VBT_STATUS_INVALID_ARGUMENT, "need 1..64 frames");
+    if (!frames || nframes <= 0 || nframes > kMaxLaunchFrames)
+        return fail(VBT_STATUS_INVALID_ARGUMENT, "need 1..128 frames");
     if (a->hdr.profile_type == 2u)
         for (int i = 0; i < nframes; ++i)
             if (frames[i] < 0 || (uint32_t)frames[i] >= a->hdr.frames)

@@ -948,7 +948,7 @@ __device__ __forceinline__ void sci_row(const DeviceAsset& a, const LeafEntry& e
 
 struct FrameList {
     int n;
-    int f[64];
+    int f[kMaxLaunchFrames];
 };
 
 template <bool DENSE, bool SCI>

@@ -40,10 +40,14 @@ struct DeviceAsset {
 // the same time.
 constexpr uint32_t kWorkSlots = 64;
 
+// Frames of one decode launch (the frame list travels as a kernel parameter).
+constexpr int kMaxLaunchFrames = 128;
+
 // Fixed shared memory of the render decode kernel besides its leaf stage (rt_kernel_leaf.cuh:
 // barrier, frame tables, axis weights, 9 warps x (x-lerp + y-lerp rows), 3072-float controls,
 // reciprocal table, axis weights as 16-byte rows).
-constexpr uint32_t kLeafFixedBytes = 16 + 256 + 128 + 576 + 9 * 196 * 8 + 9 * 112 * 16 + 3072 * 4 + 256 * 4 + 768;
+constexpr uint32_t kLeafFixedBytes =
+    16 + 6 * kMaxLaunchFrames + 576 + 9 * 196 * 8 + 9 * 112 * 16 + 3072 * 4 + 256 * 4 + 768;
 
 constexpr int kWalkThreads = 256;
 constexpr int kWalkTile = 256;   // leaves per walker CTA (one scan element per thread)
@@ -91,7 +95,7 @@ void launch_page_table(const DeviceAsset& a, uint32_t epoch, cudaStream_t s);
 // kFlagHalfPlain bits of the leaf table.  Runs at load and after every re-upload; later walks copy
 // the bits from key_sorted.
 void launch_key_order(const DeviceAsset& a, cudaStream_t s);
-// Decode `nframes` frames (frames[] on the host, <= 64) of every active leaf into the cache:
+// Decode `nframes` frames (frames[] on the host, <= kMaxLaunchFrames) of every active leaf into the cache:
 // out[f * cache_frame_stride + rank * 512 + voxel].
 void launch_decode_cache(const DeviceAsset& a, uint32_t seq, const int* frames, int nframes, float* out,
                          uint64_t cache_frame_stride, int grid, cudaStream_t s);

@@ -19,7 +19,7 @@ constexpr int kDecThreads = 32 * kDecWarps;
 constexpr int kLeafCtrlBudget = 3072;   // floats: frames x controls of one batch
 constexpr uint32_t leaf_fixed_bytes(int nw)
 {
-    return 16 + 256 + 128 + 576 + nw * 196 * 8 + nw * 112 * 16 + kLeafCtrlBudget * 4 + 256 * 4 + 768;
+    return 16 + 6 * kMaxLaunchFrames + 576 + nw * 196 * 8 + nw * 112 * 16 + kLeafCtrlBudget * 4 + 256 * 4 + 768;
 }
 constexpr uint32_t kLeafFixed = leaf_fixed_bytes(kLeafWarps);
 constexpr uint32_t kDecFixed = leaf_fixed_bytes(kDecWarps);
@@ -46,10 +46,10 @@ __device__ __forceinline__ LeafSmem leaf_layout(uint8_t* dyn)
     LeafSmem s;
     s.bar = reinterpret_cast<uint64_t*>(dyn);
     s.fr = reinterpret_cast<int*>(dyn + 16);
-    s.b8 = dyn + 16 + 256;
-    s.b4 = s.b8 + 64;
-    s.w = reinterpret_cast<AxisWeight(*)[3][8]>(dyn + 16 + 256 + 128);
-    s.x2 = reinterpret_cast<float2*>(dyn + 16 + 256 + 128 + 576);
+    s.b8 = dyn + 16 + 4 * kMaxLaunchFrames;
+    s.b4 = s.b8 + kMaxLaunchFrames;
+    s.w = reinterpret_cast<AxisWeight(*)[3][8]>(dyn + 16 + 6 * kMaxLaunchFrames);
+    s.x2 = reinterpret_cast<float2*>(dyn + 16 + 6 * kMaxLaunchFrames + 576);
     s.y4 = reinterpret_cast<float4*>(reinterpret_cast<uint8_t*>(s.x2) + NW * 196 * 8);
     s.ctrl = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(s.y4) + NW * 112 * 16);
     s.rcp = s.ctrl + kLeafCtrlBudget;

@@ -3,8 +3,8 @@
 //
 // A timeline is a page-table build followed by ceil(n / frames_per_launch) cache-decode launches.
 // The autotuner times every candidate shape on the caller's own output buffer with CUDA events
-// and keeps the fastest: leaf per CTA (the TMA-staged kernel; 16, 24, 32, 48 or 64 frames per
-// launch) or leaf per warp (8 leaves per CTA; 16, 32 or 64 frames, one or two waves).  All shapes
+// and keeps the fastest: leaf per CTA (the TMA-staged kernel; 16, 24, 32, 48, 64, 96 or 128
+// frames per launch) or leaf per warp (8 leaves per CTA; 16, 32 or 64 frames, one or two waves).  All shapes
 // write identical values.
 #include <cuda_runtime.h>
 
@@ -54,8 +54,8 @@ int cuda_fail(cudaError_t e, const char* what)
 void enqueue_timeline(vbt_asset* a, const vbt_tuning& t, int t0, int n, float* out, uint64_t stride, cudaStream_t s)
 {
     launch_page_table(a->dev, ++a->epoch, s);
-    int fr[64];
-    const int fpl = (int)std::max<uint32_t>(1u, std::min<uint32_t>(64u, t.frames_per_launch));
+    int fr[kMaxLaunchFrames];
+    const int fpl = (int)std::max<uint32_t>(1u, std::min<uint32_t>((uint32_t)kMaxLaunchFrames, t.frames_per_launch));
     for (int i = 0; i < n; i += fpl) {
         const int m = std::min(fpl, n - i);
         for (int j = 0; j < m; ++j) fr[j] = t0 + i + j;
@@ -97,7 +97,7 @@ int vbt_autotune_cache(vbt_asset* a, int nframes, float* d_out, uint64_t stride,
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int wave = decode_warp_grid();
     std::vector<vbt_tuning> cands;
-    for (uint32_t f : {16u, 24u, 32u, 48u, 64u}) cands.push_back(vbt_tuning{0u, f, 0, 0.f, 0.f});
+    for (uint32_t f : {16u, 24u, 32u, 48u, 64u, 96u, 128u}) cands.push_back(vbt_tuning{0u, f, 0, 0.f, 0.f});
     for (uint32_t f : {16u, 32u, 64u})
         for (int g : {0, 2 * wave}) cands.push_back(vbt_tuning{1u, f, g, 0.f, 0.f});
     vbt_tuning best{0u, 48u, 0, 0.f, 0.f};
@@ -123,7 +123,7 @@ int vbt_autotune_cache(vbt_asset* a, int nframes, float* d_out, uint64_t stride,
 int vbt_set_tuning(vbt_asset* a, const vbt_tuning* t)
 {
     if (!a || !t) return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "null argument");
-    if (t->variant > 1u || t->frames_per_launch == 0u || t->frames_per_launch > 64u || t->grid < 0)
+    if (t->variant > 1u || t->frames_per_launch == 0u || t->frames_per_launch > (uint32_t)kMaxLaunchFrames || t->grid < 0)
         return set_last_error(VBT_STATUS_INVALID_ARGUMENT, "tuning out of range");
     Guard guard(a->device);
     vbtb::release_timeline_graphs(a);
