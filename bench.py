@@ -165,15 +165,21 @@ def measured_peak():
     return 6650.0, "fallback 6.65 TB/s"
 
 
-def ncu_traffic():
+def ncu_traffic(frames_per_launch):
     """Per-launch DRAM bytes (read + write) of the decode kernel from the committed ncu summary
-    (profiles/decode_leaf_cfg2.md, line `traffic_bytes_per_launch: N`), if present."""
+    (profiles/decode_leaf_cfg2.md, lines `traffic_bytes_per_launch: N` and
+    `traffic_frames_per_launch: F`), if present and captured on launches of this run's shape."""
     p = os.path.join(ROOT, "profiles", "decode_leaf_cfg2.md")
-    if os.path.exists(p):
-        for line in open(p):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return int(line.split(":")[1])
-    return None
+    if not os.path.exists(p):
+        return None
+    vals = {}
+    for line in open(p):
+        for key in ("traffic_bytes_per_launch", "traffic_frames_per_launch"):
+            if line.startswith(key + ":"):
+                vals[key] = int(line.split(":")[1])
+    if vals.get("traffic_frames_per_launch") != frames_per_launch:
+        return None
+    return vals.get("traffic_bytes_per_launch")
 
 
 # ------------------------------------------------------------------------------ CPU baseline
@@ -1294,7 +1300,7 @@ def run_ours(args, rank, local_rank, world):
     mean_launch_s = statistics.mean(dec_ms) * 1e-3
     alg_per_launch = [bytes_per_frame * len(ch) for ch in chunks]
     achieved = statistics.mean(alg_per_launch) / mean_launch_s / 1e9
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(len(chunks[0])) if len({len(ch) for ch in chunks}) == 1 else None
 
     # the same step replayed from a captured CUDA graph (page table + all decode launches, one
     # cudaGraphLaunch), timed the same way
