@@ -9,7 +9,8 @@
 // of 1/7, so S' = 343 S is an integer matrix with entries <= 343.  Every entry but 343 (the eight
 // voxels that sit on a control point, weight 1) is exact in one BF16; the A operand holds S' with
 // 343 entered as 342, and the missing 1 x C term of those eight voxels is added on the CUDA cores.
-// C is computed in FP32 (compensated sum) and split into three BF16 terms c = c_hi + c_mid + c_lo
+// C is computed in FP64 (exact products, one rounding per term), rounded once to FP32 and split
+// into three BF16 terms c = c_hi + c_mid + c_lo
 // (residual below 2^-26 |c|).  The contraction is 3 tcgen05.mma products per 16-wide K step
 // (S'.c_hi + S'.c_mid + S'.c_lo), accumulated in FP32 in tensor memory: 4 M tiles (128 voxels)
 // x 4 K steps x 3 terms = 48 MMAs of 128 x N x 16 per leaf-window, N = n rounded up to 16.
