@@ -61,3 +61,17 @@ def test_max_over_ranks_without_group():
     import bench
     assert bench.max_over_ranks(3.25, None, "cpu") == 3.25
     assert os.path.exists(os.path.join(ROOT, "bench.py"))
+
+
+def test_roofline_traffic_only_for_the_captured_launch_shape():
+    """`roofline.traffic` comes from the committed ncu summary of the decode kernel; it is reported
+    only for launches of the frame count that summary was captured on."""
+    sys.path.insert(0, ROOT)
+    import bench
+    frames = None
+    for line in open(os.path.join(ROOT, "profiles", "decode_leaf_cfg2.md")):
+        if line.startswith("traffic_frames_per_launch:"):
+            frames = int(line.split(":")[1])
+    assert frames is not None
+    assert bench.ncu_traffic(frames) > 0
+    assert bench.ncu_traffic(frames + 1) is None
